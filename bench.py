@@ -1,0 +1,369 @@
+#!/usr/bin/env python
+"""Multi-source traversal benchmark (GTEPS on one B200 per rank).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl xbtrav|reference]
+                    [--workload rmat22_k1024|er335k_k256|rmat16_k64]
+
+Workload (default): undirected R-MAT scale 22, edge factor 16, a/b/c/d =
+.57/.19/.19/.05 (symmetrised, cleaned, sorted int32 CSR), 1024 seeded sources
+drawn from vertices of non-zero degree; one step = traversal of all 1024
+sources producing the int32 level and parent tables (1024 x n each) in HBM.
+GTEPS = sum over sources of sum over reached vertices of deg(v) / time (the
+"Processed Edges" unit of the reference's BFS_Throughput).  Synthetic seeded
+data stands in for the reference's real datasets (not shipped).
+
+N > 1: one process per GPU; the graph is replicated and every rank traverses
+its own 1024 sources (weak scaling, no collective on the data path; NCCL is
+used only for the barrier and the max/sum of the timing scalars).
+
+--impl reference: the reference's own CPU BFS (Ligra BFS_F + edgeMap from the
+reference sources, prebuilt in oracle/_ref/) on the same graph and metric,
+all host threads, a bounded sample of sources per step; falls back to the
+C restatement in oracle/ when oracle/_ref/ was not built.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "xblossom-sigmetrics27-ae_b200")
+for _p in (ROOT, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+WORKLOADS = {
+    "rmat22_k1024": dict(kind="rmat", scale=22, ef=16, k=1024),
+    "er335k_k256": dict(kind="er", n=335_000, pairs=1_850_000, k=256),
+    "rmat16_k64": dict(kind="rmat", scale=16, ef=16, k=64),
+}
+SEED = 0x5EED
+
+
+def make_graph(w: dict):
+    import xbtrav
+
+    if w["kind"] == "rmat":
+        return xbtrav.HostCSR.rmat(w["scale"], w["ef"], 0.57, 0.19, 0.19, seed=SEED)
+    return xbtrav.HostCSR.er(w["n"], w["pairs"], seed=SEED)
+
+
+def workload_config(name: str, w: dict, info: dict) -> dict:
+    cfg = {"workload": name, "n": info["n"], "m_directed": info["m"], "sources": w["k"], "seed": SEED,
+           "l2": "inputs larger than L2 (colIndices > 126 MB); no flush"}
+    if w["kind"] == "rmat":
+        cfg.update(graph=f"rmat scale {w['scale']} ef {w['ef']} a/b/c/d .57/.19/.19/.05")
+    else:
+        cfg.update(graph=f"uniform n {w['n']} pairs {w['pairs']}")
+    return cfg
+
+
+def measured_peaks() -> tuple[float, str]:
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.f = None
+
+    def start(self):
+        try:
+            self.f = tempfile.TemporaryFile(mode="w+")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.seek(0)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.f.read().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def traffic_from_profile(workload: str):
+    """Per-launch DRAM bytes of the dominant kernel from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", f"traffic_{workload}.json")
+    try:
+        return json.load(open(p))
+    except Exception:
+        return None
+
+
+def cpu_baseline_port(ro, ci, sources, budget_s: float = 15.0) -> dict:
+    """The C restatement (oracle/) on all host cores, a bounded sample of sources."""
+    from oracle import oracle
+
+    cores = os.cpu_count() or 1
+    sample = list(sources[: max(1, min(len(sources), cores))])
+    t0 = time.perf_counter()
+    _, _, e, _ = oracle.msbfs(ro, ci, np.array(sample, np.int32), threads=cores)
+    dt = time.perf_counter() - t0
+    # grow the sample toward the budget
+    per = dt / len(sample)
+    extra = int(min(len(sources) - len(sample), max(0, (budget_s - dt) / max(per, 1e-9))))
+    if extra > 0:
+        more = sources[len(sample): len(sample) + extra]
+        t1 = time.perf_counter()
+        _, _, e2, _ = oracle.msbfs(ro, ci, np.array(more, np.int32), threads=cores)
+        dt += time.perf_counter() - t1
+        e += e2
+        sample += list(more)
+    return {"value": e / dt / 1e9, "unit": "GTEPS", "cores": cores, "kind": "port",
+            "sample": f"{len(sample)} of the workload's sources, levels + min-id parents, {dt:.1f} s"}
+
+
+def run_reference(args, w, name) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import oracle
+
+    t_gen = time.perf_counter()
+    csr = make_graph(w)
+    ro, ci = csr.arrays()
+    info = csr.info()
+    import xbtrav
+
+    sources = xbtrav.select_sources_csr(ro, SEED + 1, w["k"])
+    cores = os.cpu_count() or 1
+    use_ligra = oracle.ligra_available()
+    per_step = 8 if w["kind"] == "rmat" and w.get("scale", 0) >= 20 else min(w["k"], 64)
+    times, edges = [], []
+    for step in range(args.warmup + args.steps):
+        sel = sources[(step * per_step) % len(sources):][:per_step]
+        if use_ligra:
+            _, secs, e = oracle.ligra_bfs(ro, ci, sel, threads=cores, want_parents=False)
+        else:
+            t0 = time.perf_counter()
+            _, _, e, _ = oracle.msbfs(ro, ci, sel, threads=cores, want_tables=False)
+            secs = time.perf_counter() - t0
+        if step >= args.warmup:
+            times.append(secs)
+            edges.append(e)
+    value = sum(edges) / sum(times) / 1e9
+    kind = "reference" if use_ligra else "port"
+    what = ("Ligra BFS_F/edgeMap from the reference sources (oracle/_ref), parents only"
+            if use_ligra else "C restatement (oracle/), levels only")
+    line = {
+        "impl": "reference", "metric": "multi-source traversal throughput", "value": value, "unit": "GTEPS",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000.0 * sum(times) / len(times), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded generator)",
+        "config": workload_config(name, w, info),
+        "cpu_baseline": {"value": value, "unit": "GTEPS", "cores": cores, "kind": kind,
+                         "sample": f"{per_step} sources per step, {what}"},
+        "e2e": {"value": value, "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "setup_s": time.perf_counter() - t_gen,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="xbtrav", choices=["xbtrav", "reference"])
+    ap.add_argument("--workload", default="rmat22_k1024", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    w = WORKLOADS[args.workload]
+    if args.impl == "reference":
+        run_reference(args, w, args.workload)
+        return
+
+    import torch
+
+    import xbtrav
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+
+    t_setup = time.perf_counter()
+    csr = make_graph(w)
+    info = csr.info()
+    ro, ci = csr.arrays()
+    ctx = xbtrav.Context(local)
+    ctx.set_tuning(timing=1)
+    g = ctx.upload(csr)
+    k = w["k"]
+    sources = g.select_sources(SEED + 1 + 7919 * rank, k)
+    src_dev = torch.from_numpy(sources).to(dev)
+    level = torch.empty((k, g.n), dtype=torch.int32, device=dev)
+    parent = torch.empty((k, g.n), dtype=torch.int32, device=dev)
+    stream = torch.cuda.ExternalStream(ctx.stream_handle(), device=dev)
+    setup_s = time.perf_counter() - t_setup
+
+    def barrier():
+        torch.cuda.synchronize(dev)
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    for _ in range(args.warmup):
+        ctx.traverse(g, src_dev, out="device", level=level, parent=parent)
+    clocks = ClockSampler(local)
+    barrier()
+    clocks.start()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    agg = {"edges_traversed": 0, "class_ms": [0.0, 0.0, 0.0], "class_bytes": [0, 0, 0], "class_launches": [0, 0, 0],
+           "levels": 0, "push_levels": 0, "pull_levels": 0, "algo_bytes": 0}
+    with torch.cuda.stream(stream):
+        ev0.record(stream)
+    for _ in range(args.steps):
+        r = ctx.traverse(g, src_dev, out="device", level=level, parent=parent)
+        s = r.stats
+        agg["edges_traversed"] += s["edges_traversed"]
+        agg["algo_bytes"] += s["algo_bytes"]
+        for i in range(3):
+            agg["class_ms"][i] += s["class_ms"][i]
+            agg["class_bytes"][i] += s["class_bytes"][i]
+            agg["class_launches"][i] += s["class_launches"][i]
+        agg["levels"] = s["levels"]
+        agg["push_levels"] += s["push_levels"]
+        agg["pull_levels"] += s["pull_levels"]
+    with torch.cuda.stream(stream):
+        ev1.record(stream)
+    barrier()
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    edges_total = agg["edges_traversed"]
+    if dist is not None:
+        t = torch.tensor([ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        e = torch.tensor([edges_total], dtype=torch.float64, device=dev)
+        dist.all_reduce(e, op=dist.ReduceOp.SUM)
+        edges_total = float(e.item())
+    value = edges_total / (ms / 1e3) / 1e9
+
+    # roofline of the dominant kernel class (event-timed inside the timed region)
+    peak, peak_kind = measured_peaks()
+    dom = 0 if agg["class_ms"][0] >= agg["class_ms"][1] else 1
+    dom_name = ["level steps (k_pull_tiles/k_push_*)", "table pass (k_tables)"][dom]
+    achieved = agg["class_bytes"][dom] / (agg["class_ms"][dom] / 1e3) / 1e9 if agg["class_ms"][dom] > 0 else None
+    tr = traffic_from_profile(args.workload)
+    roofline = {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
+                "traffic": tr.get(str(dom)) if isinstance(tr, dict) else None,
+                "class_ms_per_step": [x / args.steps for x in agg["class_ms"]],
+                "class_gbytes_per_step": [x / args.steps / 1e9 for x in agg["class_bytes"]]}
+
+    # end to end through the C ABI with host buffers (pinned), copies in the timed region
+    e2e = None
+    if not args.no_e2e:
+        try:
+            hl = torch.empty((k, g.n), dtype=torch.int32, pin_memory=True)
+            hp = torch.empty((k, g.n), dtype=torch.int32, pin_memory=True)
+            hs = torch.from_numpy(sources).pin_memory()
+            ln, pn = hl.numpy(), hp.numpy()
+            e2e_steps = max(1, min(args.steps, 3))
+            ctx.traverse(g, hs.numpy(), level=ln, parent=pn)
+            barrier()
+            t0 = time.perf_counter()
+            et = 0
+            for _ in range(e2e_steps):
+                r = ctx.traverse(g, hs.numpy(), level=ln, parent=pn)
+                et += r.stats["edges_traversed"]
+            barrier()
+            dt = time.perf_counter() - t0
+            if dist is not None:
+                t = torch.tensor([dt, et], dtype=torch.float64, device=dev)
+                tm = t.clone()
+                dist.all_reduce(tm, op=dist.ReduceOp.MAX)
+                dist.all_reduce(t, op=dist.ReduceOp.SUM)
+                dt, et = float(tm[0].item()), float(t[1].item())
+            e2e = {"value": et / dt / 1e9, "unit": "GTEPS", "h2d_bytes_per_step": 4 * k,
+                   "d2h_bytes_per_step": 8 * k * g.n, "steps": e2e_steps,
+                   "note": "xb_traverse with host source list and host level/parent tables (pinned); "
+                           "graph resident"}
+            del hl, hp
+        except Exception as ex:  # noqa: BLE001
+            e2e = {"value": None, "unit": "GTEPS", "error": str(ex)[:200]}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_port(ro, ci, sources)
+
+    if rank == 0:
+        line = {
+            "metric": "multi-source traversal throughput (plain per-call path)", "value": value, "unit": "GTEPS",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+            "data": "synthetic (seeded R-MAT / uniform generator)",
+            "config": dict(workload_config(args.workload, w, info), parallelism=f"replicas{world}",
+                           path="xb_traverse (host level loop, 64 sources per word)"),
+            "plain_gteps": value,
+            "undirected_gteps": value / 2,
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
+            "gpu_launches": sum(agg["class_launches"]),
+            "levels": agg["levels"], "push_levels_per_step": agg["push_levels"] / args.steps,
+            "pull_levels_per_step": agg["pull_levels"] / args.steps, "setup_s": setup_s,
+        }
+        print(json.dumps(line), flush=True)
+    g.close()
+    ctx.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,165 @@
+/*
+ * xbtrav.h -- C ABI of the B200 multi-source traversal engine (libxbtrav.so).
+ *
+ * The engine traverses an undirected CSR graph from many sources at once and
+ * returns, per source, an int32 level table and an int32 parent table
+ * (k x n, source-major: level[s*n + v]).  Every call returns an xb_status
+ * (0 = OK, negative = error; xb_status_str / xb_last_error explain it).
+ * Buffers are caller-owned unless a function says otherwise.  No torch or C++
+ * types cross this boundary.
+ *
+ * Reference interfaces these entry points replace (paths relative to the
+ * X-Blossom project):
+ *   CSR load            zblossom::HGraph(row_path, col_path)
+ *                       apps/xb/src/include/graph/hgraph.h:37-48, text format
+ *                       one int per line apps/xb/src/include/common/utils_cpu.h:9-23
+ *   device graph        zblossom::DGraph(const HGraph&)
+ *                       apps/xb/src/include/graph/dgraph.h:50-63
+ *   source set          exposed-vertex roots
+ *                       apps/xb/src/xblsm_gpu/xblossom_gpu_engine_10.cu:119-144;
+ *                       experiment source lists scripts/2-datasets/src_nodes/generate_src_lists.py
+ *   traversal           Engine::ExpandAlternatingForest
+ *                       apps/xb/src/xblsm_gpu/xblossom_gpu_engine_10.cu:270-359 and
+ *                       parExpand_pro_all apps/xb/src/xblsm_cpu/par_pro_pernode.cu:178-234;
+ *                       plain BFS semantics apps/ligra/apps/BFS.C:26-53
+ *   level / parent      PathTable root_distance_ / ExpandTwoNodes
+ *                       apps/xb/src/include/path_table/path_table.h:222,256-271
+ */
+#ifndef XBTRAV_H
+#define XBTRAV_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define XB_ABI_VERSION 1
+
+typedef int32_t xb_status;
+#define XB_OK 0
+#define XB_ERR_ARG (-1)      /* bad argument (null pointer, out-of-range id, size) */
+#define XB_ERR_OOM (-2)      /* device or host allocation failed */
+#define XB_ERR_CAPACITY (-3) /* a table or queue would overflow its fixed capacity */
+#define XB_ERR_TIMEOUT (-4)  /* a bounded device-side wait gave up */
+#define XB_ERR_CUDA (-5)     /* a CUDA runtime call failed */
+#define XB_ERR_IO (-6)       /* file could not be read or written */
+#define XB_ERR_NODEV (-7)    /* no usable CUDA device */
+#define XB_ERR_STATE (-8)    /* object used in the wrong state */
+
+#define XB_MODE_PLAIN 0       /* independent BFS per source */
+#define XB_MODE_ALTERNATING 1 /* reserved: alternating forest over a matching */
+
+/* xb_traverse flags */
+#define XB_OUT_DEVICE 1u     /* level/parent are device pointers (else host) */
+#define XB_SOURCES_DEVICE 2u /* sources is a device pointer (else host) */
+
+typedef struct xb_host_csr xb_host_csr; /* host-resident CSR (int64 offsets) */
+typedef struct xb_ctx xb_ctx;           /* device, stream, workspace */
+typedef struct xb_graph xb_graph;       /* device-resident CSR */
+
+/* Counters of one traversal call.  edges_traversed is the work unit of the
+ * GTEPS metric: sum over sources of sum over reached vertices of deg(v), the
+ * "Processed Edges" of apps/ligra/apps/BFS_Throughput.C:42-63. */
+typedef struct xb_stats {
+  int64_t edges_traversed;  /* GTEPS numerator */
+  int64_t reached;          /* sum over sources of reached vertices */
+  int64_t edges_scanned;    /* CSR entries read by the level steps */
+  int64_t vertices_scanned; /* vertices whose adjacency the level steps read */
+  int64_t vertices_swept;   /* vertex state words swept by the level steps */
+  int64_t parent_edges_scanned; /* CSR entries read by the parent pass */
+  int64_t algo_bytes;       /* algorithmic HBM bytes of the whole call */
+  int32_t levels;           /* max depth + 1 over all sources */
+  int32_t push_levels;
+  int32_t pull_levels;
+  int32_t batches;          /* source words processed */
+  double device_ms;         /* device time of the call (CUDA events) */
+  /* per kernel class (0 = level steps, 1 = parent/table pass, 2 = other):
+   * launches, device ms (events; only when timing is enabled) and
+   * algorithmic bytes. */
+  int64_t class_launches[3];
+  double class_ms[3];
+  int64_t class_bytes[3];
+} xb_stats;
+
+/* Tunables of the engine (the autotuner's search space). */
+typedef struct xb_tuning {
+  int32_t word_bits;       /* sources per word: 32 or 64 */
+  int32_t words;           /* words per vertex traversed together: 1, 2 or 4 */
+  float pull_alpha;        /* pull when frontier_edges*alpha > unfinished_edges */
+  int32_t heavy_degree;    /* vertices above this degree get block-wide passes */
+  int32_t timing;          /* 1 = record per-class CUDA events into xb_stats */
+} xb_tuning;
+
+/* ---- status ------------------------------------------------------------ */
+const char* xb_status_str(xb_status s);
+/* Message of the last error raised on the calling thread ("" if none). */
+const char* xb_last_error(void);
+int32_t xb_abi_version(void);
+
+/* ---- host CSR (no GPU needed) ------------------------------------------ */
+/* Seeded undirected R-MAT: n = 2^scale, n*edge_factor sampled pairs with
+ * quadrant probabilities a, b, c (d = 1-a-b-c); symmetrised, self-loops and
+ * duplicates removed, adjacency sorted ascending.  threads <= 0: all cores. */
+xb_status xb_csr_gen_rmat(int32_t scale, int32_t edge_factor, double a, double b, double c,
+                          uint64_t seed, int32_t threads, xb_host_csr** out);
+/* Seeded Erdos-Renyi style graph: m_pairs uniform vertex pairs, same cleaning. */
+xb_status xb_csr_gen_er(int64_t n, int64_t m_pairs, uint64_t seed, int32_t threads,
+                        xb_host_csr** out);
+/* Copies and validates a CSR (ids in range; offsets non-decreasing). */
+xb_status xb_csr_from_arrays(int64_t n, const int64_t* row_offsets, const int32_t* col_indices,
+                             xb_host_csr** out);
+/* Reference text format: one integer per line, row offsets file and column
+ * indices file (HGraph(row_path, col_path), hgraph.h:37-48). */
+xb_status xb_csr_load_text(const char* row_path, const char* col_path, xb_host_csr** out);
+xb_status xb_csr_save_text(const xb_host_csr* g, const char* row_path, const char* col_path);
+xb_status xb_csr_info(const xb_host_csr* g, int64_t* n, int64_t* m, int64_t* max_degree,
+                      int64_t* isolated);
+/* Borrowed pointers, valid until xb_csr_free. */
+xb_status xb_csr_arrays(const xb_host_csr* g, const int64_t** row_offsets,
+                        const int32_t** col_indices);
+void xb_csr_free(xb_host_csr* g);
+/* k distinct sources drawn uniformly without replacement from the vertices of
+ * non-zero degree, splitmix64 stream seeded by seed. */
+xb_status xb_select_sources_csr(int64_t n, const int64_t* row_offsets, uint64_t seed, int32_t k,
+                                int32_t* out);
+
+/* ---- device context and graphs ----------------------------------------- */
+xb_status xb_ctx_create(int32_t device, xb_ctx** out);
+xb_status xb_ctx_destroy(xb_ctx* ctx);
+xb_status xb_ctx_set_tuning(xb_ctx* ctx, const xb_tuning* t);
+xb_status xb_ctx_get_tuning(const xb_ctx* ctx, xb_tuning* t);
+/* Device workspace bytes currently held by the context. */
+xb_status xb_ctx_workspace_bytes(const xb_ctx* ctx, int64_t* bytes);
+/* The context's CUDA stream (a cudaStream_t), for callers that order their
+ * own work or timing events against the engine's launches. */
+xb_status xb_ctx_get_stream(const xb_ctx* ctx, void** stream);
+
+/* Uploads a CSR (row offsets int32 or int64 as offsets_are_64bit says; host
+ * pointers) and keeps it resident. */
+xb_status xb_graph_upload(xb_ctx* ctx, int64_t n, const void* row_offsets,
+                          int32_t offsets_are_64bit, int64_t m, const int32_t* col_indices,
+                          xb_graph** out);
+xb_status xb_graph_from_host_csr(xb_ctx* ctx, const xb_host_csr* g, xb_graph** out);
+xb_status xb_graph_load_csr_text(xb_ctx* ctx, const char* row_path, const char* col_path,
+                                 xb_graph** out);
+xb_status xb_graph_free(xb_graph* g);
+xb_status xb_graph_info(const xb_graph* g, int64_t* n, int64_t* m, int64_t* max_degree);
+xb_status xb_select_sources(const xb_graph* g, uint64_t seed, int32_t k, int32_t* out);
+
+/* ---- traversal ---------------------------------------------------------- */
+/* Plain per-call path (the drop-in).  k sources; level and parent receive
+ * k*n int32 each, source-major.  level = hop distance (-1 unreached); parent =
+ * the smallest-id neighbour one level closer to the source (the source's own
+ * parent is itself; -1 unreached).  Sources are processed 64 (or 32) per
+ * word, one word per launch sequence, with a host-side level loop.
+ * mode must be XB_MODE_PLAIN; matching and owner must be NULL. */
+xb_status xb_traverse(xb_ctx* ctx, const xb_graph* g, const int32_t* sources, int32_t k,
+                      int32_t mode, const int32_t* matching, int32_t* level, int32_t* parent,
+                      int32_t* owner, uint32_t flags, xb_stats* stats);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* XBTRAV_H */

@@ -1,0 +1,188 @@
+/*
+ * msbfs_oracle.c -- CPU oracle for the multi-source traversal path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is the checker: only tests/,
+ * __graft_entry__.smoke() and bench.py's cpu_baseline / --impl reference legs
+ * load it.  The product (libxbtrav.so) never links or calls it.
+ *
+ * What it restates (reference paths are relative to the X-Blossom project):
+ *
+ *  - Plain multi-source BFS.  One independent breadth-first search per source
+ *    over an undirected CSR graph, producing an int32 level table and an int32
+ *    parent table per source (k x n, source-major).
+ *      * level[s][v]  = hop distance from source s, -1 if unreached.
+ *      * parent[s][s] = s: the root convention of
+ *        apps/ligra/apps/BFS.C:47 (Parents[start] = start) and of the
+ *        reference's root initialisation apps/xb/src/xblsm_gpu/xblossom_gpu_engine_10.cu:119-144.
+ *      * parent rule ORACLE_RULE_MINID: parent[s][v] = the smallest vertex id u
+ *        adjacent to v with level[s][u] == level[s][v]-1.  This is the
+ *        deterministic rule the GPU engine implements.  The reference's own
+ *        parents (Ligra CAS, apps/ligra/apps/BFS.C:33-35; XB-Pro CAS claims,
+ *        apps/xb/src/xblsm_cpu/par_pro_pernode.cu:203-215) are first-writer-wins
+ *        and schedule dependent, so every one of them is merely *a* valid
+ *        predecessor at level-1; the min-id rule picks one of those.
+ *      * parent rule ORACLE_RULE_FIFO: the first discoverer in a FIFO queue
+ *        whose neighbours are visited in CSR order.  This is the rule of the
+ *        reference's only deterministic BFS with predecessors,
+ *        xblossom::Graph::findShortestPath, apps/xb/src/include/graph/xgraph.h:155-191
+ *        (adjacency built in CSR order by buildAdjListFromCSR, xgraph.h:347-356).
+ *  - The work unit: edges traversed = sum over sources of sum over reached
+ *    vertices of deg(v), the "Processed Edges" count of
+ *    apps/ligra/apps/BFS_Throughput.C:42-63,77 and
+ *    apps/xb/runner/xblsm_gpu/run_xb_pp_by_dataset.cu:117,152.
+ *  - Work split over host threads: the chunked fetch_add idiom of the
+ *    reference CPU engine (apps/xb/src/xblsm_cpu/par_pro_pernode.cu:111-118),
+ *    here over sources instead of frontier vertices.
+ *
+ * Parity pinning: the level rule and the FIFO parent rule are checked against
+ * the reference's own code (xgraph.h findShortestPath and Ligra BFS_F/edgeMap,
+ * compiled from the reference sources by oracle/Makefile into oracle/_ref/)
+ * through the fixtures in tests/golden/.
+ */
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#include <pthread.h>
+#include <stdatomic.h>
+
+#define ORACLE_RULE_MINID 0
+#define ORACLE_RULE_FIFO 1
+
+typedef struct {
+    int64_t n;
+    const int64_t *ro;
+    const int32_t *ci;
+    const int32_t *src;
+    int32_t k;
+    int32_t rule;
+    int32_t *level;   /* k*n or NULL */
+    int32_t *parent;  /* k*n or NULL */
+    atomic_long next; /* next source index to claim */
+    atomic_llong edges;
+    atomic_llong reached;
+    int chunk;
+} job_t;
+
+/* One BFS from s.  lvl/par are the rows for this source (n entries). */
+static void bfs_one(const job_t *j, int32_t s, int32_t *lvl, int32_t *par,
+                    int32_t *queue, long long *edges_out, long long *reached_out) {
+    const int64_t n = j->n;
+    for (int64_t v = 0; v < n; v++) { lvl[v] = -1; par[v] = -1; }
+    int64_t head = 0, tail = 0;
+    queue[tail++] = s;
+    lvl[s] = 0;
+    par[s] = s;
+    long long edges = 0;
+    while (head < tail) {
+        int32_t u = queue[head++];
+        int64_t b = j->ro[u], e = j->ro[u + 1];
+        edges += (long long)(e - b);
+        for (int64_t p = b; p < e; p++) {
+            int32_t w = j->ci[p];
+            if (lvl[w] < 0) {
+                lvl[w] = lvl[u] + 1;
+                par[w] = u; /* FIFO first discoverer */
+                queue[tail++] = w;
+            }
+        }
+    }
+    if (j->rule == ORACLE_RULE_MINID) {
+        /* parent = smallest adjacent id one level up */
+        for (int64_t q = 0; q < tail; q++) {
+            int32_t v = queue[q];
+            if (v == s) continue;
+            int32_t best = -1;
+            for (int64_t p = j->ro[v]; p < j->ro[v + 1]; p++) {
+                int32_t u = j->ci[p];
+                if (lvl[u] == lvl[v] - 1 && (best < 0 || u < best)) best = u;
+            }
+            par[v] = best;
+        }
+    }
+    *edges_out = edges;
+    *reached_out = tail;
+}
+
+static void *worker(void *arg) {
+    job_t *j = (job_t *)arg;
+    int32_t *queue = (int32_t *)malloc(sizeof(int32_t) * (size_t)(j->n > 0 ? j->n : 1));
+    int32_t *lvl_tmp = NULL, *par_tmp = NULL;
+    if (!j->level) lvl_tmp = (int32_t *)malloc(sizeof(int32_t) * (size_t)(j->n > 0 ? j->n : 1));
+    if (!j->parent) par_tmp = (int32_t *)malloc(sizeof(int32_t) * (size_t)(j->n > 0 ? j->n : 1));
+    for (;;) {
+        long b = atomic_fetch_add(&j->next, j->chunk);
+        if (b >= j->k) break;
+        long e = b + j->chunk < j->k ? b + j->chunk : j->k;
+        for (long i = b; i < e; i++) {
+            int32_t *lvl = j->level ? j->level + (size_t)i * (size_t)j->n : lvl_tmp;
+            int32_t *par = j->parent ? j->parent + (size_t)i * (size_t)j->n : par_tmp;
+            long long ed = 0, rc = 0;
+            bfs_one(j, j->src[i], lvl, par, queue, &ed, &rc);
+            atomic_fetch_add(&j->edges, ed);
+            atomic_fetch_add(&j->reached, rc);
+        }
+    }
+    free(queue);
+    free(lvl_tmp);
+    free(par_tmp);
+    return NULL;
+}
+
+/*
+ * Plain multi-source BFS.  Returns 0 on success, -1 on a bad argument.
+ * level/parent may be NULL (then the search runs but the table is dropped,
+ * used by the timed CPU baseline).  edges_traversed/reached may be NULL.
+ */
+int oracle_msbfs(int64_t n, const int64_t *row_offsets, const int32_t *col_indices,
+                 const int32_t *sources, int32_t k, int32_t rule,
+                 int32_t *level, int32_t *parent,
+                 long long *edges_traversed, long long *reached, int32_t threads) {
+    if (n < 0 || k < 0 || (k > 0 && (!sources || !row_offsets))) return -1;
+    if (rule != ORACLE_RULE_MINID && rule != ORACLE_RULE_FIFO) return -1;
+    for (int32_t i = 0; i < k; i++)
+        if (sources[i] < 0 || sources[i] >= n) return -1;
+    job_t j;
+    memset(&j, 0, sizeof(j));
+    j.n = n; j.ro = row_offsets; j.ci = col_indices; j.src = sources; j.k = k;
+    j.rule = rule; j.level = level; j.parent = parent;
+    atomic_init(&j.next, 0);
+    atomic_init(&j.edges, 0);
+    atomic_init(&j.reached, 0);
+    j.chunk = 1;
+    if (threads < 1) threads = 1;
+    if (threads > k) threads = k > 0 ? k : 1;
+    if (threads == 1) {
+        worker(&j);
+    } else {
+        pthread_t *tid = (pthread_t *)malloc(sizeof(pthread_t) * (size_t)threads);
+        for (int t = 0; t < threads; t++) pthread_create(&tid[t], NULL, worker, &j);
+        for (int t = 0; t < threads; t++) pthread_join(tid[t], NULL);
+        free(tid);
+    }
+    if (edges_traversed) *edges_traversed = atomic_load(&j.edges);
+    if (reached) *reached = atomic_load(&j.reached);
+    return 0;
+}
+
+/*
+ * Checks that parent[] (one source row) is a valid BFS predecessor table for
+ * level[] (same row): parent[s]==s at level 0, every other reached v has an
+ * edge (parent[v], v) with level[parent[v]] == level[v]-1, unreached vertices
+ * carry -1.  Returns the number of violations.  This is the acceptance rule
+ * for schedule-dependent reference parents (Ligra CAS, XB-Pro claims).
+ */
+long long oracle_check_parents(int64_t n, const int64_t *ro, const int32_t *ci,
+                               int32_t s, const int32_t *level, const int32_t *parent) {
+    long long bad = 0;
+    for (int64_t v = 0; v < n; v++) {
+        int32_t L = level[v], p = parent[v];
+        if (L < 0) { if (p != -1) bad++; continue; }
+        if (v == s) { if (L != 0 || p != s) bad++; continue; }
+        if (p < 0 || p >= n || level[p] != L - 1) { bad++; continue; }
+        int found = 0;
+        for (int64_t q = ro[v]; q < ro[v + 1]; q++)
+            if (ci[q] == p) { found = 1; break; }
+        if (!found) bad++;
+    }
+    return bad;
+}

@@ -1,0 +1,151 @@
+"""CPU oracle loader -- TEST INFRASTRUCTURE ONLY.
+
+Loads the C restatement (oracle/liboracle_msbfs.so, built from
+oracle/msbfs_oracle.c) and, where it was built, the reference's own code
+compiled from the reference sources into oracle/_ref/ (Ligra BFS and
+xblossom::Graph::findShortestPath).  Only tests/, __graft_entry__.smoke()
+and bench.py's CPU-baseline legs import this module; the product never does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "liboracle_msbfs.so")
+REF_DIR = os.path.join(HERE, "_ref")
+LIGRA_SO = os.path.join(REF_DIR, "libligra_bfs_ref.so")
+XGRAPH_SO = os.path.join(REF_DIR, "libxgraph_fifo_ref.so")
+
+RULE_MINID = 0
+RULE_FIFO = 1
+
+_o = None
+_lig = None
+_xg = None
+
+
+def build(ref_root: str | None = None) -> None:
+    """Builds the C restatement, and the reference checkers when the reference tree exists."""
+    subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
+    root = ref_root or "/root/reference"
+    if os.path.isdir(os.path.join(root, "apps")):
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF_ROOT={root}"], check=True)
+
+
+def _load() -> C.CDLL:
+    global _o
+    if _o is None:
+        if not os.path.exists(ORACLE_SO):
+            build()
+        L = C.CDLL(ORACLE_SO)
+        L.oracle_msbfs.restype = C.c_int
+        L.oracle_msbfs.argtypes = [C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32,
+                                   C.c_void_p, C.c_void_p, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong),
+                                   C.c_int32]
+        L.oracle_check_parents.restype = C.c_longlong
+        L.oracle_check_parents.argtypes = [C.c_int64, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]
+        _o = L
+    return _o
+
+
+def msbfs(ro: np.ndarray, ci: np.ndarray, sources: np.ndarray, rule: int = RULE_MINID, threads: int = 0,
+          want_tables: bool = True):
+    """Plain multi-source BFS on the CPU.  Returns (level, parent, edges_traversed, reached)."""
+    ro = np.ascontiguousarray(ro, dtype=np.int64)
+    ci = np.ascontiguousarray(ci, dtype=np.int32)
+    src = np.ascontiguousarray(sources, dtype=np.int32)
+    n, k = len(ro) - 1, len(src)
+    lvl = np.empty((k, n), np.int32) if want_tables else None
+    par = np.empty((k, n), np.int32) if want_tables else None
+    e, r = C.c_longlong(), C.c_longlong()
+    if threads <= 0:
+        threads = os.cpu_count() or 1
+    rc = _load().oracle_msbfs(n, ro.ctypes.data, ci.ctypes.data if len(ci) else None, src.ctypes.data, k, rule,
+                              lvl.ctypes.data if want_tables else None, par.ctypes.data if want_tables else None,
+                              C.byref(e), C.byref(r), threads)
+    if rc != 0:
+        raise ValueError("oracle_msbfs rejected its arguments")
+    return lvl, par, e.value, r.value
+
+
+def check_parents(ro, ci, s: int, level_row: np.ndarray, parent_row: np.ndarray) -> int:
+    """Number of entries of parent_row that are not a valid BFS predecessor under level_row."""
+    ro = np.ascontiguousarray(ro, dtype=np.int64)
+    ci = np.ascontiguousarray(ci, dtype=np.int32)
+    lv = np.ascontiguousarray(level_row, dtype=np.int32)
+    pr = np.ascontiguousarray(parent_row, dtype=np.int32)
+    return int(_load().oracle_check_parents(len(ro) - 1, ro.ctypes.data, ci.ctypes.data if len(ci) else None, s,
+                                            lv.ctypes.data, pr.ctypes.data))
+
+
+# ---- the reference's own code (built from its sources) ---------------------
+
+def ligra_available() -> bool:
+    return os.path.exists(LIGRA_SO)
+
+
+def xgraph_available() -> bool:
+    return os.path.exists(XGRAPH_SO)
+
+
+def _ligra() -> C.CDLL:
+    global _lig
+    if _lig is None:
+        L = C.CDLL(LIGRA_SO)
+        L.ligra_ref_bfs.restype = C.c_double
+        L.ligra_ref_bfs.argtypes = [C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p,
+                                    C.POINTER(C.c_int64), C.c_int32]
+        L.ligra_ref_workers.restype = C.c_int32
+        _lig = L
+    return _lig
+
+
+def ligra_bfs(ro, ci, sources, threads: int = 0, want_parents: bool = True):
+    """Reference Ligra BFS (apps/ligra/apps/BFS.C).  Returns (parents uint32 (k,n) or None, seconds, edges)."""
+    ro = np.ascontiguousarray(ro, dtype=np.int64)
+    ci = np.ascontiguousarray(ci, dtype=np.int32)
+    src = np.ascontiguousarray(sources, dtype=np.int32)
+    n, k = len(ro) - 1, len(src)
+    par = np.empty((k, n), np.uint32) if want_parents else None
+    e = C.c_int64()
+    secs = _ligra().ligra_ref_bfs(n, ro.ctypes.data, ci.ctypes.data if len(ci) else None, src.ctypes.data, k,
+                                  par.ctypes.data if want_parents else None, C.byref(e), threads)
+    if secs < 0:
+        raise ValueError("ligra_ref_bfs rejected its arguments")
+    return par, secs, e.value
+
+
+def ligra_workers() -> int:
+    return int(_ligra().ligra_ref_workers())
+
+
+def _xgraph() -> C.CDLL:
+    global _xg
+    if _xg is None:
+        L = C.CDLL(XGRAPH_SO)
+        L.xgraph_ref_paths.restype = C.c_int32
+        L.xgraph_ref_paths.argtypes = [C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64,
+                                       C.c_void_p, C.c_void_p]
+        _xg = L
+    return _xg
+
+
+def xgraph_paths(ro, ci, src: np.ndarray, dst: np.ndarray):
+    """Reference findShortestPath (apps/xb/src/include/graph/xgraph.h:155-191) per (src, dst) pair.
+
+    Returns (level, fifo_parent) per pair.  dst must be reachable from src."""
+    ro32 = np.ascontiguousarray(ro, dtype=np.int32)
+    ci32 = np.ascontiguousarray(ci, dtype=np.int32)
+    s = np.ascontiguousarray(src, dtype=np.int32)
+    d = np.ascontiguousarray(dst, dtype=np.int32)
+    lv = np.empty(len(s), np.int32)
+    pr = np.empty(len(s), np.int32)
+    rc = _xgraph().xgraph_ref_paths(len(ro32) - 1, ro32.ctypes.data, ci32.ctypes.data if len(ci32) else None,
+                                    s.ctypes.data, d.ctypes.data, len(s), lv.ctypes.data, pr.ctypes.data)
+    if rc != 0:
+        raise ValueError("xgraph_ref_paths rejected its arguments")
+    return lv, pr

@@ -1,0 +1,620 @@
+// xb_engine.cu -- device context, resident graphs and the plain per-call
+// traversal path of libxbtrav.so (C ABI in include/xbtrav.h).
+//
+// The plain path mirrors the reference engine's control structure
+// (FindAndFlipAugmentingPathInAlternatingForest's host loop,
+// apps/xb/src/xblsm_gpu/xblossom_gpu_engine_10.cu:72-185): a host-side level
+// loop that launches one level step, reads the frontier counters back and
+// decides the next step.  Unlike the reference it reads one 200-byte counter
+// block per level (instead of four D2H scalars plus a device sync per queue
+// swap) and traverses B (32 or 64) sources per launch sequence.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "xb_internal.h"
+#include "xb_kernels.cuh"
+
+using xbi::fail;
+
+#define XB_CUDA(call)                                                                        \
+  do {                                                                                       \
+    cudaError_t e_ = (call);                                                                 \
+    if (e_ != cudaSuccess) return fail(XB_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+#define XB_LAUNCH_CHECK(what)                                                                \
+  do {                                                                                       \
+    cudaError_t e_ = cudaGetLastError();                                                     \
+    if (e_ != cudaSuccess) return fail(XB_ERR_CUDA, std::string("launch ") + what + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+struct xb_ctx {
+  int device = 0;
+  int num_sms = 148;
+  cudaStream_t stream = nullptr;
+  xb_tuning tuning{};
+  // workspace
+  void* ws = nullptr;
+  size_t ws_bytes = 0;
+  xbk::Ctrs* d_ctr = nullptr;
+  xbk::Ctrs* h_ctr = nullptr;  // pinned
+  int32_t* d_src = nullptr;
+  int64_t src_cap = 0;
+  int32_t* d_stage = nullptr;  // device staging for host-bound tables
+  size_t stage_bytes = 0;
+  int32_t epoch = 1;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, evc0 = nullptr, evc1 = nullptr;
+};
+
+struct xb_graph {
+  xb_ctx* ctx = nullptr;
+  int64_t n = 0, m = 0, max_deg = 0;
+  bool off64 = false;
+  void* d_ro = nullptr;
+  int32_t* d_ci = nullptr;
+  std::vector<int64_t> h_ro;
+  int32_t* d_heavy = nullptr;  // vertices with degree > heavy_thr, ascending
+  int32_t n_heavy = 0;
+  int32_t heavy_thr = -1;
+};
+
+namespace {
+
+struct WsLayout {
+  size_t seen, F, N, planes, touched, fl_light, fl_heavy, nl_light, nl_heavy, stamp, total;
+  int64_t plane_stride;  // in words
+  int nplanes_alloc;
+};
+
+int bitlen_levels(int64_t n) {
+  // levels are in [0, n-1]; number of bits to hold n-1, at least 3
+  int b = 0;
+  int64_t x = n > 1 ? n - 1 : 0;
+  while (x) {
+    b++;
+    x >>= 1;
+  }
+  return std::max(3, b);
+}
+
+size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
+
+WsLayout layout_for(int64_t n, int word_bytes, int nw) {
+  WsLayout L{};
+  const size_t sw = align_up((size_t)n * nw * word_bytes);
+  const size_t li = align_up((size_t)std::max<int64_t>(n, 1) * 4);
+  L.nplanes_alloc = bitlen_levels(n);
+  L.plane_stride = (int64_t)(sw / word_bytes);
+  size_t o = 0;
+  L.seen = o; o += sw;
+  L.F = o; o += sw;
+  L.N = o; o += sw;
+  L.planes = o; o += sw * L.nplanes_alloc;
+  L.touched = o; o += li;
+  L.fl_light = o; o += li;
+  L.fl_heavy = o; o += li;
+  L.nl_light = o; o += li;
+  L.nl_heavy = o; o += li;
+  L.stamp = o; o += li;
+  L.total = o;
+  return L;
+}
+
+xb_status ensure_workspace(xb_ctx* c, const WsLayout& L) {
+  if (c->ws_bytes >= L.total && c->ws) return XB_OK;
+  if (c->ws) {
+    cudaFree(c->ws);
+    c->ws = nullptr;
+    c->ws_bytes = 0;
+  }
+  cudaError_t e = cudaMalloc(&c->ws, L.total);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(XB_ERR_OOM, "workspace allocation of " + std::to_string(L.total) + " bytes failed");
+  }
+  c->ws_bytes = L.total;
+  // F, N and the stamps must start zero; everything else is reset per pass
+  XB_CUDA(cudaMemsetAsync(c->ws, 0, L.total, c->stream));
+  return XB_OK;
+}
+
+xb_status ensure_sources(xb_ctx* c, int64_t k) {
+  if (c->src_cap >= k) return XB_OK;
+  if (c->d_src) cudaFree(c->d_src);
+  c->d_src = nullptr;
+  c->src_cap = 0;
+  if (cudaMalloc(&c->d_src, sizeof(int32_t) * std::max<int64_t>(k, 1)) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(XB_ERR_OOM, "source buffer allocation failed");
+  }
+  c->src_cap = k;
+  return XB_OK;
+}
+
+xb_status ensure_stage(xb_ctx* c, size_t bytes) {
+  if (c->stage_bytes >= bytes) return XB_OK;
+  if (c->d_stage) cudaFree(c->d_stage);
+  c->d_stage = nullptr;
+  c->stage_bytes = 0;
+  if (cudaMalloc(&c->d_stage, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(XB_ERR_OOM, "table staging allocation failed");
+  }
+  c->stage_bytes = bytes;
+  return XB_OK;
+}
+
+xb_status ensure_heavy(xb_graph* g, int thr) {
+  if (g->heavy_thr == thr) return XB_OK;
+  std::vector<int32_t> hv;
+  for (int64_t v = 0; v < g->n; v++)
+    if (g->h_ro[v + 1] - g->h_ro[v] > thr) hv.push_back((int32_t)v);
+  if (g->d_heavy) cudaFree(g->d_heavy);
+  g->d_heavy = nullptr;
+  if (cudaMalloc(&g->d_heavy, sizeof(int32_t) * std::max<size_t>(hv.size(), 1)) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(XB_ERR_OOM, "heavy list allocation failed");
+  }
+  if (!hv.empty())
+    XB_CUDA(cudaMemcpy(g->d_heavy, hv.data(), sizeof(int32_t) * hv.size(), cudaMemcpyHostToDevice));
+  g->n_heavy = (int32_t)hv.size();
+  g->heavy_thr = thr;
+  return XB_OK;
+}
+
+struct ClassTimer {
+  xb_ctx* c;
+  xb_stats* st;
+  bool on;
+  void begin() {
+    if (on) cudaEventRecord(c->evc0, c->stream);
+  }
+  void end(int cls, int64_t launches) {
+    if (st) st->class_launches[cls] += launches;
+    if (!on) return;
+    cudaEventRecord(c->evc1, c->stream);
+    cudaEventSynchronize(c->evc1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->evc0, c->evc1);
+    if (st) st->class_ms[cls] += ms;
+  }
+};
+
+template <typename W, int NW, typename OffT>
+xb_status run_plain(xb_ctx* c, xb_graph* g, const int32_t* d_sources, int32_t k, int32_t* level_out,
+                    int32_t* parent_out, bool out_dev, xb_stats* st) {
+  constexpr int B = xbk::WB<W>::bits;
+  constexpr int SPP = B * NW;  // sources per pass
+  const int64_t n = g->n;
+  const int heavy = std::max(32, c->tuning.heavy_degree);
+  xb_status s = ensure_heavy(g, heavy);
+  if (s != XB_OK) return s;
+  const WsLayout L = layout_for(n, (int)sizeof(W), NW);
+  s = ensure_workspace(c, L);
+  if (s != XB_OK) return s;
+  if (!out_dev) {
+    s = ensure_stage(c, sizeof(int32_t) * 2 * (size_t)B * (size_t)n);
+    if (s != XB_OK) return s;
+  }
+  char* base = (char*)c->ws;
+  W* seen = (W*)(base + L.seen);
+  W* F = (W*)(base + L.F);
+  W* N = (W*)(base + L.N);
+  W* planes = (W*)(base + L.planes);
+  int32_t* touched = (int32_t*)(base + L.touched);
+  xbk::Lists fl{(int32_t*)(base + L.fl_light), (int32_t*)(base + L.fl_heavy)};
+  xbk::Lists nl{(int32_t*)(base + L.nl_light), (int32_t*)(base + L.nl_heavy)};
+  int32_t* stamp = (int32_t*)(base + L.stamp);
+  const size_t state_bytes = (size_t)n * NW * sizeof(W);
+  const OffT* ro = (const OffT*)g->d_ro;
+  const int32_t* ci = g->d_ci;
+  const int sms = c->num_sms;
+  const float alpha = c->tuning.pull_alpha > 0 ? c->tuning.pull_alpha : 4.0f;
+  ClassTimer timer{c, st, c->tuning.timing != 0};
+  const int64_t ntiles = (n + 31) / 32;
+  constexpr int PULL_WARPS = 8;
+  constexpr int TAB_WARPS = (B == 64) ? 4 : 8;
+  const int pull_grid = (int)std::max<int64_t>(1, std::min<int64_t>((ntiles + PULL_WARPS - 1) / PULL_WARPS, (int64_t)sms * 8));
+  const int tab_grid = (int)std::max<int64_t>(1, std::min<int64_t>((ntiles + TAB_WARPS - 1) / TAB_WARPS, (int64_t)sms * 16));
+  int max_levels = 0;
+
+  for (int64_t k0 = 0; k0 < k; k0 += SPP) {
+    const int kb = (int)std::min<int64_t>(SPP, k - k0);
+    xbk::Masks<W, NW> active{};
+    for (int i = 0; i < NW; i++) {
+      const int lo = i * B, hi = std::min(kb, (i + 1) * B);
+      W m = 0;
+      for (int b = lo; b < hi; b++) m |= (W)1 << (b - lo);
+      active.w[i] = m;
+    }
+    // reset per-pass state: seen and the first three planes; counters
+    XB_CUDA(cudaMemsetAsync(seen, 0, state_bytes, c->stream));
+    XB_CUDA(cudaMemsetAsync(planes, 0, (size_t)L.plane_stride * sizeof(W) * 3, c->stream));
+    int planes_zeroed = 3;
+    std::memset(c->h_ctr, 0, sizeof(xbk::Ctrs));
+    c->h_ctr->b.m_unfinished = g->m;
+    XB_CUDA(cudaMemcpyAsync(c->d_ctr, c->h_ctr, sizeof(xbk::Ctrs), cudaMemcpyHostToDevice, c->stream));
+    timer.begin();
+    xbk::k_init_batch<W, NW, OffT><<<1, 256, 0, c->stream>>>(d_sources + k0, kb, ro, F, seen, active, heavy, fl,
+                                                              c->d_ctr);
+    XB_LAUNCH_CHECK("init");
+    timer.end(2, 1);
+    int cur = 0, level = 0;
+    for (;;) {
+      XB_CUDA(cudaMemcpyAsync(c->h_ctr, c->d_ctr, sizeof(xbk::Ctrs), cudaMemcpyDeviceToHost, c->stream));
+      XB_CUDA(cudaStreamSynchronize(c->stream));
+      const xbk::LevelCtr lc = c->h_ctr->lv[cur];
+      const long long m_unf = c->h_ctr->b.m_unfinished;
+      const int64_t fcount = (int64_t)lc.n_light + lc.n_heavy;
+      if (fcount == 0) break;
+      const int next_level = level + 1;
+      while (planes_zeroed < L.nplanes_alloc && ((int64_t)1 << planes_zeroed) <= next_level) {
+        XB_CUDA(cudaMemsetAsync(planes + (size_t)planes_zeroed * L.plane_stride, 0,
+                                (size_t)L.plane_stride * sizeof(W), c->stream));
+        planes_zeroed++;
+      }
+      XB_CUDA(cudaMemsetAsync(&c->d_ctr->lv[cur ^ 1], 0, sizeof(xbk::LevelCtr), c->stream));
+      const bool pull = (double)lc.edges * alpha > (double)m_unf;
+      timer.begin();
+      int64_t launches = 0;
+      if (!pull) {
+        if (lc.n_light > 0) {
+          const int grid = (int)std::min<int64_t>(((int64_t)lc.n_light + 7) / 8, (int64_t)sms * 16);
+          xbk::k_push_light<W, NW, OffT><<<grid, 256, 0, c->stream>>>(fl.light, &c->d_ctr->lv[cur].n_light, ro, ci,
+                                                                      F, seen, N, stamp, c->epoch, touched,
+                                                                      c->d_ctr, cur);
+          XB_LAUNCH_CHECK("push_light");
+          launches++;
+        }
+        if (lc.n_heavy > 0) {
+          const int grid = (int)std::min<int64_t>(lc.n_heavy, (int64_t)sms * 4);
+          xbk::k_push_heavy<W, NW, OffT><<<grid, 512, 0, c->stream>>>(fl.heavy, &c->d_ctr->lv[cur].n_heavy, ro, ci,
+                                                                      F, seen, N, stamp, c->epoch, touched,
+                                                                      c->d_ctr, cur);
+          XB_LAUNCH_CHECK("push_heavy");
+          launches++;
+        }
+        // the touched count is on the device; size the grid for the worst case
+        const int fgrid = (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)sms * 8));
+        xbk::k_push_finalize<W, NW, OffT><<<fgrid, 256, 0, c->stream>>>(touched, ro, N, seen, planes, L.plane_stride,
+                                                                        next_level, active, heavy, nl, c->d_ctr, cur);
+        XB_LAUNCH_CHECK("push_finalize");
+        launches++;
+        if (st) st->push_levels++;
+      } else {
+        xbk::k_pull_tiles<W, NW, OffT, PULL_WARPS><<<pull_grid, PULL_WARPS * 32, 0, c->stream>>>(
+            n, ro, ci, F, seen, N, planes, L.plane_stride, next_level, active, heavy, nl, c->d_ctr, cur);
+        XB_LAUNCH_CHECK("pull_tiles");
+        launches++;
+        if (g->n_heavy > 0) {
+          const int grid = (int)std::min<int64_t>(g->n_heavy, (int64_t)sms * 4);
+          xbk::k_pull_heavy<W, NW, OffT><<<grid, 512, 0, c->stream>>>(g->d_heavy, g->n_heavy, ro, ci, F, seen, N,
+                                                                      planes, L.plane_stride, next_level, active,
+                                                                      heavy, nl, c->d_ctr, cur);
+          XB_LAUNCH_CHECK("pull_heavy");
+          launches++;
+        }
+        // zero the consumed frontier
+        if (fcount * 16 < n) {
+          if (lc.n_light > 0) {
+            xbk::k_clear_list<W, NW><<<(int)std::min<int64_t>((lc.n_light * NW + 255) / 256, sms * 8), 256, 0,
+                                       c->stream>>>(fl.light, &c->d_ctr->lv[cur].n_light, F);
+            launches++;
+          }
+          if (lc.n_heavy > 0) {
+            xbk::k_clear_list<W, NW><<<(int)std::min<int64_t>((lc.n_heavy * NW + 255) / 256, sms * 8), 256, 0,
+                                       c->stream>>>(fl.heavy, &c->d_ctr->lv[cur].n_heavy, F);
+            launches++;
+          }
+          XB_LAUNCH_CHECK("clear_list");
+        } else {
+          XB_CUDA(cudaMemsetAsync(F, 0, state_bytes, c->stream));
+        }
+        if (st) st->pull_levels++;
+      }
+      timer.end(0, launches);
+      c->epoch++;
+      if (c->epoch == INT32_MAX) {  // stamps wrap: clear them
+        XB_CUDA(cudaMemsetAsync(stamp, 0, sizeof(int32_t) * n, c->stream));
+        c->epoch = 1;
+      }
+      std::swap(F, N);
+      std::swap(fl, nl);
+      cur ^= 1;
+      level = next_level;
+    }
+    max_levels = std::max(max_levels, level);
+    // tables, one word at a time
+    for (int wi = 0; wi < NW; wi++) {
+      const int kbw = std::min(B, kb - wi * B);
+      if (kbw <= 0) break;
+      const int64_t s0 = k0 + (int64_t)wi * B;
+      int32_t* lv_out = out_dev ? level_out + s0 * n : c->d_stage;
+      int32_t* pr_out = out_dev ? parent_out + s0 * n : c->d_stage + (size_t)B * n;
+      timer.begin();
+      xbk::k_tables<W, NW, OffT, TAB_WARPS><<<tab_grid, TAB_WARPS * 32, 0, c->stream>>>(
+          n, ro, ci, seen, planes, L.plane_stride, planes_zeroed, wi, kbw, heavy, lv_out, pr_out, c->d_ctr);
+      XB_LAUNCH_CHECK("tables");
+      int64_t launches = 1;
+      if (g->n_heavy > 0) {
+        const int grid = (int)std::min<int64_t>(g->n_heavy, (int64_t)sms * 4);
+        xbk::k_tables_heavy<W, NW, OffT><<<grid, 256, 0, c->stream>>>(g->d_heavy, g->n_heavy, n, ro, ci, seen, planes,
+                                                                       L.plane_stride, planes_zeroed, wi, kbw, lv_out,
+                                                                       pr_out, c->d_ctr);
+        XB_LAUNCH_CHECK("tables_heavy");
+        launches++;
+      }
+      timer.end(1, launches);
+      if (!out_dev) {
+        XB_CUDA(cudaMemcpyAsync(level_out + s0 * n, lv_out, sizeof(int32_t) * (size_t)kbw * n, cudaMemcpyDeviceToHost,
+                                c->stream));
+        XB_CUDA(cudaMemcpyAsync(parent_out + s0 * n, pr_out, sizeof(int32_t) * (size_t)kbw * n,
+                                cudaMemcpyDeviceToHost, c->stream));
+      }
+    }
+    XB_CUDA(cudaMemcpyAsync(c->h_ctr, c->d_ctr, sizeof(xbk::Ctrs), cudaMemcpyDeviceToHost, c->stream));
+    XB_CUDA(cudaStreamSynchronize(c->stream));
+    if (st) {
+      const xbk::BatchCtr& b = c->h_ctr->b;
+      st->edges_traversed += (int64_t)b.edges_traversed;
+      st->reached += (int64_t)b.reached;
+      st->edges_scanned += (int64_t)b.edges_scanned;
+      st->vertices_scanned += (int64_t)b.vertices_scanned;
+      st->vertices_swept += (int64_t)b.vertices_swept;
+      st->parent_edges_scanned += (int64_t)b.parent_edges;
+      st->batches += 1;
+      // algorithmic bytes (level steps): offsets pair + colIndices + gathered
+      // words per scanned edge, a three-word sweep per swept vertex
+      const int64_t R = (int64_t)sizeof(OffT) * 2;
+      const int64_t wbytes = (int64_t)sizeof(W) * NW;
+      const int64_t lvl_bytes = R * (int64_t)b.vertices_scanned + (4 + wbytes) * (int64_t)b.edges_scanned +
+                                3 * wbytes * (int64_t)b.vertices_swept;
+      // table pass: per vertex its seen+planes words and offsets, per scanned
+      // edge colIndices + three gathered words, and the written tables
+      const int64_t tab_bytes = (int64_t)n * (R + wbytes * (1 + planes_zeroed)) +
+                                (4 + 3 * (int64_t)sizeof(W)) * (int64_t)b.parent_edges + 8 * (int64_t)kb * n;
+      st->class_bytes[0] += lvl_bytes;
+      st->class_bytes[1] += tab_bytes;
+      st->algo_bytes += lvl_bytes + tab_bytes;
+    }
+  }
+  if (st) st->levels = std::max(st->levels, max_levels);
+  return XB_OK;
+}
+
+template <typename W, typename OffT>
+xb_status dispatch_nw(xb_ctx* c, xb_graph* g, const int32_t* d_src, int32_t k, int32_t* lv, int32_t* pr, bool od,
+                      xb_stats* st) {
+  switch (c->tuning.words) {
+    case 1: return run_plain<W, 1, OffT>(c, g, d_src, k, lv, pr, od, st);
+    case 2: return run_plain<W, 2, OffT>(c, g, d_src, k, lv, pr, od, st);
+    case 4: return run_plain<W, 4, OffT>(c, g, d_src, k, lv, pr, od, st);
+    default: return fail(XB_ERR_ARG, "tuning.words must be 1, 2 or 4");
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+xb_status xb_ctx_create(int32_t device, xb_ctx** out) {
+  xbi::clear_error();
+  if (!out) return fail(XB_ERR_ARG, "null out");
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return fail(XB_ERR_NODEV, std::string("no CUDA device: ") + cudaGetErrorString(e));
+  }
+  if (device < 0 || device >= ndev) return fail(XB_ERR_ARG, "device index out of range");
+  XB_CUDA(cudaSetDevice(device));
+  std::unique_ptr<xb_ctx> c(new xb_ctx());
+  c->device = device;
+  XB_CUDA(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device));
+  XB_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  XB_CUDA(cudaMalloc(&c->d_ctr, sizeof(xbk::Ctrs)));
+  XB_CUDA(cudaMallocHost(&c->h_ctr, sizeof(xbk::Ctrs)));
+  XB_CUDA(cudaEventCreate(&c->ev0));
+  XB_CUDA(cudaEventCreate(&c->ev1));
+  XB_CUDA(cudaEventCreate(&c->evc0));
+  XB_CUDA(cudaEventCreate(&c->evc1));
+  c->tuning.word_bits = 64;
+  c->tuning.words = 1;
+  c->tuning.pull_alpha = 4.0f;
+  c->tuning.heavy_degree = 2048;
+  c->tuning.timing = 0;
+  *out = c.release();
+  return XB_OK;
+}
+
+xb_status xb_ctx_destroy(xb_ctx* c) {
+  xbi::clear_error();
+  if (!c) return XB_OK;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->ws) cudaFree(c->ws);
+  if (c->d_src) cudaFree(c->d_src);
+  if (c->d_stage) cudaFree(c->d_stage);
+  if (c->d_ctr) cudaFree(c->d_ctr);
+  if (c->h_ctr) cudaFreeHost(c->h_ctr);
+  for (cudaEvent_t ev : {c->ev0, c->ev1, c->evc0, c->evc1})
+    if (ev) cudaEventDestroy(ev);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return XB_OK;
+}
+
+xb_status xb_ctx_set_tuning(xb_ctx* c, const xb_tuning* t) {
+  xbi::clear_error();
+  if (!c || !t) return fail(XB_ERR_ARG, "null argument");
+  if (t->word_bits != 32 && t->word_bits != 64) return fail(XB_ERR_ARG, "word_bits must be 32 or 64");
+  if (t->words != 1 && t->words != 2 && t->words != 4) return fail(XB_ERR_ARG, "words must be 1, 2 or 4");
+  if (!(t->pull_alpha > 0)) return fail(XB_ERR_ARG, "pull_alpha must be positive");
+  if (t->heavy_degree < 32 || t->heavy_degree > (1 << 20))
+    return fail(XB_ERR_ARG, "heavy_degree must be in [32, 2^20]");
+  c->tuning = *t;
+  return XB_OK;
+}
+
+xb_status xb_ctx_get_tuning(const xb_ctx* c, xb_tuning* t) {
+  xbi::clear_error();
+  if (!c || !t) return fail(XB_ERR_ARG, "null argument");
+  *t = c->tuning;
+  return XB_OK;
+}
+
+xb_status xb_ctx_workspace_bytes(const xb_ctx* c, int64_t* bytes) {
+  xbi::clear_error();
+  if (!c || !bytes) return fail(XB_ERR_ARG, "null argument");
+  *bytes = (int64_t)(c->ws_bytes + c->stage_bytes + sizeof(int32_t) * c->src_cap);
+  return XB_OK;
+}
+
+xb_status xb_ctx_get_stream(const xb_ctx* c, void** stream) {
+  xbi::clear_error();
+  if (!c || !stream) return fail(XB_ERR_ARG, "null argument");
+  *stream = (void*)c->stream;
+  return XB_OK;
+}
+
+xb_status xb_graph_upload(xb_ctx* c, int64_t n, const void* row_offsets, int32_t offsets_are_64bit, int64_t m,
+                          const int32_t* col_indices, xb_graph** out) {
+  xbi::clear_error();
+  if (!c || !out || !row_offsets) return fail(XB_ERR_ARG, "null argument");
+  if (n < 1 || n >= INT32_MAX) return fail(XB_ERR_ARG, "n must be in [1, 2^31-1)");
+  std::vector<int64_t> ro((size_t)n + 1);
+  if (offsets_are_64bit) {
+    std::memcpy(ro.data(), row_offsets, sizeof(int64_t) * (n + 1));
+  } else {
+    const int32_t* r32 = (const int32_t*)row_offsets;
+    for (int64_t i = 0; i <= n; i++) ro[i] = r32[i];
+  }
+  if (ro[n] != m) return fail(XB_ERR_ARG, "row_offsets[n] != m");
+  xb_status s = xbi::validate_csr(n, ro.data(), col_indices);
+  if (s != XB_OK) return s;
+  XB_CUDA(cudaSetDevice(c->device));
+  std::unique_ptr<xb_graph> g(new xb_graph());
+  g->ctx = c;
+  g->n = n;
+  g->m = m;
+  g->off64 = m >= (int64_t)INT32_MAX;
+  for (int64_t v = 0; v < n; v++) g->max_deg = std::max(g->max_deg, ro[v + 1] - ro[v]);
+  const size_t ro_bytes = (g->off64 ? 8 : 4) * (size_t)(n + 1);
+  if (cudaMalloc(&g->d_ro, ro_bytes) != cudaSuccess ||
+      cudaMalloc(&g->d_ci, sizeof(int32_t) * (size_t)std::max<int64_t>(m, 1)) != cudaSuccess) {
+    cudaGetLastError();
+    if (g->d_ro) cudaFree(g->d_ro);
+    if (g->d_ci) cudaFree(g->d_ci);
+    return fail(XB_ERR_OOM, "graph allocation failed");
+  }
+  if (g->off64) {
+    XB_CUDA(cudaMemcpy(g->d_ro, ro.data(), ro_bytes, cudaMemcpyHostToDevice));
+  } else {
+    std::vector<int32_t> r32((size_t)n + 1);
+    for (int64_t i = 0; i <= n; i++) r32[i] = (int32_t)ro[i];
+    XB_CUDA(cudaMemcpy(g->d_ro, r32.data(), ro_bytes, cudaMemcpyHostToDevice));
+  }
+  if (m > 0) XB_CUDA(cudaMemcpy(g->d_ci, col_indices, sizeof(int32_t) * (size_t)m, cudaMemcpyHostToDevice));
+  g->h_ro = std::move(ro);
+  *out = g.release();
+  return XB_OK;
+}
+
+xb_status xb_graph_from_host_csr(xb_ctx* c, const xb_host_csr* h, xb_graph** out) {
+  xbi::clear_error();
+  if (!h) return fail(XB_ERR_ARG, "null host csr");
+  return xb_graph_upload(c, h->n, h->ro.data(), 1, h->ro[h->n], h->ci.data(), out);
+}
+
+xb_status xb_graph_load_csr_text(xb_ctx* c, const char* row_path, const char* col_path, xb_graph** out) {
+  xb_host_csr* h = nullptr;
+  xb_status s = xb_csr_load_text(row_path, col_path, &h);
+  if (s != XB_OK) return s;
+  s = xb_graph_from_host_csr(c, h, out);
+  xb_csr_free(h);
+  return s;
+}
+
+xb_status xb_graph_free(xb_graph* g) {
+  xbi::clear_error();
+  if (!g) return XB_OK;
+  cudaSetDevice(g->ctx->device);
+  if (g->d_ro) cudaFree(g->d_ro);
+  if (g->d_ci) cudaFree(g->d_ci);
+  if (g->d_heavy) cudaFree(g->d_heavy);
+  delete g;
+  return XB_OK;
+}
+
+xb_status xb_graph_info(const xb_graph* g, int64_t* n, int64_t* m, int64_t* max_degree) {
+  xbi::clear_error();
+  if (!g) return fail(XB_ERR_ARG, "null graph");
+  if (n) *n = g->n;
+  if (m) *m = g->m;
+  if (max_degree) *max_degree = g->max_deg;
+  return XB_OK;
+}
+
+xb_status xb_select_sources(const xb_graph* g, uint64_t seed, int32_t k, int32_t* out) {
+  xbi::clear_error();
+  if (!g) return fail(XB_ERR_ARG, "null graph");
+  return xbi::select_sources(g->n, g->h_ro.data(), seed, k, out);
+}
+
+xb_status xb_traverse(xb_ctx* c, const xb_graph* gc, const int32_t* sources, int32_t k, int32_t mode,
+                      const int32_t* matching, int32_t* level, int32_t* parent, int32_t* owner, uint32_t flags,
+                      xb_stats* st) {
+  xbi::clear_error();
+  xb_graph* g = const_cast<xb_graph*>(gc);
+  if (!c || !g) return fail(XB_ERR_ARG, "null context or graph");
+  if (g->ctx->device != c->device) return fail(XB_ERR_ARG, "graph lives on another device");
+  if (mode != XB_MODE_PLAIN) return fail(XB_ERR_ARG, "only XB_MODE_PLAIN is supported by xb_traverse");
+  if (matching || owner) return fail(XB_ERR_ARG, "matching/owner must be NULL in plain mode");
+  if (k < 0) return fail(XB_ERR_ARG, "negative source count");
+  if (k > 0 && (!sources || !level || !parent)) return fail(XB_ERR_ARG, "null sources or output tables");
+  if (st) std::memset(st, 0, sizeof(*st));
+  if (k == 0) return XB_OK;
+  XB_CUDA(cudaSetDevice(c->device));
+  const bool src_dev = (flags & XB_SOURCES_DEVICE) != 0;
+  const bool out_dev = (flags & XB_OUT_DEVICE) != 0;
+  // validate sources (host copy)
+  std::vector<int32_t> hs((size_t)k);
+  if (src_dev) {
+    XB_CUDA(cudaMemcpy(hs.data(), sources, sizeof(int32_t) * k, cudaMemcpyDeviceToHost));
+  } else {
+    std::memcpy(hs.data(), sources, sizeof(int32_t) * k);
+  }
+  for (int32_t i = 0; i < k; i++)
+    if (hs[i] < 0 || hs[i] >= g->n) return fail(XB_ERR_ARG, "source " + std::to_string(i) + " out of range");
+  xb_status s = ensure_sources(c, k);
+  if (s != XB_OK) return s;
+  XB_CUDA(cudaMemcpyAsync(c->d_src, hs.data(), sizeof(int32_t) * k, cudaMemcpyHostToDevice, c->stream));
+  XB_CUDA(cudaEventRecord(c->ev0, c->stream));
+  if (c->tuning.word_bits == 64) {
+    s = g->off64 ? dispatch_nw<unsigned long long, int64_t>(c, g, c->d_src, k, level, parent, out_dev, st)
+                 : dispatch_nw<unsigned long long, int32_t>(c, g, c->d_src, k, level, parent, out_dev, st);
+  } else {
+    s = g->off64 ? dispatch_nw<unsigned int, int64_t>(c, g, c->d_src, k, level, parent, out_dev, st)
+                 : dispatch_nw<unsigned int, int32_t>(c, g, c->d_src, k, level, parent, out_dev, st);
+  }
+  if (s != XB_OK) {
+    cudaStreamSynchronize(c->stream);
+    return s;
+  }
+  XB_CUDA(cudaEventRecord(c->ev1, c->stream));
+  XB_CUDA(cudaEventSynchronize(c->ev1));
+  if (st) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    st->device_ms = ms;
+  }
+  return XB_OK;
+}
+
+}  // extern "C"

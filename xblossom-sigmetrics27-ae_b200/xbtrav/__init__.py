@@ -1,0 +1,366 @@
+"""xbtrav -- Python binding of libxbtrav.so over its C ABI (include/xbtrav.h).
+
+The binding is a thin ctypes layer: every call goes through the extern "C"
+entry points of the in-tree shared library, the same ones a C/C++ caller of
+the reference-style API binds.  There is no Python or CPU fallback for the
+traversal: if the library or a CUDA device is missing the calls raise.
+
+Reference-facing names (paths relative to the X-Blossom project):
+  HostCSR.load_text(row, col)   <- zblossom::HGraph(row_path, col_path)
+                                   apps/xb/src/include/graph/hgraph.h:37-48
+  Context.upload(csr)           <- zblossom::DGraph(const HGraph&)
+                                   apps/xb/src/include/graph/dgraph.h:50-63
+  Context.traverse(...)         <- the expand phase of
+                                   apps/xb/src/xblsm_gpu/xblossom_gpu_engine_10.cu:270-359
+                                   returning level (root_distance_) and parent
+                                   (PathTable) tables per source.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(_HERE), "libxbtrav.so")
+
+XB_OK = 0
+XB_ERR_ARG = -1
+XB_ERR_OOM = -2
+XB_ERR_CAPACITY = -3
+XB_ERR_TIMEOUT = -4
+XB_ERR_CUDA = -5
+XB_ERR_IO = -6
+XB_ERR_NODEV = -7
+XB_ERR_STATE = -8
+
+XB_MODE_PLAIN = 0
+XB_MODE_ALTERNATING = 1
+XB_OUT_DEVICE = 1
+XB_SOURCES_DEVICE = 2
+
+
+class XbError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"xbtrav status {status}: {msg}")
+        self.status = status
+
+
+class XbStats(C.Structure):
+    _fields_ = [
+        ("edges_traversed", C.c_int64),
+        ("reached", C.c_int64),
+        ("edges_scanned", C.c_int64),
+        ("vertices_scanned", C.c_int64),
+        ("vertices_swept", C.c_int64),
+        ("parent_edges_scanned", C.c_int64),
+        ("algo_bytes", C.c_int64),
+        ("levels", C.c_int32),
+        ("push_levels", C.c_int32),
+        ("pull_levels", C.c_int32),
+        ("batches", C.c_int32),
+        ("device_ms", C.c_double),
+        ("class_launches", C.c_int64 * 3),
+        ("class_ms", C.c_double * 3),
+        ("class_bytes", C.c_int64 * 3),
+    ]
+
+    def as_dict(self) -> dict:
+        d = {}
+        for name, _ in self._fields_:
+            v = getattr(self, name)
+            d[name] = list(v) if hasattr(v, "__len__") else v
+        return d
+
+
+class XbTuning(C.Structure):
+    _fields_ = [
+        ("word_bits", C.c_int32),
+        ("words", C.c_int32),
+        ("pull_alpha", C.c_float),
+        ("heavy_degree", C.c_int32),
+        ("timing", C.c_int32),
+    ]
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Loads libxbtrav.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise FileNotFoundError(f"{LIB_PATH} is missing: build it with __graft_entry__.build()")
+    L = C.CDLL(LIB_PATH)
+    vp, i32, i64, u64, u32 = C.c_void_p, C.c_int32, C.c_int64, C.c_uint64, C.c_uint32
+    P = C.POINTER
+    sig = {
+        "xb_status_str": (C.c_char_p, [i32]),
+        "xb_last_error": (C.c_char_p, []),
+        "xb_abi_version": (i32, []),
+        "xb_csr_gen_rmat": (i32, [i32, i32, C.c_double, C.c_double, C.c_double, u64, i32, P(vp)]),
+        "xb_csr_gen_er": (i32, [i64, i64, u64, i32, P(vp)]),
+        "xb_csr_from_arrays": (i32, [i64, vp, vp, P(vp)]),
+        "xb_csr_load_text": (i32, [C.c_char_p, C.c_char_p, P(vp)]),
+        "xb_csr_save_text": (i32, [vp, C.c_char_p, C.c_char_p]),
+        "xb_csr_info": (i32, [vp, P(i64), P(i64), P(i64), P(i64)]),
+        "xb_csr_arrays": (i32, [vp, P(vp), P(vp)]),
+        "xb_csr_free": (None, [vp]),
+        "xb_select_sources_csr": (i32, [i64, vp, u64, i32, vp]),
+        "xb_ctx_create": (i32, [i32, P(vp)]),
+        "xb_ctx_destroy": (i32, [vp]),
+        "xb_ctx_set_tuning": (i32, [vp, P(XbTuning)]),
+        "xb_ctx_get_tuning": (i32, [vp, P(XbTuning)]),
+        "xb_ctx_workspace_bytes": (i32, [vp, P(i64)]),
+        "xb_ctx_get_stream": (i32, [vp, P(vp)]),
+        "xb_graph_upload": (i32, [vp, i64, vp, i32, i64, vp, P(vp)]),
+        "xb_graph_from_host_csr": (i32, [vp, vp, P(vp)]),
+        "xb_graph_load_csr_text": (i32, [vp, C.c_char_p, C.c_char_p, P(vp)]),
+        "xb_graph_free": (i32, [vp]),
+        "xb_graph_info": (i32, [vp, P(i64), P(i64), P(i64)]),
+        "xb_select_sources": (i32, [vp, u64, i32, vp]),
+        "xb_traverse": (i32, [vp, vp, vp, i32, i32, vp, vp, vp, vp, u32, P(XbStats)]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = L
+    return L
+
+
+def declared_symbols() -> list[str]:
+    """Function names declared in include/*.h (parsed from the headers)."""
+    import re
+
+    inc = os.path.join(os.path.dirname(os.path.dirname(_HERE)), "include")
+    names = []
+    for fn in sorted(os.listdir(inc)):
+        if not fn.endswith(".h"):
+            continue
+        text = open(os.path.join(inc, fn)).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        for m in re.finditer(r"^\s*(?:const\s+)?[A-Za-z_][A-Za-z0-9_]*\s*\*?\s*(xb_[a-z0-9_]+)\s*\(", text, re.M):
+            names.append(m.group(1))
+    return names
+
+
+def _check(st: int) -> None:
+    if st != XB_OK:
+        L = lib()
+        msg = L.xb_last_error().decode() or L.xb_status_str(st).decode()
+        raise XbError(st, msg)
+
+
+class HostCSR:
+    """Host-resident CSR (int64 row offsets, int32 column indices)."""
+
+    def __init__(self, handle: int):
+        self._h = C.c_void_p(handle)
+
+    @classmethod
+    def rmat(cls, scale: int, edge_factor: int, a=0.57, b=0.19, c=0.19, seed=0x5EED, threads=0) -> "HostCSR":
+        h = C.c_void_p()
+        _check(lib().xb_csr_gen_rmat(scale, edge_factor, a, b, c, seed, threads, C.byref(h)))
+        return cls(h.value)
+
+    @classmethod
+    def er(cls, n: int, m_pairs: int, seed=0x5EED, threads=0) -> "HostCSR":
+        h = C.c_void_p()
+        _check(lib().xb_csr_gen_er(n, m_pairs, seed, threads, C.byref(h)))
+        return cls(h.value)
+
+    @classmethod
+    def from_arrays(cls, row_offsets, col_indices) -> "HostCSR":
+        ro = np.ascontiguousarray(row_offsets, dtype=np.int64)
+        ci = np.ascontiguousarray(col_indices, dtype=np.int32)
+        h = C.c_void_p()
+        _check(lib().xb_csr_from_arrays(len(ro) - 1, ro.ctypes.data, ci.ctypes.data if len(ci) else None,
+                                        C.byref(h)))
+        return cls(h.value)
+
+    @classmethod
+    def load_text(cls, row_path: str, col_path: str) -> "HostCSR":
+        h = C.c_void_p()
+        _check(lib().xb_csr_load_text(row_path.encode(), col_path.encode(), C.byref(h)))
+        return cls(h.value)
+
+    def save_text(self, row_path: str, col_path: str) -> None:
+        _check(lib().xb_csr_save_text(self._h, row_path.encode(), col_path.encode()))
+
+    def info(self) -> dict:
+        n, m, md, iso = C.c_int64(), C.c_int64(), C.c_int64(), C.c_int64()
+        _check(lib().xb_csr_info(self._h, C.byref(n), C.byref(m), C.byref(md), C.byref(iso)))
+        return {"n": n.value, "m": m.value, "max_degree": md.value, "isolated": iso.value}
+
+    def arrays(self) -> tuple[np.ndarray, np.ndarray]:
+        """Copies of (row_offsets int64[n+1], col_indices int32[m])."""
+        inf = self.info()
+        ro, ci = C.c_void_p(), C.c_void_p()
+        _check(lib().xb_csr_arrays(self._h, C.byref(ro), C.byref(ci)))
+        r = np.ctypeslib.as_array(C.cast(ro, C.POINTER(C.c_int64)), shape=(inf["n"] + 1,)).copy()
+        if inf["m"]:
+            c = np.ctypeslib.as_array(C.cast(ci, C.POINTER(C.c_int32)), shape=(inf["m"],)).copy()
+        else:
+            c = np.zeros(0, np.int32)
+        return r, c
+
+    def close(self) -> None:
+        if self._h and self._h.value:
+            lib().xb_csr_free(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def select_sources_csr(row_offsets: np.ndarray, seed: int, k: int) -> np.ndarray:
+    ro = np.ascontiguousarray(row_offsets, dtype=np.int64)
+    out = np.zeros(k, np.int32)
+    _check(lib().xb_select_sources_csr(len(ro) - 1, ro.ctypes.data, seed, k, out.ctypes.data))
+    return out
+
+
+class Graph:
+    """Device-resident CSR owned by a Context."""
+
+    def __init__(self, ctx: "Context", handle: int):
+        self.ctx = ctx
+        self._h = C.c_void_p(handle)
+        n, m, md = C.c_int64(), C.c_int64(), C.c_int64()
+        _check(lib().xb_graph_info(self._h, C.byref(n), C.byref(m), C.byref(md)))
+        self.n, self.m, self.max_degree = n.value, m.value, md.value
+
+    def select_sources(self, seed: int, k: int) -> np.ndarray:
+        out = np.zeros(k, np.int32)
+        _check(lib().xb_select_sources(self._h, seed, k, out.ctypes.data))
+        return out
+
+    def close(self) -> None:
+        if self._h and self._h.value:
+            _check(lib().xb_graph_free(self._h))
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+@dataclass
+class TraversalResult:
+    level: object  # np.ndarray (host) or torch.Tensor (device), shape (k, n)
+    parent: object
+    stats: dict = field(default_factory=dict)
+
+
+class Context:
+    """A device context: stream, workspace, tuning (xb_ctx)."""
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        _check(lib().xb_ctx_create(device, C.byref(h)))
+        self._h = h
+        self.device = device
+
+    # tuning -----------------------------------------------------------------
+    def tuning(self) -> dict:
+        t = XbTuning()
+        _check(lib().xb_ctx_get_tuning(self._h, C.byref(t)))
+        return {f: getattr(t, f) for f, _ in XbTuning._fields_}
+
+    def set_tuning(self, **kw) -> None:
+        cur = self.tuning()
+        cur.update(kw)
+        t = XbTuning(**cur)
+        _check(lib().xb_ctx_set_tuning(self._h, C.byref(t)))
+
+    def workspace_bytes(self) -> int:
+        b = C.c_int64()
+        _check(lib().xb_ctx_workspace_bytes(self._h, C.byref(b)))
+        return b.value
+
+    def stream_handle(self) -> int:
+        """The engine's cudaStream_t as an integer (for torch.cuda.ExternalStream)."""
+        p = C.c_void_p()
+        _check(lib().xb_ctx_get_stream(self._h, C.byref(p)))
+        return p.value or 0
+
+    # graphs -----------------------------------------------------------------
+    def upload(self, csr: HostCSR) -> Graph:
+        h = C.c_void_p()
+        _check(lib().xb_graph_from_host_csr(self._h, csr._h, C.byref(h)))
+        return Graph(self, h.value)
+
+    def upload_arrays(self, row_offsets, col_indices) -> Graph:
+        ro = np.ascontiguousarray(row_offsets, dtype=np.int64)
+        ci = np.ascontiguousarray(col_indices, dtype=np.int32)
+        h = C.c_void_p()
+        _check(lib().xb_graph_upload(self._h, len(ro) - 1, ro.ctypes.data, 1, int(ro[-1]),
+                                     ci.ctypes.data if len(ci) else None, C.byref(h)))
+        return Graph(self, h.value)
+
+    def load_text(self, row_path: str, col_path: str) -> Graph:
+        h = C.c_void_p()
+        _check(lib().xb_graph_load_csr_text(self._h, row_path.encode(), col_path.encode(), C.byref(h)))
+        return Graph(self, h.value)
+
+    # traversal --------------------------------------------------------------
+    def traverse(self, graph: Graph, sources, out: str = "host", level=None, parent=None) -> TraversalResult:
+        """Plain multi-source traversal through xb_traverse.
+
+        out="host": numpy (k, n) int32 tables (host buffers, the drop-in path);
+        out="device": torch int32 CUDA tensors (k, n) (allocated here unless
+        given).  sources: numpy int32 (host) or a torch int32 CUDA tensor.
+        """
+        st = XbStats()
+        flags = 0
+        src_keep = sources
+        if hasattr(sources, "data_ptr"):
+            flags |= XB_SOURCES_DEVICE
+            k = int(sources.numel())
+            sptr = sources.data_ptr()
+        else:
+            src_keep = np.ascontiguousarray(sources, dtype=np.int32)
+            k = len(src_keep)
+            sptr = src_keep.ctypes.data
+        n = graph.n
+        if out == "device":
+            import torch
+
+            flags |= XB_OUT_DEVICE
+            dev = torch.device("cuda", self.device)
+            if level is None:
+                level = torch.empty((k, n), dtype=torch.int32, device=dev)
+            if parent is None:
+                parent = torch.empty((k, n), dtype=torch.int32, device=dev)
+            torch.cuda.synchronize(dev)
+            lp, pp = level.data_ptr(), parent.data_ptr()
+        else:
+            if level is None:
+                level = np.empty((k, n), np.int32)
+            if parent is None:
+                parent = np.empty((k, n), np.int32)
+            lp, pp = level.ctypes.data, parent.ctypes.data
+        _check(lib().xb_traverse(self._h, graph._h, sptr, k, XB_MODE_PLAIN, None, lp, pp, None, flags,
+                                 C.byref(st)))
+        return TraversalResult(level, parent, st.as_dict())
+
+    def close(self) -> None:
+        if self._h and self._h.value:
+            _check(lib().xb_ctx_destroy(self._h))
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
