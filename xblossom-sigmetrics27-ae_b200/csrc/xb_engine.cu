@@ -42,6 +42,7 @@ struct xb_ctx {
   // workspace
   void* ws = nullptr;
   size_t ws_bytes = 0;
+  int64_t ws_key[3] = {-1, -1, -1};  // (n, word bytes, words) of the current layout
   xbk::Ctrs* d_ctr = nullptr;
   xbk::Ctrs* h_ctr = nullptr;  // pinned
   int32_t* d_src = nullptr;
@@ -106,8 +107,21 @@ WsLayout layout_for(int64_t n, int word_bytes, int nw) {
   return L;
 }
 
-xb_status ensure_workspace(xb_ctx* c, const WsLayout& L) {
-  if (c->ws_bytes >= L.total && c->ws) return XB_OK;
+// The F/N "all zero between calls" invariant and the epoch stamps hold per
+// layout; a call with another (n, word size, words) places the regions at
+// other offsets, so the used range is cleared whenever the layout changes.
+xb_status ensure_workspace(xb_ctx* c, const WsLayout& L, int64_t n, int wbytes, int nw) {
+  const int64_t key[3] = {n, wbytes, nw};
+  if (c->ws_bytes >= L.total && c->ws) {
+    if (std::memcmp(key, c->ws_key, sizeof(key)) != 0) {
+      XB_CUDA(cudaMemsetAsync(c->ws, 0, L.total, c->stream));
+      std::memcpy(c->ws_key, key, sizeof(key));
+      c->epoch = 1;
+    }
+    return XB_OK;
+  }
+  std::memcpy(c->ws_key, key, sizeof(key));
+  c->epoch = 1;
   if (c->ws) {
     cudaFree(c->ws);
     c->ws = nullptr;
@@ -196,7 +210,7 @@ xb_status run_plain(xb_ctx* c, xb_graph* g, const int32_t* d_sources, int32_t k,
   xb_status s = ensure_heavy(g, heavy);
   if (s != XB_OK) return s;
   const WsLayout L = layout_for(n, (int)sizeof(W), NW);
-  s = ensure_workspace(c, L);
+  s = ensure_workspace(c, L, n, (int)sizeof(W), NW);
   if (s != XB_OK) return s;
   if (!out_dev) {
     s = ensure_stage(c, sizeof(int32_t) * 2 * (size_t)B * (size_t)n);
@@ -605,6 +619,7 @@ xb_status xb_traverse(xb_ctx* c, const xb_graph* gc, const int32_t* sources, int
   }
   if (s != XB_OK) {
     cudaStreamSynchronize(c->stream);
+    c->ws_key[0] = -1;  // the zero invariants may be broken: clear on the next call
     return s;
   }
   XB_CUDA(cudaEventRecord(c->ev1, c->stream));
