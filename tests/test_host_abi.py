@@ -134,3 +134,27 @@ def test_context_without_device_reports_nodev():
     with pytest.raises(xbtrav.XbError) as e:
         xbtrav.Context(0)
     assert e.value.status == xbtrav.XB_ERR_NODEV
+
+
+def _build_example(tmp_path):
+    import os
+    import subprocess
+
+    import xbtrav as X
+
+    pkg = os.path.dirname(X.LIB_PATH)
+    root = os.path.dirname(pkg)
+    exe = str(tmp_path / "example_traverse")
+    subprocess.run(["g++", "-std=c++17", "-O2", "-I", os.path.join(root, "include"), "-I", os.path.join(pkg, "host"),
+                    os.path.join(pkg, "host", "example_traverse.cpp"), "-L", pkg, "-lxbtrav",
+                    f"-Wl,-rpath,{pkg}", "-o", exe], check=True)
+    return exe
+
+
+def test_cpp_host_api_compiles_and_links(tmp_path):
+    import subprocess
+
+    exe = _build_example(tmp_path)
+    # usage error path runs without a GPU
+    r = subprocess.run([exe], capture_output=True, text=True)
+    assert r.returncode == 2 and "usage" in r.stderr

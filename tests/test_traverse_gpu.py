@@ -162,3 +162,28 @@ def test_rmat20_k128_levels_and_parents(ctx):
     _tune(ctx, timing=1)
     r = _assert_parity(ctx, ro, ci, src)
     assert r.stats["pull_levels"] > 0 and r.stats["push_levels"] > 0
+
+
+def test_cpp_host_api_matches_python_binding(ctx, tmp_path):
+    """The reference-style C++ layer (host/xbtrav.hpp) gives the same tables."""
+    import subprocess
+
+    from test_host_abi import _build_example
+
+    exe = _build_example(tmp_path)
+    out = subprocess.run([exe, "--rmat", "12", "16", "64", "0x77"], capture_output=True, text=True, check=True).stdout
+    kv = dict(x.split("=") for x in out.split())
+    csr = xbtrav.HostCSR.rmat(12, 16, seed=0x5EED)
+    ro, ci = csr.arrays()
+    src = xbtrav.select_sources_csr(ro, 0x77, 64)
+    _tune(ctx)
+    g = ctx.upload(csr)
+    r = ctx.traverse(g, src)
+    h = np.uint64(1469598103934665603)
+    prime = np.uint64(1099511628211)
+    with np.errstate(over="ignore"):
+        for x in np.concatenate([r.level.ravel(), r.parent.ravel()]).astype(np.uint32):
+            h = (h ^ np.uint64(x)) * prime
+    assert kv["checksum"] == f"{int(h):016x}"
+    assert int(kv["edges_traversed"]) == r.stats["edges_traversed"]
+    g.close()
