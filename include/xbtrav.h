@@ -158,6 +158,28 @@ xb_status xb_traverse(xb_ctx* ctx, const xb_graph* g, const int32_t* sources, in
                       int32_t mode, const int32_t* matching, int32_t* level, int32_t* parent,
                       int32_t* owner, uint32_t flags, xb_stats* stats);
 
+/* ---- traversal without device allocation -------------------------------- */
+/* No counterpart in the reference (whose engine allocates all its device
+ * buffers itself): an entry point for callers that may not allocate device
+ * memory -- a plugin whose host owns the GPU's memory through its own pool,
+ * or a latency-critical path where cudaMalloc/cudaFree and their implicit
+ * device synchronisation are not allowed.  Same results as xb_traverse in
+ * plain mode (64 sources per word).  Every pointer is a device pointer the
+ * caller owns: int32 CSR (row_offsets n+1, col_indices row_offsets[n]),
+ * k sources, level and parent tables k*n each, source-major.  stream is a
+ * cudaStream_t (NULL = the legacy default stream); the call returns after
+ * the work on it has finished.  Working state lives in one fixed array of
+ * about 23 MiB compiled into the library, held by every GPU that loads the
+ * library until exit; graphs above XB_NOALLOC_MAX_VERTICES vertices are
+ * rejected with XB_ERR_CAPACITY.  The first call on a device looks up the
+ * array's address (do it before any stream capture on that device).  Calls
+ * share the array: calls that overlap on the GPU race and must be
+ * serialised by the caller.  stats may be NULL. */
+#define XB_NOALLOC_MAX_VERTICES 131072
+xb_status xb_traverse_noalloc(int64_t n, const int32_t* row_offsets, const int32_t* col_indices,
+                              const int32_t* sources, int32_t k, int32_t* level, int32_t* parent,
+                              void* stream, xb_stats* stats);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,269 @@
+// xb_noalloc.cu -- xb_traverse_noalloc: the plain multi-source traversal for
+// callers that must not allocate device memory.
+//
+// Who needs it: a host that owns all of the GPU's memory through its own pool
+// (a plugin inside a database or analytics engine, a framework with a caching
+// allocator that hands out every byte) may not call cudaMalloc behind that
+// pool's back, and a latency-critical serving path may forbid cudaMalloc and
+// cudaFree because they can synchronise the device and stall other streams.
+// Such a caller already holds the graph, the sources and the output tables in
+// memory it owns; this entry point takes only device pointers to those and
+// keeps its own working state in one fixed array compiled into the library.
+//
+// The array (g_noalloc_scratch, about 23 MiB) lives in every GPU that loads
+// the library until the process exits.  It bounds the graph to
+// XB_NOALLOC_MAX_VERTICES vertices; larger graphs are rejected with
+// XB_ERR_CAPACITY.  Every call on a device shares the one array and leaves
+// its contents behind; each call clears what must start at zero before it
+// uses it.  Calls whose work overlaps on the GPU (two host threads, or two
+// streams, at once on the same device) race on the array and give wrong
+// results: serialise them.
+//
+// The device address of the array is looked up once per device, on the first
+// call made with that device current (cudaGetSymbolAddress); make that first
+// call before any stream capture begins on the device.
+//
+// No cudaMalloc, cudaFree, cudaMallocHost or allocating library routine is
+// called here, on the host or the device.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <mutex>
+#include <string>
+
+#include "xb_internal.h"
+#include "xb_kernels.cuh"
+
+using xbi::fail;
+
+namespace {
+
+constexpr int64_t kMaxN = XB_NOALLOC_MAX_VERTICES;  // 131072
+constexpr int kPlanes = 17;                          // levels < kMaxN <= 2^17
+constexpr size_t kW = (size_t)kMaxN;                 // 8-byte words per state array
+// layout in 8-byte words
+constexpr size_t kSeenOff = 0;
+constexpr size_t kFOff = kSeenOff + kW;
+constexpr size_t kNOff = kFOff + kW;
+constexpr size_t kPlanesOff = kNOff + kW;
+constexpr size_t kListsOff = kPlanesOff + (size_t)kPlanes * kW;  // 6 int32 lists of kMaxN
+constexpr size_t kCtrOff = kListsOff + 3 * kW;
+constexpr size_t kCtrWords = (sizeof(xbk::Ctrs) + 7) / 8;
+constexpr size_t kMiscOff = kCtrOff + kCtrWords;  // int32 heavy count, int32 error flag
+constexpr size_t kTotalWords = kMiscOff + 4;
+
+constexpr int kHeavy = 2048;
+constexpr float kAlpha = 4.0f;
+constexpr int kMaxDevices = 64;
+
+}  // namespace
+
+static __device__ __align__(256) unsigned long long g_noalloc_scratch[kTotalWords];
+
+namespace {
+
+std::mutex g_setup_mu;
+unsigned long long* g_scratch_ptr[kMaxDevices] = {};
+
+// One-time, per-device lookup of the array's device address.
+xb_status scratch_for_current_device(unsigned long long** out) {
+  int dev = -1;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return fail(XB_ERR_NODEV, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+  if (dev < 0 || dev >= kMaxDevices) return fail(XB_ERR_ARG, "device index beyond the supported range");
+  std::lock_guard<std::mutex> lock(g_setup_mu);
+  if (!g_scratch_ptr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+      return fail(XB_ERR_CUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
+    g_scratch_ptr[dev] = (unsigned long long*)p;
+  }
+  *out = g_scratch_ptr[dev];
+  return XB_OK;
+}
+
+// Checks the caller's CSR and sources on the device; sets *err on the first
+// violation: 1 = offsets, 2 = column index, 3 = source id.
+__global__ void k_validate(int64_t n, const int32_t* __restrict__ ro, const int32_t* __restrict__ ci,
+                           const int32_t* __restrict__ src, int32_t k, int32_t* err) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int32_t m = ro[n];
+  if (tid == 0 && (ro[0] != 0 || m < 0)) atomicCAS(err, 0, 1);
+  for (int64_t v = tid; v < n; v += stride)
+    if (ro[v + 1] < ro[v]) atomicCAS(err, 0, 1);
+  for (int64_t i = tid; i < (int64_t)k; i += stride)
+    if (src[i] < 0 || src[i] >= n) atomicCAS(err, 0, 3);
+  if (m < 0) return;
+  for (int64_t e = tid; e < m; e += stride)
+    if (ci[e] < 0 || ci[e] >= n) atomicCAS(err, 0, 2);
+}
+
+// Vertices of degree > thr, appended in any order (the kernels that read the
+// list reduce per vertex, so the order does not matter).
+__global__ void k_heavy_list(int64_t n, const int32_t* __restrict__ ro, int thr, int32_t* list, int32_t* count) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < n; base += stride) {
+    const int64_t v = base + threadIdx.x;
+    const bool hv = v < n && ro[v + 1] - ro[v] > thr;
+    xbk::warp_append(hv, (int32_t)v, list, count);
+  }
+}
+
+#define NA_CUDA(call)                                                                                    \
+  do {                                                                                                   \
+    cudaError_t e_ = (call);                                                                             \
+    if (e_ != cudaSuccess) return fail(XB_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+}  // namespace
+
+extern "C" xb_status xb_traverse_noalloc(int64_t n, const int32_t* row_offsets, const int32_t* col_indices,
+                                         const int32_t* sources, int32_t k, int32_t* level, int32_t* parent,
+                                         void* stream_handle, xb_stats* st) {
+  using W = unsigned long long;
+  constexpr int B = 64;
+  xbi::clear_error();
+  if (st) std::memset(st, 0, sizeof(*st));
+  if (n < 1) return fail(XB_ERR_ARG, "n must be at least 1");
+  if (n > kMaxN)
+    return fail(XB_ERR_CAPACITY, "graph has " + std::to_string(n) + " vertices; xb_traverse_noalloc holds at most " +
+                                     std::to_string(kMaxN) + " (its scratch array is fixed at build time)");
+  if (k < 0) return fail(XB_ERR_ARG, "negative source count");
+  if (!row_offsets || (k > 0 && (!sources || !level || !parent)))
+    return fail(XB_ERR_ARG, "null device pointer");
+  if (k == 0) return XB_OK;
+  cudaStream_t sm = (cudaStream_t)stream_handle;
+  unsigned long long* scratch = nullptr;
+  xb_status s = scratch_for_current_device(&scratch);
+  if (s != XB_OK) return s;
+  int dev = 0, sms = 148;
+  NA_CUDA(cudaGetDevice(&dev));
+  NA_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+
+  W* seen = scratch + kSeenOff;
+  W* F = scratch + kFOff;
+  W* N = scratch + kNOff;
+  W* planes = scratch + kPlanesOff;
+  int32_t* lists = (int32_t*)(scratch + kListsOff);
+  xbk::Lists fl{lists + 0 * kW, lists + 1 * kW};
+  xbk::Lists nl{lists + 2 * kW, lists + 3 * kW};
+  int32_t* touched = lists + 4 * kW;
+  int32_t* heavy_list = lists + 5 * kW;
+  xbk::Ctrs* ctr = (xbk::Ctrs*)(scratch + kCtrOff);
+  int32_t* misc = (int32_t*)(scratch + kMiscOff);  // [0] heavy count, [1] validation error
+  const int64_t plane_stride = (int64_t)kW;
+  const size_t state_bytes = sizeof(W) * (size_t)n;
+
+  // validate the caller's arrays on the device (a bad id would fault the kernels)
+  int32_t m32 = 0;
+  NA_CUDA(cudaMemcpyAsync(&m32, row_offsets + n, sizeof(int32_t), cudaMemcpyDeviceToHost, sm));
+  NA_CUDA(cudaStreamSynchronize(sm));
+  if (m32 < 0) return fail(XB_ERR_ARG, "row_offsets[n] is negative");
+  if (m32 > 0 && !col_indices) return fail(XB_ERR_ARG, "null column indices");
+  NA_CUDA(cudaMemsetAsync(misc, 0, 4 * sizeof(int32_t), sm));
+  const int vgrid = sms * 4;
+  k_validate<<<vgrid, 256, 0, sm>>>(n, row_offsets, col_indices, sources, k, misc + 1);
+  NA_CUDA(cudaGetLastError());
+  int32_t hmisc[2] = {0, 0};
+  NA_CUDA(cudaMemcpyAsync(hmisc, misc, sizeof(hmisc), cudaMemcpyDeviceToHost, sm));
+  NA_CUDA(cudaStreamSynchronize(sm));
+  if (hmisc[1] == 1) return fail(XB_ERR_ARG, "row offsets must start at 0 and not decrease");
+  if (hmisc[1] == 2) return fail(XB_ERR_ARG, "a column index is out of range");
+  if (hmisc[1] == 3) return fail(XB_ERR_ARG, "a source id is out of range");
+  k_heavy_list<<<(int)std::min<int64_t>((n + 255) / 256, (int64_t)sms * 8), 256, 0, sm>>>(n, row_offsets, kHeavy,
+                                                                                        heavy_list, misc);
+  NA_CUDA(cudaGetLastError());
+  NA_CUDA(cudaMemcpyAsync(hmisc, misc, sizeof(int32_t), cudaMemcpyDeviceToHost, sm));
+  NA_CUDA(cudaStreamSynchronize(sm));
+  const int32_t n_heavy = hmisc[0];
+
+  // F and N must start zero: the array keeps whatever the last call left
+  NA_CUDA(cudaMemsetAsync(F, 0, state_bytes, sm));
+  NA_CUDA(cudaMemsetAsync(N, 0, state_bytes, sm));
+
+  const int64_t ntiles = (n + 31) / 32;
+  constexpr int PULL_WARPS = 8, TAB_WARPS = 4;
+  const int pull_grid = (int)std::max<int64_t>(1, std::min<int64_t>((ntiles + PULL_WARPS - 1) / PULL_WARPS, (int64_t)sms * 8));
+  const int tab_grid = (int)std::max<int64_t>(1, std::min<int64_t>((ntiles + TAB_WARPS - 1) / TAB_WARPS, (int64_t)sms * 16));
+  xbk::Ctrs h{};
+  int max_levels = 0;
+  for (int64_t k0 = 0; k0 < k; k0 += B) {
+    const int kb = (int)std::min<int64_t>(B, k - k0);
+    xbk::Masks<W, 1> active{};
+    active.w[0] = kb == 64 ? ~0ull : ((1ull << kb) - 1ull);
+    NA_CUDA(cudaMemsetAsync(seen, 0, state_bytes, sm));
+    NA_CUDA(cudaMemsetAsync(planes, 0, sizeof(W) * (size_t)plane_stride * 3, sm));
+    int planes_zeroed = 3;
+    std::memset(&h, 0, sizeof(h));
+    h.b.m_unfinished = m32;
+    NA_CUDA(cudaMemcpyAsync(ctr, &h, sizeof(h), cudaMemcpyHostToDevice, sm));
+    xbk::k_init_batch<W, 1, int32_t><<<1, 256, 0, sm>>>(sources + k0, kb, row_offsets, F, seen, active, kHeavy, fl,
+                                                         ctr);
+    NA_CUDA(cudaGetLastError());
+    int cur = 0, lvl = 0;
+    for (;;) {
+      NA_CUDA(cudaMemcpyAsync(&h, ctr, sizeof(h), cudaMemcpyDeviceToHost, sm));
+      NA_CUDA(cudaStreamSynchronize(sm));
+      const xbk::LevelCtr lc = h.lv[cur];
+      const int64_t fcount = (int64_t)lc.n_light + lc.n_heavy;
+      if (fcount == 0) break;
+      const int next = lvl + 1;
+      while (planes_zeroed < kPlanes && ((int64_t)1 << planes_zeroed) <= next) {
+        NA_CUDA(cudaMemsetAsync(planes + (size_t)planes_zeroed * plane_stride, 0, sizeof(W) * (size_t)plane_stride, sm));
+        planes_zeroed++;
+      }
+      NA_CUDA(cudaMemsetAsync(&ctr->lv[cur ^ 1], 0, sizeof(xbk::LevelCtr), sm));
+      const bool pull = (double)lc.edges * kAlpha > (double)h.b.m_unfinished;
+      if (!pull) {
+        if (lc.n_light > 0)
+          xbk::k_push_light<W, 1, int32_t><<<(int)std::min<int64_t>((lc.n_light + 7) / 8, (int64_t)sms * 16), 256, 0,
+                                             sm>>>(fl.light, &ctr->lv[cur].n_light, row_offsets, col_indices, F, seen, N,
+                                                   nullptr, 0, touched, ctr, cur);
+        if (lc.n_heavy > 0)
+          xbk::k_push_heavy<W, 1, int32_t><<<(int)std::min<int64_t>(lc.n_heavy, (int64_t)sms * 4), 512, 0, sm>>>(
+              fl.heavy, &ctr->lv[cur].n_heavy, row_offsets, col_indices, F, seen, N, nullptr, 0, touched, ctr, cur);
+        xbk::k_push_finalize<W, 1, int32_t><<<(int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)sms * 8)),
+                                              256, 0, sm>>>(touched, row_offsets, N, seen, planes, plane_stride, next,
+                                                            active, kHeavy, nl, ctr, cur);
+      } else {
+        xbk::k_pull_tiles<W, 1, int32_t, PULL_WARPS><<<pull_grid, PULL_WARPS * 32, 0, sm>>>(
+            n, row_offsets, col_indices, F, seen, N, planes, plane_stride, next, active, kHeavy, nl, ctr, cur);
+        if (n_heavy > 0)
+          xbk::k_pull_heavy<W, 1, int32_t><<<(int)std::min<int64_t>(n_heavy, (int64_t)sms * 4), 512, 0, sm>>>(
+              heavy_list, n_heavy, row_offsets, col_indices, F, seen, N, planes, plane_stride, next, active, kHeavy,
+              nl, ctr, cur);
+        NA_CUDA(cudaMemsetAsync(F, 0, state_bytes, sm));
+      }
+      NA_CUDA(cudaGetLastError());
+      std::swap(F, N);
+      std::swap(fl, nl);
+      cur ^= 1;
+      lvl = next;
+    }
+    max_levels = std::max(max_levels, lvl);
+    xbk::k_tables<W, 1, int32_t, TAB_WARPS><<<tab_grid, TAB_WARPS * 32, 0, sm>>>(
+        n, row_offsets, col_indices, seen, planes, plane_stride, planes_zeroed, 0, kb, kHeavy, level + k0 * n,
+        parent + k0 * n, ctr);
+    if (n_heavy > 0)
+      xbk::k_tables_heavy<W, 1, int32_t><<<(int)std::min<int64_t>(n_heavy, (int64_t)sms * 4), 256, 0, sm>>>(
+          heavy_list, n_heavy, n, row_offsets, col_indices, seen, planes, plane_stride, planes_zeroed, 0, kb,
+          level + k0 * n, parent + k0 * n, ctr);
+    NA_CUDA(cudaGetLastError());
+    NA_CUDA(cudaMemcpyAsync(&h, ctr, sizeof(h), cudaMemcpyDeviceToHost, sm));
+    NA_CUDA(cudaStreamSynchronize(sm));
+    if (st) {
+      st->edges_traversed += (int64_t)h.b.edges_traversed;
+      st->reached += (int64_t)h.b.reached;
+      st->edges_scanned += (int64_t)h.b.edges_scanned;
+      st->vertices_scanned += (int64_t)h.b.vertices_scanned;
+      st->vertices_swept += (int64_t)h.b.vertices_swept;
+      st->parent_edges_scanned += (int64_t)h.b.parent_edges;
+      st->batches += 1;
+    }
+  }
+  if (st) st->levels = max_levels;
+  return XB_OK;
+}
