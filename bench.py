@@ -43,6 +43,8 @@ WORKLOADS = {
     "rmat22_k1024": dict(kind="rmat", scale=22, ef=16, k=1024),
     "er335k_k256": dict(kind="er", n=335_000, pairs=1_850_000, k=256),
     "rmat16_k64": dict(kind="rmat", scale=16, ef=16, k=64),
+    # smaller case for kernel profiles (graph > L2, a few hundred MB on the device)
+    "rmat20_k64": dict(kind="rmat", scale=20, ef=16, k=64),
 }
 SEED = 0x5EED
 

@@ -61,14 +61,20 @@ struct xb_graph {
   int32_t* d_ci = nullptr;
   std::vector<int64_t> h_ro;
   int32_t* d_heavy = nullptr;  // vertices with degree > heavy_thr, ascending
+  int32_t* d_hpar = nullptr;   // per heavy vertex, 64 parent slots of the table pass
+  int2* d_hitems = nullptr;    // (heavy index, chunk) items of the table pass
+  int64_t n_hitems = 0;
   int32_t n_heavy = 0;
   int32_t heavy_thr = -1;
 };
 
 namespace {
 
+// Edges per work item of the heavy-vertex table scan.
+constexpr int kTableChunk = 4096;
+
 struct WsLayout {
-  size_t seen, F, N, planes, touched, fl_light, fl_heavy, nl_light, nl_heavy, stamp, total;
+  size_t seen, F, N, p01, ph, touched, fl_light, fl_heavy, nl_light, nl_heavy, stamp, total;
   int64_t plane_stride;  // in words
   int nplanes_alloc;
 };
@@ -96,7 +102,8 @@ WsLayout layout_for(int64_t n, int word_bytes, int nw) {
   L.seen = o; o += sw;
   L.F = o; o += sw;
   L.N = o; o += sw;
-  L.planes = o; o += sw * L.nplanes_alloc;
+  L.p01 = o; o += 2 * sw;
+  L.ph = o; o += sw * (L.nplanes_alloc - 2);
   L.touched = o; o += li;
   L.fl_light = o; o += li;
   L.fl_heavy = o; o += li;
@@ -170,13 +177,34 @@ xb_status ensure_heavy(xb_graph* g, int thr) {
   for (int64_t v = 0; v < g->n; v++)
     if (g->h_ro[v + 1] - g->h_ro[v] > thr) hv.push_back((int32_t)v);
   if (g->d_heavy) cudaFree(g->d_heavy);
+  if (g->d_hpar) cudaFree(g->d_hpar);
   g->d_heavy = nullptr;
-  if (cudaMalloc(&g->d_heavy, sizeof(int32_t) * std::max<size_t>(hv.size(), 1)) != cudaSuccess) {
+  g->d_hpar = nullptr;
+  g->heavy_thr = -1;
+  if (cudaMalloc(&g->d_heavy, sizeof(int32_t) * std::max<size_t>(hv.size(), 1)) != cudaSuccess ||
+      cudaMalloc(&g->d_hpar, sizeof(int32_t) * 64 * std::max<size_t>(hv.size(), 1)) != cudaSuccess) {
     cudaGetLastError();
     return fail(XB_ERR_OOM, "heavy list allocation failed");
   }
   if (!hv.empty())
     XB_CUDA(cudaMemcpy(g->d_heavy, hv.data(), sizeof(int32_t) * hv.size(), cudaMemcpyHostToDevice));
+  // (heavy index, chunk) work items of the table pass, heaviest vertices first
+  // (ids ascend roughly with falling degree in R-MAT-like graphs, so this is
+  // the list order)
+  std::vector<int2> items;
+  for (size_t i = 0; i < hv.size(); i++) {
+    const int64_t d = g->h_ro[hv[i] + 1] - g->h_ro[hv[i]];
+    for (int64_t c = 0; c * kTableChunk < d; c++) items.push_back(make_int2((int)i, (int)c));
+  }
+  if (g->d_hitems) cudaFree(g->d_hitems);
+  g->d_hitems = nullptr;
+  if (cudaMalloc(&g->d_hitems, sizeof(int2) * std::max<size_t>(items.size(), 1)) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(XB_ERR_OOM, "heavy item list allocation failed");
+  }
+  if (!items.empty())
+    XB_CUDA(cudaMemcpy(g->d_hitems, items.data(), sizeof(int2) * items.size(), cudaMemcpyHostToDevice));
+  g->n_hitems = (int64_t)items.size();
   g->n_heavy = (int32_t)hv.size();
   g->heavy_thr = thr;
   return XB_OK;
@@ -220,22 +248,25 @@ xb_status run_plain(xb_ctx* c, xb_graph* g, const int32_t* d_sources, int32_t k,
   W* seen = (W*)(base + L.seen);
   W* F = (W*)(base + L.F);
   W* N = (W*)(base + L.N);
-  W* planes = (W*)(base + L.planes);
+  const xbk::Planes<W, NW> pl{(W*)(base + L.p01), (W*)(base + L.ph), L.plane_stride};
   int32_t* touched = (int32_t*)(base + L.touched);
   xbk::Lists fl{(int32_t*)(base + L.fl_light), (int32_t*)(base + L.fl_heavy)};
   xbk::Lists nl{(int32_t*)(base + L.nl_light), (int32_t*)(base + L.nl_heavy)};
   int32_t* stamp = (int32_t*)(base + L.stamp);
   const size_t state_bytes = (size_t)n * NW * sizeof(W);
+  const size_t plane_bytes = (size_t)L.plane_stride * sizeof(W);
   const OffT* ro = (const OffT*)g->d_ro;
   const int32_t* ci = g->d_ci;
   const int sms = c->num_sms;
   const float alpha = c->tuning.pull_alpha > 0 ? c->tuning.pull_alpha : 4.0f;
   ClassTimer timer{c, st, c->tuning.timing != 0};
   const int64_t ntiles = (n + 31) / 32;
-  constexpr int PULL_WARPS = 8;
-  constexpr int TAB_WARPS = (B == 64) ? 4 : 8;
+  constexpr int PULL_WARPS = 8, PULL_U = 4;
+  constexpr int TAB_WARPS = (B == 64) ? 4 : 8, TAB_U = 4;
+  constexpr int PUSH_CHUNK = 2048;
   const int pull_grid = (int)std::max<int64_t>(1, std::min<int64_t>((ntiles + PULL_WARPS - 1) / PULL_WARPS, (int64_t)sms * 8));
   const int tab_grid = (int)std::max<int64_t>(1, std::min<int64_t>((ntiles + TAB_WARPS - 1) / TAB_WARPS, (int64_t)sms * 16));
+  const int heavy_chunks = (int)std::max<int64_t>(1, std::min<int64_t>((g->max_deg + PUSH_CHUNK - 1) / PUSH_CHUNK, 64));
   int max_levels = 0;
 
   for (int64_t k0 = 0; k0 < k; k0 += SPP) {
@@ -247,15 +278,16 @@ xb_status run_plain(xb_ctx* c, xb_graph* g, const int32_t* d_sources, int32_t k,
       for (int b = lo; b < hi; b++) m |= (W)1 << (b - lo);
       active.w[i] = m;
     }
-    // reset per-pass state: seen and the first three planes; counters
+    // reset per-pass state: seen, planes 0-2; counters
     XB_CUDA(cudaMemsetAsync(seen, 0, state_bytes, c->stream));
-    XB_CUDA(cudaMemsetAsync(planes, 0, (size_t)L.plane_stride * sizeof(W) * 3, c->stream));
+    XB_CUDA(cudaMemsetAsync(pl.p01, 0, 2 * plane_bytes, c->stream));
+    XB_CUDA(cudaMemsetAsync(pl.ph, 0, plane_bytes, c->stream));
     int planes_zeroed = 3;
     std::memset(c->h_ctr, 0, sizeof(xbk::Ctrs));
     c->h_ctr->b.m_unfinished = g->m;
     XB_CUDA(cudaMemcpyAsync(c->d_ctr, c->h_ctr, sizeof(xbk::Ctrs), cudaMemcpyHostToDevice, c->stream));
     timer.begin();
-    xbk::k_init_batch<W, NW, OffT><<<1, 256, 0, c->stream>>>(d_sources + k0, kb, ro, F, seen, active, heavy, fl,
+    xbk::k_init_batch<W, NW, OffT><<<1, 256, 0, c->stream>>>(d_sources + k0, kb, ro, F, seen, pl, active, heavy, fl,
                                                               c->d_ctr);
     XB_LAUNCH_CHECK("init");
     timer.end(2, 1);
@@ -269,8 +301,7 @@ xb_status run_plain(xb_ctx* c, xb_graph* g, const int32_t* d_sources, int32_t k,
       if (fcount == 0) break;
       const int next_level = level + 1;
       while (planes_zeroed < L.nplanes_alloc && ((int64_t)1 << planes_zeroed) <= next_level) {
-        XB_CUDA(cudaMemsetAsync(planes + (size_t)planes_zeroed * L.plane_stride, 0,
-                                (size_t)L.plane_stride * sizeof(W), c->stream));
+        XB_CUDA(cudaMemsetAsync(pl.ph + (size_t)(planes_zeroed - 2) * L.plane_stride, 0, plane_bytes, c->stream));
         planes_zeroed++;
       }
       XB_CUDA(cudaMemsetAsync(&c->d_ctr->lv[cur ^ 1], 0, sizeof(xbk::LevelCtr), c->stream));
@@ -287,30 +318,32 @@ xb_status run_plain(xb_ctx* c, xb_graph* g, const int32_t* d_sources, int32_t k,
           launches++;
         }
         if (lc.n_heavy > 0) {
-          const int grid = (int)std::min<int64_t>(lc.n_heavy, (int64_t)sms * 4);
-          xbk::k_push_heavy<W, NW, OffT><<<grid, 512, 0, c->stream>>>(fl.heavy, &c->d_ctr->lv[cur].n_heavy, ro, ci,
+          const dim3 grid(heavy_chunks, (unsigned)std::min<int64_t>(lc.n_heavy, 65535));
+          xbk::k_push_heavy<W, NW, OffT><<<grid, 256, 0, c->stream>>>(fl.heavy, &c->d_ctr->lv[cur].n_heavy, ro, ci,
                                                                       F, seen, N, stamp, c->epoch, touched,
-                                                                      c->d_ctr, cur);
+                                                                      c->d_ctr, cur, PUSH_CHUNK);
           XB_LAUNCH_CHECK("push_heavy");
-          launches++;
+          xbk::k_clear_list<W, NW><<<(int)std::min<int64_t>((lc.n_heavy * NW + 255) / 256, sms * 8), 256, 0,
+                                     c->stream>>>(fl.heavy, &c->d_ctr->lv[cur].n_heavy, F);
+          XB_LAUNCH_CHECK("clear_heavy");
+          launches += 2;
         }
         // the touched count is on the device; size the grid for the worst case
         const int fgrid = (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)sms * 8));
-        xbk::k_push_finalize<W, NW, OffT><<<fgrid, 256, 0, c->stream>>>(touched, ro, N, seen, planes, L.plane_stride,
-                                                                        next_level, active, heavy, nl, c->d_ctr, cur);
+        xbk::k_push_finalize<W, NW, OffT><<<fgrid, 256, 0, c->stream>>>(touched, ro, N, seen, pl, next_level, active,
+                                                                        heavy, nl, c->d_ctr, cur);
         XB_LAUNCH_CHECK("push_finalize");
         launches++;
         if (st) st->push_levels++;
       } else {
-        xbk::k_pull_tiles<W, NW, OffT, PULL_WARPS><<<pull_grid, PULL_WARPS * 32, 0, c->stream>>>(
-            n, ro, ci, F, seen, N, planes, L.plane_stride, next_level, active, heavy, nl, c->d_ctr, cur);
+        xbk::k_pull_tiles<W, NW, OffT, PULL_WARPS, PULL_U><<<pull_grid, PULL_WARPS * 32, 0, c->stream>>>(
+            n, ro, ci, F, seen, N, pl, next_level, active, heavy, nl, c->d_ctr, cur);
         XB_LAUNCH_CHECK("pull_tiles");
         launches++;
         if (g->n_heavy > 0) {
           const int grid = (int)std::min<int64_t>(g->n_heavy, (int64_t)sms * 4);
-          xbk::k_pull_heavy<W, NW, OffT><<<grid, 512, 0, c->stream>>>(g->d_heavy, g->n_heavy, ro, ci, F, seen, N,
-                                                                      planes, L.plane_stride, next_level, active,
-                                                                      heavy, nl, c->d_ctr, cur);
+          xbk::k_pull_heavy<W, NW, OffT><<<grid, 512, 0, c->stream>>>(g->d_heavy, g->n_heavy, ro, ci, F, seen, N, pl,
+                                                                      next_level, active, heavy, nl, c->d_ctr, cur);
           XB_LAUNCH_CHECK("pull_heavy");
           launches++;
         }
@@ -352,17 +385,22 @@ xb_status run_plain(xb_ctx* c, xb_graph* g, const int32_t* d_sources, int32_t k,
       int32_t* lv_out = out_dev ? level_out + s0 * n : c->d_stage;
       int32_t* pr_out = out_dev ? parent_out + s0 * n : c->d_stage + (size_t)B * n;
       timer.begin();
-      xbk::k_tables<W, NW, OffT, TAB_WARPS><<<tab_grid, TAB_WARPS * 32, 0, c->stream>>>(
-          n, ro, ci, seen, planes, L.plane_stride, planes_zeroed, wi, kbw, heavy, lv_out, pr_out, c->d_ctr);
+      xbk::k_tables<W, NW, OffT, TAB_WARPS, TAB_U><<<tab_grid, TAB_WARPS * 32, 0, c->stream>>>(
+          n, ro, ci, seen, pl, planes_zeroed, wi, kbw, heavy, lv_out, pr_out, c->d_ctr);
       XB_LAUNCH_CHECK("tables");
       int64_t launches = 1;
       if (g->n_heavy > 0) {
-        const int grid = (int)std::min<int64_t>(g->n_heavy, (int64_t)sms * 4);
-        xbk::k_tables_heavy<W, NW, OffT><<<grid, 256, 0, c->stream>>>(g->d_heavy, g->n_heavy, n, ro, ci, seen, planes,
-                                                                       L.plane_stride, planes_zeroed, wi, kbw, lv_out,
-                                                                       pr_out, c->d_ctr);
+        const int64_t hcount = (int64_t)g->n_heavy * B;
+        xbk::k_fill<int32_t><<<(int)std::min<int64_t>((hcount + 255) / 256, sms * 8), 256, 0, c->stream>>>(g->d_hpar, hcount,
+                                                                                                    INT32_MAX);
+        const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(g->n_hitems, (int64_t)sms * 8));
+        xbk::k_tables_heavy_scan<W, NW, OffT><<<grid, 256, 0, c->stream>>>(g->d_heavy, g->d_hitems, g->n_hitems, ro,
+                                                                           ci, seen, pl, planes_zeroed, wi, kTableChunk,
+                                                                           g->d_hpar, c->d_ctr);
+        xbk::k_tables_heavy_write<W, NW><<<(int)std::min<int64_t>(g->n_heavy, (int64_t)sms * 8), 64, 0, c->stream>>>(
+            g->d_heavy, g->n_heavy, n, seen, pl, planes_zeroed, wi, kbw, g->d_hpar, lv_out, pr_out);
         XB_LAUNCH_CHECK("tables_heavy");
-        launches++;
+        launches += 3;
       }
       timer.end(1, launches);
       if (!out_dev) {
@@ -389,10 +427,10 @@ xb_status run_plain(xb_ctx* c, xb_graph* g, const int32_t* d_sources, int32_t k,
       const int64_t wbytes = (int64_t)sizeof(W) * NW;
       const int64_t lvl_bytes = R * (int64_t)b.vertices_scanned + (4 + wbytes) * (int64_t)b.edges_scanned +
                                 3 * wbytes * (int64_t)b.vertices_swept;
-      // table pass: per vertex its seen+planes words and offsets, per scanned
-      // edge colIndices + three gathered words, and the written tables
-      const int64_t tab_bytes = (int64_t)n * (R + wbytes * (1 + planes_zeroed)) +
-                                (4 + 3 * (int64_t)sizeof(W)) * (int64_t)b.parent_edges + 8 * (int64_t)kb * n;
+      // table pass: per vertex offsets + seen + its planes (per word), per
+      // scanned edge colIndices + the gathered plane pair, and the tables
+      const int64_t tab_bytes = (int64_t)NW * n * (R + (int64_t)sizeof(W) * (1 + planes_zeroed)) +
+                                (4 + 2 * (int64_t)sizeof(W)) * (int64_t)b.parent_edges + 8 * (int64_t)kb * n;
       st->class_bytes[0] += lvl_bytes;
       st->class_bytes[1] += tab_bytes;
       st->algo_bytes += lvl_bytes + tab_bytes;
@@ -441,7 +479,7 @@ xb_status xb_ctx_create(int32_t device, xb_ctx** out) {
   c->tuning.word_bits = 64;
   c->tuning.words = 1;
   c->tuning.pull_alpha = 4.0f;
-  c->tuning.heavy_degree = 2048;
+  c->tuning.heavy_degree = 256;
   c->tuning.timing = 0;
   *out = c.release();
   return XB_OK;
@@ -562,6 +600,8 @@ xb_status xb_graph_free(xb_graph* g) {
   if (g->d_ro) cudaFree(g->d_ro);
   if (g->d_ci) cudaFree(g->d_ci);
   if (g->d_heavy) cudaFree(g->d_heavy);
+  if (g->d_hpar) cudaFree(g->d_hpar);
+  if (g->d_hitems) cudaFree(g->d_hitems);
   delete g;
   return XB_OK;
 }

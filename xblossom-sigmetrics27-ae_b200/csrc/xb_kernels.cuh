@@ -1,13 +1,16 @@
 // xb_kernels.cuh -- sm_100a device code of the multi-source traversal.
 //
 // Data layout in HBM (one traversal pass = NW words of B bits per vertex,
-// B*NW sources traversed together):
+// B*NW sources traversed together; word i of vertex v at index v*NW+i):
 //   seen[v*NW+i]      bits of the sources that have reached v
 //   F[v*NW+i]         bits newly reached at the current level (the frontier)
 //   N[v*NW+i]         bits reached at the next level (all zero between levels
 //                     except at next-frontier vertices)
-//   plane[j][v*NW+i]  bit j of the level of (source, v), bit-sliced: the level
-//                     of source s at v is sum_j bit_s(plane[j][v]) << j
+//   level planes      the level bit-sliced: bit j of the level of every source
+//                     at v.  Planes 0 and 1 are interleaved per word
+//                     (p01[2*(v*NW+i)] = plane 0, +1 = plane 1) so one
+//                     16-byte load returns "level mod 4" of 64 sources; planes
+//                     j >= 2 are separate arrays ph[(j-2)*stride + v*NW+i].
 //   FL/NL             frontier vertex lists, split by degree (light / heavy)
 //
 // One level step (level L -> L+1) is either
@@ -25,11 +28,14 @@
 //
 // Parents are resolved after the search by the table pass: for vertex v at
 // level L for source s, parent = smallest-id neighbour u with level L-1.  Two
-// adjacent reached vertices differ in level by at most one, so level mod 4
-// (planes 0 and 1) decides "u is one level up"; the bit-sliced compare does
-// it for all B sources of a word at once.  The pass transposes a 32-vertex x
-// B-source tile in shared memory and writes whole 128-byte rows of the
-// source-major level and parent tables with streaming stores.
+// adjacent reached vertices differ in level by at most one, and every
+// neighbour of a vertex reached by s is reached by s, so "level(u) == L-1"
+// reduces to a bit-sliced compare of level mod 4 (planes 0 and 1), done for
+// all B sources of a word at once.  The pass walks each 32-vertex tile's
+// adjacency edge-parallel in ascending order (per-vertex early exit once every
+// needed bit has a parent), transposes the 32-vertex x B-source tile in shared
+// memory and writes whole 128-byte rows of the source-major tables with
+// streaming stores.
 #pragma once
 
 #include <cstdint>
@@ -106,6 +112,80 @@ struct Lists {
   int32_t* heavy;
 };
 
+// Vector types for loading NW consecutive words / a plane pair at once.
+template <typename W, int K>
+struct Vec;
+template <>
+struct Vec<unsigned long long, 1> {
+  using T = unsigned long long;
+};
+template <>
+struct Vec<unsigned long long, 2> {
+  using T = ulonglong2;
+};
+template <>
+struct Vec<unsigned int, 1> {
+  using T = unsigned int;
+};
+template <>
+struct Vec<unsigned int, 2> {
+  using T = uint2;
+};
+template <>
+struct Vec<unsigned int, 4> {
+  using T = uint4;
+};
+
+// Loads K consecutive words starting at p (p aligned to K words).
+template <typename W, int K>
+__device__ __forceinline__ void load_words(const W* __restrict__ p, W (&out)[K]) {
+  if constexpr (K == 1) {
+    out[0] = __ldg(p);
+  } else if constexpr (sizeof(W) == 8 && K == 2) {
+    const ulonglong2 x = __ldg(reinterpret_cast<const ulonglong2*>(p));
+    out[0] = x.x;
+    out[1] = x.y;
+  } else if constexpr (sizeof(W) == 8 && K == 4) {
+    const ulonglong2 x = __ldg(reinterpret_cast<const ulonglong2*>(p));
+    const ulonglong2 y = __ldg(reinterpret_cast<const ulonglong2*>(p) + 1);
+    out[0] = x.x;
+    out[1] = x.y;
+    out[2] = y.x;
+    out[3] = y.y;
+  } else if constexpr (sizeof(W) == 4 && K == 2) {
+    const uint2 x = __ldg(reinterpret_cast<const uint2*>(p));
+    out[0] = x.x;
+    out[1] = x.y;
+  } else {
+    static_assert(sizeof(W) == 4 && K == 4, "unsupported word vector");
+    const uint4 x = __ldg(reinterpret_cast<const uint4*>(p));
+    out[0] = x.x;
+    out[1] = x.y;
+    out[2] = x.z;
+    out[3] = x.w;
+  }
+}
+
+// Level planes of one traversal pass.
+template <typename W, int NW>
+struct Planes {
+  W* p01;          // planes 0 and 1, interleaved per word
+  W* ph;           // planes 2.. : ph[(j-2)*stride + v*NW + i]
+  int64_t stride;  // words per plane array
+
+  __device__ __forceinline__ W get(int j, int64_t v, int i) const {
+    return j < 2 ? p01[((v * NW + i) << 1) + j] : ph[(int64_t)(j - 2) * stride + v * NW + i];
+  }
+  // ORs `bits` into the planes of the bits set in `level`.
+  __device__ __forceinline__ void add(int level, int64_t v, int i, W bits) const {
+    const int64_t q = (v * NW + i) << 1;
+    if (level & 1) p01[q] |= bits;
+    if (level & 2) p01[q + 1] |= bits;
+    for (int j = 2; (level >> j) != 0; j++)
+      if ((level >> j) & 1) ph[(int64_t)(j - 2) * stride + v * NW + i] |= bits;
+  }
+};
+
 template <typename OffT>
 __device__ __forceinline__ int64_t deg_of(const OffT* ro, int32_t v) {
   return (int64_t)ro[v + 1] - (int64_t)ro[v];
@@ -141,46 +221,59 @@ __device__ __forceinline__ W warp_or(W x) {
   return x;
 }
 
+// Per-lane counter increments, kept in registers until the kernel ends.
+template <typename W, int NW>
+struct StatAcc {
+  unsigned long long e_tr = 0, rch = 0, fe = 0;
+  long long fin = 0;
+  W live[NW] = {};
+};
+
 // Records a newly reached vertex (all lanes call; `has` marks lanes that own
-// one): folds new bits into seen and the level planes, updates the counters
-// and appends the vertex to the next frontier's light/heavy list.
+// one): folds new bits into seen and the level planes, accumulates the
+// counters and appends the vertex to the next frontier's light/heavy list.
 template <typename W, int NW, typename OffT>
 __device__ __forceinline__ void commit_new(bool has, int32_t w, const W (&nw)[NW], const W (&sw)[NW],
-                                           int64_t dg, int level, W* seen, W* planes, int64_t plane_stride,
+                                           int64_t dg, int level, W* seen, const Planes<W, NW>& pl,
                                            const Masks<W, NW>& active, int heavy, Lists nl, LevelCtr* nctr,
-                                           BatchCtr* bc) {
-  int cnt = 0;
-  bool fin_now = false;
+                                           StatAcc<W, NW>& acc) {
   if (has) {
     bool full = true;
+    int cnt = 0;
 #pragma unroll
     for (int i = 0; i < NW; i++) {
       const W s2 = sw[i] | nw[i];
       if (nw[i]) {
         seen[(int64_t)w * NW + i] = s2;
-        for (int j = 0; (level >> j) != 0; j++)
-          if ((level >> j) & 1) planes[j * plane_stride + (int64_t)w * NW + i] |= nw[i];
+        pl.add(level, w, i, nw[i]);
       }
       cnt += popc(nw[i]);
       full = full && (s2 == active.w[i]);
+      acc.live[i] |= nw[i];
     }
-    fin_now = full;
+    acc.rch += (unsigned long long)cnt;
+    acc.e_tr += (unsigned long long)dg * (unsigned long long)cnt;
+    acc.fe += (unsigned long long)dg;
+    if (full) acc.fin -= dg;
   }
   const bool light = has && dg <= heavy;
   const bool hv = has && dg > heavy;
   warp_append(light, w, nl.light, &nctr->n_light);
   warp_append(hv, w, nl.heavy, &nctr->n_heavy);
-  unsigned long long e_tr = has ? (unsigned long long)dg * (unsigned long long)cnt : 0ull;
-  unsigned long long rch = (unsigned long long)cnt;
-  unsigned long long fe = has ? (unsigned long long)dg : 0ull;
-  long long fin = fin_now ? -(long long)dg : 0ll;
-  e_tr = warp_sum_u64(e_tr);
-  rch = warp_sum_u64(rch);
-  fe = warp_sum_u64(fe);
-  fin = warp_sum_i64(fin);
+}
+
+// Folds a warp's accumulated counters into the level / batch counters: one
+// set of atomics per warp per kernel instead of per committed tile (all 32
+// lanes must call it).
+template <typename W, int NW>
+__device__ __forceinline__ void flush_stats(StatAcc<W, NW>& acc, LevelCtr* nctr, BatchCtr* bc) {
+  const unsigned long long e_tr = warp_sum_u64(acc.e_tr);
+  const unsigned long long rch = warp_sum_u64(acc.rch);
+  const unsigned long long fe = warp_sum_u64(acc.fe);
+  const long long fin = warp_sum_i64(acc.fin);
   W lv[NW];
 #pragma unroll
-  for (int i = 0; i < NW; i++) lv[i] = warp_or<W>(has ? nw[i] : (W)0);
+  for (int i = 0; i < NW; i++) lv[i] = warp_or<W>(acc.live[i]);
   if ((threadIdx.x & 31) == 0) {
     if (rch) {
       atomicAdd(&bc->reached, rch);
@@ -198,7 +291,7 @@ __device__ __forceinline__ void commit_new(bool has, int32_t w, const W (&nw)[NW
 // Batch initialisation: one block; thread t owns source slot t.
 template <typename W, int NW, typename OffT>
 __global__ void k_init_batch(const int32_t* __restrict__ src, int kb, const OffT* __restrict__ ro, W* F,
-                             W* seen, Masks<W, NW> active, int heavy, Lists fl, Ctrs* ctr) {
+                             W* seen, Planes<W, NW> pl, Masks<W, NW> active, int heavy, Lists fl, Ctrs* ctr) {
   constexpr int B = WB<W>::bits;
   const int t = threadIdx.x;
   int32_t v = -1;
@@ -220,14 +313,41 @@ __global__ void k_init_batch(const int32_t* __restrict__ src, int kb, const OffT
 #pragma unroll
   for (int i = 0; i < NW; i++) {
     nw[i] = first ? F[(int64_t)v * NW + i] : (W)0;
-    sw[i] = 0;  // seen already holds the bits; commit_new must not add planes (level 0)
+    sw[i] = 0;
   }
   const int64_t dg = first ? deg_of(ro, v) : 0;
-  // level 0: no plane bits; commit_new with level 0 only counts and appends.
-  // seen was set above, so pass seen-before = 0 and a dummy seen pointer write
-  // of the same value is harmless.
-  commit_new<W, NW, OffT>(first, v, nw, sw, dg, 0, seen, seen, 0, active, heavy, fl, &ctr->lv[0],
-                          &ctr->b);
+  // level 0 sets no plane bits; seen already holds the bits and commit_new
+  // rewrites the same value.
+  StatAcc<W, NW> acc;
+  commit_new<W, NW, OffT>(first, v, nw, sw, dg, 0, seen, pl, active, heavy, fl, &ctr->lv[0], acc);
+  flush_stats<W, NW>(acc, &ctr->lv[0], &ctr->b);
+}
+
+// Push body for one edge (v -> w) with frontier words f.  Returns true when
+// this thread is the first toucher of w in this level.
+template <typename W, int NW>
+__device__ __forceinline__ bool push_edge(int32_t w, const W (&f)[NW], const W* __restrict__ seen, W* N,
+                                          int32_t* stamp, int32_t epoch) {
+  bool app = false, added = false;
+  W sw[NW];
+  load_words<W, NW>(seen + (int64_t)w * NW, sw);
+#pragma unroll
+  for (int i = 0; i < NW; i++) {
+    const W m = f[i] & ~sw[i];
+    if (m) {
+      const W cur_n = N[(int64_t)w * NW + i];
+      if ((cur_n & m) != m) {
+        const W old = atomicOr(&N[(int64_t)w * NW + i], m);
+        if (NW == 1) {
+          app = (old == 0);
+        } else if ((old & m) != m) {
+          added = true;
+        }
+      }
+    }
+  }
+  if (NW > 1 && added) app = atomicExch(&stamp[w], epoch) != epoch;
+  return app;
 }
 
 // ---------------------------------------------------------------------------
@@ -261,23 +381,7 @@ __global__ void k_push_light(const int32_t* __restrict__ list, const int32_t* __
       int32_t w = 0;
       if (e < end) {
         w = __ldg(&ci[e]);
-        bool added = false;
-#pragma unroll
-        for (int i = 0; i < NW; i++) {
-          const W m = f[i] & ~seen[(int64_t)w * NW + i];
-          if (m) {
-            const W cur_n = N[(int64_t)w * NW + i];
-            if ((cur_n & m) != m) {
-              const W old = atomicOr(&N[(int64_t)w * NW + i], m);
-              if (NW == 1) {
-                app = (old == 0);
-              } else if ((old & m) != m) {
-                added = true;
-              }
-            }
-          }
-        }
-        if (NW > 1 && added) app = atomicExch(&stamp[w], epoch) != epoch;
+        app = push_edge<W, NW>(w, f, seen, N, stamp, epoch);
       }
       warp_append(app, w, touched, &nctr->n_touched);
     }
@@ -288,53 +392,39 @@ __global__ void k_push_light(const int32_t* __restrict__ list, const int32_t* __
   }
 }
 
-// Push, heavy frontier vertices: one block per vertex.
+// Push, heavy frontier vertices: blockIdx.y walks the heavy list, blockIdx.x
+// splits each adjacency into chunks of `chunk` edges so a hub spreads over
+// many SMs.  F of heavy vertices is cleared afterwards by k_clear_list.
 template <typename W, int NW, typename OffT>
 __global__ void k_push_heavy(const int32_t* __restrict__ list, const int32_t* __restrict__ count,
-                             const OffT* __restrict__ ro, const int32_t* __restrict__ ci, W* F,
-                             const W* __restrict__ seen, W* N, int32_t* stamp, int32_t epoch,
-                             int32_t* touched, Ctrs* ctr, int cur) {
+                             const OffT* __restrict__ ro, const int32_t* __restrict__ ci, const W* __restrict__ F,
+                             const W* __restrict__ seen, W* N, int32_t* stamp, int32_t epoch, int32_t* touched,
+                             Ctrs* ctr, int cur, int chunk) {
   const int32_t cnt = *count;
   LevelCtr* nctr = &ctr->lv[cur ^ 1];
-  for (int64_t idx = blockIdx.x; idx < cnt; idx += gridDim.x) {
+  for (int64_t idx = blockIdx.y; idx < cnt; idx += gridDim.y) {
     const int32_t v = list[idx];
     W f[NW];
 #pragma unroll
     for (int i = 0; i < NW; i++) f[i] = F[(int64_t)v * NW + i];
-    __syncthreads();
-    if (threadIdx.x < NW) F[(int64_t)v * NW + threadIdx.x] = 0;
     const int64_t beg = ro[v], end = ro[v + 1];
-    if (threadIdx.x == 0) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
       atomicAdd(&ctr->b.edges_scanned, (unsigned long long)(end - beg));
       atomicAdd(&ctr->b.vertices_scanned, 1ull);
     }
-    for (int64_t base = beg; base < end; base += blockDim.x) {
-      const int64_t e = base + threadIdx.x;
-      bool app = false;
-      int32_t w = 0;
-      if (e < end) {
-        w = __ldg(&ci[e]);
-        bool added = false;
-#pragma unroll
-        for (int i = 0; i < NW; i++) {
-          const W m = f[i] & ~seen[(int64_t)w * NW + i];
-          if (m) {
-            const W cur_n = N[(int64_t)w * NW + i];
-            if ((cur_n & m) != m) {
-              const W old = atomicOr(&N[(int64_t)w * NW + i], m);
-              if (NW == 1) {
-                app = (old == 0);
-              } else if ((old & m) != m) {
-                added = true;
-              }
-            }
-          }
+    for (int64_t cb = beg + (int64_t)blockIdx.x * chunk; cb < end; cb += (int64_t)gridDim.x * chunk) {
+      const int64_t ce = imin64(end, cb + chunk);
+      for (int64_t base = cb; base < ce; base += blockDim.x) {
+        const int64_t e = base + threadIdx.x;
+        bool app = false;
+        int32_t w = 0;
+        if (e < ce) {
+          w = __ldg(&ci[e]);
+          app = push_edge<W, NW>(w, f, seen, N, stamp, epoch);
         }
-        if (NW > 1 && added) app = atomicExch(&stamp[w], epoch) != epoch;
+        warp_append(app, w, touched, &nctr->n_touched);
       }
-      warp_append(app, w, touched, &nctr->n_touched);
     }
-    __syncthreads();
   }
 }
 
@@ -342,11 +432,12 @@ __global__ void k_push_heavy(const int32_t* __restrict__ list, const int32_t* __
 // next frontier.
 template <typename W, int NW, typename OffT>
 __global__ void k_push_finalize(const int32_t* __restrict__ touched, const OffT* __restrict__ ro, const W* N,
-                                W* seen, W* planes, int64_t plane_stride, int level, Masks<W, NW> active,
-                                int heavy, Lists nl, Ctrs* ctr, int cur) {
+                                W* seen, Planes<W, NW> pl, int level, Masks<W, NW> active, int heavy, Lists nl,
+                                Ctrs* ctr, int cur) {
   LevelCtr* nctr = &ctr->lv[cur ^ 1];
   const int32_t cnt = nctr->n_touched;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  StatAcc<W, NW> acc;
   for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < cnt; base += stride) {
     const int64_t idx = base + threadIdx.x;
     const bool has = idx < cnt;
@@ -365,9 +456,9 @@ __global__ void k_push_finalize(const int32_t* __restrict__ touched, const OffT*
 #pragma unroll
       for (int i = 0; i < NW; i++) nw[i] = sw[i] = 0;
     }
-    commit_new<W, NW, OffT>(has, w, nw, sw, dg, level, seen, planes, plane_stride, active, heavy, nl, nctr,
-                            &ctr->b);
+    commit_new<W, NW, OffT>(has, w, nw, sw, dg, level, seen, pl, active, heavy, nl, nctr, acc);
   }
+  flush_stats<W, NW>(acc, nctr, &ctr->b);
 }
 
 // Segmented inclusive OR scan over a warp, segments = equal consecutive keys.
@@ -383,15 +474,25 @@ __device__ __forceinline__ W seg_or_scan(W x, int key) {
   return x;
 }
 
+// Owner lane of flat edge e: last j in [0,31] with off[j] <= e.
+__device__ __forceinline__ int flat_owner(const int32_t* __restrict__ off, int32_t e) {
+  int lo = 0;
+#pragma unroll
+  for (int step = 16; step > 0; step >>= 1)
+    if (off[lo + step] <= e) lo += step;
+  return lo;
+}
+
 // ---------------------------------------------------------------------------
 // Pull, light vertices: one warp per tile of 32 consecutive vertices.  The
 // tile's wanted adjacency ranges are flattened and read edge-parallel
-// (coalesced colIndices), F is gathered per edge, a segmented OR scan folds
-// the words per owner vertex into shared memory.
-template <typename W, int NW, typename OffT, int WARPS>
+// (coalesced colIndices), U x 32 edges per round with all loads issued before
+// any is consumed; F is gathered per edge and a segmented OR scan folds the
+// words per owner vertex into shared memory.
+template <typename W, int NW, typename OffT, int WARPS, int U>
 __global__ void __launch_bounds__(WARPS * 32) k_pull_tiles(int64_t n, const OffT* __restrict__ ro,
                                                            const int32_t* __restrict__ ci, const W* __restrict__ F,
-                                                           W* seen, W* N, W* planes, int64_t plane_stride, int level,
+                                                           W* seen, W* N, Planes<W, NW> pl, int level,
                                                            Masks<W, NW> active, int heavy, Lists nl, Ctrs* ctr,
                                                            int cur) {
   __shared__ int32_t s_off[WARPS][33];
@@ -408,6 +509,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_pull_tiles(int64_t n, const OffT
 #pragma unroll
   for (int i = 0; i < NW; i++) live[i] = (W)cctr->live[i] & active.w[i];
   unsigned long long e_scan = 0, v_scan = 0, v_sweep = 0;
+  StatAcc<W, NW> acc;
   for (int64_t tile = warp; tile < ntiles; tile += nwarps) {
     const int64_t v = tile * 32 + lane;
     const bool valid = v < n;
@@ -417,9 +519,9 @@ __global__ void __launch_bounds__(WARPS * 32) k_pull_tiles(int64_t n, const OffT
     if (valid) {
       beg = ro[v];
       dg = (int64_t)ro[v + 1] - beg;
+      load_words<W, NW>(seen + v * NW, sw);
 #pragma unroll
       for (int i = 0; i < NW; i++) {
-        sw[i] = seen[v * NW + i];
         want[i] = live[i] & ~sw[i];
         any = any || want[i] != 0;
       }
@@ -430,8 +532,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_pull_tiles(int64_t n, const OffT
     v_sweep += valid ? 1 : 0;
     const bool scan_me = any && dg > 0 && dg <= heavy;
     v_scan += scan_me ? 1 : 0;
-    int32_t d = scan_me ? (int32_t)dg : 0;
-    // exclusive scan of d over the warp
+    const int32_t d = scan_me ? (int32_t)dg : 0;
     int32_t inc = d;
 #pragma unroll
     for (int s = 1; s < 32; s <<= 1) {
@@ -446,39 +547,41 @@ __global__ void __launch_bounds__(WARPS * 32) k_pull_tiles(int64_t n, const OffT
     for (int i = 0; i < NW; i++) s_acc[wib][lane][i] = 0;
     __syncwarp();
     e_scan += (unsigned long long)(lane == 0 ? total : 0);
-    for (int32_t base = 0; base < total; base += 32) {
-      const int32_t e = base + lane;
-      int key = 32 + lane;  // unique key for idle lanes
-      W f[NW];
+    for (int32_t base = 0; base < total; base += 32 * U) {
+      int key[U];
+      int32_t col[U];
 #pragma unroll
-      for (int i = 0; i < NW; i++) f[i] = 0;
-      if (e < total) {
-        // owner: last j with s_off[j] <= e (binary search over 33 offsets)
-        int lo = 0, hi = 31;
-        while (lo < hi) {
-          const int mid = (lo + hi + 1) >> 1;
-          if (s_off[wib][mid] <= e)
-            lo = mid;
-          else
-            hi = mid - 1;
+      for (int u = 0; u < U; u++) {
+        const int32_t e = base + u * 32 + lane;
+        key[u] = 32 + lane;  // unique key for idle lanes
+        col[u] = -1;
+        if (e < total) {
+          const int o = flat_owner(s_off[wib], e);
+          key[u] = o;
+          col[u] = __ldg(&ci[s_beg[wib][o] + (e - s_off[wib][o])]);
         }
-        key = lo;
-        const int32_t u = __ldg(&ci[s_beg[wib][lo] + (e - s_off[wib][lo])]);
-        if (NW == 1) {
-          f[0] = __ldg(&F[u]);
+      }
+      W f[U][NW];
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        if (col[u] >= 0) {
+          load_words<W, NW>(F + (int64_t)col[u] * NW, f[u]);
         } else {
 #pragma unroll
-          for (int i = 0; i < NW; i++) f[i] = __ldg(&F[(int64_t)u * NW + i]);
+          for (int i = 0; i < NW; i++) f[u][i] = 0;
         }
       }
-      const int next_key = __shfl_down_sync(0xffffffffu, key, 1);
-      const bool tail = (lane == 31) || (next_key != key);
 #pragma unroll
-      for (int i = 0; i < NW; i++) {
-        const W r = seg_or_scan<W>(f[i], key);
-        if (tail && key < 32) s_acc[wib][key][i] |= r;
+      for (int u = 0; u < U; u++) {
+        const int next_key = __shfl_down_sync(0xffffffffu, key[u], 1);
+        const bool tail = (lane == 31) || (next_key != key[u]);
+#pragma unroll
+        for (int i = 0; i < NW; i++) {
+          const W r = seg_or_scan<W>(f[u][i], key[u]);
+          if (tail && key[u] < 32) s_acc[wib][key[u]][i] |= r;
+        }
+        __syncwarp();
       }
-      __syncwarp();
     }
     W nw[NW];
     bool has = false;
@@ -491,10 +594,10 @@ __global__ void __launch_bounds__(WARPS * 32) k_pull_tiles(int64_t n, const OffT
 #pragma unroll
       for (int i = 0; i < NW; i++) N[v * NW + i] = nw[i];
     }
-    commit_new<W, NW, OffT>(has, (int32_t)v, nw, sw, dg, level, seen, planes, plane_stride, active, heavy, nl,
-                            nctr, &ctr->b);
+    commit_new<W, NW, OffT>(has, (int32_t)v, nw, sw, dg, level, seen, pl, active, heavy, nl, nctr, acc);
     __syncwarp();
   }
+  flush_stats<W, NW>(acc, nctr, &ctr->b);
   e_scan = warp_sum_u64(e_scan);
   v_scan = warp_sum_u64(v_scan);
   v_sweep = warp_sum_u64(v_sweep);
@@ -528,12 +631,13 @@ __device__ __forceinline__ void block_or(W (&x)[NW], W (*s_red)[NW]) {
 // once every wanted bit is found.
 template <typename W, int NW, typename OffT>
 __global__ void k_pull_heavy(const int32_t* __restrict__ hlist, int32_t nh, const OffT* __restrict__ ro,
-                             const int32_t* __restrict__ ci, const W* __restrict__ F, W* seen, W* N, W* planes,
-                             int64_t plane_stride, int level, Masks<W, NW> active, int heavy, Lists nl, Ctrs* ctr,
+                             const int32_t* __restrict__ ci, const W* __restrict__ F, W* seen, W* N,
+                             Planes<W, NW> pl, int level, Masks<W, NW> active, int heavy, Lists nl, Ctrs* ctr,
                              int cur) {
   __shared__ W s_red[32][NW];
   LevelCtr* cctr = &ctr->lv[cur];
   LevelCtr* nctr = &ctr->lv[cur ^ 1];
+  StatAcc<W, NW> sacc;
   for (int64_t idx = blockIdx.x; idx < nh; idx += gridDim.x) {
     const int32_t v = hlist[idx];
     W sw[NW], want[NW];
@@ -550,14 +654,23 @@ __global__ void k_pull_heavy(const int32_t* __restrict__ hlist, int32_t nh, cons
 #pragma unroll
     for (int i = 0; i < NW; i++) acc[i] = 0;
     int64_t scanned = 0;
-    for (int64_t base = beg; base < end; base += blockDim.x) {
-      const int64_t e = base + threadIdx.x;
-      if (e < end) {
-        const int32_t u = __ldg(&ci[e]);
+    for (int64_t base = beg; base < end; base += 4 * (int64_t)blockDim.x) {
+      int32_t col[4];
 #pragma unroll
-        for (int i = 0; i < NW; i++) acc[i] |= __ldg(&F[(int64_t)u * NW + i]);
+      for (int u = 0; u < 4; u++) {
+        const int64_t e = base + u * (int64_t)blockDim.x + threadIdx.x;
+        col[u] = e < end ? __ldg(&ci[e]) : -1;
       }
-      scanned += imin64((int64_t)blockDim.x, end - base);
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        if (col[u] >= 0) {
+          W f[NW];
+          load_words<W, NW>(F + (int64_t)col[u] * NW, f);
+#pragma unroll
+          for (int i = 0; i < NW; i++) acc[i] |= f[i];
+        }
+      }
+      scanned += imin64(4 * (int64_t)blockDim.x, end - base);
       block_or<W, NW>(acc, s_red);
       bool done = true;
 #pragma unroll
@@ -579,8 +692,7 @@ __global__ void k_pull_heavy(const int32_t* __restrict__ hlist, int32_t nh, cons
       W s0[NW];
 #pragma unroll
       for (int i = 0; i < NW; i++) s0[i] = sw[i];
-      commit_new<W, NW, OffT>(has, v, nw, s0, end - beg, level, seen, planes, plane_stride, active, heavy, nl,
-                              nctr, &ctr->b);
+      commit_new<W, NW, OffT>(has, v, nw, s0, end - beg, level, seen, pl, active, heavy, nl, nctr, sacc);
       if (threadIdx.x == 0) {
         atomicAdd(&ctr->b.edges_scanned, (unsigned long long)scanned);
         atomicAdd(&ctr->b.vertices_scanned, 1ull);
@@ -588,6 +700,7 @@ __global__ void k_pull_heavy(const int32_t* __restrict__ hlist, int32_t nh, cons
     }
     __syncthreads();
   }
+  flush_stats<W, NW>(sacc, nctr, &ctr->b);
 }
 
 // Zeroes F at the vertices of a frontier list.
@@ -599,22 +712,49 @@ __global__ void k_clear_list(const int32_t* __restrict__ list, const int32_t* __
     F[(int64_t)list[i / NW] * NW + (i % NW)] = 0;
 }
 
-// ---------------------------------------------------------------------------
-// Table pass.  Word wi of the pass (sources word_base .. word_base+kbw-1).
-// One warp per 32-vertex tile; level[s*n + v] and parent[s*n + v].
-template <typename W, int NW>
-__device__ __forceinline__ W plane_at(const W* planes, int64_t plane_stride, int j, int64_t v, int wi) {
-  return planes[j * plane_stride + v * NW + wi];
+template <typename T>
+__global__ void k_fill(T* p, int64_t count, T value) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += (int64_t)gridDim.x * blockDim.x)
+    p[i] = value;
 }
 
-template <typename W, int NW, typename OffT, int WARPS>
+// ---------------------------------------------------------------------------
+// Table pass, word wi of the pass (sources word_base .. word_base+kbw-1; the
+// output pointers are already offset to row word_base).
+//
+// The vertex's own level and "needed" bits: need = reached and not the
+// source itself (level 0 is the only level with every plane bit clear).
+template <typename W, int NW>
+__device__ __forceinline__ void vertex_levels(const W* __restrict__ seen, const Planes<W, NW>& pl, int nplanes,
+                                              int64_t v, int wi, W& sv, W& p0, W& p1, W& root) {
+  sv = seen[v * NW + wi];
+  W pr[2];
+  load_words<W, 2>(pl.p01 + ((v * NW + wi) << 1), pr);
+  p0 = pr[0];
+  p1 = pr[1];
+  W anyp = p0 | p1;
+  for (int j = 2; j < nplanes; j++) anyp |= pl.get(j, v, wi);
+  root = sv & ~anyp;
+}
+
+// One warp per 32-vertex tile.  Parent search: rounds over the flattened,
+// still-needed adjacency (ascending within each vertex), U x 32 edges per
+// round, loads issued up front; a segmented exclusive prefix OR in edge order
+// hands each needed bit to its first (= smallest-id) matching neighbour.
+template <typename W, int NW, typename OffT, int WARPS, int U>
 __global__ void __launch_bounds__(WARPS * 32) k_tables(int64_t n, const OffT* __restrict__ ro,
                                                        const int32_t* __restrict__ ci, const W* __restrict__ seen,
-                                                       const W* __restrict__ planes, int64_t plane_stride, int nplanes,
-                                                       int wi, int kbw, int heavy, int32_t* __restrict__ level_out,
+                                                       Planes<W, NW> pl, int nplanes, int wi, int kbw, int heavy,
+                                                       int32_t* __restrict__ level_out,
                                                        int32_t* __restrict__ parent_out, Ctrs* ctr) {
   constexpr int B = WB<W>::bits;
   __shared__ int32_t s_par[WARPS][B][32];
+  __shared__ int32_t s_off[WARPS][33];
+  __shared__ int64_t s_pos[WARPS][32];
+  __shared__ W s_need[WARPS][32];
+  __shared__ W s_t0[WARPS][32];
+  __shared__ W s_t1[WARPS][32];
+  __shared__ W s_found[WARPS][32];
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
   const int64_t ntiles = (n + 31) >> 5;
@@ -624,96 +764,115 @@ __global__ void __launch_bounds__(WARPS * 32) k_tables(int64_t n, const OffT* __
   for (int64_t tile = warp; tile < ntiles; tile += nwarps) {
     const int64_t v = tile * 32 + lane;
     const bool valid = v < n;
-    W sv = 0, p0 = 0, p1 = 0, anyp = 0;
+    W sv = 0, p0 = 0, p1 = 0, root = 0;
     int64_t beg = 0, dg = 0;
     if (valid) {
-      sv = seen[v * NW + wi];
-      p0 = plane_at<W, NW>(planes, plane_stride, 0, v, wi);
-      p1 = plane_at<W, NW>(planes, plane_stride, 1, v, wi);
-      anyp = p0 | p1;
-      for (int j = 2; j < nplanes; j++) anyp |= plane_at<W, NW>(planes, plane_stride, j, v, wi);
+      vertex_levels<W, NW>(seen, pl, nplanes, v, wi, sv, p0, p1, root);
       beg = ro[v];
       dg = (int64_t)ro[v + 1] - beg;
     }
-    const W root = sv & ~anyp;
-    const W need = sv & ~root;
-    const W t0 = ~p0, t1 = ~(p0 ^ p1);  // bit-sliced (level - 1) mod 4
     const bool is_heavy = dg > heavy;
-    // light: lane-private scan with early exit
-    W found = 0;
-    if (valid && need && !is_heavy && dg <= 32) {
-      for (int64_t e = beg; e < beg + dg; e++) {
-        const int32_t u = __ldg(&ci[e]);
-        pe++;
-        const W su = seen[(int64_t)u * NW + wi];
-        const W q0 = plane_at<W, NW>(planes, plane_stride, 0, u, wi);
-        const W q1 = plane_at<W, NW>(planes, plane_stride, 1, u, wi);
-        W eq = su & ~(q0 ^ t0) & ~(q1 ^ t1) & need & ~found;
-        found |= eq;
-        while (eq) {
-          const int b = ffs0(eq);
-          s_par[wib][b][lane] = u;
-          eq &= eq - 1;
-        }
-        if (found == need) break;
+    const W need = (valid && !is_heavy) ? (sv & ~root) : (W)0;
+    s_need[wib][lane] = need;
+    s_t0[wib][lane] = ~p0;         // bit-sliced (level - 1) mod 4, plane 0
+    s_t1[wib][lane] = ~(p0 ^ p1);  // plane 1
+    s_found[wib][lane] = 0;
+    int64_t pos = beg;
+    const int64_t end = beg + dg;
+    __syncwarp();
+    for (;;) {
+      const W fnd = s_found[wib][lane];
+      const int32_t r = (need & ~fnd) ? (int32_t)(end - pos) : 0;
+      int32_t inc = r;
+#pragma unroll
+      for (int s = 1; s < 32; s <<= 1) {
+        const int32_t y = __shfl_up_sync(0xffffffffu, inc, s);
+        if (lane >= s) inc += y;
       }
-    }
-    // medium: warp-cooperative scan, one vertex at a time
-    unsigned med = __ballot_sync(0xffffffffu, valid && need && !is_heavy && dg > 32);
-    while (med) {
-      const int j = __ffs(med) - 1;
-      med &= med - 1;
-      const W nd = shfl_idx<W>(need, j);
-      const W a0 = shfl_idx<W>(t0, j), a1 = shfl_idx<W>(t1, j);
-      const int64_t b0 = __shfl_sync(0xffffffffu, beg, j);
-      const int64_t d0 = __shfl_sync(0xffffffffu, dg, j);
-      W fnd = 0;
-      for (int64_t base = 0; base < d0; base += 32) {
-        const int64_t e = base + lane;
-        W eq = 0;
-        int32_t u = 0;
-        if (e < d0) {
-          u = __ldg(&ci[b0 + e]);
-          const W su = seen[(int64_t)u * NW + wi];
-          const W q0 = plane_at<W, NW>(planes, plane_stride, 0, u, wi);
-          const W q1 = plane_at<W, NW>(planes, plane_stride, 1, u, wi);
-          eq = su & ~(q0 ^ a0) & ~(q1 ^ a1) & nd & ~fnd;
+      const int32_t total = __shfl_sync(0xffffffffu, inc, 31);
+      if (total == 0) break;
+      const int32_t off = inc - r;
+      s_off[wib][lane] = off;
+      if (lane == 31) s_off[wib][32] = inc;
+      s_pos[wib][lane] = pos;
+      __syncwarp();
+      const int32_t take = total < 32 * U ? total : 32 * U;
+      int key[U];
+      int32_t col[U];
+      W q0[U], q1[U];
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        const int32_t e = u * 32 + lane;
+        key[u] = 32 + lane;
+        col[u] = -1;
+        if (e < take) {
+          const int o = flat_owner(s_off[wib], e);
+          key[u] = o;
+          col[u] = __ldg(&ci[s_pos[wib][o] + (e - s_off[wib][o])]);
         }
-        // exclusive prefix OR in lane (= neighbour) order: the lowest lane wins
-        W inc = eq;
+      }
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        q0[u] = q1[u] = 0;
+        if (col[u] >= 0) {
+          W pr[2];
+          load_words<W, 2>(pl.p01 + (((int64_t)col[u] * NW + wi) << 1), pr);
+          q0[u] = pr[0];
+          q1[u] = pr[1];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        const int k = key[u];
+        const bool act = k < 32;
+        W eq = 0;
+        if (act) eq = ~(q0[u] ^ s_t0[wib][k]) & ~(q1[u] ^ s_t1[wib][k]) & s_need[wib][k];
+        W incl = eq;
 #pragma unroll
         for (int s = 1; s < 32; s <<= 1) {
-          const W y = shfl_up<W>(inc, s);
-          if (lane >= s) inc |= y;
+          const W y = shfl_up<W>(incl, s);
+          const int k2 = __shfl_up_sync(0xffffffffu, k, s);
+          if (lane >= s && k2 == k) incl |= y;
         }
-        W excl = shfl_up<W>(inc, 1);
-        if (lane == 0) excl = 0;
-        W mine = eq & ~excl;
-        while (mine) {
-          const int b = ffs0(mine);
-          s_par[wib][b][j] = u;
-          mine &= mine - 1;
+        const W prev = shfl_up<W>(incl, 1);
+        const int kprev = __shfl_up_sync(0xffffffffu, k, 1);
+        const W excl = (lane > 0 && kprev == k) ? prev : (W)0;
+        const int knext = __shfl_down_sync(0xffffffffu, k, 1);
+        const bool tail = (lane == 31) || (knext != k);
+        if (act) {
+          W mine = eq & ~excl & ~s_found[wib][k];
+          while (mine) {
+            const int b = ffs0(mine);
+            s_par[wib][b][k] = col[u];
+            mine &= mine - 1;
+          }
         }
-        fnd |= shfl_idx<W>(inc, 31);
-        if (lane == 0) pe += (unsigned long long)imin64(32, d0 - base);
-        if (fnd == nd) break;
+        __syncwarp();
+        if (act && tail) s_found[wib][k] |= incl;
+        __syncwarp();
       }
+      // advance this lane's vertex by the edges the round consumed
+      int32_t used = take - off;
+      used = used < 0 ? 0 : (used > r ? r : used);
+      pos += used;
+      if (lane == 0) pe += (unsigned long long)take;
+      __syncwarp();
     }
-    __syncwarp();
     // write rows: level and parent of sources 0..kbw-1 at vertices tile*32 + lane
     if (valid && !is_heavy) {
       constexpr int RP = 8;  // planes held in registers; deeper levels read on demand
-      W pl[RP];
+      W plr[RP];
+      plr[0] = p0;
+      plr[1] = p1;
 #pragma unroll
-      for (int j = 0; j < RP; j++) pl[j] = j < nplanes ? plane_at<W, NW>(planes, plane_stride, j, v, wi) : (W)0;
+      for (int j = 2; j < RP; j++) plr[j] = j < nplanes ? pl.get(j, v, wi) : (W)0;
       for (int s = 0; s < kbw; s++) {
         int32_t lv = -1, pr = -1;
         if ((sv >> s) & 1) {
           lv = 0;
 #pragma unroll
-          for (int j = 0; j < RP; j++) lv |= (int32_t)((pl[j] >> s) & 1) << j;
-          for (int j = RP; j < nplanes; j++)
-            lv |= (int32_t)((plane_at<W, NW>(planes, plane_stride, j, v, wi) >> s) & 1) << j;
+          for (int j = 0; j < RP; j++) lv |= (int32_t)((plr[j] >> s) & 1) << j;
+          for (int j = RP; j < nplanes; j++) lv |= (int32_t)((pl.get(j, v, wi) >> s) & 1) << j;
           pr = ((root >> s) & 1) ? (int32_t)v : s_par[wib][s][lane];
         }
         __stcs(&level_out[(int64_t)s * n + v], lv);
@@ -726,84 +885,120 @@ __global__ void __launch_bounds__(WARPS * 32) k_tables(int64_t n, const OffT* __
   if (lane == 0 && pe) atomicAdd(&ctr->b.parent_edges, pe);
 }
 
-// Table pass for heavy vertices: one block per vertex, block-wide ordered
-// scan of the adjacency with early exit.
+// Table pass for heavy vertices, scan step: the blocks walk a per-graph list
+// of (heavy index, chunk) items, each chunk `chunk` edges of one adjacency.
+// Each block hands every needed bit to the first matching neighbour of its
+// chunk (block-wide exclusive prefix OR in edge order) and folds it into
+// hpar[idx*B + bit] with atomicMin, so the smallest id over all chunks wins
+// regardless of schedule.  hpar must hold INT32_MAX beforehand.
 template <typename W, int NW, typename OffT>
-__global__ void k_tables_heavy(const int32_t* __restrict__ hlist, int32_t nh, int64_t n, const OffT* __restrict__ ro,
-                               const int32_t* __restrict__ ci, const W* __restrict__ seen, const W* __restrict__ planes,
-                               int64_t plane_stride, int nplanes, int wi, int kbw, int32_t* __restrict__ level_out,
-                               int32_t* __restrict__ parent_out, Ctrs* ctr) {
-  __shared__ W s_wor[32];
-  __shared__ W s_found;
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nwb = blockDim.x >> 5;
-  for (int64_t idx = blockIdx.x; idx < nh; idx += gridDim.x) {
+__global__ void __launch_bounds__(256) k_tables_heavy_scan(const int32_t* __restrict__ hlist,
+                                                           const int2* __restrict__ items, int64_t nitems,
+                                                           const OffT* __restrict__ ro, const int32_t* __restrict__ ci,
+                                                           const W* __restrict__ seen, Planes<W, NW> pl, int nplanes,
+                                                           int wi, int chunk, int32_t* hpar, Ctrs* ctr) {
+  constexpr int B = WB<W>::bits;
+  __shared__ W s_wor[8];
+  __shared__ W s_claimed;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int64_t it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const int2 item = items[it];
+    const int64_t idx = item.x;
     const int64_t v = hlist[idx];
-    const W sv = seen[v * NW + wi];
-    const W p0 = plane_at<W, NW>(planes, plane_stride, 0, v, wi);
-    const W p1 = plane_at<W, NW>(planes, plane_stride, 1, v, wi);
-    W anyp = p0 | p1;
-    for (int j = 2; j < nplanes; j++) anyp |= plane_at<W, NW>(planes, plane_stride, j, v, wi);
-    const W root = sv & ~anyp;
+    W sv, p0, p1, root;
+    vertex_levels<W, NW>(seen, pl, nplanes, v, wi, sv, p0, p1, root);
     const W need = sv & ~root;
+    if (!need) continue;  // uniform
     const W t0 = ~p0, t1 = ~(p0 ^ p1);
     const int64_t beg = ro[v], end = ro[v + 1];
-    W fnd = 0;
-    unsigned long long pe = 0;
-    if (need) {
-      for (int64_t base = beg; base < end; base += blockDim.x) {
-        const int64_t e = base + threadIdx.x;
-        W eq = 0;
-        int32_t u = 0;
-        if (e < end) {
-          u = __ldg(&ci[e]);
-          const W su = seen[(int64_t)u * NW + wi];
-          const W q0 = plane_at<W, NW>(planes, plane_stride, 0, u, wi);
-          const W q1 = plane_at<W, NW>(planes, plane_stride, 1, u, wi);
-          eq = su & ~(q0 ^ t0) & ~(q1 ^ t1) & need & ~fnd;
-        }
-        // block-wide exclusive prefix OR in thread order
-        W inc = eq;
+    const int64_t c0 = beg + (int64_t)item.y * chunk;
+    for (int64_t cb = c0; cb < end && cb < c0 + chunk; cb += chunk) {  // one chunk
+      const int64_t ce = imin64(end, cb + chunk);
+      if (threadIdx.x == 0) s_claimed = 0;
+      __syncthreads();
+      unsigned long long pe = 0;
+      for (int64_t base = cb; base < ce; base += 4 * 256) {
+        int32_t col[4];
+        W q0[4], q1[4];
 #pragma unroll
-        for (int s = 1; s < 32; s <<= 1) {
-          const W y = shfl_up<W>(inc, s);
-          if (lane >= s) inc |= y;
+        for (int u = 0; u < 4; u++) {
+          const int64_t e = base + u * 256 + threadIdx.x;
+          col[u] = e < ce ? __ldg(&ci[e]) : -1;
         }
-        if (lane == 31) s_wor[wid] = inc;
-        __syncthreads();
-        W before = 0;
-        for (int k = 0; k < wid; k++) before |= s_wor[k];
-        W all = 0;
-        for (int k = 0; k < nwb; k++) all |= s_wor[k];
-        const W lane_excl = shfl_up<W>(inc, 1);
-        const W excl = before | (lane ? lane_excl : (W)0);
-        W mine = eq & ~excl;
-        while (mine) {
-          const int b = ffs0(mine);
-          parent_out[(int64_t)b * n + v] = u;
-          mine &= mine - 1;
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          q0[u] = q1[u] = 0;
+          if (col[u] >= 0) {
+            W pr[2];
+            load_words<W, 2>(pl.p01 + (((int64_t)col[u] * NW + wi) << 1), pr);
+            q0[u] = pr[0];
+            q1[u] = pr[1];
+          }
         }
-        pe += (unsigned long long)imin64((int64_t)blockDim.x, end - base);
-        fnd |= all;
-        __syncthreads();
-        if (fnd == need) break;
+        bool all_done = false;
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          const W claimed = s_claimed;
+          const W eq = col[u] >= 0 ? (~(q0[u] ^ t0) & ~(q1[u] ^ t1) & need & ~claimed) : (W)0;
+          W incl = eq;
+#pragma unroll
+          for (int s = 1; s < 32; s <<= 1) {
+            const W y = shfl_up<W>(incl, s);
+            if (lane >= s) incl |= y;
+          }
+          if (lane == 31) s_wor[wid] = incl;
+          __syncthreads();
+          W before = 0, all = 0;
+#pragma unroll
+          for (int k = 0; k < 8; k++) {
+            const W x = s_wor[k];
+            if (k < wid) before |= x;
+            all |= x;
+          }
+          W lp = shfl_up<W>(incl, 1);
+          const W excl = before | (lane ? lp : (W)0);
+          W mine = eq & ~excl;
+          while (mine) {
+            const int b = ffs0(mine);
+            atomicMin(&hpar[idx * B + b], col[u]);
+            mine &= mine - 1;
+          }
+          __syncthreads();
+          if (threadIdx.x == 0) s_claimed = claimed | all;
+          __syncthreads();
+          all_done = ((claimed | all) & need) == need;
+        }
+        pe += (unsigned long long)imin64(4 * 256, ce - base);
+        if (all_done) break;  // later edges of this chunk have larger ids
       }
+      if (threadIdx.x == 0) atomicAdd(&ctr->b.parent_edges, pe);
+      __syncthreads();
     }
-    if (threadIdx.x == 0) {
-      s_found = fnd;
-      if (pe) atomicAdd(&ctr->b.parent_edges, pe);
-    }
+  }
+}
+
+// Table pass for heavy vertices, write step: block per heavy vertex, thread
+// per source of the word.
+template <typename W, int NW>
+__global__ void k_tables_heavy_write(const int32_t* __restrict__ hlist, int32_t nh, int64_t n,
+                                     const W* __restrict__ seen, Planes<W, NW> pl, int nplanes, int wi, int kbw,
+                                     const int32_t* __restrict__ hpar, int32_t* __restrict__ level_out,
+                                     int32_t* __restrict__ parent_out) {
+  constexpr int B = WB<W>::bits;
+  for (int64_t idx = blockIdx.x; idx < nh; idx += gridDim.x) {
+    const int64_t v = hlist[idx];
+    W sv, p0, p1, root;
+    vertex_levels<W, NW>(seen, pl, nplanes, v, wi, sv, p0, p1, root);
     for (int s = threadIdx.x; s < kbw; s += blockDim.x) {
-      int32_t lv = -1;
+      int32_t lv = -1, pr = -1;
       if ((sv >> s) & 1) {
         lv = 0;
-        for (int j = 0; j < nplanes; j++) lv |= (int32_t)((plane_at<W, NW>(planes, plane_stride, j, v, wi) >> s) & 1) << j;
-        if ((root >> s) & 1) parent_out[(int64_t)s * n + v] = (int32_t)v;
-      } else {
-        parent_out[(int64_t)s * n + v] = -1;
+        for (int j = 0; j < nplanes; j++) lv |= (int32_t)((pl.get(j, v, wi) >> s) & 1) << j;
+        pr = ((root >> s) & 1) ? (int32_t)v : hpar[idx * B + s];
       }
       level_out[(int64_t)s * n + v] = lv;
+      parent_out[(int64_t)s * n + v] = pr;
     }
-    __syncthreads();
   }
 }
 

@@ -146,7 +146,8 @@ extern "C" xb_status xb_traverse_noalloc(int64_t n, const int32_t* row_offsets, 
   W* seen = scratch + kSeenOff;
   W* F = scratch + kFOff;
   W* N = scratch + kNOff;
-  W* planes = scratch + kPlanesOff;
+  // planes 0-1 interleaved (2 words per vertex), planes 2.. separate
+  const xbk::Planes<W, 1> pl{scratch + kPlanesOff, scratch + kPlanesOff + 2 * kW, (int64_t)kW};
   int32_t* lists = (int32_t*)(scratch + kListsOff);
   xbk::Lists fl{lists + 0 * kW, lists + 1 * kW};
   xbk::Lists nl{lists + 2 * kW, lists + 3 * kW};
@@ -154,7 +155,7 @@ extern "C" xb_status xb_traverse_noalloc(int64_t n, const int32_t* row_offsets, 
   int32_t* heavy_list = lists + 5 * kW;
   xbk::Ctrs* ctr = (xbk::Ctrs*)(scratch + kCtrOff);
   int32_t* misc = (int32_t*)(scratch + kMiscOff);  // [0] heavy count, [1] validation error
-  const int64_t plane_stride = (int64_t)kW;
+  const size_t plane_bytes = sizeof(W) * kW;
   const size_t state_bytes = sizeof(W) * (size_t)n;
 
   // validate the caller's arrays on the device (a bad id would fault the kernels)
@@ -185,7 +186,8 @@ extern "C" xb_status xb_traverse_noalloc(int64_t n, const int32_t* row_offsets, 
   NA_CUDA(cudaMemsetAsync(N, 0, state_bytes, sm));
 
   const int64_t ntiles = (n + 31) / 32;
-  constexpr int PULL_WARPS = 8, TAB_WARPS = 4;
+  constexpr int PULL_WARPS = 8, TAB_WARPS = 4, U = 4;
+  constexpr int PUSH_CHUNK = 2048;
   const int pull_grid = (int)std::max<int64_t>(1, std::min<int64_t>((ntiles + PULL_WARPS - 1) / PULL_WARPS, (int64_t)sms * 8));
   const int tab_grid = (int)std::max<int64_t>(1, std::min<int64_t>((ntiles + TAB_WARPS - 1) / TAB_WARPS, (int64_t)sms * 16));
   xbk::Ctrs h{};
@@ -195,13 +197,14 @@ extern "C" xb_status xb_traverse_noalloc(int64_t n, const int32_t* row_offsets, 
     xbk::Masks<W, 1> active{};
     active.w[0] = kb == 64 ? ~0ull : ((1ull << kb) - 1ull);
     NA_CUDA(cudaMemsetAsync(seen, 0, state_bytes, sm));
-    NA_CUDA(cudaMemsetAsync(planes, 0, sizeof(W) * (size_t)plane_stride * 3, sm));
+    NA_CUDA(cudaMemsetAsync(pl.p01, 0, 2 * plane_bytes, sm));
+    NA_CUDA(cudaMemsetAsync(pl.ph, 0, plane_bytes, sm));
     int planes_zeroed = 3;
     std::memset(&h, 0, sizeof(h));
     h.b.m_unfinished = m32;
     NA_CUDA(cudaMemcpyAsync(ctr, &h, sizeof(h), cudaMemcpyHostToDevice, sm));
-    xbk::k_init_batch<W, 1, int32_t><<<1, 256, 0, sm>>>(sources + k0, kb, row_offsets, F, seen, active, kHeavy, fl,
-                                                         ctr);
+    xbk::k_init_batch<W, 1, int32_t><<<1, 256, 0, sm>>>(sources + k0, kb, row_offsets, F, seen, pl, active, kHeavy,
+                                                         fl, ctr);
     NA_CUDA(cudaGetLastError());
     int cur = 0, lvl = 0;
     for (;;) {
@@ -212,7 +215,7 @@ extern "C" xb_status xb_traverse_noalloc(int64_t n, const int32_t* row_offsets, 
       if (fcount == 0) break;
       const int next = lvl + 1;
       while (planes_zeroed < kPlanes && ((int64_t)1 << planes_zeroed) <= next) {
-        NA_CUDA(cudaMemsetAsync(planes + (size_t)planes_zeroed * plane_stride, 0, sizeof(W) * (size_t)plane_stride, sm));
+        NA_CUDA(cudaMemsetAsync(pl.ph + (size_t)(planes_zeroed - 2) * kW, 0, plane_bytes, sm));
         planes_zeroed++;
       }
       NA_CUDA(cudaMemsetAsync(&ctr->lv[cur ^ 1], 0, sizeof(xbk::LevelCtr), sm));
@@ -222,19 +225,24 @@ extern "C" xb_status xb_traverse_noalloc(int64_t n, const int32_t* row_offsets, 
           xbk::k_push_light<W, 1, int32_t><<<(int)std::min<int64_t>((lc.n_light + 7) / 8, (int64_t)sms * 16), 256, 0,
                                              sm>>>(fl.light, &ctr->lv[cur].n_light, row_offsets, col_indices, F, seen, N,
                                                    nullptr, 0, touched, ctr, cur);
-        if (lc.n_heavy > 0)
-          xbk::k_push_heavy<W, 1, int32_t><<<(int)std::min<int64_t>(lc.n_heavy, (int64_t)sms * 4), 512, 0, sm>>>(
-              fl.heavy, &ctr->lv[cur].n_heavy, row_offsets, col_indices, F, seen, N, nullptr, 0, touched, ctr, cur);
+        if (lc.n_heavy > 0) {
+          const dim3 hgrid((unsigned)std::max<int64_t>(1, std::min<int64_t>((n + PUSH_CHUNK - 1) / PUSH_CHUNK, 64)),
+                           (unsigned)std::min<int64_t>(lc.n_heavy, 65535));
+          xbk::k_push_heavy<W, 1, int32_t><<<hgrid, 256, 0, sm>>>(fl.heavy, &ctr->lv[cur].n_heavy, row_offsets,
+                                                                  col_indices, F, seen, N, nullptr, 0, touched, ctr,
+                                                                  cur, PUSH_CHUNK);
+          xbk::k_clear_list<W, 1><<<(int)std::min<int64_t>((lc.n_heavy + 255) / 256, (int64_t)sms * 8), 256, 0, sm>>>(
+              fl.heavy, &ctr->lv[cur].n_heavy, F);
+        }
         xbk::k_push_finalize<W, 1, int32_t><<<(int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)sms * 8)),
-                                              256, 0, sm>>>(touched, row_offsets, N, seen, planes, plane_stride, next,
-                                                            active, kHeavy, nl, ctr, cur);
+                                              256, 0, sm>>>(touched, row_offsets, N, seen, pl, next, active, kHeavy,
+                                                            nl, ctr, cur);
       } else {
-        xbk::k_pull_tiles<W, 1, int32_t, PULL_WARPS><<<pull_grid, PULL_WARPS * 32, 0, sm>>>(
-            n, row_offsets, col_indices, F, seen, N, planes, plane_stride, next, active, kHeavy, nl, ctr, cur);
+        xbk::k_pull_tiles<W, 1, int32_t, PULL_WARPS, U><<<pull_grid, PULL_WARPS * 32, 0, sm>>>(
+            n, row_offsets, col_indices, F, seen, N, pl, next, active, kHeavy, nl, ctr, cur);
         if (n_heavy > 0)
           xbk::k_pull_heavy<W, 1, int32_t><<<(int)std::min<int64_t>(n_heavy, (int64_t)sms * 4), 512, 0, sm>>>(
-              heavy_list, n_heavy, row_offsets, col_indices, F, seen, N, planes, plane_stride, next, active, kHeavy,
-              nl, ctr, cur);
+              heavy_list, n_heavy, row_offsets, col_indices, F, seen, N, pl, next, active, kHeavy, nl, ctr, cur);
         NA_CUDA(cudaMemsetAsync(F, 0, state_bytes, sm));
       }
       NA_CUDA(cudaGetLastError());
@@ -244,13 +252,9 @@ extern "C" xb_status xb_traverse_noalloc(int64_t n, const int32_t* row_offsets, 
       lvl = next;
     }
     max_levels = std::max(max_levels, lvl);
-    xbk::k_tables<W, 1, int32_t, TAB_WARPS><<<tab_grid, TAB_WARPS * 32, 0, sm>>>(
-        n, row_offsets, col_indices, seen, planes, plane_stride, planes_zeroed, 0, kb, kHeavy, level + k0 * n,
-        parent + k0 * n, ctr);
-    if (n_heavy > 0)
-      xbk::k_tables_heavy<W, 1, int32_t><<<(int)std::min<int64_t>(n_heavy, (int64_t)sms * 4), 256, 0, sm>>>(
-          heavy_list, n_heavy, n, row_offsets, col_indices, seen, planes, plane_stride, planes_zeroed, 0, kb,
-          level + k0 * n, parent + k0 * n, ctr);
+    // every vertex takes the edge-flat table path here (no heavy-vertex staging)
+    xbk::k_tables<W, 1, int32_t, TAB_WARPS, U><<<tab_grid, TAB_WARPS * 32, 0, sm>>>(
+        n, row_offsets, col_indices, seen, pl, planes_zeroed, 0, kb, INT32_MAX, level + k0 * n, parent + k0 * n, ctr);
     NA_CUDA(cudaGetLastError());
     NA_CUDA(cudaMemcpyAsync(&h, ctr, sizeof(h), cudaMemcpyDeviceToHost, sm));
     NA_CUDA(cudaStreamSynchronize(sm));
