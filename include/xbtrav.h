@@ -169,7 +169,7 @@ xb_status xb_traverse(xb_ctx* ctx, const xb_graph* g, const int32_t* sources, in
  * k sources, level and parent tables k*n each, source-major.  stream is a
  * cudaStream_t (NULL = the legacy default stream); the call returns after
  * the work on it has finished.  Working state lives in one fixed array of
- * about 23 MiB compiled into the library, held by every GPU that loads the
+ * about 32 MiB compiled into the library, held by every GPU that loads the
  * library until exit; graphs above XB_NOALLOC_MAX_VERTICES vertices are
  * rejected with XB_ERR_CAPACITY.  The first call on a device looks up the
  * array's address (do it before any stream capture on that device).  Calls

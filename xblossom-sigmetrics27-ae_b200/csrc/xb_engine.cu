@@ -64,6 +64,9 @@ struct xb_graph {
   int32_t* d_hpar = nullptr;   // per heavy vertex, 64 parent slots of the table pass
   int2* d_hitems = nullptr;    // (heavy index, chunk) items of the table pass
   int64_t n_hitems = 0;
+  int2* d_hub_items = nullptr;  // (heavy index, chunk) items of the hub pull
+  int64_t n_hub_items = 0;
+  int32_t* d_hidx_of = nullptr;  // vertex -> index in the heavy list (-1 for light)
   int32_t n_heavy = 0;
   int32_t heavy_thr = -1;
 };
@@ -72,9 +75,15 @@ namespace {
 
 // Edges per work item of the heavy-vertex table scan.
 constexpr int kTableChunk = 4096;
+// Vertices above this degree (hubs) are pulled in chunks by many warps; the
+// other heavy vertices by one warp each.
+constexpr int kHubDegree = 4096;
+constexpr int kHubChunk = 2048;
+// Parent slots per heavy vertex: up to 64 sources x 4 words.
+constexpr int kHparRow = 256;
 
 struct WsLayout {
-  size_t seen, F, N, p01, ph, touched, fl_light, fl_heavy, nl_light, nl_heavy, stamp, total;
+  size_t seen, F, N, p01, ph, pushed, p8, touched, fl_light, fl_heavy, nl_light, nl_heavy, stamp, total;
   int64_t plane_stride;  // in words
   int nplanes_alloc;
 };
@@ -104,6 +113,8 @@ WsLayout layout_for(int64_t n, int word_bytes, int nw) {
   L.N = o; o += sw;
   L.p01 = o; o += 2 * sw;
   L.ph = o; o += sw * (L.nplanes_alloc - 2);
+  L.pushed = o; o += sw;
+  L.p8 = o; o += align_up((size_t)n * nw * word_bytes * 8);  // one byte per (vertex, source)
   L.touched = o; o += li;
   L.fl_light = o; o += li;
   L.fl_heavy = o; o += li;
@@ -182,12 +193,23 @@ xb_status ensure_heavy(xb_graph* g, int thr) {
   g->d_hpar = nullptr;
   g->heavy_thr = -1;
   if (cudaMalloc(&g->d_heavy, sizeof(int32_t) * std::max<size_t>(hv.size(), 1)) != cudaSuccess ||
-      cudaMalloc(&g->d_hpar, sizeof(int32_t) * 64 * std::max<size_t>(hv.size(), 1)) != cudaSuccess) {
+      cudaMalloc(&g->d_hpar, sizeof(int32_t) * kHparRow * std::max<size_t>(hv.size(), 1)) != cudaSuccess) {
     cudaGetLastError();
     return fail(XB_ERR_OOM, "heavy list allocation failed");
   }
   if (!hv.empty())
     XB_CUDA(cudaMemcpy(g->d_heavy, hv.data(), sizeof(int32_t) * hv.size(), cudaMemcpyHostToDevice));
+  {
+    std::vector<int32_t> hidx_of((size_t)g->n, -1);
+    for (size_t i = 0; i < hv.size(); i++) hidx_of[hv[i]] = (int32_t)i;
+    if (g->d_hidx_of) cudaFree(g->d_hidx_of);
+    g->d_hidx_of = nullptr;
+    if (cudaMalloc(&g->d_hidx_of, sizeof(int32_t) * (size_t)g->n) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(XB_ERR_OOM, "heavy index map allocation failed");
+    }
+    XB_CUDA(cudaMemcpy(g->d_hidx_of, hidx_of.data(), sizeof(int32_t) * (size_t)g->n, cudaMemcpyHostToDevice));
+  }
   // (heavy index, chunk) work items of the table pass, heaviest vertices first
   // (ids ascend roughly with falling degree in R-MAT-like graphs, so this is
   // the list order)
@@ -205,6 +227,22 @@ xb_status ensure_heavy(xb_graph* g, int thr) {
   if (!items.empty())
     XB_CUDA(cudaMemcpy(g->d_hitems, items.data(), sizeof(int2) * items.size(), cudaMemcpyHostToDevice));
   g->n_hitems = (int64_t)items.size();
+  // (heavy index, chunk) items of the hub pull
+  std::vector<int2> hub_items;
+  for (size_t i = 0; i < hv.size(); i++) {
+    const int64_t d = g->h_ro[hv[i] + 1] - g->h_ro[hv[i]];
+    if (d <= kHubDegree) continue;
+    for (int64_t c = 0; c * kHubChunk < d; c++) hub_items.push_back(make_int2((int)i, (int)c));
+  }
+  if (g->d_hub_items) cudaFree(g->d_hub_items);
+  g->d_hub_items = nullptr;
+  if (cudaMalloc(&g->d_hub_items, sizeof(int2) * std::max<size_t>(hub_items.size(), 1)) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(XB_ERR_OOM, "hub item list allocation failed");
+  }
+  if (!hub_items.empty())
+    XB_CUDA(cudaMemcpy(g->d_hub_items, hub_items.data(), sizeof(int2) * hub_items.size(), cudaMemcpyHostToDevice));
+  g->n_hub_items = (int64_t)hub_items.size();
   g->n_heavy = (int32_t)hv.size();
   g->heavy_thr = thr;
   return XB_OK;
@@ -249,6 +287,8 @@ xb_status run_plain(xb_ctx* c, xb_graph* g, const int32_t* d_sources, int32_t k,
   W* F = (W*)(base + L.F);
   W* N = (W*)(base + L.N);
   const xbk::Planes<W, NW> pl{(W*)(base + L.p01), (W*)(base + L.ph), L.plane_stride};
+  W* pushed = (W*)(base + L.pushed);
+  uint8_t* p8 = (uint8_t*)(base + L.p8);
   int32_t* touched = (int32_t*)(base + L.touched);
   xbk::Lists fl{(int32_t*)(base + L.fl_light), (int32_t*)(base + L.fl_heavy)};
   xbk::Lists nl{(int32_t*)(base + L.nl_light), (int32_t*)(base + L.nl_heavy)};
@@ -261,7 +301,8 @@ xb_status run_plain(xb_ctx* c, xb_graph* g, const int32_t* d_sources, int32_t k,
   const float alpha = c->tuning.pull_alpha > 0 ? c->tuning.pull_alpha : 4.0f;
   ClassTimer timer{c, st, c->tuning.timing != 0};
   const int64_t ntiles = (n + 31) / 32;
-  constexpr int PULL_WARPS = 8, PULL_U = 4;
+  // the pull tile keeps a B*NW-byte parent-index row per lane in shared memory
+  constexpr int PULL_WARPS = (B * NW * 32 * 8 > 40 * 1024) ? 4 : 8, PULL_U = 4;
   constexpr int TAB_WARPS = (B == 64) ? 4 : 8, TAB_U = 4;
   constexpr int PUSH_CHUNK = 2048;
   const int pull_grid = (int)std::max<int64_t>(1, std::min<int64_t>((ntiles + PULL_WARPS - 1) / PULL_WARPS, (int64_t)sms * 8));
@@ -282,6 +323,13 @@ xb_status run_plain(xb_ctx* c, xb_graph* g, const int32_t* d_sources, int32_t k,
     XB_CUDA(cudaMemsetAsync(seen, 0, state_bytes, c->stream));
     XB_CUDA(cudaMemsetAsync(pl.p01, 0, 2 * plane_bytes, c->stream));
     XB_CUDA(cudaMemsetAsync(pl.ph, 0, plane_bytes, c->stream));
+    XB_CUDA(cudaMemsetAsync(pushed, 0, state_bytes, c->stream));
+    if (g->n_heavy > 0) {  // parent slots of the heavy vertices (hub pulls fold in with atomicMin)
+      const int64_t hcount = (int64_t)g->n_heavy * kHparRow;
+      xbk::k_fill<int32_t><<<(int)std::min<int64_t>((hcount + 255) / 256, sms * 8), 256, 0, c->stream>>>(
+          g->d_hpar, hcount, INT32_MAX);
+      XB_LAUNCH_CHECK("hpar_fill");
+    }
     int planes_zeroed = 3;
     std::memset(c->h_ctr, 0, sizeof(xbk::Ctrs));
     c->h_ctr->b.m_unfinished = g->m;
@@ -292,6 +340,7 @@ xb_status run_plain(xb_ctx* c, xb_graph* g, const int32_t* d_sources, int32_t k,
     XB_LAUNCH_CHECK("init");
     timer.end(2, 1);
     int cur = 0, level = 0;
+    bool pushed_deep = false;  // a push step reached level >= 2 (its parents need a search)
     for (;;) {
       XB_CUDA(cudaMemcpyAsync(c->h_ctr, c->d_ctr, sizeof(xbk::Ctrs), cudaMemcpyDeviceToHost, c->stream));
       XB_CUDA(cudaStreamSynchronize(c->stream));
@@ -331,21 +380,37 @@ xb_status run_plain(xb_ctx* c, xb_graph* g, const int32_t* d_sources, int32_t k,
         // the touched count is on the device; size the grid for the worst case
         const int fgrid = (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)sms * 8));
         xbk::k_push_finalize<W, NW, OffT><<<fgrid, 256, 0, c->stream>>>(touched, ro, N, seen, pl, next_level, active,
-                                                                        heavy, nl, c->d_ctr, cur);
+                                                                        heavy, nl, c->d_ctr, cur, pushed);
         XB_LAUNCH_CHECK("push_finalize");
         launches++;
         if (st) st->push_levels++;
+        if (next_level >= 2) pushed_deep = true;
       } else {
         xbk::k_pull_tiles<W, NW, OffT, PULL_WARPS, PULL_U><<<pull_grid, PULL_WARPS * 32, 0, c->stream>>>(
-            n, ro, ci, F, seen, N, pl, next_level, active, heavy, nl, c->d_ctr, cur);
+            n, ro, ci, F, seen, N, pl, next_level, active, heavy, nl, c->d_ctr, cur, p8);
         XB_LAUNCH_CHECK("pull_tiles");
         launches++;
         if (g->n_heavy > 0) {
-          const int grid = (int)std::min<int64_t>(g->n_heavy, (int64_t)sms * 4);
-          xbk::k_pull_heavy<W, NW, OffT><<<grid, 512, 0, c->stream>>>(g->d_heavy, g->n_heavy, ro, ci, F, seen, N, pl,
-                                                                      next_level, active, heavy, nl, c->d_ctr, cur);
+          // one warp per heavy vertex of degree <= kHubDegree
+          const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((g->n_heavy + 7) / 8, (int64_t)sms * 16));
+          xbk::k_pull_heavy<W, NW, OffT, 4><<<grid, 256, 0, c->stream>>>(g->d_heavy, g->n_heavy, ro, ci, F, seen, N,
+                                                                         pl, next_level, active, heavy, kHubDegree, nl,
+                                                                         c->d_ctr, cur, g->d_hpar);
           XB_LAUNCH_CHECK("pull_heavy");
           launches++;
+          if (g->n_hub_items > 0) {
+            const int hgrid = (int)std::max<int64_t>(1, std::min<int64_t>((g->n_hub_items + 7) / 8, (int64_t)sms * 16));
+            xbk::k_pull_hubs<W, NW, OffT, 4><<<hgrid, 256, 0, c->stream>>>(g->d_heavy, g->d_hub_items, g->n_hub_items,
+                                                                           ro, ci, F, seen, N, active, c->d_ctr, cur,
+                                                                           kHubChunk, g->d_hpar);
+            xbk::k_pull_hub_commit<W, NW, OffT><<<(int)std::max<int64_t>(1, std::min<int64_t>((g->n_heavy + 255) / 256,
+                                                                                                (int64_t)sms * 4)),
+                                                  256, 0, c->stream>>>(g->d_heavy, g->n_heavy, ro, seen, N, pl,
+                                                                       next_level, active, heavy, kHubDegree, nl,
+                                                                       c->d_ctr, cur);
+            XB_LAUNCH_CHECK("pull_hubs");
+            launches += 2;
+          }
         }
         // zero the consumed frontier
         if (fcount * 16 < n) {
@@ -385,23 +450,22 @@ xb_status run_plain(xb_ctx* c, xb_graph* g, const int32_t* d_sources, int32_t k,
       int32_t* lv_out = out_dev ? level_out + s0 * n : c->d_stage;
       int32_t* pr_out = out_dev ? parent_out + s0 * n : c->d_stage + (size_t)B * n;
       timer.begin();
-      xbk::k_tables<W, NW, OffT, TAB_WARPS, TAB_U><<<tab_grid, TAB_WARPS * 32, 0, c->stream>>>(
-          n, ro, ci, seen, pl, planes_zeroed, wi, kbw, heavy, lv_out, pr_out, c->d_ctr);
-      XB_LAUNCH_CHECK("tables");
-      int64_t launches = 1;
-      if (g->n_heavy > 0) {
-        const int64_t hcount = (int64_t)g->n_heavy * B;
-        xbk::k_fill<int32_t><<<(int)std::min<int64_t>((hcount + 255) / 256, sms * 8), 256, 0, c->stream>>>(g->d_hpar, hcount,
-                                                                                                    INT32_MAX);
+      const int32_t* wsrc = d_sources + s0;
+      int64_t launches = 0;
+      if (g->n_heavy > 0 && pushed_deep) {
+        // heavy vertices reached by a push step at level >= 2: search their parents
         const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(g->n_hitems, (int64_t)sms * 8));
         xbk::k_tables_heavy_scan<W, NW, OffT><<<grid, 256, 0, c->stream>>>(g->d_heavy, g->d_hitems, g->n_hitems, ro,
                                                                            ci, seen, pl, planes_zeroed, wi, kTableChunk,
-                                                                           g->d_hpar, c->d_ctr);
-        xbk::k_tables_heavy_write<W, NW><<<(int)std::min<int64_t>(g->n_heavy, (int64_t)sms * 8), 64, 0, c->stream>>>(
-            g->d_heavy, g->n_heavy, n, seen, pl, planes_zeroed, wi, kbw, g->d_hpar, lv_out, pr_out);
-        XB_LAUNCH_CHECK("tables_heavy");
-        launches += 3;
+                                                                           g->d_hpar, c->d_ctr, pushed);
+        XB_LAUNCH_CHECK("tables_heavy_scan");
+        launches++;
       }
+      xbk::k_tables<W, NW, OffT, TAB_WARPS, TAB_U><<<tab_grid, TAB_WARPS * 32, 0, c->stream>>>(
+          n, ro, ci, seen, pl, planes_zeroed, wi, kbw, heavy, lv_out, pr_out, c->d_ctr, p8, pushed, wsrc,
+          g->d_hidx_of, g->d_hpar);
+      XB_LAUNCH_CHECK("tables");
+      launches++;
       timer.end(1, launches);
       if (!out_dev) {
         XB_CUDA(cudaMemcpyAsync(level_out + s0 * n, lv_out, sizeof(int32_t) * (size_t)kbw * n, cudaMemcpyDeviceToHost,
@@ -478,7 +542,9 @@ xb_status xb_ctx_create(int32_t device, xb_ctx** out) {
   XB_CUDA(cudaEventCreate(&c->evc1));
   c->tuning.word_bits = 64;
   c->tuning.words = 1;
-  c->tuning.pull_alpha = 4.0f;
+  // pull unless the frontier's edges are under 1/64 of the unfinished edges:
+  // pull steps record parents as they go, push steps leave them to a search
+  c->tuning.pull_alpha = 64.0f;
   c->tuning.heavy_degree = 256;
   c->tuning.timing = 0;
   *out = c.release();
@@ -602,6 +668,8 @@ xb_status xb_graph_free(xb_graph* g) {
   if (g->d_heavy) cudaFree(g->d_heavy);
   if (g->d_hpar) cudaFree(g->d_hpar);
   if (g->d_hitems) cudaFree(g->d_hitems);
+  if (g->d_hub_items) cudaFree(g->d_hub_items);
+  if (g->d_hidx_of) cudaFree(g->d_hidx_of);
   delete g;
   return XB_OK;
 }

@@ -54,6 +54,10 @@ struct WB<unsigned long long> {
   static constexpr int bits = 64;
 };
 
+// Vertices of degree <= this keep their pull-step parents as one-byte
+// adjacency positions (0..255).
+constexpr int kP8MaxDegree = 256;
+
 __device__ __forceinline__ int64_t imin64(int64_t a, int64_t b) { return a < b ? a : b; }
 __device__ __forceinline__ int popc(unsigned int x) { return __popc(x); }
 __device__ __forceinline__ int popc(unsigned long long x) { return __popcll(x); }
@@ -433,7 +437,7 @@ __global__ void k_push_heavy(const int32_t* __restrict__ list, const int32_t* __
 template <typename W, int NW, typename OffT>
 __global__ void k_push_finalize(const int32_t* __restrict__ touched, const OffT* __restrict__ ro, const W* N,
                                 W* seen, Planes<W, NW> pl, int level, Masks<W, NW> active, int heavy, Lists nl,
-                                Ctrs* ctr, int cur) {
+                                Ctrs* ctr, int cur, W* pushed) {
   LevelCtr* nctr = &ctr->lv[cur ^ 1];
   const int32_t cnt = nctr->n_touched;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
@@ -450,6 +454,9 @@ __global__ void k_push_finalize(const int32_t* __restrict__ touched, const OffT*
       for (int i = 0; i < NW; i++) {
         nw[i] = N[(int64_t)w * NW + i];
         sw[i] = seen[(int64_t)w * NW + i];
+        // bits reached by a push step have no recorded parent index: the
+        // table pass searches their parents
+        pushed[(int64_t)w * NW + i] |= nw[i];
       }
       dg = deg_of(ro, w);
     } else {
@@ -483,21 +490,57 @@ __device__ __forceinline__ int flat_owner(const int32_t* __restrict__ off, int32
   return lo;
 }
 
+// Flat-window bookkeeping of a warp tile: lane j owns a run of d_j edges at
+// flat offsets [off_j, off_j + d_j).  For the 32 flat positions starting at
+// wb, returns the owner lane of this lane's position and the lane index of the
+// first position of that owner's run inside the window (-1 when the run began
+// in an earlier window).  Lanes past the end get owner -1.
+struct WinOwner {
+  int owner;
+  int head;
+};
+__device__ __forceinline__ WinOwner window_owner(int32_t off, int32_t d, int32_t wb, int32_t total,
+                                                 const int8_t* __restrict__ r2l) {
+  const int lane = threadIdx.x & 31;
+  const bool in_win = d > 0 && off >= wb && off < wb + 32;
+  const unsigned starts = __reduce_or_sync(0xffffffffu, in_win ? (1u << (off - wb)) : 0u);
+  const int before = __popc(__ballot_sync(0xffffffffu, d > 0 && off < wb));
+  WinOwner r{-1, -1};
+  if (wb + lane < total) {
+    const unsigned upto = starts & (0xffffffffu >> (31 - lane));  // starts at positions <= lane
+    const int cnt = before + __popc(upto);
+    r.owner = r2l[cnt - 1];
+    r.head = upto ? 31 - __clz(upto) : -1;
+  }
+  return r;
+}
+
 // ---------------------------------------------------------------------------
 // Pull, light vertices: one warp per tile of 32 consecutive vertices.  The
 // tile's wanted adjacency ranges are flattened and read edge-parallel
 // (coalesced colIndices), U x 32 edges per round with all loads issued before
-// any is consumed; F is gathered per edge and a segmented OR scan folds the
-// words per owner vertex into shared memory.
+// any is consumed; F is gathered per edge and a segmented OR scan (head flags
+// from one warp reduction per window) folds the words per owner vertex into
+// shared memory.  The same scan gives, for every newly reached bit, its first
+// frontier neighbour in ascending (= smallest-id) order: that neighbour's
+// position in the owner's adjacency is recorded as the bit's parent index in
+// p8 (one byte per source, vertex-major rows of B*NW bytes; vertices of degree
+// <= kP8MaxDegree only), so the table pass reads parents instead of searching
+// for them.
 template <typename W, int NW, typename OffT, int WARPS, int U>
 __global__ void __launch_bounds__(WARPS * 32) k_pull_tiles(int64_t n, const OffT* __restrict__ ro,
                                                            const int32_t* __restrict__ ci, const W* __restrict__ F,
                                                            W* seen, W* N, Planes<W, NW> pl, int level,
                                                            Masks<W, NW> active, int heavy, Lists nl, Ctrs* ctr,
-                                                           int cur) {
-  __shared__ int32_t s_off[WARPS][33];
-  __shared__ int64_t s_beg[WARPS][32];
+                                                           int cur, uint8_t* __restrict__ p8) {
+  constexpr int B = WB<W>::bits;
+  constexpr int ROW = B * NW;  // p8 bytes per vertex
+  __shared__ int64_t s_base[WARPS][32];  // colIndices index of flat position 0 of each lane's run
+  __shared__ int32_t s_off[WARPS][32];
+  __shared__ int8_t s_r2l[WARPS][32];    // rank among non-empty runs -> lane
   __shared__ W s_acc[WARPS][32][NW];
+  __shared__ W s_want[WARPS][32][NW];
+  __shared__ __align__(16) uint8_t s_pidx[WARPS][32][ROW];
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
   const int64_t ntiles = (n + 31) >> 5;
@@ -540,26 +583,26 @@ __global__ void __launch_bounds__(WARPS * 32) k_pull_tiles(int64_t n, const OffT
       if (lane >= s) inc += y;
     }
     const int32_t total = __shfl_sync(0xffffffffu, inc, 31);
-    s_off[wib][lane] = inc - d;
-    if (lane == 31) s_off[wib][32] = inc;
-    s_beg[wib][lane] = beg;
+    const int32_t off = inc - d;
+    const unsigned nz = __ballot_sync(0xffffffffu, d > 0);
+    if (d > 0) s_r2l[wib][__popc(nz & ((1u << lane) - 1u))] = (int8_t)lane;
+    s_off[wib][lane] = off;
+    s_base[wib][lane] = beg - off;
 #pragma unroll
-    for (int i = 0; i < NW; i++) s_acc[wib][lane][i] = 0;
+    for (int i = 0; i < NW; i++) {
+      s_acc[wib][lane][i] = 0;
+      s_want[wib][lane][i] = want[i];
+    }
     __syncwarp();
     e_scan += (unsigned long long)(lane == 0 ? total : 0);
     for (int32_t base = 0; base < total; base += 32 * U) {
-      int key[U];
+      WinOwner wo[U];
       int32_t col[U];
 #pragma unroll
       for (int u = 0; u < U; u++) {
-        const int32_t e = base + u * 32 + lane;
-        key[u] = 32 + lane;  // unique key for idle lanes
-        col[u] = -1;
-        if (e < total) {
-          const int o = flat_owner(s_off[wib], e);
-          key[u] = o;
-          col[u] = __ldg(&ci[s_beg[wib][o] + (e - s_off[wib][o])]);
-        }
+        const int32_t wb = base + u * 32;
+        wo[u] = window_owner(off, d, wb, total, s_r2l[wib]);
+        col[u] = wo[u].owner >= 0 ? __ldg(&ci[s_base[wib][wo[u].owner] + wb + lane]) : -1;
       }
       W f[U][NW];
 #pragma unroll
@@ -573,14 +616,36 @@ __global__ void __launch_bounds__(WARPS * 32) k_pull_tiles(int64_t n, const OffT
       }
 #pragma unroll
       for (int u = 0; u < U; u++) {
-        const int next_key = __shfl_down_sync(0xffffffffu, key[u], 1);
-        const bool tail = (lane == 31) || (next_key != key[u]);
+        const int o = wo[u].owner, h = wo[u].head;
+        const int32_t e = base + u * 32 + lane;
+        // tail = last position of its run in this window
+        const int o_next = __shfl_down_sync(0xffffffffu, o, 1);
+        const bool tail = o >= 0 && (lane == 31 || o_next != o);
+        const int32_t pos = o >= 0 ? e - s_off[wib][o] : 0;  // position in the owner's adjacency
 #pragma unroll
         for (int i = 0; i < NW; i++) {
-          const W r = seg_or_scan<W>(f[u][i], key[u]);
-          if (tail && key[u] < 32) s_acc[wib][key[u]][i] |= r;
+          W x = f[u][i];
+#pragma unroll
+          for (int s = 1; s < 32; s <<= 1) {
+            const W y = shfl_up<W>(x, s);
+            if (lane - s >= h && lane >= s) x |= y;
+          }
+          W ex = shfl_up<W>(x, 1);
+          if (!(lane >= 1 && lane - 1 >= h)) ex = 0;
+          if (o >= 0) {
+            W claim = f[u][i] & s_want[wib][o][i] & ~ex & ~s_acc[wib][o][i];
+            if (pos <= 255) {
+              while (claim) {
+                const int b = ffs0(claim);
+                s_pidx[wib][o][i * B + b] = (uint8_t)pos;
+                claim &= claim - 1;
+              }
+            }
+          }
+          __syncwarp();
+          if (tail) s_acc[wib][o][i] |= x;
+          __syncwarp();
         }
-        __syncwarp();
       }
     }
     W nw[NW];
@@ -593,6 +658,32 @@ __global__ void __launch_bounds__(WARPS * 32) k_pull_tiles(int64_t n, const OffT
     if (has) {
 #pragma unroll
       for (int i = 0; i < NW; i++) N[v * NW + i] = nw[i];
+      // merge the new parent indices into this vertex's p8 row, 16 bytes at a time
+      if (dg <= kP8MaxDegree) {
+        uint4* row = reinterpret_cast<uint4*>(p8 + v * ROW);
+        const uint4* srow = reinterpret_cast<const uint4*>(s_pidx[wib][lane]);
+#pragma unroll
+        for (int q = 0; q < ROW / 16; q++) {
+          const W word = nw[(q * 16) / B];
+          const unsigned bits = (unsigned)(word >> ((q * 16) % B)) & 0xffffu;
+          if (!bits) continue;
+          uint4 cur = bits == 0xffffu ? srow[q] : row[q];
+          if (bits != 0xffffu) {
+            const uint4 nv = srow[q];
+            unsigned* c = reinterpret_cast<unsigned*>(&cur);
+            const unsigned* nn = reinterpret_cast<const unsigned*>(&nv);
+#pragma unroll
+            for (int w4 = 0; w4 < 4; w4++) {
+              const unsigned nib = (bits >> (4 * w4)) & 0xfu;
+              // byte mask of the new sources in this 4-byte word
+              const unsigned bm = ((nib & 1u) ? 0xffu : 0u) | ((nib & 2u) ? 0xff00u : 0u) |
+                                  ((nib & 4u) ? 0xff0000u : 0u) | ((nib & 8u) ? 0xff000000u : 0u);
+              c[w4] = (c[w4] & ~bm) | (nn[w4] & bm);
+            }
+          }
+          row[q] = cur;
+        }
+      }
     }
     commit_new<W, NW, OffT>(has, (int32_t)v, nw, sw, dg, level, seen, pl, active, heavy, nl, nctr, acc);
     __syncwarp();
@@ -608,97 +699,232 @@ __global__ void __launch_bounds__(WARPS * 32) k_pull_tiles(int64_t n, const OffT
   }
 }
 
-// Block-wide OR reduce (all threads get the result).  s_red: W[32][NW].
-template <typename W, int NW>
-__device__ __forceinline__ void block_or(W (&x)[NW], W (*s_red)[NW]) {
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+// First occurrence inside a warp group of 32 consecutive edges (lane order =
+// edge order): returns the bits of f that no earlier lane and no earlier group
+// (`before`) has; *grp receives the OR of the whole group.
+template <typename W>
+__device__ __forceinline__ W first_bits(W f, W before, W* grp) {
+  const int lane = threadIdx.x & 31;
+  W x = f;
 #pragma unroll
-  for (int i = 0; i < NW; i++) x[i] = warp_or<W>(x[i]);
-  __syncthreads();
-  if (lane == 0)
-#pragma unroll
-    for (int i = 0; i < NW; i++) s_red[wid][i] = x[i];
-  __syncthreads();
-#pragma unroll
-  for (int i = 0; i < NW; i++) {
-    W r = 0;
-    for (int k = 0; k < nw; k++) r |= s_red[k][i];
-    x[i] = r;
+  for (int s = 1; s < 32; s <<= 1) {
+    const W y = shfl_up<W>(x, s);
+    if (lane >= s) x |= y;
   }
+  W ex = shfl_up<W>(x, 1);
+  if (lane == 0) ex = 0;
+  *grp = shfl_idx<W>(x, 31);
+  return f & ~ex & ~before;
 }
 
-// Pull, heavy vertices (degree > heavy): one block per vertex, early exit
-// once every wanted bit is found.
-template <typename W, int NW, typename OffT>
+// Pull, heavy vertices of degree <= hub: one warp per vertex, U x 32 edges per
+// round in ascending order with all loads issued up front, early exit once
+// every wanted bit is found.  The first frontier neighbour of each newly
+// reached bit is its min-id parent; it is stored in hpar[idx*ROW + bit] (ROW =
+// B*NW) for the table pass.  Hubs (degree > hub) are left to k_pull_hubs.
+template <typename W, int NW, typename OffT, int U>
 __global__ void k_pull_heavy(const int32_t* __restrict__ hlist, int32_t nh, const OffT* __restrict__ ro,
                              const int32_t* __restrict__ ci, const W* __restrict__ F, W* seen, W* N,
-                             Planes<W, NW> pl, int level, Masks<W, NW> active, int heavy, Lists nl, Ctrs* ctr,
-                             int cur) {
-  __shared__ W s_red[32][NW];
+                             Planes<W, NW> pl, int level, Masks<W, NW> active, int heavy, int hub, Lists nl,
+                             Ctrs* ctr, int cur, int32_t* __restrict__ hpar) {
+  constexpr int B = WB<W>::bits;
+  constexpr int ROW = B * NW;
+  const int lane = threadIdx.x & 31;
+  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
   LevelCtr* cctr = &ctr->lv[cur];
   LevelCtr* nctr = &ctr->lv[cur ^ 1];
+  W live[NW];
+#pragma unroll
+  for (int i = 0; i < NW; i++) live[i] = (W)cctr->live[i] & active.w[i];
   StatAcc<W, NW> sacc;
-  for (int64_t idx = blockIdx.x; idx < nh; idx += gridDim.x) {
+  unsigned long long scanned = 0, vcount = 0;
+  for (int64_t idx = warp; idx < nh; idx += nwarps) {
     const int32_t v = hlist[idx];
+    const int64_t beg = ro[v], end = ro[v + 1];
+    if (end - beg > hub) continue;  // warp-uniform
     W sw[NW], want[NW];
+    load_words<W, NW>(seen + (int64_t)v * NW, sw);
     bool any = false;
 #pragma unroll
     for (int i = 0; i < NW; i++) {
-      sw[i] = seen[(int64_t)v * NW + i];
-      want[i] = ((W)cctr->live[i] & active.w[i]) & ~sw[i];
+      want[i] = live[i] & ~sw[i];
       any = any || want[i] != 0;
     }
-    if (!any) continue;  // uniform across the block
-    const int64_t beg = ro[v], end = ro[v + 1];
+    if (!any) continue;  // warp-uniform
+    vcount++;
     W acc[NW];
 #pragma unroll
     for (int i = 0; i < NW; i++) acc[i] = 0;
-    int64_t scanned = 0;
-    for (int64_t base = beg; base < end; base += 4 * (int64_t)blockDim.x) {
-      int32_t col[4];
+    for (int64_t base = beg; base < end; base += 32 * U) {
+      int32_t col[U];
 #pragma unroll
-      for (int u = 0; u < 4; u++) {
-        const int64_t e = base + u * (int64_t)blockDim.x + threadIdx.x;
+      for (int u = 0; u < U; u++) {
+        const int64_t e = base + u * 32 + lane;
         col[u] = e < end ? __ldg(&ci[e]) : -1;
       }
+      W f[U][NW];
 #pragma unroll
-      for (int u = 0; u < 4; u++) {
+      for (int u = 0; u < U; u++) {
         if (col[u] >= 0) {
-          W f[NW];
-          load_words<W, NW>(F + (int64_t)col[u] * NW, f);
+          load_words<W, NW>(F + (int64_t)col[u] * NW, f[u]);
+        } else {
 #pragma unroll
-          for (int i = 0; i < NW; i++) acc[i] |= f[i];
+          for (int i = 0; i < NW; i++) f[u][i] = 0;
         }
       }
-      scanned += imin64(4 * (int64_t)blockDim.x, end - base);
-      block_or<W, NW>(acc, s_red);
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+#pragma unroll
+        for (int i = 0; i < NW; i++) {
+          W grp;
+          W claim = first_bits<W>(f[u][i], acc[i], &grp) & want[i];
+          if (hpar == nullptr) claim = 0;  // caller searches these parents later
+          while (claim) {
+            const int b = ffs0(claim);
+            hpar[idx * ROW + i * B + b] = col[u];
+            claim &= claim - 1;
+          }
+          acc[i] |= grp;
+        }
+      }
+      scanned += (unsigned long long)imin64(32 * U, end - base);
       bool done = true;
 #pragma unroll
       for (int i = 0; i < NW; i++) done = done && ((acc[i] & want[i]) == want[i]);
       if (done) break;
     }
-    if (threadIdx.x < 32) {
-      W nw[NW];
-      bool has = false;
+    W nw[NW];
+    bool has = false;
+#pragma unroll
+    for (int i = 0; i < NW; i++) {
+      nw[i] = lane == 0 ? (acc[i] & want[i]) : (W)0;
+      has = has || nw[i] != 0;
+    }
+    if (has) {
+#pragma unroll
+      for (int i = 0; i < NW; i++) N[(int64_t)v * NW + i] = nw[i];
+    }
+    commit_new<W, NW, OffT>(has, v, nw, sw, end - beg, level, seen, pl, active, heavy, nl, nctr, sacc);
+  }
+  flush_stats<W, NW>(sacc, nctr, &ctr->b);
+  if (lane == 0 && vcount) {
+    atomicAdd(&ctr->b.edges_scanned, scanned);
+    atomicAdd(&ctr->b.vertices_scanned, vcount);
+  }
+}
+
+// Pull, hubs (degree > hub): one warp per (heavy index, chunk) item, no early
+// exit; found bits go to N[v] with atomicOr and each bit's first neighbour in
+// the chunk to hpar with atomicMin (hpar rows start at INT32_MAX), so the
+// smallest id over all chunks wins.  k_pull_hub_commit then records them.
+template <typename W, int NW, typename OffT, int U>
+__global__ void k_pull_hubs(const int32_t* __restrict__ hlist, const int2* __restrict__ items, int64_t nitems,
+                            const OffT* __restrict__ ro, const int32_t* __restrict__ ci, const W* __restrict__ F,
+                            const W* __restrict__ seen, W* N, Masks<W, NW> active, Ctrs* ctr, int cur, int chunk,
+                            int32_t* __restrict__ hpar) {
+  constexpr int B = WB<W>::bits;
+  constexpr int ROW = B * NW;
+  const int lane = threadIdx.x & 31;
+  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  LevelCtr* cctr = &ctr->lv[cur];
+  W live[NW];
+#pragma unroll
+  for (int i = 0; i < NW; i++) live[i] = (W)cctr->live[i] & active.w[i];
+  unsigned long long scanned = 0;
+  for (int64_t it = warp; it < nitems; it += nwarps) {
+    const int2 item = items[it];
+    const int64_t idx = item.x;
+    const int32_t v = hlist[idx];
+    W sw[NW], want[NW];
+    load_words<W, NW>(seen + (int64_t)v * NW, sw);
+    bool any = false;
+#pragma unroll
+    for (int i = 0; i < NW; i++) {
+      want[i] = live[i] & ~sw[i];
+      any = any || want[i] != 0;
+    }
+    if (!any) continue;  // warp-uniform
+    const int64_t end = ro[v + 1];
+    const int64_t cb = (int64_t)ro[v] + (int64_t)item.y * chunk;
+    const int64_t ce = imin64(end, cb + chunk);
+    W acc[NW];
+#pragma unroll
+    for (int i = 0; i < NW; i++) acc[i] = 0;
+    for (int64_t base = cb; base < ce; base += 32 * U) {
+      int32_t col[U];
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        const int64_t e = base + u * 32 + lane;
+        col[u] = e < ce ? __ldg(&ci[e]) : -1;
+      }
+      W f[U][NW];
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        if (col[u] >= 0) {
+          load_words<W, NW>(F + (int64_t)col[u] * NW, f[u]);
+        } else {
+#pragma unroll
+          for (int i = 0; i < NW; i++) f[u][i] = 0;
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+#pragma unroll
+        for (int i = 0; i < NW; i++) {
+          W grp;
+          W claim = first_bits<W>(f[u][i], acc[i], &grp) & want[i];
+          while (claim) {
+            const int b = ffs0(claim);
+            atomicMin(&hpar[idx * ROW + i * B + b], col[u]);
+            claim &= claim - 1;
+          }
+          acc[i] |= grp;
+        }
+      }
+      scanned += (unsigned long long)imin64(32 * U, ce - base);
+    }
+    if (lane == 0) {
 #pragma unroll
       for (int i = 0; i < NW; i++) {
-        nw[i] = threadIdx.x == 0 ? (acc[i] & want[i]) : (W)0;
-        has = has || nw[i] != 0;
-      }
-      if (has) {
-#pragma unroll
-        for (int i = 0; i < NW; i++) N[(int64_t)v * NW + i] = nw[i];
-      }
-      W s0[NW];
-#pragma unroll
-      for (int i = 0; i < NW; i++) s0[i] = sw[i];
-      commit_new<W, NW, OffT>(has, v, nw, s0, end - beg, level, seen, pl, active, heavy, nl, nctr, sacc);
-      if (threadIdx.x == 0) {
-        atomicAdd(&ctr->b.edges_scanned, (unsigned long long)scanned);
-        atomicAdd(&ctr->b.vertices_scanned, 1ull);
+        const W found = acc[i] & want[i];
+        if (found) atomicOr(&N[(int64_t)v * NW + i], found);
       }
     }
-    __syncthreads();
+  }
+  if (lane == 0 && scanned) atomicAdd(&ctr->b.edges_scanned, scanned);
+}
+
+// Records the level's new bits of the hubs (after k_pull_hubs).
+template <typename W, int NW, typename OffT>
+__global__ void k_pull_hub_commit(const int32_t* __restrict__ hlist, int32_t nh, const OffT* __restrict__ ro,
+                                  W* seen, const W* N, Planes<W, NW> pl, int level, Masks<W, NW> active,
+                                  int heavy, int hub, Lists nl, Ctrs* ctr, int cur) {
+  LevelCtr* nctr = &ctr->lv[cur ^ 1];
+  StatAcc<W, NW> sacc;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < nh; base += stride) {
+    const int64_t idx = base + threadIdx.x;
+    int32_t v = 0;
+    int64_t dg = 0;
+    bool has = false;
+    W nw[NW], sw[NW];
+#pragma unroll
+    for (int i = 0; i < NW; i++) nw[i] = sw[i] = 0;
+    if (idx < nh) {
+      v = hlist[idx];
+      dg = deg_of(ro, v);
+      if (dg > hub) {
+#pragma unroll
+        for (int i = 0; i < NW; i++) {
+          nw[i] = N[(int64_t)v * NW + i];
+          sw[i] = seen[(int64_t)v * NW + i];
+          has = has || nw[i] != 0;
+        }
+      }
+    }
+    commit_new<W, NW, OffT>(has, v, nw, sw, dg, level, seen, pl, active, heavy, nl, nctr, sacc);
   }
   flush_stats<W, NW>(sacc, nctr, &ctr->b);
 }
@@ -722,33 +948,46 @@ __global__ void k_fill(T* p, int64_t count, T value) {
 // Table pass, word wi of the pass (sources word_base .. word_base+kbw-1; the
 // output pointers are already offset to row word_base).
 //
-// The vertex's own level and "needed" bits: need = reached and not the
-// source itself (level 0 is the only level with every plane bit clear).
+// The vertex's own level classes: root = the vertex is the source (level 0 is
+// the only level with every plane bit clear); lvl1 = level exactly 1, whose
+// only possible parent is the source itself.
 template <typename W, int NW>
 __device__ __forceinline__ void vertex_levels(const W* __restrict__ seen, const Planes<W, NW>& pl, int nplanes,
-                                              int64_t v, int wi, W& sv, W& p0, W& p1, W& root) {
+                                              int64_t v, int wi, W& sv, W& p0, W& p1, W& root, W& lvl1) {
   sv = seen[v * NW + wi];
   W pr[2];
   load_words<W, 2>(pl.p01 + ((v * NW + wi) << 1), pr);
   p0 = pr[0];
   p1 = pr[1];
-  W anyp = p0 | p1;
-  for (int j = 2; j < nplanes; j++) anyp |= pl.get(j, v, wi);
-  root = sv & ~anyp;
+  W hi = 0;
+  for (int j = 2; j < nplanes; j++) hi |= pl.get(j, v, wi);
+  root = sv & ~(p0 | p1 | hi);
+  lvl1 = sv & p0 & ~p1 & ~hi;
 }
 
-// One warp per 32-vertex tile.  Parent search: rounds over the flattened,
-// still-needed adjacency (ascending within each vertex), U x 32 edges per
-// round, loads issued up front; a segmented exclusive prefix OR in edge order
-// hands each needed bit to its first (= smallest-id) matching neighbour.
+// One warp per 32-vertex tile.  Parents of bits reached by a pull step come
+// from the recorded p8 index (ci[ro[v] + p8[v][s]]).  Bits reached by a push
+// step (and every bit of a vertex whose degree exceeds 256) are searched:
+// rounds over the flattened, still-needed adjacency (ascending within each
+// vertex), U x 32 edges per round, loads issued up front; a segmented
+// exclusive prefix OR in edge order hands each needed bit to its first
+// (= smallest-id) matching neighbour.
 template <typename W, int NW, typename OffT, int WARPS, int U>
 __global__ void __launch_bounds__(WARPS * 32) k_tables(int64_t n, const OffT* __restrict__ ro,
                                                        const int32_t* __restrict__ ci, const W* __restrict__ seen,
                                                        Planes<W, NW> pl, int nplanes, int wi, int kbw, int heavy,
                                                        int32_t* __restrict__ level_out,
-                                                       int32_t* __restrict__ parent_out, Ctrs* ctr) {
+                                                       int32_t* __restrict__ parent_out, Ctrs* ctr,
+                                                       const uint8_t* __restrict__ p8, const W* __restrict__ pushed,
+                                                       const int32_t* __restrict__ wsrc,
+                                                       const int32_t* __restrict__ hidx_of,
+                                                       const int32_t* __restrict__ hpar) {
   constexpr int B = WB<W>::bits;
+  constexpr int ROW = B * NW;
   __shared__ int32_t s_par[WARPS][B][32];
+  __shared__ int32_t s_src[B];
+  for (int s = threadIdx.x; s < B; s += blockDim.x) s_src[s] = s < kbw ? wsrc[s] : -1;
+  __syncthreads();
   __shared__ int32_t s_off[WARPS][33];
   __shared__ int64_t s_pos[WARPS][32];
   __shared__ W s_need[WARPS][32];
@@ -764,15 +1003,19 @@ __global__ void __launch_bounds__(WARPS * 32) k_tables(int64_t n, const OffT* __
   for (int64_t tile = warp; tile < ntiles; tile += nwarps) {
     const int64_t v = tile * 32 + lane;
     const bool valid = v < n;
-    W sv = 0, p0 = 0, p1 = 0, root = 0;
+    W sv = 0, p0 = 0, p1 = 0, root = 0, lvl1 = 0;
     int64_t beg = 0, dg = 0;
     if (valid) {
-      vertex_levels<W, NW>(seen, pl, nplanes, v, wi, sv, p0, p1, root);
+      vertex_levels<W, NW>(seen, pl, nplanes, v, wi, sv, p0, p1, root, lvl1);
       beg = ro[v];
       dg = (int64_t)ro[v + 1] - beg;
     }
     const bool is_heavy = dg > heavy;
-    const W need = (valid && !is_heavy) ? (sv & ~root) : (W)0;
+    const bool has_p8 = dg <= kP8MaxDegree;
+    W pw = 0;
+    if (valid && !is_heavy && has_p8) pw = pushed[v * NW + wi];
+    // bits whose parent must be searched (level-1 bits: the source itself)
+    const W need = (valid && !is_heavy) ? (sv & ~root & ~lvl1 & (has_p8 ? pw : ~(W)0)) : (W)0;
     s_need[wib][lane] = need;
     s_t0[wib][lane] = ~p0;         // bit-sliced (level - 1) mod 4, plane 0
     s_t1[wib][lane] = ~(p0 ^ p1);  // plane 1
@@ -859,24 +1102,47 @@ __global__ void __launch_bounds__(WARPS * 32) k_tables(int64_t n, const OffT* __
       __syncwarp();
     }
     // write rows: level and parent of sources 0..kbw-1 at vertices tile*32 + lane
-    if (valid && !is_heavy) {
+    if (valid) {
       constexpr int RP = 8;  // planes held in registers; deeper levels read on demand
       W plr[RP];
       plr[0] = p0;
       plr[1] = p1;
 #pragma unroll
       for (int j = 2; j < RP; j++) plr[j] = j < nplanes ? pl.get(j, v, wi) : (W)0;
-      for (int s = 0; s < kbw; s++) {
-        int32_t lv = -1, pr = -1;
-        if ((sv >> s) & 1) {
-          lv = 0;
+      // parent sources: recorded byte index (light, pulled), recorded id
+      // (heavy), searched (s_par), the source itself (levels 0 and 1)
+      const unsigned* prow32 =
+          (!is_heavy && has_p8) ? reinterpret_cast<const unsigned*>(p8 + v * ROW + wi * B) : nullptr;
+      const int32_t* hrow = is_heavy ? hpar + (int64_t)hidx_of[v] * ROW + wi * B : nullptr;
+      const W searched = need;
+      for (int s4 = 0; s4 < kbw; s4 += 4) {
+        const unsigned pw4 = prow32 ? prow32[s4 >> 2] : 0u;
 #pragma unroll
-          for (int j = 0; j < RP; j++) lv |= (int32_t)((plr[j] >> s) & 1) << j;
-          for (int j = RP; j < nplanes; j++) lv |= (int32_t)((pl.get(j, v, wi) >> s) & 1) << j;
-          pr = ((root >> s) & 1) ? (int32_t)v : s_par[wib][s][lane];
+        for (int j4 = 0; j4 < 4; j4++) {
+          const int s = s4 + j4;
+          if (s < kbw) {
+            int32_t lv = -1, pr = -1;
+            if ((sv >> s) & 1) {
+              lv = 0;
+#pragma unroll
+              for (int j = 0; j < RP; j++) lv |= (int32_t)((plr[j] >> s) & 1) << j;
+              for (int j = RP; j < nplanes; j++) lv |= (int32_t)((pl.get(j, v, wi) >> s) & 1) << j;
+              if ((root >> s) & 1) {
+                pr = (int32_t)v;
+              } else if ((lvl1 >> s) & 1) {
+                pr = s_src[s];
+              } else if (hrow) {
+                pr = hrow[s];
+              } else if ((searched >> s) & 1) {
+                pr = s_par[wib][s][lane];
+              } else {
+                pr = __ldg(&ci[beg + ((pw4 >> (8 * j4)) & 0xffu)]);
+              }
+            }
+            __stcs(&level_out[(int64_t)s * n + v], lv);
+            __stcs(&parent_out[(int64_t)s * n + v], pr);
+          }
         }
-        __stcs(&level_out[(int64_t)s * n + v], lv);
-        __stcs(&parent_out[(int64_t)s * n + v], pr);
       }
     }
     __syncwarp();
@@ -885,19 +1151,23 @@ __global__ void __launch_bounds__(WARPS * 32) k_tables(int64_t n, const OffT* __
   if (lane == 0 && pe) atomicAdd(&ctr->b.parent_edges, pe);
 }
 
-// Table pass for heavy vertices, scan step: the blocks walk a per-graph list
-// of (heavy index, chunk) items, each chunk `chunk` edges of one adjacency.
-// Each block hands every needed bit to the first matching neighbour of its
-// chunk (block-wide exclusive prefix OR in edge order) and folds it into
-// hpar[idx*B + bit] with atomicMin, so the smallest id over all chunks wins
-// regardless of schedule.  hpar must hold INT32_MAX beforehand.
+// Table pass for heavy vertices, scan step, for the bits a push step reached
+// at level >= 2 (the pull steps recorded every other parent in hpar): the
+// blocks walk a per-graph list of (heavy index, chunk) items, each chunk
+// `chunk` edges of one adjacency.  Each block hands every needed bit to the
+// first matching neighbour of its chunk (block-wide exclusive prefix OR in
+// edge order) and folds it into hpar[idx*ROW + wi*B + bit] with atomicMin, so
+// the smallest id over all chunks wins regardless of schedule.  Those hpar
+// slots still hold the INT32_MAX written at the start of the pass.
 template <typename W, int NW, typename OffT>
 __global__ void __launch_bounds__(256) k_tables_heavy_scan(const int32_t* __restrict__ hlist,
                                                            const int2* __restrict__ items, int64_t nitems,
                                                            const OffT* __restrict__ ro, const int32_t* __restrict__ ci,
                                                            const W* __restrict__ seen, Planes<W, NW> pl, int nplanes,
-                                                           int wi, int chunk, int32_t* hpar, Ctrs* ctr) {
+                                                           int wi, int chunk, int32_t* hpar, Ctrs* ctr,
+                                                           const W* __restrict__ pushed) {
   constexpr int B = WB<W>::bits;
+  constexpr int ROW = B * NW;
   __shared__ W s_wor[8];
   __shared__ W s_claimed;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -905,9 +1175,9 @@ __global__ void __launch_bounds__(256) k_tables_heavy_scan(const int32_t* __rest
     const int2 item = items[it];
     const int64_t idx = item.x;
     const int64_t v = hlist[idx];
-    W sv, p0, p1, root;
-    vertex_levels<W, NW>(seen, pl, nplanes, v, wi, sv, p0, p1, root);
-    const W need = sv & ~root;
+    W sv, p0, p1, root, lvl1;
+    vertex_levels<W, NW>(seen, pl, nplanes, v, wi, sv, p0, p1, root, lvl1);
+    const W need = sv & ~root & ~lvl1 & pushed[v * NW + wi];
     if (!need) continue;  // uniform
     const W t0 = ~p0, t1 = ~(p0 ^ p1);
     const int64_t beg = ro[v], end = ro[v + 1];
@@ -960,7 +1230,7 @@ __global__ void __launch_bounds__(256) k_tables_heavy_scan(const int32_t* __rest
           W mine = eq & ~excl;
           while (mine) {
             const int b = ffs0(mine);
-            atomicMin(&hpar[idx * B + b], col[u]);
+            atomicMin(&hpar[idx * ROW + wi * B + b], col[u]);
             mine &= mine - 1;
           }
           __syncthreads();
@@ -973,31 +1243,6 @@ __global__ void __launch_bounds__(256) k_tables_heavy_scan(const int32_t* __rest
       }
       if (threadIdx.x == 0) atomicAdd(&ctr->b.parent_edges, pe);
       __syncthreads();
-    }
-  }
-}
-
-// Table pass for heavy vertices, write step: block per heavy vertex, thread
-// per source of the word.
-template <typename W, int NW>
-__global__ void k_tables_heavy_write(const int32_t* __restrict__ hlist, int32_t nh, int64_t n,
-                                     const W* __restrict__ seen, Planes<W, NW> pl, int nplanes, int wi, int kbw,
-                                     const int32_t* __restrict__ hpar, int32_t* __restrict__ level_out,
-                                     int32_t* __restrict__ parent_out) {
-  constexpr int B = WB<W>::bits;
-  for (int64_t idx = blockIdx.x; idx < nh; idx += gridDim.x) {
-    const int64_t v = hlist[idx];
-    W sv, p0, p1, root;
-    vertex_levels<W, NW>(seen, pl, nplanes, v, wi, sv, p0, p1, root);
-    for (int s = threadIdx.x; s < kbw; s += blockDim.x) {
-      int32_t lv = -1, pr = -1;
-      if ((sv >> s) & 1) {
-        lv = 0;
-        for (int j = 0; j < nplanes; j++) lv |= (int32_t)((pl.get(j, v, wi) >> s) & 1) << j;
-        pr = ((root >> s) & 1) ? (int32_t)v : hpar[idx * B + s];
-      }
-      level_out[(int64_t)s * n + v] = lv;
-      parent_out[(int64_t)s * n + v] = pr;
     }
   }
 }

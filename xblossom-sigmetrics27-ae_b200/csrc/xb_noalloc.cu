@@ -10,7 +10,7 @@
 // memory it owns; this entry point takes only device pointers to those and
 // keeps its own working state in one fixed array compiled into the library.
 //
-// The array (g_noalloc_scratch, about 23 MiB) lives in every GPU that loads
+// The array (g_noalloc_scratch, about 32 MiB) lives in every GPU that loads
 // the library until the process exits.  It bounds the graph to
 // XB_NOALLOC_MAX_VERTICES vertices; larger graphs are rejected with
 // XB_ERR_CAPACITY.  Every call on a device shares the one array and leaves
@@ -47,7 +47,9 @@ constexpr size_t kSeenOff = 0;
 constexpr size_t kFOff = kSeenOff + kW;
 constexpr size_t kNOff = kFOff + kW;
 constexpr size_t kPlanesOff = kNOff + kW;
-constexpr size_t kListsOff = kPlanesOff + (size_t)kPlanes * kW;  // 6 int32 lists of kMaxN
+constexpr size_t kPushedOff = kPlanesOff + (size_t)kPlanes * kW;  // bits reached by push steps
+constexpr size_t kP8Off = kPushedOff + kW;                        // 64 parent-index bytes per vertex
+constexpr size_t kListsOff = kP8Off + 8 * kW;                     // 6 int32 lists of kMaxN
 constexpr size_t kCtrOff = kListsOff + 3 * kW;
 constexpr size_t kCtrWords = (sizeof(xbk::Ctrs) + 7) / 8;
 constexpr size_t kMiscOff = kCtrOff + kCtrWords;  // int32 heavy count, int32 error flag
@@ -148,6 +150,8 @@ extern "C" xb_status xb_traverse_noalloc(int64_t n, const int32_t* row_offsets, 
   W* N = scratch + kNOff;
   // planes 0-1 interleaved (2 words per vertex), planes 2.. separate
   const xbk::Planes<W, 1> pl{scratch + kPlanesOff, scratch + kPlanesOff + 2 * kW, (int64_t)kW};
+  W* pushed = scratch + kPushedOff;
+  uint8_t* p8 = (uint8_t*)(scratch + kP8Off);
   int32_t* lists = (int32_t*)(scratch + kListsOff);
   xbk::Lists fl{lists + 0 * kW, lists + 1 * kW};
   xbk::Lists nl{lists + 2 * kW, lists + 3 * kW};
@@ -199,6 +203,7 @@ extern "C" xb_status xb_traverse_noalloc(int64_t n, const int32_t* row_offsets, 
     NA_CUDA(cudaMemsetAsync(seen, 0, state_bytes, sm));
     NA_CUDA(cudaMemsetAsync(pl.p01, 0, 2 * plane_bytes, sm));
     NA_CUDA(cudaMemsetAsync(pl.ph, 0, plane_bytes, sm));
+    NA_CUDA(cudaMemsetAsync(pushed, 0, state_bytes, sm));
     int planes_zeroed = 3;
     std::memset(&h, 0, sizeof(h));
     h.b.m_unfinished = m32;
@@ -236,13 +241,15 @@ extern "C" xb_status xb_traverse_noalloc(int64_t n, const int32_t* row_offsets, 
         }
         xbk::k_push_finalize<W, 1, int32_t><<<(int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)sms * 8)),
                                               256, 0, sm>>>(touched, row_offsets, N, seen, pl, next, active, kHeavy,
-                                                            nl, ctr, cur);
+                                                            nl, ctr, cur, pushed);
       } else {
         xbk::k_pull_tiles<W, 1, int32_t, PULL_WARPS, U><<<pull_grid, PULL_WARPS * 32, 0, sm>>>(
-            n, row_offsets, col_indices, F, seen, N, pl, next, active, kHeavy, nl, ctr, cur);
+            n, row_offsets, col_indices, F, seen, N, pl, next, active, kHeavy, nl, ctr, cur, p8);
+        // one warp per heavy vertex; their parents are searched by the table pass
         if (n_heavy > 0)
-          xbk::k_pull_heavy<W, 1, int32_t><<<(int)std::min<int64_t>(n_heavy, (int64_t)sms * 4), 512, 0, sm>>>(
-              heavy_list, n_heavy, row_offsets, col_indices, F, seen, N, pl, next, active, kHeavy, nl, ctr, cur);
+          xbk::k_pull_heavy<W, 1, int32_t, 4><<<(int)std::min<int64_t>((n_heavy + 7) / 8, (int64_t)sms * 16), 256, 0,
+                                                sm>>>(heavy_list, n_heavy, row_offsets, col_indices, F, seen, N, pl,
+                                                      next, active, kHeavy, INT32_MAX, nl, ctr, cur, nullptr);
         NA_CUDA(cudaMemsetAsync(F, 0, state_bytes, sm));
       }
       NA_CUDA(cudaGetLastError());
@@ -254,7 +261,8 @@ extern "C" xb_status xb_traverse_noalloc(int64_t n, const int32_t* row_offsets, 
     max_levels = std::max(max_levels, lvl);
     // every vertex takes the edge-flat table path here (no heavy-vertex staging)
     xbk::k_tables<W, 1, int32_t, TAB_WARPS, U><<<tab_grid, TAB_WARPS * 32, 0, sm>>>(
-        n, row_offsets, col_indices, seen, pl, planes_zeroed, 0, kb, INT32_MAX, level + k0 * n, parent + k0 * n, ctr);
+        n, row_offsets, col_indices, seen, pl, planes_zeroed, 0, kb, INT32_MAX, level + k0 * n, parent + k0 * n, ctr,
+        p8, pushed, sources + k0, nullptr, nullptr);
     NA_CUDA(cudaGetLastError());
     NA_CUDA(cudaMemcpyAsync(&h, ctr, sizeof(h), cudaMemcpyDeviceToHost, sm));
     NA_CUDA(cudaStreamSynchronize(sm));

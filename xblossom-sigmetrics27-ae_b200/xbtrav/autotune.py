@@ -19,7 +19,7 @@ DEFAULT_SPACE = {
     "word_bits": [64, 32],
     "words": [1, 2, 4],
     "heavy_degree": [128, 256, 512, 1024],
-    "pull_alpha": [1.0, 4.0, 16.0],
+    "pull_alpha": [4.0, 32.0, 128.0],
 }
 
 
