@@ -114,7 +114,7 @@ WsLayout layout_for(int64_t n, int word_bytes, int nw) {
   L.p01 = o; o += 2 * sw;
   L.ph = o; o += sw * (L.nplanes_alloc - 2);
   L.pushed = o; o += sw;
-  L.p8 = o; o += align_up((size_t)n * nw * word_bytes * 8);  // one byte per (vertex, source)
+  L.p8 = o; o += align_up((size_t)n * nw * word_bytes * 8);  // 8 position planes per (vertex, word)
   L.touched = o; o += li;
   L.fl_light = o; o += li;
   L.fl_heavy = o; o += li;
@@ -288,7 +288,8 @@ xb_status run_plain(xb_ctx* c, xb_graph* g, const int32_t* d_sources, int32_t k,
   W* N = (W*)(base + L.N);
   const xbk::Planes<W, NW> pl{(W*)(base + L.p01), (W*)(base + L.ph), L.plane_stride};
   W* pushed = (W*)(base + L.pushed);
-  uint8_t* p8 = (uint8_t*)(base + L.p8);
+  W* ppos = (W*)(base + L.p8);
+  const size_t ppos_bytes = (size_t)n * NW * sizeof(W) * 8;
   int32_t* touched = (int32_t*)(base + L.touched);
   xbk::Lists fl{(int32_t*)(base + L.fl_light), (int32_t*)(base + L.fl_heavy)};
   xbk::Lists nl{(int32_t*)(base + L.nl_light), (int32_t*)(base + L.nl_heavy)};
@@ -324,6 +325,7 @@ xb_status run_plain(xb_ctx* c, xb_graph* g, const int32_t* d_sources, int32_t k,
     XB_CUDA(cudaMemsetAsync(pl.p01, 0, 2 * plane_bytes, c->stream));
     XB_CUDA(cudaMemsetAsync(pl.ph, 0, plane_bytes, c->stream));
     XB_CUDA(cudaMemsetAsync(pushed, 0, state_bytes, c->stream));
+    XB_CUDA(cudaMemsetAsync(ppos, 0, ppos_bytes, c->stream));
     if (g->n_heavy > 0) {  // parent slots of the heavy vertices (hub pulls fold in with atomicMin)
       const int64_t hcount = (int64_t)g->n_heavy * kHparRow;
       xbk::k_fill<int32_t><<<(int)std::min<int64_t>((hcount + 255) / 256, sms * 8), 256, 0, c->stream>>>(
@@ -387,7 +389,7 @@ xb_status run_plain(xb_ctx* c, xb_graph* g, const int32_t* d_sources, int32_t k,
         if (next_level >= 2) pushed_deep = true;
       } else {
         xbk::k_pull_tiles<W, NW, OffT, PULL_WARPS, PULL_U><<<pull_grid, PULL_WARPS * 32, 0, c->stream>>>(
-            n, ro, ci, F, seen, N, pl, next_level, active, heavy, nl, c->d_ctr, cur, p8);
+            n, ro, ci, F, seen, N, pl, next_level, active, heavy, nl, c->d_ctr, cur, ppos);
         XB_LAUNCH_CHECK("pull_tiles");
         launches++;
         if (g->n_heavy > 0) {
@@ -462,7 +464,7 @@ xb_status run_plain(xb_ctx* c, xb_graph* g, const int32_t* d_sources, int32_t k,
         launches++;
       }
       xbk::k_tables<W, NW, OffT, TAB_WARPS, TAB_U><<<tab_grid, TAB_WARPS * 32, 0, c->stream>>>(
-          n, ro, ci, seen, pl, planes_zeroed, wi, kbw, heavy, lv_out, pr_out, c->d_ctr, p8, pushed, wsrc,
+          n, ro, ci, seen, pl, planes_zeroed, wi, kbw, heavy, lv_out, pr_out, c->d_ctr, ppos, pushed, wsrc,
           g->d_hidx_of, g->d_hpar);
       XB_LAUNCH_CHECK("tables");
       launches++;

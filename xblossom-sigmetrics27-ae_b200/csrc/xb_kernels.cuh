@@ -523,24 +523,23 @@ __device__ __forceinline__ WinOwner window_owner(int32_t off, int32_t d, int32_t
 // from one warp reduction per window) folds the words per owner vertex into
 // shared memory.  The same scan gives, for every newly reached bit, its first
 // frontier neighbour in ascending (= smallest-id) order: that neighbour's
-// position in the owner's adjacency is recorded as the bit's parent index in
-// p8 (one byte per source, vertex-major rows of B*NW bytes; vertices of degree
-// <= kP8MaxDegree only), so the table pass reads parents instead of searching
-// for them.
+// position in the owner's adjacency (< 256 for vertices of degree <=
+// kP8MaxDegree) is recorded bit-sliced in ppos (8 words per vertex and word:
+// word k holds bit k of every source's position), so one claim of any number
+// of sources costs at most 8 ORs and the table pass reads parents instead of
+// searching for them.  ppos must be zero at the start of the pass.
 template <typename W, int NW, typename OffT, int WARPS, int U>
 __global__ void __launch_bounds__(WARPS * 32) k_pull_tiles(int64_t n, const OffT* __restrict__ ro,
                                                            const int32_t* __restrict__ ci, const W* __restrict__ F,
                                                            W* seen, W* N, Planes<W, NW> pl, int level,
                                                            Masks<W, NW> active, int heavy, Lists nl, Ctrs* ctr,
-                                                           int cur, uint8_t* __restrict__ p8) {
-  constexpr int B = WB<W>::bits;
-  constexpr int ROW = B * NW;  // p8 bytes per vertex
+                                                           int cur, W* __restrict__ ppos) {
   __shared__ int64_t s_base[WARPS][32];  // colIndices index of flat position 0 of each lane's run
   __shared__ int32_t s_off[WARPS][32];
   __shared__ int8_t s_r2l[WARPS][32];    // rank among non-empty runs -> lane
   __shared__ W s_acc[WARPS][32][NW];
   __shared__ W s_want[WARPS][32][NW];
-  __shared__ __align__(16) uint8_t s_pidx[WARPS][32][ROW];
+  __shared__ W s_pp[WARPS][32][NW][8];   // bit-sliced positions of this level's claims
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
   const int64_t ntiles = (n + 31) >> 5;
@@ -592,6 +591,8 @@ __global__ void __launch_bounds__(WARPS * 32) k_pull_tiles(int64_t n, const OffT
     for (int i = 0; i < NW; i++) {
       s_acc[wib][lane][i] = 0;
       s_want[wib][lane][i] = want[i];
+#pragma unroll
+      for (int k = 0; k < 8; k++) s_pp[wib][lane][i][k] = 0;
     }
     __syncwarp();
     e_scan += (unsigned long long)(lane == 0 ? total : 0);
@@ -633,13 +634,12 @@ __global__ void __launch_bounds__(WARPS * 32) k_pull_tiles(int64_t n, const OffT
           W ex = shfl_up<W>(x, 1);
           if (!(lane >= 1 && lane - 1 >= h)) ex = 0;
           if (o >= 0) {
-            W claim = f[u][i] & s_want[wib][o][i] & ~ex & ~s_acc[wib][o][i];
-            if (pos <= 255) {
-              while (claim) {
-                const int b = ffs0(claim);
-                s_pidx[wib][o][i * B + b] = (uint8_t)pos;
-                claim &= claim - 1;
-              }
+            const W claim = f[u][i] & s_want[wib][o][i] & ~ex & ~s_acc[wib][o][i];
+            if (claim && pos < kP8MaxDegree) {
+              // bit k of this position goes to plane k of every claimed source
+#pragma unroll
+              for (int k = 0; k < 8; k++)
+                if ((pos >> k) & 1) atomicOr(&s_pp[wib][o][i][k], claim);
             }
           }
           __syncwarp();
@@ -658,30 +658,17 @@ __global__ void __launch_bounds__(WARPS * 32) k_pull_tiles(int64_t n, const OffT
     if (has) {
 #pragma unroll
       for (int i = 0; i < NW; i++) N[v * NW + i] = nw[i];
-      // merge the new parent indices into this vertex's p8 row, 16 bytes at a time
+      // fold this level's claimed positions into the vertex's position planes
       if (dg <= kP8MaxDegree) {
-        uint4* row = reinterpret_cast<uint4*>(p8 + v * ROW);
-        const uint4* srow = reinterpret_cast<const uint4*>(s_pidx[wib][lane]);
 #pragma unroll
-        for (int q = 0; q < ROW / 16; q++) {
-          const W word = nw[(q * 16) / B];
-          const unsigned bits = (unsigned)(word >> ((q * 16) % B)) & 0xffffu;
-          if (!bits) continue;
-          uint4 cur = bits == 0xffffu ? srow[q] : row[q];
-          if (bits != 0xffffu) {
-            const uint4 nv = srow[q];
-            unsigned* c = reinterpret_cast<unsigned*>(&cur);
-            const unsigned* nn = reinterpret_cast<const unsigned*>(&nv);
+        for (int i = 0; i < NW; i++) {
+          if (!nw[i]) continue;
+          W* prow = ppos + (v * NW + i) * 8;
 #pragma unroll
-            for (int w4 = 0; w4 < 4; w4++) {
-              const unsigned nib = (bits >> (4 * w4)) & 0xfu;
-              // byte mask of the new sources in this 4-byte word
-              const unsigned bm = ((nib & 1u) ? 0xffu : 0u) | ((nib & 2u) ? 0xff00u : 0u) |
-                                  ((nib & 4u) ? 0xff0000u : 0u) | ((nib & 8u) ? 0xff000000u : 0u);
-              c[w4] = (c[w4] & ~bm) | (nn[w4] & bm);
-            }
+          for (int k = 0; k < 8; k++) {
+            const W add = s_pp[wib][lane][i][k];
+            if (add) prow[k] |= add;
           }
-          row[q] = cur;
         }
       }
     }
@@ -978,7 +965,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_tables(int64_t n, const OffT* __
                                                        Planes<W, NW> pl, int nplanes, int wi, int kbw, int heavy,
                                                        int32_t* __restrict__ level_out,
                                                        int32_t* __restrict__ parent_out, Ctrs* ctr,
-                                                       const uint8_t* __restrict__ p8, const W* __restrict__ pushed,
+                                                       const W* __restrict__ ppos, const W* __restrict__ pushed,
                                                        const int32_t* __restrict__ wsrc,
                                                        const int32_t* __restrict__ hidx_of,
                                                        const int32_t* __restrict__ hpar) {
@@ -1109,14 +1096,21 @@ __global__ void __launch_bounds__(WARPS * 32) k_tables(int64_t n, const OffT* __
       plr[1] = p1;
 #pragma unroll
       for (int j = 2; j < RP; j++) plr[j] = j < nplanes ? pl.get(j, v, wi) : (W)0;
-      // parent sources: recorded byte index (light, pulled), recorded id
-      // (heavy), searched (s_par), the source itself (levels 0 and 1)
-      const unsigned* prow32 =
-          (!is_heavy && has_p8) ? reinterpret_cast<const unsigned*>(p8 + v * ROW + wi * B) : nullptr;
+      // parent sources: recorded position (light, pulled; bit-sliced in 8
+      // planes), recorded id (heavy), searched (s_par), the source itself
+      // (levels 0 and 1)
+      W pp[8];
+      const bool use_pp = !is_heavy && has_p8;
+#pragma unroll
+      for (int k2 = 0; k2 < 8; k2 += 2) {
+        W t2[2] = {0, 0};
+        if (use_pp) load_words<W, 2>(ppos + (v * NW + wi) * 8 + k2, t2);
+        pp[k2] = t2[0];
+        pp[k2 + 1] = t2[1];
+      }
       const int32_t* hrow = is_heavy ? hpar + (int64_t)hidx_of[v] * ROW + wi * B : nullptr;
       const W searched = need;
       for (int s4 = 0; s4 < kbw; s4 += 4) {
-        const unsigned pw4 = prow32 ? prow32[s4 >> 2] : 0u;
 #pragma unroll
         for (int j4 = 0; j4 < 4; j4++) {
           const int s = s4 + j4;
@@ -1133,10 +1127,13 @@ __global__ void __launch_bounds__(WARPS * 32) k_tables(int64_t n, const OffT* __
                 pr = s_src[s];
               } else if (hrow) {
                 pr = hrow[s];
-              } else if ((searched >> s) & 1) {
+              } else if ((searched >> s) & 1 || !use_pp) {
                 pr = s_par[wib][s][lane];
               } else {
-                pr = __ldg(&ci[beg + ((pw4 >> (8 * j4)) & 0xffu)]);
+                int32_t idx = 0;
+#pragma unroll
+                for (int k = 0; k < 8; k++) idx |= (int32_t)((pp[k] >> s) & 1) << k;
+                pr = __ldg(&ci[beg + idx]);
               }
             }
             __stcs(&level_out[(int64_t)s * n + v], lv);

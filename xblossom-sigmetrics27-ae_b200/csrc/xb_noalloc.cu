@@ -151,7 +151,7 @@ extern "C" xb_status xb_traverse_noalloc(int64_t n, const int32_t* row_offsets, 
   // planes 0-1 interleaved (2 words per vertex), planes 2.. separate
   const xbk::Planes<W, 1> pl{scratch + kPlanesOff, scratch + kPlanesOff + 2 * kW, (int64_t)kW};
   W* pushed = scratch + kPushedOff;
-  uint8_t* p8 = (uint8_t*)(scratch + kP8Off);
+  W* ppos = scratch + kP8Off;  // 8 position planes per vertex
   int32_t* lists = (int32_t*)(scratch + kListsOff);
   xbk::Lists fl{lists + 0 * kW, lists + 1 * kW};
   xbk::Lists nl{lists + 2 * kW, lists + 3 * kW};
@@ -204,6 +204,7 @@ extern "C" xb_status xb_traverse_noalloc(int64_t n, const int32_t* row_offsets, 
     NA_CUDA(cudaMemsetAsync(pl.p01, 0, 2 * plane_bytes, sm));
     NA_CUDA(cudaMemsetAsync(pl.ph, 0, plane_bytes, sm));
     NA_CUDA(cudaMemsetAsync(pushed, 0, state_bytes, sm));
+    NA_CUDA(cudaMemsetAsync(ppos, 0, 8 * state_bytes, sm));
     int planes_zeroed = 3;
     std::memset(&h, 0, sizeof(h));
     h.b.m_unfinished = m32;
@@ -244,7 +245,7 @@ extern "C" xb_status xb_traverse_noalloc(int64_t n, const int32_t* row_offsets, 
                                                             nl, ctr, cur, pushed);
       } else {
         xbk::k_pull_tiles<W, 1, int32_t, PULL_WARPS, U><<<pull_grid, PULL_WARPS * 32, 0, sm>>>(
-            n, row_offsets, col_indices, F, seen, N, pl, next, active, kHeavy, nl, ctr, cur, p8);
+            n, row_offsets, col_indices, F, seen, N, pl, next, active, kHeavy, nl, ctr, cur, ppos);
         // one warp per heavy vertex; their parents are searched by the table pass
         if (n_heavy > 0)
           xbk::k_pull_heavy<W, 1, int32_t, 4><<<(int)std::min<int64_t>((n_heavy + 7) / 8, (int64_t)sms * 16), 256, 0,
@@ -262,7 +263,7 @@ extern "C" xb_status xb_traverse_noalloc(int64_t n, const int32_t* row_offsets, 
     // every vertex takes the edge-flat table path here (no heavy-vertex staging)
     xbk::k_tables<W, 1, int32_t, TAB_WARPS, U><<<tab_grid, TAB_WARPS * 32, 0, sm>>>(
         n, row_offsets, col_indices, seen, pl, planes_zeroed, 0, kb, INT32_MAX, level + k0 * n, parent + k0 * n, ctr,
-        p8, pushed, sources + k0, nullptr, nullptr);
+        ppos, pushed, sources + k0, nullptr, nullptr);
     NA_CUDA(cudaGetLastError());
     NA_CUDA(cudaMemcpyAsync(&h, ctr, sizeof(h), cudaMemcpyDeviceToHost, sm));
     NA_CUDA(cudaStreamSynchronize(sm));
