@@ -266,6 +266,239 @@ struct ClassTimer {
   }
 };
 
+// Algorithmic bytes of a pass's level steps: the row-offset pair of every
+// scanned vertex, colIndices + the gathered frontier words of every scanned
+// edge, and a three-word sweep (seen read, seen and next-frontier write) of
+// every swept vertex.
+template <typename W, int NW, typename OffT>
+int64_t level_bytes(const xbk::BatchCtr& b) {
+  const int64_t R = (int64_t)sizeof(OffT) * 2;
+  const int64_t wbytes = (int64_t)sizeof(W) * NW;
+  return R * (int64_t)b.vertices_scanned + (4 + wbytes) * (int64_t)b.edges_scanned +
+         3 * wbytes * (int64_t)b.vertices_swept;
+}
+
+// Algorithmic bytes of a pass's table pass: per vertex its row offsets, seen,
+// level planes and parent-position planes (per word), the colIndices entry of
+// every recorded parent, colIndices + gathered plane pair of every searched
+// edge, and the two written tables.
+template <typename W, int NW, typename OffT>
+int64_t table_bytes(const xbk::BatchCtr& b, int64_t n, int kb) {
+  const int64_t R = (int64_t)sizeof(OffT) * 2;
+  return (int64_t)NW * n * (R + (int64_t)sizeof(W) * (1 + b.nplanes + 8)) + 4 * (int64_t)b.reached +
+         (4 + 2 * (int64_t)sizeof(W)) * (int64_t)b.parent_edges + 8 * (int64_t)kb * n;
+}
+
+// Pointers and constants of one traversal pass (a workspace + counters).
+template <typename W, int NW, typename OffT>
+struct PassRes {
+  int64_t n = 0;
+  const OffT* ro = nullptr;
+  const int32_t* ci = nullptr;
+  W* seen = nullptr;
+  W* buf[2] = {nullptr, nullptr};  // frontier words; buf[cur] = F, buf[cur ^ 1] = N
+  xbk::Planes<W, NW> pl{};
+  W* pushed = nullptr;
+  W* ppos = nullptr;
+  int32_t* touched = nullptr;
+  xbk::Lists lists[2] = {};  // lists[cur] = current frontier, lists[cur ^ 1] = next
+  int32_t* stamp = nullptr;
+  xbk::Ctrs* ctr = nullptr;
+  int32_t* hpar = nullptr;
+  int heavy = 256;
+  size_t state_bytes = 0, plane_bytes = 0, ppos_bytes = 0;
+  int nplanes_alloc = 3;
+};
+
+template <typename W, int NW, typename OffT>
+PassRes<W, NW, OffT> pass_res(const xb_graph* g, void* ws, const WsLayout& L, xbk::Ctrs* ctr, int32_t* hpar,
+                              int heavy) {
+  PassRes<W, NW, OffT> p;
+  char* base = (char*)ws;
+  p.n = g->n;
+  p.ro = (const OffT*)g->d_ro;
+  p.ci = g->d_ci;
+  p.seen = (W*)(base + L.seen);
+  p.buf[0] = (W*)(base + L.F);
+  p.buf[1] = (W*)(base + L.N);
+  p.pl = xbk::Planes<W, NW>{(W*)(base + L.p01), (W*)(base + L.ph), L.plane_stride};
+  p.pushed = (W*)(base + L.pushed);
+  p.ppos = (W*)(base + L.p8);
+  p.touched = (int32_t*)(base + L.touched);
+  p.lists[0] = xbk::Lists{(int32_t*)(base + L.fl_light), (int32_t*)(base + L.fl_heavy)};
+  p.lists[1] = xbk::Lists{(int32_t*)(base + L.nl_light), (int32_t*)(base + L.nl_heavy)};
+  p.stamp = (int32_t*)(base + L.stamp);
+  p.ctr = ctr;
+  p.hpar = hpar;
+  p.heavy = heavy;
+  p.state_bytes = (size_t)g->n * NW * sizeof(W);
+  p.plane_bytes = (size_t)L.plane_stride * sizeof(W);
+  p.ppos_bytes = p.state_bytes * 8;
+  p.nplanes_alloc = L.nplanes_alloc;
+  return p;
+}
+
+template <typename W, int NW>
+xbk::Masks<W, NW> active_mask(int kb) {
+  constexpr int B = xbk::WB<W>::bits;
+  xbk::Masks<W, NW> a{};
+  for (int i = 0; i < NW; i++) {
+    const int lo = i * B, hi = std::min(kb, (i + 1) * B);
+    W m = 0;
+    for (int b = lo; b < hi; b++) m |= (W)1 << (b - lo);
+    a.w[i] = m;
+  }
+  return a;
+}
+
+// Launch shapes of the level-step kernels.
+struct StepShape {
+  int push_light_grid;   // 0: skip
+  dim3 push_heavy_grid;  // .y == 0: skip
+  int finalize_grid;
+  int pull_grid;
+  int heavy_grid;
+  int hub_grid;
+  int commit_grid;
+  int clear_grid;
+};
+
+template <typename W, int NW>
+constexpr int pull_warps() {
+  // the pull tile keeps 8 position words per lane and word in shared memory
+  return (xbk::WB<W>::bits * NW * 32 * 8 > 40 * 1024) ? 4 : 8;
+}
+
+// Pass start: clear the per-pass state, reset counters, seed the sources.
+template <typename W, int NW, typename OffT>
+xb_status emit_pass_init(const PassRes<W, NW, OffT>& p, const xb_graph* g, const int32_t* src, int kb,
+                         cudaStream_t s, int sms) {
+  XB_CUDA(cudaMemsetAsync(p.seen, 0, p.state_bytes, s));
+  XB_CUDA(cudaMemsetAsync(p.pl.p01, 0, 2 * p.plane_bytes, s));
+  XB_CUDA(cudaMemsetAsync(p.pl.ph, 0, p.plane_bytes, s));
+  XB_CUDA(cudaMemsetAsync(p.pushed, 0, p.state_bytes, s));
+  XB_CUDA(cudaMemsetAsync(p.ppos, 0, p.ppos_bytes, s));
+  if (g->n_heavy > 0) {  // parent slots of the heavy vertices (hub pulls fold in with atomicMin)
+    const int64_t hcount = (int64_t)g->n_heavy * kHparRow;
+    xbk::k_fill<int32_t><<<(int)std::min<int64_t>((hcount + 255) / 256, (int64_t)sms * 8), 256, 0, s>>>(p.hpar, hcount,
+                                                                                                   INT32_MAX);
+  }
+  xbk::k_pass_init<<<1, 1, 0, s>>>(p.ctr, (long long)g->m);
+  xbk::k_init_batch<W, NW, OffT><<<1, 256, 0, s>>>(src, kb, p.ro, p.buf[0], p.seen, p.pl, active_mask<W, NW>(kb),
+                                                   p.heavy, p.lists[0], p.ctr);
+  XB_LAUNCH_CHECK("pass init");
+  return XB_OK;
+}
+
+template <typename W, int NW, typename OffT>
+xb_status emit_push(const PassRes<W, NW, OffT>& p, const xb_graph* g, int cur, const StepShape& sh, int kb,
+                    cudaStream_t s, int64_t* launches) {
+  constexpr int PUSH_CHUNK = 2048;
+  W* F = p.buf[cur];
+  W* N = p.buf[cur ^ 1];
+  const xbk::Lists fl = p.lists[cur], nl = p.lists[cur ^ 1];
+  if (sh.push_light_grid > 0) {
+    xbk::k_push_light<W, NW, OffT><<<sh.push_light_grid, 256, 0, s>>>(fl.light, &p.ctr->lv[cur].n_light, p.ro, p.ci, F,
+                                                                      p.seen, N, p.stamp, p.touched, p.ctr, cur);
+    (*launches)++;
+  }
+  if (sh.push_heavy_grid.y > 0) {
+    xbk::k_push_heavy<W, NW, OffT><<<sh.push_heavy_grid, 256, 0, s>>>(fl.heavy, &p.ctr->lv[cur].n_heavy, p.ro, p.ci, F,
+                                                                      p.seen, N, p.stamp, p.touched, p.ctr, cur,
+                                                                      PUSH_CHUNK);
+    xbk::k_clear_list<W, NW><<<sh.clear_grid, 256, 0, s>>>(fl.heavy, &p.ctr->lv[cur].n_heavy, F);
+    *launches += 2;
+  }
+  xbk::k_push_finalize<W, NW, OffT><<<sh.finalize_grid, 256, 0, s>>>(p.touched, p.ro, N, p.seen, p.pl,
+                                                                     active_mask<W, NW>(kb), p.heavy, nl, p.ctr, cur,
+                                                                     p.pushed);
+  (*launches)++;
+  XB_LAUNCH_CHECK("push step");
+  return XB_OK;
+}
+
+template <typename W, int NW, typename OffT>
+xb_status emit_pull(const PassRes<W, NW, OffT>& p, const xb_graph* g, int cur, const StepShape& sh, int kb,
+                    cudaStream_t s, int64_t* launches) {
+  constexpr int PW = pull_warps<W, NW>();
+  W* F = p.buf[cur];
+  W* N = p.buf[cur ^ 1];
+  const xbk::Lists fl = p.lists[cur], nl = p.lists[cur ^ 1];
+  const xbk::Masks<W, NW> active = active_mask<W, NW>(kb);
+  xbk::k_pull_tiles<W, NW, OffT, PW, 4><<<sh.pull_grid, PW * 32, 0, s>>>(p.n, p.ro, p.ci, F, p.seen, N, p.pl, active,
+                                                                         p.heavy, nl, p.ctr, cur, p.ppos);
+  (*launches)++;
+  if (g->n_heavy > 0) {
+    xbk::k_pull_heavy<W, NW, OffT, 4><<<sh.heavy_grid, 256, 0, s>>>(g->d_heavy, g->n_heavy, p.ro, p.ci, F, p.seen, N,
+                                                                    p.pl, active, p.heavy, kHubDegree, nl, p.ctr, cur,
+                                                                    p.hpar);
+    (*launches)++;
+    if (g->n_hub_items > 0) {
+      xbk::k_pull_hubs<W, NW, OffT, 4><<<sh.hub_grid, 256, 0, s>>>(g->d_heavy, g->d_hub_items, g->n_hub_items, p.ro,
+                                                                   p.ci, F, p.seen, N, active, p.ctr, cur, kHubChunk,
+                                                                   p.hpar);
+      xbk::k_pull_hub_commit<W, NW, OffT><<<sh.commit_grid, 256, 0, s>>>(g->d_heavy, g->n_heavy, p.ro, p.seen, N, p.pl,
+                                                                        active, p.heavy, kHubDegree, nl, p.ctr, cur);
+      *launches += 2;
+    }
+  }
+  xbk::k_clear_frontier<W, NW><<<sh.clear_grid, 256, 0, s>>>(F, p.n, fl, p.ctr, cur);
+  (*launches)++;
+  XB_LAUNCH_CHECK("pull step");
+  return XB_OK;
+}
+
+// Table pass of one pass (all its words).  Row s of a word's tables starts at
+// lv_base + (wi*B + s) * row_stride.
+template <typename W, int NW, typename OffT>
+xb_status emit_tables(const PassRes<W, NW, OffT>& p, const xb_graph* g, const int32_t* src, int kb, int32_t* lv_base,
+                      int32_t* pr_base, bool search_heavy, cudaStream_t s, int sms, int64_t* launches) {
+  constexpr int B = xbk::WB<W>::bits;
+  constexpr int TAB_WARPS = (B == 64) ? 4 : 8;
+  const int64_t ntiles = (p.n + 31) / 32;
+  const int tab_grid = (int)std::max<int64_t>(1, std::min<int64_t>((ntiles + TAB_WARPS - 1) / TAB_WARPS, (int64_t)sms * 16));
+  for (int wi = 0; wi < NW; wi++) {
+    const int kbw = std::min(B, kb - wi * B);
+    if (kbw <= 0) break;
+    int32_t* lv_out = lv_base + (int64_t)wi * B * p.n;
+    int32_t* pr_out = pr_base + (int64_t)wi * B * p.n;
+    const int32_t* wsrc = src + wi * B;
+    if (g->n_heavy > 0 && search_heavy) {
+      // heavy vertices reached by a push step at level >= 2: search their parents
+      const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(g->n_hitems, (int64_t)sms * 8));
+      xbk::k_tables_heavy_scan<W, NW, OffT><<<grid, 256, 0, s>>>(g->d_heavy, g->d_hitems, g->n_hitems, p.ro, p.ci,
+                                                                 p.seen, p.pl, wi, kTableChunk, p.hpar, p.ctr,
+                                                                 p.pushed);
+      (*launches)++;
+    }
+    xbk::k_tables<W, NW, OffT, TAB_WARPS, 4><<<tab_grid, TAB_WARPS * 32, 0, s>>>(
+        p.n, p.ro, p.ci, p.seen, p.pl, wi, kbw, p.heavy, lv_out, pr_out, p.ctr, p.ppos, p.pushed, wsrc, g->d_hidx_of,
+        p.hpar);
+    (*launches)++;
+  }
+  XB_LAUNCH_CHECK("tables");
+  return XB_OK;
+}
+
+template <typename W, int NW, typename OffT>
+StepShape max_shape(const xb_graph* g, int sms) {
+  constexpr int PW = pull_warps<W, NW>();
+  StepShape sh{};
+  const int64_t n = g->n;
+  const int64_t ntiles = (n + 31) / 32;
+  sh.push_light_grid = sms * 16;
+  sh.push_heavy_grid = dim3((unsigned)std::max<int64_t>(1, std::min<int64_t>((g->max_deg + 2047) / 2048, 64)),
+                            (unsigned)std::max<int64_t>(1, std::min<int64_t>(g->n_heavy, 65535)));
+  if (g->n_heavy == 0) sh.push_heavy_grid.y = 0;
+  sh.finalize_grid = (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)sms * 8));
+  sh.pull_grid = (int)std::max<int64_t>(1, std::min<int64_t>((ntiles + PW - 1) / PW, (int64_t)sms * 8));
+  sh.heavy_grid = (int)std::max<int64_t>(1, std::min<int64_t>((g->n_heavy + 7) / 8, (int64_t)sms * 16));
+  sh.hub_grid = (int)std::max<int64_t>(1, std::min<int64_t>((g->n_hub_items + 7) / 8, (int64_t)sms * 16));
+  sh.commit_grid = (int)std::max<int64_t>(1, std::min<int64_t>((g->n_heavy + 255) / 256, (int64_t)sms * 4));
+  sh.clear_grid = sms * 8;
+  return sh;
+}
+
 template <typename W, int NW, typename OffT>
 xb_status run_plain(xb_ctx* c, xb_graph* g, const int32_t* d_sources, int32_t k, int32_t* level_out,
                     int32_t* parent_out, bool out_dev, xb_stats* st) {
@@ -279,204 +512,69 @@ xb_status run_plain(xb_ctx* c, xb_graph* g, const int32_t* d_sources, int32_t k,
   s = ensure_workspace(c, L, n, (int)sizeof(W), NW);
   if (s != XB_OK) return s;
   if (!out_dev) {
-    s = ensure_stage(c, sizeof(int32_t) * 2 * (size_t)B * (size_t)n);
+    s = ensure_stage(c, sizeof(int32_t) * 2 * (size_t)SPP * (size_t)n);
     if (s != XB_OK) return s;
   }
-  char* base = (char*)c->ws;
-  W* seen = (W*)(base + L.seen);
-  W* F = (W*)(base + L.F);
-  W* N = (W*)(base + L.N);
-  const xbk::Planes<W, NW> pl{(W*)(base + L.p01), (W*)(base + L.ph), L.plane_stride};
-  W* pushed = (W*)(base + L.pushed);
-  W* ppos = (W*)(base + L.p8);
-  const size_t ppos_bytes = (size_t)n * NW * sizeof(W) * 8;
-  int32_t* touched = (int32_t*)(base + L.touched);
-  xbk::Lists fl{(int32_t*)(base + L.fl_light), (int32_t*)(base + L.fl_heavy)};
-  xbk::Lists nl{(int32_t*)(base + L.nl_light), (int32_t*)(base + L.nl_heavy)};
-  int32_t* stamp = (int32_t*)(base + L.stamp);
-  const size_t state_bytes = (size_t)n * NW * sizeof(W);
-  const size_t plane_bytes = (size_t)L.plane_stride * sizeof(W);
-  const OffT* ro = (const OffT*)g->d_ro;
-  const int32_t* ci = g->d_ci;
+  PassRes<W, NW, OffT> p = pass_res<W, NW, OffT>(g, c->ws, L, c->d_ctr, g->d_hpar, heavy);
   const int sms = c->num_sms;
-  const float alpha = c->tuning.pull_alpha > 0 ? c->tuning.pull_alpha : 4.0f;
+  const float alpha = c->tuning.pull_alpha > 0 ? c->tuning.pull_alpha : 64.0f;
   ClassTimer timer{c, st, c->tuning.timing != 0};
-  const int64_t ntiles = (n + 31) / 32;
-  // the pull tile keeps a B*NW-byte parent-index row per lane in shared memory
-  constexpr int PULL_WARPS = (B * NW * 32 * 8 > 40 * 1024) ? 4 : 8, PULL_U = 4;
-  constexpr int TAB_WARPS = (B == 64) ? 4 : 8, TAB_U = 4;
-  constexpr int PUSH_CHUNK = 2048;
-  const int pull_grid = (int)std::max<int64_t>(1, std::min<int64_t>((ntiles + PULL_WARPS - 1) / PULL_WARPS, (int64_t)sms * 8));
-  const int tab_grid = (int)std::max<int64_t>(1, std::min<int64_t>((ntiles + TAB_WARPS - 1) / TAB_WARPS, (int64_t)sms * 16));
-  const int heavy_chunks = (int)std::max<int64_t>(1, std::min<int64_t>((g->max_deg + PUSH_CHUNK - 1) / PUSH_CHUNK, 64));
+  const StepShape mx = max_shape<W, NW, OffT>(g, sms);
   int max_levels = 0;
 
   for (int64_t k0 = 0; k0 < k; k0 += SPP) {
     const int kb = (int)std::min<int64_t>(SPP, k - k0);
-    xbk::Masks<W, NW> active{};
-    for (int i = 0; i < NW; i++) {
-      const int lo = i * B, hi = std::min(kb, (i + 1) * B);
-      W m = 0;
-      for (int b = lo; b < hi; b++) m |= (W)1 << (b - lo);
-      active.w[i] = m;
-    }
-    // reset per-pass state: seen, planes 0-2; counters
-    XB_CUDA(cudaMemsetAsync(seen, 0, state_bytes, c->stream));
-    XB_CUDA(cudaMemsetAsync(pl.p01, 0, 2 * plane_bytes, c->stream));
-    XB_CUDA(cudaMemsetAsync(pl.ph, 0, plane_bytes, c->stream));
-    XB_CUDA(cudaMemsetAsync(pushed, 0, state_bytes, c->stream));
-    XB_CUDA(cudaMemsetAsync(ppos, 0, ppos_bytes, c->stream));
-    if (g->n_heavy > 0) {  // parent slots of the heavy vertices (hub pulls fold in with atomicMin)
-      const int64_t hcount = (int64_t)g->n_heavy * kHparRow;
-      xbk::k_fill<int32_t><<<(int)std::min<int64_t>((hcount + 255) / 256, sms * 8), 256, 0, c->stream>>>(
-          g->d_hpar, hcount, INT32_MAX);
-      XB_LAUNCH_CHECK("hpar_fill");
-    }
-    int planes_zeroed = 3;
-    std::memset(c->h_ctr, 0, sizeof(xbk::Ctrs));
-    c->h_ctr->b.m_unfinished = g->m;
-    XB_CUDA(cudaMemcpyAsync(c->d_ctr, c->h_ctr, sizeof(xbk::Ctrs), cudaMemcpyHostToDevice, c->stream));
     timer.begin();
-    xbk::k_init_batch<W, NW, OffT><<<1, 256, 0, c->stream>>>(d_sources + k0, kb, ro, F, seen, pl, active, heavy, fl,
-                                                              c->d_ctr);
-    XB_LAUNCH_CHECK("init");
-    timer.end(2, 1);
-    int cur = 0, level = 0;
-    bool pushed_deep = false;  // a push step reached level >= 2 (its parents need a search)
+    s = emit_pass_init<W, NW, OffT>(p, g, d_sources + k0, kb, c->stream, sms);
+    if (s != XB_OK) return s;
+    timer.end(2, 3);
+    int cur = 0;
     for (;;) {
-      XB_CUDA(cudaMemcpyAsync(c->h_ctr, c->d_ctr, sizeof(xbk::Ctrs), cudaMemcpyDeviceToHost, c->stream));
+      // the device decides the step; the host reads the decision back
+      xbk::k_step_begin<<<1, 1, 0, c->stream>>>(p.ctr, cur, alpha, p.nplanes_alloc, 0, 0);
+      XB_LAUNCH_CHECK("step begin");
+      XB_CUDA(cudaMemcpyAsync(c->h_ctr, p.ctr, sizeof(xbk::Ctrs), cudaMemcpyDeviceToHost, c->stream));
       XB_CUDA(cudaStreamSynchronize(c->stream));
+      const xbk::BatchCtr bc = c->h_ctr->b;
+      if (bc.dir == 2) break;
       const xbk::LevelCtr lc = c->h_ctr->lv[cur];
-      const long long m_unf = c->h_ctr->b.m_unfinished;
-      const int64_t fcount = (int64_t)lc.n_light + lc.n_heavy;
-      if (fcount == 0) break;
-      const int next_level = level + 1;
-      while (planes_zeroed < L.nplanes_alloc && ((int64_t)1 << planes_zeroed) <= next_level) {
-        XB_CUDA(cudaMemsetAsync(pl.ph + (size_t)(planes_zeroed - 2) * L.plane_stride, 0, plane_bytes, c->stream));
-        planes_zeroed++;
-      }
-      XB_CUDA(cudaMemsetAsync(&c->d_ctr->lv[cur ^ 1], 0, sizeof(xbk::LevelCtr), c->stream));
-      const bool pull = (double)lc.edges * alpha > (double)m_unf;
       timer.begin();
-      int64_t launches = 0;
-      if (!pull) {
-        if (lc.n_light > 0) {
-          const int grid = (int)std::min<int64_t>(((int64_t)lc.n_light + 7) / 8, (int64_t)sms * 16);
-          xbk::k_push_light<W, NW, OffT><<<grid, 256, 0, c->stream>>>(fl.light, &c->d_ctr->lv[cur].n_light, ro, ci,
-                                                                      F, seen, N, stamp, c->epoch, touched,
-                                                                      c->d_ctr, cur);
-          XB_LAUNCH_CHECK("push_light");
-          launches++;
-        }
-        if (lc.n_heavy > 0) {
-          const dim3 grid(heavy_chunks, (unsigned)std::min<int64_t>(lc.n_heavy, 65535));
-          xbk::k_push_heavy<W, NW, OffT><<<grid, 256, 0, c->stream>>>(fl.heavy, &c->d_ctr->lv[cur].n_heavy, ro, ci,
-                                                                      F, seen, N, stamp, c->epoch, touched,
-                                                                      c->d_ctr, cur, PUSH_CHUNK);
-          XB_LAUNCH_CHECK("push_heavy");
-          xbk::k_clear_list<W, NW><<<(int)std::min<int64_t>((lc.n_heavy * NW + 255) / 256, sms * 8), 256, 0,
-                                     c->stream>>>(fl.heavy, &c->d_ctr->lv[cur].n_heavy, F);
-          XB_LAUNCH_CHECK("clear_heavy");
-          launches += 2;
-        }
-        // the touched count is on the device; size the grid for the worst case
-        const int fgrid = (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)sms * 8));
-        xbk::k_push_finalize<W, NW, OffT><<<fgrid, 256, 0, c->stream>>>(touched, ro, N, seen, pl, next_level, active,
-                                                                        heavy, nl, c->d_ctr, cur, pushed);
-        XB_LAUNCH_CHECK("push_finalize");
+      int64_t launches = 1;
+      if (bc.zero_plane >= 3) {
+        xbk::k_zero_plane<W><<<sms * 8, 256, 0, c->stream>>>(p.pl.ph, p.pl.stride, n * NW, p.ctr);
         launches++;
+      }
+      StepShape sh = mx;
+      if (bc.dir == 0) {
+        sh.push_light_grid = lc.n_light > 0 ? (int)std::min<int64_t>(((int64_t)lc.n_light + 7) / 8, (int64_t)sms * 16) : 0;
+        sh.push_heavy_grid.y = lc.n_heavy > 0 ? (unsigned)std::min<int64_t>(lc.n_heavy, 65535) : 0;
+        sh.clear_grid = (int)std::max<int64_t>(1, std::min<int64_t>((lc.n_heavy * NW + 255) / 256, (int64_t)sms * 8));
+        s = emit_push<W, NW, OffT>(p, g, cur, sh, kb, c->stream, &launches);
         if (st) st->push_levels++;
-        if (next_level >= 2) pushed_deep = true;
       } else {
-        xbk::k_pull_tiles<W, NW, OffT, PULL_WARPS, PULL_U><<<pull_grid, PULL_WARPS * 32, 0, c->stream>>>(
-            n, ro, ci, F, seen, N, pl, next_level, active, heavy, nl, c->d_ctr, cur, ppos);
-        XB_LAUNCH_CHECK("pull_tiles");
-        launches++;
-        if (g->n_heavy > 0) {
-          // one warp per heavy vertex of degree <= kHubDegree
-          const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((g->n_heavy + 7) / 8, (int64_t)sms * 16));
-          xbk::k_pull_heavy<W, NW, OffT, 4><<<grid, 256, 0, c->stream>>>(g->d_heavy, g->n_heavy, ro, ci, F, seen, N,
-                                                                         pl, next_level, active, heavy, kHubDegree, nl,
-                                                                         c->d_ctr, cur, g->d_hpar);
-          XB_LAUNCH_CHECK("pull_heavy");
-          launches++;
-          if (g->n_hub_items > 0) {
-            const int hgrid = (int)std::max<int64_t>(1, std::min<int64_t>((g->n_hub_items + 7) / 8, (int64_t)sms * 16));
-            xbk::k_pull_hubs<W, NW, OffT, 4><<<hgrid, 256, 0, c->stream>>>(g->d_heavy, g->d_hub_items, g->n_hub_items,
-                                                                           ro, ci, F, seen, N, active, c->d_ctr, cur,
-                                                                           kHubChunk, g->d_hpar);
-            xbk::k_pull_hub_commit<W, NW, OffT><<<(int)std::max<int64_t>(1, std::min<int64_t>((g->n_heavy + 255) / 256,
-                                                                                                (int64_t)sms * 4)),
-                                                  256, 0, c->stream>>>(g->d_heavy, g->n_heavy, ro, seen, N, pl,
-                                                                       next_level, active, heavy, kHubDegree, nl,
-                                                                       c->d_ctr, cur);
-            XB_LAUNCH_CHECK("pull_hubs");
-            launches += 2;
-          }
-        }
-        // zero the consumed frontier
-        if (fcount * 16 < n) {
-          if (lc.n_light > 0) {
-            xbk::k_clear_list<W, NW><<<(int)std::min<int64_t>((lc.n_light * NW + 255) / 256, sms * 8), 256, 0,
-                                       c->stream>>>(fl.light, &c->d_ctr->lv[cur].n_light, F);
-            launches++;
-          }
-          if (lc.n_heavy > 0) {
-            xbk::k_clear_list<W, NW><<<(int)std::min<int64_t>((lc.n_heavy * NW + 255) / 256, sms * 8), 256, 0,
-                                       c->stream>>>(fl.heavy, &c->d_ctr->lv[cur].n_heavy, F);
-            launches++;
-          }
-          XB_LAUNCH_CHECK("clear_list");
-        } else {
-          XB_CUDA(cudaMemsetAsync(F, 0, state_bytes, c->stream));
-        }
+        s = emit_pull<W, NW, OffT>(p, g, cur, sh, kb, c->stream, &launches);
         if (st) st->pull_levels++;
       }
+      if (s != XB_OK) return s;
       timer.end(0, launches);
-      c->epoch++;
-      if (c->epoch == INT32_MAX) {  // stamps wrap: clear them
-        XB_CUDA(cudaMemsetAsync(stamp, 0, sizeof(int32_t) * n, c->stream));
-        c->epoch = 1;
-      }
-      std::swap(F, N);
-      std::swap(fl, nl);
       cur ^= 1;
-      level = next_level;
     }
-    max_levels = std::max(max_levels, level);
-    // tables, one word at a time
-    for (int wi = 0; wi < NW; wi++) {
-      const int kbw = std::min(B, kb - wi * B);
-      if (kbw <= 0) break;
-      const int64_t s0 = k0 + (int64_t)wi * B;
-      int32_t* lv_out = out_dev ? level_out + s0 * n : c->d_stage;
-      int32_t* pr_out = out_dev ? parent_out + s0 * n : c->d_stage + (size_t)B * n;
-      timer.begin();
-      const int32_t* wsrc = d_sources + s0;
-      int64_t launches = 0;
-      if (g->n_heavy > 0 && pushed_deep) {
-        // heavy vertices reached by a push step at level >= 2: search their parents
-        const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(g->n_hitems, (int64_t)sms * 8));
-        xbk::k_tables_heavy_scan<W, NW, OffT><<<grid, 256, 0, c->stream>>>(g->d_heavy, g->d_hitems, g->n_hitems, ro,
-                                                                           ci, seen, pl, planes_zeroed, wi, kTableChunk,
-                                                                           g->d_hpar, c->d_ctr, pushed);
-        XB_LAUNCH_CHECK("tables_heavy_scan");
-        launches++;
-      }
-      xbk::k_tables<W, NW, OffT, TAB_WARPS, TAB_U><<<tab_grid, TAB_WARPS * 32, 0, c->stream>>>(
-          n, ro, ci, seen, pl, planes_zeroed, wi, kbw, heavy, lv_out, pr_out, c->d_ctr, ppos, pushed, wsrc,
-          g->d_hidx_of, g->d_hpar);
-      XB_LAUNCH_CHECK("tables");
-      launches++;
-      timer.end(1, launches);
-      if (!out_dev) {
-        XB_CUDA(cudaMemcpyAsync(level_out + s0 * n, lv_out, sizeof(int32_t) * (size_t)kbw * n, cudaMemcpyDeviceToHost,
-                                c->stream));
-        XB_CUDA(cudaMemcpyAsync(parent_out + s0 * n, pr_out, sizeof(int32_t) * (size_t)kbw * n,
-                                cudaMemcpyDeviceToHost, c->stream));
-      }
+    max_levels = std::max(max_levels, c->h_ctr->b.level);
+    timer.begin();
+    int64_t launches = 0;
+    int32_t* lv_base = out_dev ? level_out + k0 * n : c->d_stage;
+    int32_t* pr_base = out_dev ? parent_out + k0 * n : c->d_stage + (size_t)SPP * n;
+    s = emit_tables<W, NW, OffT>(p, g, d_sources + k0, kb, lv_base, pr_base, c->h_ctr->b.pushed_deep != 0, c->stream,
+                                 sms, &launches);
+    if (s != XB_OK) return s;
+    timer.end(1, launches);
+    if (!out_dev) {
+      XB_CUDA(cudaMemcpyAsync(level_out + k0 * n, lv_base, sizeof(int32_t) * (size_t)kb * n, cudaMemcpyDeviceToHost,
+                              c->stream));
+      XB_CUDA(cudaMemcpyAsync(parent_out + k0 * n, pr_base, sizeof(int32_t) * (size_t)kb * n, cudaMemcpyDeviceToHost,
+                              c->stream));
     }
-    XB_CUDA(cudaMemcpyAsync(c->h_ctr, c->d_ctr, sizeof(xbk::Ctrs), cudaMemcpyDeviceToHost, c->stream));
+    XB_CUDA(cudaMemcpyAsync(c->h_ctr, p.ctr, sizeof(xbk::Ctrs), cudaMemcpyDeviceToHost, c->stream));
     XB_CUDA(cudaStreamSynchronize(c->stream));
     if (st) {
       const xbk::BatchCtr& b = c->h_ctr->b;
@@ -487,16 +585,8 @@ xb_status run_plain(xb_ctx* c, xb_graph* g, const int32_t* d_sources, int32_t k,
       st->vertices_swept += (int64_t)b.vertices_swept;
       st->parent_edges_scanned += (int64_t)b.parent_edges;
       st->batches += 1;
-      // algorithmic bytes (level steps): offsets pair + colIndices + gathered
-      // words per scanned edge, a three-word sweep per swept vertex
-      const int64_t R = (int64_t)sizeof(OffT) * 2;
-      const int64_t wbytes = (int64_t)sizeof(W) * NW;
-      const int64_t lvl_bytes = R * (int64_t)b.vertices_scanned + (4 + wbytes) * (int64_t)b.edges_scanned +
-                                3 * wbytes * (int64_t)b.vertices_swept;
-      // table pass: per vertex offsets + seen + its planes (per word), per
-      // scanned edge colIndices + the gathered plane pair, and the tables
-      const int64_t tab_bytes = (int64_t)NW * n * (R + (int64_t)sizeof(W) * (1 + planes_zeroed)) +
-                                (4 + 2 * (int64_t)sizeof(W)) * (int64_t)b.parent_edges + 8 * (int64_t)kb * n;
+      const int64_t lvl_bytes = level_bytes<W, NW, OffT>(b);
+      const int64_t tab_bytes = table_bytes<W, NW, OffT>(b, n, kb);
       st->class_bytes[0] += lvl_bytes;
       st->class_bytes[1] += tab_bytes;
       st->algo_bytes += lvl_bytes + tab_bytes;
@@ -537,6 +627,7 @@ xb_status xb_ctx_create(int32_t device, xb_ctx** out) {
   XB_CUDA(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device));
   XB_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
   XB_CUDA(cudaMalloc(&c->d_ctr, sizeof(xbk::Ctrs)));
+  XB_CUDA(cudaMemset(c->d_ctr, 0, sizeof(xbk::Ctrs)));  // epoch 0: below every step's stamp
   XB_CUDA(cudaMallocHost(&c->h_ctr, sizeof(xbk::Ctrs)));
   XB_CUDA(cudaEventCreate(&c->ev0));
   XB_CUDA(cudaEventCreate(&c->ev1));

@@ -97,12 +97,20 @@ struct BatchCtr {
   unsigned long long parent_edges;
   long long m_unfinished;  // sum of degrees of vertices not reached by every source
   int32_t err;
-  int32_t pad;
+  int32_t level;        // level discovered by the current step (0 after init)
+  int32_t nplanes;      // level planes in use (all levels < 2^nplanes)
+  int32_t zero_plane;   // plane the current step must clear first (-1: none)
+  int32_t dir;          // current step: 0 push, 1 pull, 2 none (frontier empty)
+  int32_t pushed_deep;  // a push step reached level >= 2
+  int32_t push_levels;
+  int32_t pull_levels;
 };
 
 struct Ctrs {
   LevelCtr lv[2];
   BatchCtr b;
+  int32_t epoch;  // stamp of the current step; grows across passes and calls
+  int32_t pad;
 };
 
 template <typename W, int NW>
@@ -361,8 +369,9 @@ __device__ __forceinline__ bool push_edge(int32_t w, const W (&f)[NW], const W* 
 template <typename W, int NW, typename OffT>
 __global__ void k_push_light(const int32_t* __restrict__ list, const int32_t* __restrict__ count,
                              const OffT* __restrict__ ro, const int32_t* __restrict__ ci, W* F,
-                             const W* __restrict__ seen, W* N, int32_t* stamp, int32_t epoch,
-                             int32_t* touched, Ctrs* ctr, int cur) {
+                             const W* __restrict__ seen, W* N, int32_t* stamp, int32_t* touched, Ctrs* ctr,
+                             int cur) {
+  const int32_t epoch = ctr->epoch;
   const int lane = threadIdx.x & 31;
   const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -402,8 +411,9 @@ __global__ void k_push_light(const int32_t* __restrict__ list, const int32_t* __
 template <typename W, int NW, typename OffT>
 __global__ void k_push_heavy(const int32_t* __restrict__ list, const int32_t* __restrict__ count,
                              const OffT* __restrict__ ro, const int32_t* __restrict__ ci, const W* __restrict__ F,
-                             const W* __restrict__ seen, W* N, int32_t* stamp, int32_t epoch, int32_t* touched,
-                             Ctrs* ctr, int cur, int chunk) {
+                             const W* __restrict__ seen, W* N, int32_t* stamp, int32_t* touched, Ctrs* ctr,
+                             int cur, int chunk) {
+  const int32_t epoch = ctr->epoch;
   const int32_t cnt = *count;
   LevelCtr* nctr = &ctr->lv[cur ^ 1];
   for (int64_t idx = blockIdx.y; idx < cnt; idx += gridDim.y) {
@@ -436,8 +446,9 @@ __global__ void k_push_heavy(const int32_t* __restrict__ list, const int32_t* __
 // next frontier.
 template <typename W, int NW, typename OffT>
 __global__ void k_push_finalize(const int32_t* __restrict__ touched, const OffT* __restrict__ ro, const W* N,
-                                W* seen, Planes<W, NW> pl, int level, Masks<W, NW> active, int heavy, Lists nl,
-                                Ctrs* ctr, int cur, W* pushed) {
+                                W* seen, Planes<W, NW> pl, Masks<W, NW> active, int heavy, Lists nl, Ctrs* ctr,
+                                int cur, W* pushed) {
+  const int level = ctr->b.level;
   LevelCtr* nctr = &ctr->lv[cur ^ 1];
   const int32_t cnt = nctr->n_touched;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
@@ -531,9 +542,10 @@ __device__ __forceinline__ WinOwner window_owner(int32_t off, int32_t d, int32_t
 template <typename W, int NW, typename OffT, int WARPS, int U>
 __global__ void __launch_bounds__(WARPS * 32) k_pull_tiles(int64_t n, const OffT* __restrict__ ro,
                                                            const int32_t* __restrict__ ci, const W* __restrict__ F,
-                                                           W* seen, W* N, Planes<W, NW> pl, int level,
-                                                           Masks<W, NW> active, int heavy, Lists nl, Ctrs* ctr,
-                                                           int cur, W* __restrict__ ppos) {
+                                                           W* seen, W* N, Planes<W, NW> pl, Masks<W, NW> active,
+                                                           int heavy, Lists nl, Ctrs* ctr, int cur,
+                                                           W* __restrict__ ppos) {
+  const int level = ctr->b.level;
   __shared__ int64_t s_base[WARPS][32];  // colIndices index of flat position 0 of each lane's run
   __shared__ int32_t s_off[WARPS][32];
   __shared__ int8_t s_r2l[WARPS][32];    // rank among non-empty runs -> lane
@@ -712,8 +724,9 @@ __device__ __forceinline__ W first_bits(W f, W before, W* grp) {
 template <typename W, int NW, typename OffT, int U>
 __global__ void k_pull_heavy(const int32_t* __restrict__ hlist, int32_t nh, const OffT* __restrict__ ro,
                              const int32_t* __restrict__ ci, const W* __restrict__ F, W* seen, W* N,
-                             Planes<W, NW> pl, int level, Masks<W, NW> active, int heavy, int hub, Lists nl,
-                             Ctrs* ctr, int cur, int32_t* __restrict__ hpar) {
+                             Planes<W, NW> pl, Masks<W, NW> active, int heavy, int hub, Lists nl, Ctrs* ctr,
+                             int cur, int32_t* __restrict__ hpar) {
+  const int level = ctr->b.level;
   constexpr int B = WB<W>::bits;
   constexpr int ROW = B * NW;
   const int lane = threadIdx.x & 31;
@@ -886,8 +899,9 @@ __global__ void k_pull_hubs(const int32_t* __restrict__ hlist, const int2* __res
 // Records the level's new bits of the hubs (after k_pull_hubs).
 template <typename W, int NW, typename OffT>
 __global__ void k_pull_hub_commit(const int32_t* __restrict__ hlist, int32_t nh, const OffT* __restrict__ ro,
-                                  W* seen, const W* N, Planes<W, NW> pl, int level, Masks<W, NW> active,
-                                  int heavy, int hub, Lists nl, Ctrs* ctr, int cur) {
+                                  W* seen, const W* N, Planes<W, NW> pl, Masks<W, NW> active, int heavy,
+                                  int hub, Lists nl, Ctrs* ctr, int cur) {
+  const int level = ctr->b.level;
   LevelCtr* nctr = &ctr->lv[cur ^ 1];
   StatAcc<W, NW> sacc;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
@@ -962,7 +976,7 @@ __device__ __forceinline__ void vertex_levels(const W* __restrict__ seen, const 
 template <typename W, int NW, typename OffT, int WARPS, int U>
 __global__ void __launch_bounds__(WARPS * 32) k_tables(int64_t n, const OffT* __restrict__ ro,
                                                        const int32_t* __restrict__ ci, const W* __restrict__ seen,
-                                                       Planes<W, NW> pl, int nplanes, int wi, int kbw, int heavy,
+                                                       Planes<W, NW> pl, int wi, int kbw, int heavy,
                                                        int32_t* __restrict__ level_out,
                                                        int32_t* __restrict__ parent_out, Ctrs* ctr,
                                                        const W* __restrict__ ppos, const W* __restrict__ pushed,
@@ -971,6 +985,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_tables(int64_t n, const OffT* __
                                                        const int32_t* __restrict__ hpar) {
   constexpr int B = WB<W>::bits;
   constexpr int ROW = B * NW;
+  const int nplanes = ctr->b.nplanes;
   __shared__ int32_t s_par[WARPS][B][32];
   __shared__ int32_t s_src[B];
   for (int s = threadIdx.x; s < B; s += blockDim.x) s_src[s] = s < kbw ? wsrc[s] : -1;
@@ -1160,11 +1175,13 @@ template <typename W, int NW, typename OffT>
 __global__ void __launch_bounds__(256) k_tables_heavy_scan(const int32_t* __restrict__ hlist,
                                                            const int2* __restrict__ items, int64_t nitems,
                                                            const OffT* __restrict__ ro, const int32_t* __restrict__ ci,
-                                                           const W* __restrict__ seen, Planes<W, NW> pl, int nplanes,
-                                                           int wi, int chunk, int32_t* hpar, Ctrs* ctr,
+                                                           const W* __restrict__ seen, Planes<W, NW> pl, int wi,
+                                                           int chunk, int32_t* hpar, Ctrs* ctr,
                                                            const W* __restrict__ pushed) {
   constexpr int B = WB<W>::bits;
   constexpr int ROW = B * NW;
+  if (!ctr->b.pushed_deep) return;  // no push step reached level >= 2: nothing to search
+  const int nplanes = ctr->b.nplanes;
   __shared__ W s_wor[8];
   __shared__ W s_claimed;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -1242,6 +1259,114 @@ __global__ void __launch_bounds__(256) k_tables_heavy_scan(const int32_t* __rest
       __syncthreads();
     }
   }
+}
+
+// ---------------------------------------------------------------------------
+// Level-loop control.  The same single-thread kernels drive the host loop of
+// xb_traverse (which reads the decision back) and the device loop of
+// xb_traverse_batched (which feeds it to conditional nodes of a CUDA graph).
+
+// Resets the counters of a pass; the unfinished-edge estimate starts at m.
+static __global__ void k_pass_init(Ctrs* ctr, long long m) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  LevelCtr z{};
+  ctr->lv[0] = z;
+  ctr->lv[1] = z;
+  BatchCtr b{};
+  b.m_unfinished = m;
+  b.nplanes = 3;  // planes 0-2 are cleared with the pass
+  b.zero_plane = -1;
+  ctr->b = b;
+}
+
+// Decides the next step from the current frontier's counters lv[cur]:
+// dir = 0 push, 1 pull (frontier edges * alpha > unfinished edges), 2 done.
+// Advances the level, picks the level plane to clear, bumps the stamp epoch
+// and zeroes the next frontier's counters.
+static __global__ void k_step_begin(Ctrs* ctr, int cur, float alpha, int nplanes_alloc, int graph_mode,
+                                    cudaGraphConditionalHandle hswitch) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  BatchCtr& b = ctr->b;
+  const LevelCtr& lc = ctr->lv[cur];
+  int dir = 2;
+  if (b.dir != 2 && b.err == 0 && (long long)lc.n_light + lc.n_heavy > 0) {
+    dir = ((double)lc.edges * (double)alpha > (double)b.m_unfinished) ? 1 : 0;
+    b.level += 1;
+    b.zero_plane = -1;
+    if (b.nplanes < nplanes_alloc && (1 << b.nplanes) <= b.level) {
+      b.zero_plane = b.nplanes;
+      b.nplanes += 1;
+    }
+    if (dir == 0) {
+      b.push_levels += 1;
+      if (b.level >= 2) b.pushed_deep = 1;
+    } else {
+      b.pull_levels += 1;
+    }
+    ctr->epoch += 1;
+    LevelCtr z{};
+    ctr->lv[cur ^ 1] = z;
+  }
+  b.dir = dir;
+  if (graph_mode) cudaGraphSetConditional(hswitch, (unsigned)dir);
+}
+
+// Clears the level plane k_step_begin picked (planes >= 3 live in ph).
+template <typename W>
+__global__ void k_zero_plane(W* ph, int64_t stride, int64_t words, const Ctrs* ctr) {
+  const int zp = ctr->b.zero_plane;
+  if (zp < 3) return;
+  W* p = ph + (int64_t)(zp - 2) * stride;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < words; i += (int64_t)gridDim.x * blockDim.x)
+    p[i] = 0;
+}
+
+// Zeroes the consumed frontier after a pull step: the listed vertices when
+// the frontier is small, the whole array otherwise.
+template <typename W, int NW>
+__global__ void k_clear_frontier(W* F, int64_t n, Lists fl, const Ctrs* ctr, int cur) {
+  const int32_t nlight = ctr->lv[cur].n_light, nheavy = ctr->lv[cur].n_heavy;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (((int64_t)nlight + nheavy) * 16 < n) {
+    for (int64_t i = tid; i < ((int64_t)nlight + nheavy) * NW; i += stride) {
+      const int64_t j = i / NW;
+      const int32_t v = j < nlight ? fl.light[j] : fl.heavy[j - nlight];
+      F[(int64_t)v * NW + (i % NW)] = 0;
+    }
+  } else {
+    for (int64_t i = tid; i < n * NW; i += stride) F[i] = 0;
+  }
+}
+
+// After the second step of a loop body: keep looping while the traversal has
+// a frontier.
+static __global__ void k_loop_end(const Ctrs* ctr, int cur_next, cudaGraphConditionalHandle hwhile) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const bool more = ctr->b.dir != 2 && ctr->b.err == 0 &&
+                    (long long)ctr->lv[cur_next].n_light + ctr->lv[cur_next].n_heavy > 0;
+  cudaGraphSetConditional(hwhile, more ? 1u : 0u);
+}
+
+// Per-call totals over passes (device).
+struct PassSum {
+  unsigned long long edges_traversed, reached, edges_scanned, vertices_scanned, vertices_swept, parent_edges;
+  int32_t max_level, push_levels, pull_levels, passes;
+};
+
+static __global__ void k_pass_accum(const Ctrs* ctr, PassSum* sum) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const BatchCtr& b = ctr->b;
+  sum->edges_traversed += b.edges_traversed;
+  sum->reached += b.reached;
+  sum->edges_scanned += b.edges_scanned;
+  sum->vertices_scanned += b.vertices_scanned;
+  sum->vertices_swept += b.vertices_swept;
+  sum->parent_edges += b.parent_edges;
+  if (b.level > sum->max_level) sum->max_level = b.level;  // levels with a non-empty frontier
+  sum->push_levels += b.push_levels;
+  sum->pull_levels += b.pull_levels;
+  sum->passes += 1;
 }
 
 }  // namespace xbk

@@ -205,65 +205,57 @@ extern "C" xb_status xb_traverse_noalloc(int64_t n, const int32_t* row_offsets, 
     NA_CUDA(cudaMemsetAsync(pl.ph, 0, plane_bytes, sm));
     NA_CUDA(cudaMemsetAsync(pushed, 0, state_bytes, sm));
     NA_CUDA(cudaMemsetAsync(ppos, 0, 8 * state_bytes, sm));
-    int planes_zeroed = 3;
-    std::memset(&h, 0, sizeof(h));
-    h.b.m_unfinished = m32;
-    NA_CUDA(cudaMemcpyAsync(ctr, &h, sizeof(h), cudaMemcpyHostToDevice, sm));
+    xbk::k_pass_init<<<1, 1, 0, sm>>>(ctr, (long long)m32);
     xbk::k_init_batch<W, 1, int32_t><<<1, 256, 0, sm>>>(sources + k0, kb, row_offsets, F, seen, pl, active, kHeavy,
                                                          fl, ctr);
     NA_CUDA(cudaGetLastError());
-    int cur = 0, lvl = 0;
+    int cur = 0;
     for (;;) {
+      // the device picks the step (push / pull / done); the host reads it back
+      xbk::k_step_begin<<<1, 1, 0, sm>>>(ctr, cur, kAlpha, kPlanes, 0, 0);
       NA_CUDA(cudaMemcpyAsync(&h, ctr, sizeof(h), cudaMemcpyDeviceToHost, sm));
       NA_CUDA(cudaStreamSynchronize(sm));
+      if (h.b.dir == 2) break;
       const xbk::LevelCtr lc = h.lv[cur];
-      const int64_t fcount = (int64_t)lc.n_light + lc.n_heavy;
-      if (fcount == 0) break;
-      const int next = lvl + 1;
-      while (planes_zeroed < kPlanes && ((int64_t)1 << planes_zeroed) <= next) {
-        NA_CUDA(cudaMemsetAsync(pl.ph + (size_t)(planes_zeroed - 2) * kW, 0, plane_bytes, sm));
-        planes_zeroed++;
-      }
-      NA_CUDA(cudaMemsetAsync(&ctr->lv[cur ^ 1], 0, sizeof(xbk::LevelCtr), sm));
-      const bool pull = (double)lc.edges * kAlpha > (double)h.b.m_unfinished;
-      if (!pull) {
+      if (h.b.zero_plane >= 3)
+        NA_CUDA(cudaMemsetAsync(pl.ph + (size_t)(h.b.zero_plane - 2) * kW, 0, plane_bytes, sm));
+      if (h.b.dir == 0) {
         if (lc.n_light > 0)
           xbk::k_push_light<W, 1, int32_t><<<(int)std::min<int64_t>((lc.n_light + 7) / 8, (int64_t)sms * 16), 256, 0,
                                              sm>>>(fl.light, &ctr->lv[cur].n_light, row_offsets, col_indices, F, seen, N,
-                                                   nullptr, 0, touched, ctr, cur);
+                                                   nullptr, touched, ctr, cur);
         if (lc.n_heavy > 0) {
           const dim3 hgrid((unsigned)std::max<int64_t>(1, std::min<int64_t>((n + PUSH_CHUNK - 1) / PUSH_CHUNK, 64)),
                            (unsigned)std::min<int64_t>(lc.n_heavy, 65535));
           xbk::k_push_heavy<W, 1, int32_t><<<hgrid, 256, 0, sm>>>(fl.heavy, &ctr->lv[cur].n_heavy, row_offsets,
-                                                                  col_indices, F, seen, N, nullptr, 0, touched, ctr,
-                                                                  cur, PUSH_CHUNK);
+                                                                  col_indices, F, seen, N, nullptr, touched, ctr, cur,
+                                                                  PUSH_CHUNK);
           xbk::k_clear_list<W, 1><<<(int)std::min<int64_t>((lc.n_heavy + 255) / 256, (int64_t)sms * 8), 256, 0, sm>>>(
               fl.heavy, &ctr->lv[cur].n_heavy, F);
         }
         xbk::k_push_finalize<W, 1, int32_t><<<(int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)sms * 8)),
-                                              256, 0, sm>>>(touched, row_offsets, N, seen, pl, next, active, kHeavy,
-                                                            nl, ctr, cur, pushed);
+                                              256, 0, sm>>>(touched, row_offsets, N, seen, pl, active, kHeavy, nl, ctr,
+                                                            cur, pushed);
       } else {
         xbk::k_pull_tiles<W, 1, int32_t, PULL_WARPS, U><<<pull_grid, PULL_WARPS * 32, 0, sm>>>(
-            n, row_offsets, col_indices, F, seen, N, pl, next, active, kHeavy, nl, ctr, cur, ppos);
+            n, row_offsets, col_indices, F, seen, N, pl, active, kHeavy, nl, ctr, cur, ppos);
         // one warp per heavy vertex; their parents are searched by the table pass
         if (n_heavy > 0)
           xbk::k_pull_heavy<W, 1, int32_t, 4><<<(int)std::min<int64_t>((n_heavy + 7) / 8, (int64_t)sms * 16), 256, 0,
                                                 sm>>>(heavy_list, n_heavy, row_offsets, col_indices, F, seen, N, pl,
-                                                      next, active, kHeavy, INT32_MAX, nl, ctr, cur, nullptr);
+                                                      active, kHeavy, INT32_MAX, nl, ctr, cur, nullptr);
         NA_CUDA(cudaMemsetAsync(F, 0, state_bytes, sm));
       }
       NA_CUDA(cudaGetLastError());
       std::swap(F, N);
       std::swap(fl, nl);
       cur ^= 1;
-      lvl = next;
     }
-    max_levels = std::max(max_levels, lvl);
+    max_levels = std::max(max_levels, h.b.level);
     // every vertex takes the edge-flat table path here (no heavy-vertex staging)
     xbk::k_tables<W, 1, int32_t, TAB_WARPS, U><<<tab_grid, TAB_WARPS * 32, 0, sm>>>(
-        n, row_offsets, col_indices, seen, pl, planes_zeroed, 0, kb, INT32_MAX, level + k0 * n, parent + k0 * n, ctr,
-        ppos, pushed, sources + k0, nullptr, nullptr);
+        n, row_offsets, col_indices, seen, pl, 0, kb, INT32_MAX, level + k0 * n, parent + k0 * n, ctr, ppos, pushed,
+        sources + k0, nullptr, nullptr);
     NA_CUDA(cudaGetLastError());
     NA_CUDA(cudaMemcpyAsync(&h, ctr, sizeof(h), cudaMemcpyDeviceToHost, sm));
     NA_CUDA(cudaStreamSynchronize(sm));
@@ -274,6 +266,8 @@ extern "C" xb_status xb_traverse_noalloc(int64_t n, const int32_t* row_offsets, 
       st->vertices_scanned += (int64_t)h.b.vertices_scanned;
       st->vertices_swept += (int64_t)h.b.vertices_swept;
       st->parent_edges_scanned += (int64_t)h.b.parent_edges;
+      st->push_levels += h.b.push_levels;
+      st->pull_levels += h.b.pull_levels;
       st->batches += 1;
     }
   }
