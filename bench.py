@@ -2,12 +2,15 @@
 """Multi-source traversal benchmark (GTEPS on one B200 per rank).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl xbtrav|reference]
-                    [--workload rmat22_k1024|er335k_k256|rmat16_k64]
+                    [--workload rmat22_k1024|er335k_k256|rmat16_k64] [--path batched|plain]
 
 Workload (default): undirected R-MAT scale 22, edge factor 16, a/b/c/d =
 .57/.19/.19/.05 (symmetrised, cleaned, sorted int32 CSR), 1024 seeded sources
 drawn from vertices of non-zero degree; one step = traversal of all 1024
 sources producing the int32 level and parent tables (1024 x n each) in HBM.
+Both paths are timed on the same inputs in the same run: the batched path
+(xb_traverse_batched, one CUDA-graph launch per step; the headline `value`)
+and the plain per-call path (xb_traverse, `plain_gteps`).
 GTEPS = sum over sources of sum over reached vertices of deg(v) / time (the
 "Processed Edges" unit of the reference's BFS_Throughput).  Synthetic seeded
 data stands in for the reference's real datasets (not shipped).
@@ -47,6 +50,7 @@ WORKLOADS = {
     "rmat20_k64": dict(kind="rmat", scale=20, ef=16, k=64),
 }
 SEED = 0x5EED
+METRIC = "multi-source GTEPS at 1 B200, batched vs plain; p50/p99 query latency"
 
 
 def make_graph(w: dict):
@@ -190,7 +194,7 @@ def run_reference(args, w, name) -> None:
     what = ("Ligra BFS_F/edgeMap from the reference sources (oracle/_ref), parents only"
             if use_ligra else "C restatement (oracle/), levels only")
     line = {
-        "impl": "reference", "metric": "multi-source traversal throughput", "value": value, "unit": "GTEPS",
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "GTEPS",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1000.0 * sum(times) / len(times), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded generator)",
@@ -210,6 +214,9 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="xbtrav", choices=["xbtrav", "reference"])
     ap.add_argument("--workload", default="rmat22_k1024", choices=sorted(WORKLOADS))
+    ap.add_argument("--path", default="batched", choices=["batched", "plain"],
+                    help="path the headline value measures (both are timed)")
+    ap.add_argument("--chains", type=int, default=0, help="batched chains (0: tuned default)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
@@ -242,7 +249,8 @@ def main() -> None:
     info = csr.info()
     ro, ci = csr.arrays()
     ctx = xbtrav.Context(local)
-    ctx.set_tuning(timing=1)
+    if args.chains:
+        ctx.set_tuning(chains=args.chains)
     g = ctx.upload(csr)
     k = w["k"]
     sources = g.select_sources(SEED + 1 + 7919 * rank, k)
@@ -258,85 +266,124 @@ def main() -> None:
             dist.barrier()
         torch.cuda.synchronize(dev)
 
-    for _ in range(args.warmup):
-        ctx.traverse(g, src_dev, out="device", level=level, parent=parent)
-    clocks = ClockSampler(local)
-    barrier()
-    clocks.start()
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
-    agg = {"edges_traversed": 0, "class_ms": [0.0, 0.0, 0.0], "class_bytes": [0, 0, 0], "class_launches": [0, 0, 0],
-           "levels": 0, "push_levels": 0, "pull_levels": 0, "algo_bytes": 0}
-    with torch.cuda.stream(stream):
-        ev0.record(stream)
-    for _ in range(args.steps):
-        r = ctx.traverse(g, src_dev, out="device", level=level, parent=parent)
-        s = r.stats
-        agg["edges_traversed"] += s["edges_traversed"]
-        agg["algo_bytes"] += s["algo_bytes"]
-        for i in range(3):
-            agg["class_ms"][i] += s["class_ms"][i]
-            agg["class_bytes"][i] += s["class_bytes"][i]
-            agg["class_launches"][i] += s["class_launches"][i]
-        agg["levels"] = s["levels"]
-        agg["push_levels"] += s["push_levels"]
-        agg["pull_levels"] += s["pull_levels"]
-    with torch.cuda.stream(stream):
-        ev1.record(stream)
-    barrier()
-    clk = clocks.stop()
-    ms = ev0.elapsed_time(ev1)
-    edges_total = agg["edges_traversed"]
-    if dist is not None:
-        t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-        e = torch.tensor([edges_total], dtype=torch.float64, device=dev)
-        dist.all_reduce(e, op=dist.ReduceOp.SUM)
-        edges_total = float(e.item())
-    value = edges_total / (ms / 1e3) / 1e9
+        return float(t.item())
 
-    # roofline of the dominant kernel class (event-timed inside the timed region)
+    def sum_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        return float(t.item())
+
+    def plain_step():
+        return ctx.traverse(g, src_dev, out="device", level=level, parent=parent).stats
+
+    def batched_step():
+        return ctx.traverse_batched([(g, src_dev)], outputs=[(level, parent)])[1]
+
+    def timed(step, steps, sampler=None):
+        """steps of `step` between CUDA events on the engine's stream; returns (ms, summed stats)."""
+        barrier()
+        if sampler is not None:
+            sampler.start()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        agg = {"edges_traversed": 0, "class_ms": [0.0, 0.0, 0.0], "class_bytes": [0, 0, 0],
+               "class_launches": [0, 0, 0], "levels": 0, "push_levels": 0, "pull_levels": 0, "algo_bytes": 0}
+        with torch.cuda.stream(stream):
+            ev0.record(stream)
+        for _ in range(steps):
+            s = step()
+            agg["edges_traversed"] += s["edges_traversed"]
+            agg["algo_bytes"] += s["algo_bytes"]
+            for i in range(3):
+                agg["class_ms"][i] += s["class_ms"][i]
+                agg["class_bytes"][i] += s["class_bytes"][i]
+                agg["class_launches"][i] += s["class_launches"][i]
+            agg["levels"] = s["levels"]
+            agg["push_levels"] += s["push_levels"]
+            agg["pull_levels"] += s["pull_levels"]
+        with torch.cuda.stream(stream):
+            ev1.record(stream)
+        barrier()
+        clk = sampler.stop() if sampler is not None else None
+        return max_over_ranks(ev0.elapsed_time(ev1)), agg, clk
+
+    # plain per-call path (the drop-in): one word per launch sequence, host level loop
+    ctx.set_tuning(timing=0)
+    for _ in range(args.warmup):
+        plain_step()
+    plain_ms, plain_agg, _ = timed(plain_step, args.steps)
+    plain_gteps = sum_over_ranks(plain_agg["edges_traversed"]) / (plain_ms / 1e3) / 1e9
+
+    # per-kernel-class device times of the same kernels (one step, event-timed per class)
+    ctx.set_tuning(timing=1)
+    _, cls_agg, _ = timed(plain_step, 1)
+    ctx.set_tuning(timing=0)
+
+    # batched path: the whole step is one CUDA-graph launch
+    for _ in range(args.warmup):
+        batched_step()
+    clocks = ClockSampler(local)
+    b_ms, b_agg, clk = timed(batched_step, args.steps, clocks)
+    edges_total = sum_over_ranks(b_agg["edges_traversed"])
+    value = edges_total / (b_ms / 1e3) / 1e9
+    headline = value if args.path == "batched" else plain_gteps
+    ms = b_ms if args.path == "batched" else plain_ms
+
+    # roofline of the dominant kernel class (its kernels event-timed per class)
     peak, peak_kind = measured_peaks()
-    dom = 0 if agg["class_ms"][0] >= agg["class_ms"][1] else 1
+    dom = 0 if cls_agg["class_ms"][0] >= cls_agg["class_ms"][1] else 1
     dom_name = ["level steps (k_pull_tiles/k_push_*)", "table pass (k_tables)"][dom]
-    achieved = agg["class_bytes"][dom] / (agg["class_ms"][dom] / 1e3) / 1e9 if agg["class_ms"][dom] > 0 else None
+    achieved = (cls_agg["class_bytes"][dom] / (cls_agg["class_ms"][dom] / 1e3) / 1e9
+                if cls_agg["class_ms"][dom] > 0 else None)
     tr = traffic_from_profile(args.workload)
+    engine_gbs = b_agg["algo_bytes"] / (b_ms / 1e3) / 1e9
     roofline = {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
                 "traffic": tr.get(str(dom)) if isinstance(tr, dict) else None,
-                "class_ms_per_step": [x / args.steps for x in agg["class_ms"]],
-                "class_gbytes_per_step": [x / args.steps / 1e9 for x in agg["class_bytes"]]}
+                "class_ms_per_step": cls_agg["class_ms"],
+                "class_gbytes_per_step": [x / 1e9 for x in cls_agg["class_bytes"]],
+                "batched_engine_gbs": engine_gbs, "batched_engine_frac": engine_gbs / peak}
 
     # end to end through the C ABI with host buffers (pinned), copies in the timed region
+    def e2e_run(batched: bool, steps: int):
+        hl = torch.empty((k, g.n), dtype=torch.int32, pin_memory=True)
+        hp = torch.empty((k, g.n), dtype=torch.int32, pin_memory=True)
+        hs = torch.from_numpy(sources).pin_memory().numpy()
+        ln, pn = hl.numpy(), hp.numpy()
+
+        def one():
+            if batched:
+                return ctx.traverse_batched([(g, hs)], out="host", outputs=[(hl, hp)])[1]["edges_traversed"]
+            return ctx.traverse(g, hs, level=ln, parent=pn).stats["edges_traversed"]
+
+        one()
+        barrier()
+        t0 = time.perf_counter()
+        et = 0
+        for _ in range(steps):
+            et += one()
+        barrier()
+        dt = max_over_ranks(time.perf_counter() - t0)
+        et = sum_over_ranks(et)
+        del hl, hp
+        return et / dt / 1e9
+
     e2e = None
     if not args.no_e2e:
         try:
-            hl = torch.empty((k, g.n), dtype=torch.int32, pin_memory=True)
-            hp = torch.empty((k, g.n), dtype=torch.int32, pin_memory=True)
-            hs = torch.from_numpy(sources).pin_memory()
-            ln, pn = hl.numpy(), hp.numpy()
             e2e_steps = max(1, min(args.steps, 3))
-            ctx.traverse(g, hs.numpy(), level=ln, parent=pn)
-            barrier()
-            t0 = time.perf_counter()
-            et = 0
-            for _ in range(e2e_steps):
-                r = ctx.traverse(g, hs.numpy(), level=ln, parent=pn)
-                et += r.stats["edges_traversed"]
-            barrier()
-            dt = time.perf_counter() - t0
-            if dist is not None:
-                t = torch.tensor([dt, et], dtype=torch.float64, device=dev)
-                tm = t.clone()
-                dist.all_reduce(tm, op=dist.ReduceOp.MAX)
-                dist.all_reduce(t, op=dist.ReduceOp.SUM)
-                dt, et = float(tm[0].item()), float(t[1].item())
-            e2e = {"value": et / dt / 1e9, "unit": "GTEPS", "h2d_bytes_per_step": 4 * k,
-                   "d2h_bytes_per_step": 8 * k * g.n, "steps": e2e_steps,
-                   "note": "xb_traverse with host source list and host level/parent tables (pinned); "
-                           "graph resident"}
-            del hl, hp
+            e2e = {"value": e2e_run(args.path == "batched", e2e_steps), "unit": "GTEPS",
+                   "h2d_bytes_per_step": 4 * k, "d2h_bytes_per_step": 8 * k * g.n, "steps": e2e_steps,
+                   "note": ("xb_traverse_batched" if args.path == "batched" else "xb_traverse") +
+                           " with a host source list and page-locked host level/parent tables; graph resident"}
+            e2e["plain_value"] = e2e_run(False, 1) if args.path == "batched" else e2e["value"]
         except Exception as ex:  # noqa: BLE001
             e2e = {"value": None, "unit": "GTEPS", "error": str(ex)[:200]}
 
@@ -345,15 +392,20 @@ def main() -> None:
         cpu = cpu_baseline_port(ro, ci, sources)
 
     if rank == 0:
+        tun = ctx.tuning()
+        path_desc = (f"xb_traverse_batched (one CUDA-graph launch per step, device level loop, "
+                     f"{tun['chains']} chains, {tun['word_bits']} sources per word x {tun['words']})"
+                     if args.path == "batched" else "xb_traverse (host level loop, one word per launch sequence)")
+        agg = b_agg if args.path == "batched" else plain_agg
         line = {
-            "metric": "multi-source traversal throughput (plain per-call path)", "value": value, "unit": "GTEPS",
+            "metric": METRIC, "value": headline, "unit": "GTEPS",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
             "data": "synthetic (seeded R-MAT / uniform generator)",
-            "config": dict(workload_config(args.workload, w, info), parallelism=f"replicas{world}",
-                           path="xb_traverse (host level loop, 64 sources per word)"),
-            "plain_gteps": value,
-            "undirected_gteps": value / 2,
+            "config": dict(workload_config(args.workload, w, info), parallelism=f"replicas{world}", path=path_desc),
+            "batched_gteps": value, "plain_gteps": plain_gteps, "batched_over_plain": value / plain_gteps,
+            "plain_ms_per_step": plain_ms / args.steps,
+            "undirected_gteps": headline / 2,
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
             "gpu_launches": sum(agg["class_launches"]),
             "levels": agg["levels"], "push_levels_per_step": agg["push_levels"] / args.steps,

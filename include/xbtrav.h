@@ -89,6 +89,8 @@ typedef struct xb_tuning {
   float pull_alpha;        /* pull when frontier_edges*alpha > unfinished_edges */
   int32_t heavy_degree;    /* vertices above this degree get block-wide passes */
   int32_t timing;          /* 1 = record per-class CUDA events into xb_stats */
+  int32_t chains;          /* xb_traverse_batched: passes in flight at once, each with its
+                              own workspace (1..16; 0 = default 2) */
 } xb_tuning;
 
 /* ---- status ------------------------------------------------------------ */
@@ -157,6 +159,37 @@ xb_status xb_select_sources(const xb_graph* g, uint64_t seed, int32_t k, int32_t
 xb_status xb_traverse(xb_ctx* ctx, const xb_graph* g, const int32_t* sources, int32_t k,
                       int32_t mode, const int32_t* matching, int32_t* level, int32_t* parent,
                       int32_t* owner, uint32_t flags, xb_stats* stats);
+
+/* ---- batched traversal ------------------------------------------------- */
+/* One query of a batch: k sources on a resident graph, tables k*n int32 each
+ * (source-major), with the same meaning as xb_traverse's.  flags:
+ * XB_SOURCES_DEVICE (sources is a device pointer) and XB_OUT_DEVICE (level /
+ * parent are device pointers; otherwise they must be page-locked host memory,
+ * from cudaHostAlloc or cudaHostRegister, so the copies can run inside the
+ * launch). */
+typedef struct xb_batch_item {
+  const xb_graph* graph;
+  const int32_t* sources;
+  int32_t k;
+  uint32_t flags;
+  int32_t* level;
+  int32_t* parent;
+} xb_batch_item;
+
+/* Batched path (the reference has none: its engine runs one source set per
+ * host-driven loop, xblossom_gpu_engine_10.cu:72-185).  All queries of the
+ * batch -- on one graph or several, of any sizes -- run as ONE CUDA-graph
+ * launch: the sources of queries on the same graph are packed 64 (or 32) per
+ * word regardless of which query they come from, the words ("passes") are
+ * spread over tuning.chains concurrent chains, and each pass's level loop runs
+ * on the device (conditional WHILE / SWITCH nodes pick push or pull per level
+ * from the frontier counters; no host round trip per level).  The launch is
+ * cached: calls with the same queries shape (graphs, k per query, flags and,
+ * for host outputs, the output pointers) reuse it; sources and device output
+ * pointers may change freely between such calls.  Results are identical to
+ * xb_traverse's.  stats (may be NULL) sums over the whole batch. */
+xb_status xb_traverse_batched(xb_ctx* ctx, const xb_batch_item* items, int32_t nitems,
+                              xb_stats* stats);
 
 /* ---- traversal without device allocation -------------------------------- */
 /* No counterpart in the reference (whose engine allocates all its device

@@ -1,0 +1,691 @@
+// xb_batched.cu -- xb_traverse_batched: every query of a batch traversed by
+// one launch of a cached CUDA graph.
+//
+// Plan.  The sources of all queries on the same graph are concatenated and cut
+// into passes of B*NW sources (B = 32 or 64 per word), so small queries share
+// words; each source row of a pass carries its own output row pointers (the
+// table pass writes through a row table), which is what lets one word serve
+// several queries.  Passes are spread over C chains by longest-processing-time
+// first; a chain owns a workspace, counters and heavy-parent slots and runs its
+// passes back to back, while the chains run concurrently.
+//
+// Graph.  Per pass: the pass init (memsets, counters, sources) at top level,
+// then a WHILE node whose body holds two level steps (even and odd frontier
+// buffers); each step is k_step_begin (a one-thread kernel that decides push /
+// pull / done from the frontier counters and sets the SWITCH handle), the
+// level-plane clear, and a SWITCH node with a push body and a pull body whose
+// kernels take fixed grids and stride over whatever the frontier holds.
+// k_loop_end sets the WHILE handle.  After the loop come the table pass and
+// the pass's fold into the per-chain totals; for host outputs the table pass
+// writes one of two staging slots of the chain and a D2H copy of that slot
+// runs beside the chain's next pass.
+//
+// The reference drives every level from the host (four D2H scalars and a
+// device sync per frontier swap, xblossom_gpu_engine_10.cu:72-185 and
+// enode_queue.h:40-64); nothing here returns to the host until the batch ends.
+#include <map>
+#include <memory>
+
+#include "xb_engine_common.cuh"
+
+using xbi::fail;
+
+namespace xbe {
+
+constexpr int kMaxChains = 16;
+constexpr size_t kMaxCached = 8;
+
+struct Chain {
+  void* ws = nullptr;
+  size_t ws_bytes = 0;
+  xbk::Ctrs* ctr = nullptr;
+  int32_t* hpar = nullptr;
+  size_t hpar_count = 0;
+  int32_t* stage = nullptr;  // two slots of 2*SPP rows of n_max int32 (level rows, then parent rows)
+  size_t stage_bytes = 0;
+  cudaStream_t cs = nullptr, cps = nullptr;  // capture streams: compute, copies
+  cudaEvent_t ev_tab = nullptr, ev_free[2] = {nullptr, nullptr}, ev_join = nullptr, ev_join_cp = nullptr;
+};
+
+struct CachedGraph {
+  std::vector<uint64_t> key;
+  cudaGraphExec_t exec = nullptr;
+  std::vector<const xb_graph*> graphs;
+  uint64_t last_use = 0;
+};
+
+struct BatchState {
+  int device = 0;
+  Chain chains[kMaxChains];
+  xbk::PassSum* d_sums = nullptr;  // one per chain
+  xbk::PassSum* h_sums = nullptr;  // pinned
+  int32_t* d_src = nullptr;
+  int32_t* h_src = nullptr;  // pinned
+  int64_t src_cap = 0;
+  int32_t** d_rows = nullptr;
+  int32_t** h_rows = nullptr;  // pinned
+  int64_t rows_cap = 0;
+  cudaStream_t origin = nullptr, body[2] = {nullptr, nullptr};
+  cudaEvent_t ev_fork = nullptr;
+  uint64_t gen = 1;  // bumped whenever a buffer a cached graph points at is reallocated
+  uint64_t tick = 0;
+  std::vector<CachedGraph> cache;
+};
+
+namespace {
+
+void drop_cache(BatchState* b) {
+  for (auto& e : b->cache)
+    if (e.exec) cudaGraphExecDestroy(e.exec);
+  b->cache.clear();
+}
+
+xb_status make_state(xb_ctx* c) {
+  if (c->batch) return XB_OK;
+  std::unique_ptr<BatchState> b(new BatchState());
+  b->device = c->device;
+  XB_CUDA(cudaMalloc(&b->d_sums, sizeof(xbk::PassSum) * kMaxChains));
+  XB_CUDA(cudaMallocHost(&b->h_sums, sizeof(xbk::PassSum) * kMaxChains));
+  XB_CUDA(cudaStreamCreateWithFlags(&b->origin, cudaStreamNonBlocking));
+  for (auto& s : b->body) XB_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  XB_CUDA(cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming));
+  for (auto& ch : b->chains) {
+    XB_CUDA(cudaStreamCreateWithFlags(&ch.cs, cudaStreamNonBlocking));
+    XB_CUDA(cudaStreamCreateWithFlags(&ch.cps, cudaStreamNonBlocking));
+    for (cudaEvent_t* e : {&ch.ev_tab, &ch.ev_free[0], &ch.ev_free[1], &ch.ev_join, &ch.ev_join_cp})
+      XB_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+  }
+  c->batch = b.release();
+  return XB_OK;
+}
+
+// Grows a device buffer to at least `bytes` (contents not kept).
+template <typename T>
+xb_status grow(T** p, size_t* cap_bytes, size_t bytes, uint64_t* gen, const char* what) {
+  if (*cap_bytes >= bytes && *p) return XB_OK;
+  if (*p) cudaFree(*p);
+  *p = nullptr;
+  *cap_bytes = 0;
+  (*gen)++;
+  if (cudaMalloc((void**)p, std::max<size_t>(bytes, 256)) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(XB_ERR_OOM, std::string(what) + " allocation of " + std::to_string(bytes) + " bytes failed");
+  }
+  *cap_bytes = bytes;
+  return XB_OK;
+}
+
+// Where one source row of a pass goes.
+struct RowDst {
+  int32_t item;  // query index
+  int32_t idx;   // source index within the query
+};
+
+struct PassPlan {
+  const xb_graph* g = nullptr;
+  int kb = 0;
+  int64_t src_off = 0;  // into the batch's source buffer
+  std::vector<RowDst> rows;
+  bool host = false;  // some row goes to host memory (through a staging slot)
+  int chain = 0, slot = 0;
+  double cost = 0;
+};
+
+// Creates a conditional handle in the graph stream s is capturing into.
+xb_status make_handle(cudaStream_t s, unsigned dflt, unsigned flags, cudaGraphConditionalHandle* h) {
+  cudaStreamCaptureStatus cst = cudaStreamCaptureStatusNone;
+  cudaGraph_t g = nullptr;
+  XB_CUDA(cudaStreamGetCaptureInfo(s, &cst, nullptr, &g, nullptr, nullptr));
+  if (cst != cudaStreamCaptureStatusActive) return fail(XB_ERR_STATE, "stream is not capturing");
+  XB_CUDA(cudaGraphConditionalHandleCreate(h, g, dflt, flags));
+  return XB_OK;
+}
+
+// Adds a conditional node on handle h after the work captured so far on s and
+// makes it the stream's only dependency; returns its body graphs.
+xb_status add_conditional(cudaStream_t s, cudaGraphConditionalHandle h, cudaGraphConditionalNodeType type,
+                          unsigned size, cudaGraph_t* bodies) {
+  cudaStreamCaptureStatus cst = cudaStreamCaptureStatusNone;
+  cudaGraph_t g = nullptr;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t nd = 0;
+  XB_CUDA(cudaStreamGetCaptureInfo(s, &cst, nullptr, &g, &deps, &nd));
+  if (cst != cudaStreamCaptureStatusActive) return fail(XB_ERR_STATE, "stream is not capturing");
+  cudaGraphNodeParams np = {};
+  np.type = cudaGraphNodeTypeConditional;
+  np.conditional.handle = h;
+  np.conditional.type = type;
+  np.conditional.size = size;
+  cudaGraphNode_t node = nullptr;
+  XB_CUDA(cudaGraphAddNode(&node, g, deps, nd, &np));
+  for (unsigned i = 0; i < size; i++) bodies[i] = np.conditional.phGraph_out[i];
+  XB_CUDA(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
+  return XB_OK;
+}
+
+// Ends a capture into a body graph whatever happened inside it; keeps the
+// first error.
+xb_status end_body(cudaStream_t s, xb_status st) {
+  cudaGraph_t out = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(s, &out);
+  if (st != XB_OK) return st;
+  if (e != cudaSuccess) return fail(XB_ERR_CUDA, std::string("body capture: ") + cudaGetErrorString(e));
+  return XB_OK;
+}
+
+// One level step inside the WHILE body (captured on b0): decide, clear the
+// new level plane, then SWITCH into the push or the pull body (captured on b1).
+template <typename W, int NW, typename OffT>
+xb_status capture_step(BatchState* bs, const PassRes<W, NW, OffT>& p, const xb_graph* g, int cur, int kb,
+                       float alpha, const StepShape& sh, int sms) {
+  cudaStream_t b0 = bs->body[0], b1 = bs->body[1];
+  cudaGraphConditionalHandle hsw;
+  xb_status st = make_handle(b0, 2, cudaGraphCondAssignDefault, &hsw);
+  if (st != XB_OK) return st;
+  xbk::k_step_begin<<<1, 1, 0, b0>>>(p.ctr, cur, alpha, p.nplanes_alloc, 1, hsw);
+  xbk::k_zero_plane<W><<<(int)std::max<int64_t>(1, std::min<int64_t>((p.n * NW + 255) / 256, (int64_t)sms * 8)), 256,
+                         0, b0>>>(p.pl.ph, p.pl.stride, p.n * NW, p.ctr);
+  XB_LAUNCH_CHECK("step control");
+  cudaGraph_t br[2];
+  st = add_conditional(b0, hsw, cudaGraphCondTypeSwitch, 2, br);
+  if (st != XB_OK) return st;
+  int64_t launches = 0;
+  XB_CUDA(cudaStreamBeginCaptureToGraph(b1, br[0], nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+  st = end_body(b1, emit_push<W, NW, OffT>(p, g, cur, sh, kb, b1, &launches));
+  if (st != XB_OK) return st;
+  XB_CUDA(cudaStreamBeginCaptureToGraph(b1, br[1], nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+  return end_body(b1, emit_pull<W, NW, OffT>(p, g, cur, sh, kb, b1, &launches));
+}
+
+// The level loop of one pass, as a WHILE node on stream s: each iteration
+// takes the step on the even buffers, then on the odd ones.
+template <typename W, int NW, typename OffT>
+xb_status capture_level_loop(BatchState* bs, const PassRes<W, NW, OffT>& p, const xb_graph* g, int kb, float alpha,
+                             const StepShape& sh, cudaStream_t s, int sms) {
+  cudaGraphConditionalHandle hwhile;
+  xb_status st = make_handle(s, 1, cudaGraphCondAssignDefault, &hwhile);
+  if (st != XB_OK) return st;
+  cudaGraph_t wbody;
+  st = add_conditional(s, hwhile, cudaGraphCondTypeWhile, 1, &wbody);
+  if (st != XB_OK) return st;
+  cudaStream_t b0 = bs->body[0];
+  XB_CUDA(cudaStreamBeginCaptureToGraph(b0, wbody, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+  for (int cur = 0; cur < 2 && st == XB_OK; cur++) st = capture_step<W, NW, OffT>(bs, p, g, cur, kb, alpha, sh, sms);
+  if (st == XB_OK) {
+    xbk::k_loop_end<<<1, 1, 0, b0>>>(p.ctr, 0, hwhile);
+    if (cudaGetLastError() != cudaSuccess) st = fail(XB_ERR_CUDA, "launch k_loop_end failed");
+  }
+  return end_body(b0, st);
+}
+
+// One pass on its chain's compute stream (and copy stream for host rows).
+template <typename W, int NW, typename OffT>
+xb_status capture_pass(xb_ctx* c, BatchState* bs, const PassPlan& pp, int64_t rows_off, int64_t n_stage,
+                       const std::vector<xb_batch_item>& items, bool slot_used[kMaxChains][2]) {
+  constexpr int B = xbk::WB<W>::bits;
+  constexpr int SPP = B * NW;
+  Chain& ch = bs->chains[pp.chain];
+  const xb_graph* g = pp.g;
+  const int sms = c->num_sms;
+  const int heavy = std::max(32, c->tuning.heavy_degree);
+  const float alpha = c->tuning.pull_alpha > 0 ? c->tuning.pull_alpha : 64.0f;
+  const WsLayout L = layout_for(g->n, (int)sizeof(W), NW);
+  const PassRes<W, NW, OffT> p = pass_res<W, NW, OffT>(g, ch.ws, L, ch.ctr, ch.hpar, heavy);
+  const StepShape sh = graph_shape<W, NW, OffT>(g, sms);
+  const int32_t* src = bs->d_src + pp.src_off;
+  xb_status st = emit_pass_init<W, NW, OffT>(p, g, src, pp.kb, ch.cs, sms, true);
+  if (st != XB_OK) return st;
+  st = capture_level_loop<W, NW, OffT>(bs, p, g, pp.kb, alpha, sh, ch.cs, sms);
+  if (st != XB_OK) return st;
+  if (pp.host && slot_used[pp.chain][pp.slot]) XB_CUDA(cudaStreamWaitEvent(ch.cs, ch.ev_free[pp.slot], 0));
+  int64_t launches = 0;
+  st = emit_tables<W, NW, OffT>(p, g, src, pp.kb, bs->d_rows + rows_off, true, ch.cs, sms, &launches);
+  if (st != XB_OK) return st;
+  const int hv = g->n_heavy > 0 ? 1 : 0;
+  const int words = (pp.kb + B - 1) / B;
+  const int fixed_k = hv + 2 + words * (1 + hv) + 1;
+  const int push_k = 2 + 2 * hv;
+  const int pull_k = 2 + hv + (g->n_hub_items > 0 ? 2 : 0);
+  xbk::k_pass_accum<<<1, 1, 0, ch.cs>>>(p.ctr, bs->d_sums + pp.chain, (long long)g->n, pp.kb,
+                                        (int)sizeof(OffT) * 2, (int)sizeof(W), NW, fixed_k, push_k, pull_k);
+  XB_LAUNCH_CHECK("pass accumulate");
+  if (pp.host) {
+    XB_CUDA(cudaEventRecord(ch.ev_tab, ch.cs));
+    XB_CUDA(cudaStreamWaitEvent(ch.cps, ch.ev_tab, 0));
+    // runs of consecutive rows of the same host query become one copy each
+    const int32_t* lv_slot = ch.stage + (size_t)pp.slot * 2 * SPP * n_stage;
+    const int32_t* pr_slot = lv_slot + (size_t)SPP * n_stage;
+    const int64_t n = g->n;
+    for (int j = 0; j < pp.kb;) {
+      const xb_batch_item& it = items[pp.rows[j].item];
+      if (it.flags & XB_OUT_DEVICE) {
+        j++;
+        continue;
+      }
+      int r = j + 1;
+      while (r < pp.kb && pp.rows[r].item == pp.rows[j].item && pp.rows[r].idx == pp.rows[r - 1].idx + 1) r++;
+      const size_t bytes = sizeof(int32_t) * (size_t)(r - j) * (size_t)n;
+      // staging rows are n_stage apart; copy row by row when that differs from n
+      if (n_stage == n) {
+        XB_CUDA(cudaMemcpyAsync(it.level + (int64_t)pp.rows[j].idx * n, lv_slot + (size_t)j * n_stage, bytes,
+                                cudaMemcpyDeviceToHost, ch.cps));
+        XB_CUDA(cudaMemcpyAsync(it.parent + (int64_t)pp.rows[j].idx * n, pr_slot + (size_t)j * n_stage, bytes,
+                                cudaMemcpyDeviceToHost, ch.cps));
+      } else {
+        XB_CUDA(cudaMemcpy2DAsync(it.level + (int64_t)pp.rows[j].idx * n, sizeof(int32_t) * n,
+                                  lv_slot + (size_t)j * n_stage, sizeof(int32_t) * n_stage, sizeof(int32_t) * n,
+                                  (size_t)(r - j), cudaMemcpyDeviceToHost, ch.cps));
+        XB_CUDA(cudaMemcpy2DAsync(it.parent + (int64_t)pp.rows[j].idx * n, sizeof(int32_t) * n,
+                                  pr_slot + (size_t)j * n_stage, sizeof(int32_t) * n_stage, sizeof(int32_t) * n,
+                                  (size_t)(r - j), cudaMemcpyDeviceToHost, ch.cps));
+      }
+      j = r;
+    }
+    XB_CUDA(cudaEventRecord(ch.ev_free[pp.slot], ch.cps));
+    slot_used[pp.chain][pp.slot] = true;
+  }
+  return XB_OK;
+}
+
+template <typename W, int NW>
+xb_status capture_pass_any(xb_ctx* c, BatchState* bs, const PassPlan& pp, int64_t rows_off, int64_t n_stage,
+                           const std::vector<xb_batch_item>& items, bool slot_used[kMaxChains][2]) {
+  return pp.g->off64 ? capture_pass<W, NW, int64_t>(c, bs, pp, rows_off, n_stage, items, slot_used)
+                     : capture_pass<W, NW, int32_t>(c, bs, pp, rows_off, n_stage, items, slot_used);
+}
+
+// Captures the whole plan into an executable graph.
+template <typename W, int NW>
+xb_status capture_plan(xb_ctx* c, BatchState* bs, const std::vector<PassPlan>& plan, int nch,
+                       const std::vector<int64_t>& n_stage, const std::vector<xb_batch_item>& items,
+                       cudaGraphExec_t* exec) {
+  constexpr int SPP = xbk::WB<W>::bits * NW;
+  cudaStream_t os = bs->origin;
+  XB_CUDA(cudaStreamBeginCapture(os, cudaStreamCaptureModeRelaxed));
+  xb_status st = XB_OK;
+  bool host_chain[kMaxChains] = {};
+  for (const auto& pp : plan) host_chain[pp.chain] |= pp.host;
+  auto body = [&]() -> xb_status {
+    XB_CUDA(cudaMemsetAsync(bs->d_sums, 0, sizeof(xbk::PassSum) * kMaxChains, os));
+    XB_CUDA(cudaEventRecord(bs->ev_fork, os));
+    for (int i = 0; i < nch; i++) {
+      XB_CUDA(cudaStreamWaitEvent(bs->chains[i].cs, bs->ev_fork, 0));
+      if (host_chain[i]) XB_CUDA(cudaStreamWaitEvent(bs->chains[i].cps, bs->ev_fork, 0));
+    }
+    bool slot_used[kMaxChains][2] = {};
+    for (size_t j = 0; j < plan.size(); j++) {
+      const xb_status s2 = capture_pass_any<W, NW>(c, bs, plan[j], (int64_t)j * 2 * SPP, n_stage[plan[j].chain],
+                                                   items, slot_used);
+      if (s2 != XB_OK) return s2;
+    }
+    for (int i = 0; i < nch; i++) {
+      XB_CUDA(cudaEventRecord(bs->chains[i].ev_join, bs->chains[i].cs));
+      XB_CUDA(cudaStreamWaitEvent(os, bs->chains[i].ev_join, 0));
+      if (host_chain[i]) {
+        XB_CUDA(cudaEventRecord(bs->chains[i].ev_join_cp, bs->chains[i].cps));
+        XB_CUDA(cudaStreamWaitEvent(os, bs->chains[i].ev_join_cp, 0));
+      }
+    }
+    return XB_OK;
+  };
+  st = body();
+  cudaGraph_t graph = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(os, &graph);
+  if (st == XB_OK && e != cudaSuccess) st = fail(XB_ERR_CUDA, std::string("batch capture: ") + cudaGetErrorString(e));
+  if (st == XB_OK) {
+    const cudaError_t ei = cudaGraphInstantiate(exec, graph, 0);
+    if (ei != cudaSuccess) st = fail(XB_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ei));
+  }
+  if (graph) cudaGraphDestroy(graph);
+  cudaGetLastError();
+  return st;
+}
+
+template <typename W, int NW>
+xb_status run_batched(xb_ctx* c, const std::vector<xb_batch_item>& items, const std::vector<std::vector<int32_t>>& hsrc,
+                      xb_stats* stats) {
+  constexpr int B = xbk::WB<W>::bits;
+  constexpr int SPP = B * NW;
+  xb_status st = make_state(c);
+  if (st != XB_OK) return st;
+  BatchState* bs = c->batch;
+  const int heavy = std::max(32, c->tuning.heavy_degree);
+
+  // ---- plan: group by graph (first appearance), pack sources into passes
+  std::vector<const xb_graph*> graphs;
+  std::map<const xb_graph*, std::vector<RowDst>> by_graph;
+  for (size_t i = 0; i < items.size(); i++) {
+    const xb_graph* g = items[i].graph;
+    if (items[i].k == 0) continue;
+    if (!by_graph.count(g)) graphs.push_back(g);
+    auto& v = by_graph[g];
+    for (int32_t s = 0; s < items[i].k; s++) v.push_back(RowDst{(int32_t)i, s});
+  }
+  std::vector<PassPlan> plan;
+  int64_t nsrc = 0;
+  for (const xb_graph* g : graphs) {
+    st = ensure_heavy(const_cast<xb_graph*>(g), heavy);
+    if (st != XB_OK) return st;
+    const auto& v = by_graph[g];
+    for (size_t j0 = 0; j0 < v.size(); j0 += SPP) {
+      PassPlan pp;
+      pp.g = g;
+      pp.kb = (int)std::min<size_t>(SPP, v.size() - j0);
+      pp.src_off = nsrc;
+      pp.rows.assign(v.begin() + (ptrdiff_t)j0, v.begin() + (ptrdiff_t)(j0 + pp.kb));
+      for (const auto& r : pp.rows) pp.host |= !(items[r.item].flags & XB_OUT_DEVICE);
+      pp.cost = (double)g->m + 4.0 * (double)g->n;
+      nsrc += pp.kb;
+      plan.push_back(std::move(pp));
+    }
+  }
+  if (plan.empty()) return XB_OK;
+  const int nch = (int)std::min<int64_t>(std::max(1, c->tuning.chains), (int64_t)plan.size());
+  {  // longest processing time first; within a chain, passes keep plan order
+    std::vector<size_t> order(plan.size());
+    for (size_t j = 0; j < order.size(); j++) order[j] = j;
+    std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return plan[a].cost > plan[b].cost; });
+    std::vector<double> load((size_t)nch, 0.0);
+    for (size_t j : order) {
+      const int ci = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+      plan[j].chain = ci;
+      load[(size_t)ci] += plan[j].cost;
+    }
+    std::vector<PassPlan> sorted;
+    sorted.reserve(plan.size());
+    for (int ci = 0; ci < nch; ci++)
+      for (auto& pp : plan)
+        if (pp.chain == ci) sorted.push_back(pp);
+    plan.swap(sorted);
+    int next_slot[kMaxChains] = {};
+    for (auto& pp : plan)
+      if (pp.host) {
+        pp.slot = next_slot[pp.chain];
+        next_slot[pp.chain] ^= 1;
+      }
+  }
+
+  // ---- per-chain resources
+  std::vector<int64_t> n_stage((size_t)nch, 0);
+  for (int ci = 0; ci < nch; ci++) {
+    size_t ws = 0, hp = 1;
+    int64_t nmax_host = 0;
+    for (const auto& pp : plan) {
+      if (pp.chain != ci) continue;
+      ws = std::max(ws, layout_for(pp.g->n, (int)sizeof(W), NW).total);
+      hp = std::max(hp, (size_t)std::max(pp.g->n_heavy, 1) * kHparRow);
+      if (pp.host) nmax_host = std::max(nmax_host, pp.g->n);
+    }
+    Chain& ch = bs->chains[ci];
+    size_t cap = ch.ws_bytes;
+    st = grow(&ch.ws, &cap, ws, &bs->gen, "chain workspace");
+    ch.ws_bytes = cap;
+    if (st != XB_OK) return st;
+    if (!ch.ctr) {
+      XB_CUDA(cudaMalloc(&ch.ctr, sizeof(xbk::Ctrs)));
+      XB_CUDA(cudaMemset(ch.ctr, 0, sizeof(xbk::Ctrs)));
+      bs->gen++;
+    }
+    size_t hcap = ch.hpar_count * sizeof(int32_t);
+    st = grow(&ch.hpar, &hcap, hp * sizeof(int32_t), &bs->gen, "heavy parent slots");
+    ch.hpar_count = hcap / sizeof(int32_t);
+    if (st != XB_OK) return st;
+    if (nmax_host > 0) {
+      size_t scap = ch.stage_bytes;
+      st = grow(&ch.stage, &scap, sizeof(int32_t) * 2 * 2 * (size_t)SPP * (size_t)nmax_host, &bs->gen,
+                "chain staging");
+      ch.stage_bytes = scap;
+      if (st != XB_OK) return st;
+      n_stage[(size_t)ci] = (int64_t)(ch.stage_bytes / (sizeof(int32_t) * 4 * (size_t)SPP));
+    }
+  }
+  // sources and row tables (pinned host mirrors, uploaded every call)
+  const int64_t nrows = (int64_t)plan.size() * 2 * SPP;
+  if (bs->src_cap < nsrc) {
+    if (bs->d_src) cudaFree(bs->d_src);
+    if (bs->h_src) cudaFreeHost(bs->h_src);
+    bs->d_src = nullptr;
+    bs->h_src = nullptr;
+    bs->src_cap = 0;
+    bs->gen++;
+    if (cudaMalloc(&bs->d_src, sizeof(int32_t) * (size_t)nsrc) != cudaSuccess ||
+        cudaMallocHost(&bs->h_src, sizeof(int32_t) * (size_t)nsrc) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(XB_ERR_OOM, "batch source buffer allocation failed");
+    }
+    bs->src_cap = nsrc;
+  }
+  if (bs->rows_cap < nrows) {
+    if (bs->d_rows) cudaFree(bs->d_rows);
+    if (bs->h_rows) cudaFreeHost(bs->h_rows);
+    bs->d_rows = nullptr;
+    bs->h_rows = nullptr;
+    bs->rows_cap = 0;
+    bs->gen++;
+    if (cudaMalloc(&bs->d_rows, sizeof(int32_t*) * (size_t)nrows) != cudaSuccess ||
+        cudaMallocHost(&bs->h_rows, sizeof(int32_t*) * (size_t)nrows) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(XB_ERR_OOM, "batch row table allocation failed");
+    }
+    bs->rows_cap = nrows;
+  }
+  // the previous launch has finished (every call ends synchronised), so the
+  // pinned mirrors may be rewritten
+  for (size_t j = 0; j < plan.size(); j++) {
+    const PassPlan& pp = plan[j];
+    int32_t** rows = bs->h_rows + (int64_t)j * 2 * SPP;
+    const int64_t ns = n_stage[(size_t)pp.chain];
+    int32_t* lv_slot = pp.host ? bs->chains[pp.chain].stage + (size_t)pp.slot * 2 * SPP * ns : nullptr;
+    int32_t* pr_slot = pp.host ? lv_slot + (size_t)SPP * ns : nullptr;
+    for (int s = 0; s < SPP; s++) {
+      const int wi = s / B, b = s % B;
+      int32_t* lv = nullptr;
+      int32_t* pr = nullptr;
+      if (s < pp.kb) {
+        const RowDst r = pp.rows[s];
+        const xb_batch_item& it = items[r.item];
+        bs->h_src[pp.src_off + s] = hsrc[r.item][r.idx];
+        if (it.flags & XB_OUT_DEVICE) {
+          lv = it.level + (int64_t)r.idx * pp.g->n;
+          pr = it.parent + (int64_t)r.idx * pp.g->n;
+        } else {
+          lv = lv_slot + (size_t)s * ns;
+          pr = pr_slot + (size_t)s * ns;
+        }
+      }
+      rows[wi * 2 * B + b] = lv;
+      rows[wi * 2 * B + B + b] = pr;
+    }
+  }
+
+  // ---- cached executable graph for this plan shape
+  std::vector<uint64_t> key = {bs->gen,
+                               (uint64_t)sizeof(W),
+                               (uint64_t)NW,
+                               (uint64_t)heavy,
+                               0,
+                               (uint64_t)nch,
+                               (uint64_t)items.size()};
+  {
+    uint32_t abits = 0;
+    std::memcpy(&abits, &c->tuning.pull_alpha, sizeof(abits));
+    key[4] = abits;
+  }
+  for (const auto& it : items) {
+    key.push_back((uint64_t)(uintptr_t)it.graph);
+    key.push_back(it.graph->version);
+    key.push_back((uint64_t)it.k);
+    key.push_back((uint64_t)(it.flags & XB_OUT_DEVICE));
+    if (!(it.flags & XB_OUT_DEVICE) && it.k > 0) {
+      key.push_back((uint64_t)(uintptr_t)it.level);
+      key.push_back((uint64_t)(uintptr_t)it.parent);
+    }
+  }
+  CachedGraph* hit = nullptr;
+  for (auto& e : bs->cache)
+    if (e.key == key) hit = &e;
+  if (!hit) {
+    // entries made before a reallocation point at freed buffers
+    for (size_t i = 0; i < bs->cache.size();) {
+      if (bs->cache[i].key[0] != bs->gen) {
+        cudaGraphExecDestroy(bs->cache[i].exec);
+        bs->cache.erase(bs->cache.begin() + (ptrdiff_t)i);
+      } else {
+        i++;
+      }
+    }
+    if (bs->cache.size() >= kMaxCached) {
+      auto lru = std::min_element(bs->cache.begin(), bs->cache.end(),
+                                  [](const CachedGraph& a, const CachedGraph& b) { return a.last_use < b.last_use; });
+      cudaGraphExecDestroy(lru->exec);
+      bs->cache.erase(lru);
+    }
+    // the capture streams must not hold work of an earlier call
+    XB_CUDA(cudaStreamSynchronize(c->stream));
+    CachedGraph e;
+    e.key = key;
+    e.graphs = graphs;
+    st = capture_plan<W, NW>(c, bs, plan, nch, n_stage, items, &e.exec);
+    if (st != XB_OK) return st;
+    bs->cache.push_back(std::move(e));
+    hit = &bs->cache.back();
+  }
+  hit->last_use = ++bs->tick;
+
+  // ---- launch
+  XB_CUDA(cudaMemcpyAsync(bs->d_src, bs->h_src, sizeof(int32_t) * (size_t)nsrc, cudaMemcpyHostToDevice, c->stream));
+  XB_CUDA(cudaMemcpyAsync(bs->d_rows, bs->h_rows, sizeof(int32_t*) * (size_t)nrows, cudaMemcpyHostToDevice,
+                          c->stream));
+  XB_CUDA(cudaEventRecord(c->ev0, c->stream));
+  XB_CUDA(cudaGraphLaunch(hit->exec, c->stream));
+  XB_CUDA(cudaEventRecord(c->ev1, c->stream));
+  XB_CUDA(cudaMemcpyAsync(bs->h_sums, bs->d_sums, sizeof(xbk::PassSum) * kMaxChains, cudaMemcpyDeviceToHost,
+                          c->stream));
+  XB_CUDA(cudaStreamSynchronize(c->stream));
+  for (int ci = 0; ci < nch; ci++)
+    if (bs->h_sums[ci].errors)
+      return fail(XB_ERR_STATE, "a pass's level loop ran past the level bound (corrupted traversal state)");
+  if (stats) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    stats->device_ms = ms;
+    for (int ci = 0; ci < nch; ci++) {
+      const xbk::PassSum& s = bs->h_sums[ci];
+      stats->edges_traversed += (int64_t)s.edges_traversed;
+      stats->reached += (int64_t)s.reached;
+      stats->edges_scanned += (int64_t)s.edges_scanned;
+      stats->vertices_scanned += (int64_t)s.vertices_scanned;
+      stats->vertices_swept += (int64_t)s.vertices_swept;
+      stats->parent_edges_scanned += (int64_t)s.parent_edges;
+      stats->class_bytes[0] += (int64_t)s.level_bytes;
+      stats->class_bytes[1] += (int64_t)s.table_bytes;
+      stats->algo_bytes += (int64_t)(s.level_bytes + s.table_bytes);
+      stats->levels = std::max(stats->levels, s.max_level);
+      stats->push_levels += s.push_levels;
+      stats->pull_levels += s.pull_levels;
+      stats->batches += s.passes;
+    }
+    for (int ci = 0; ci < nch; ci++) stats->class_launches[2] += (int64_t)bs->h_sums[ci].launches;
+  }
+  return XB_OK;
+}
+
+}  // namespace
+
+void batch_state_free(BatchState* b) {
+  if (!b) return;
+  cudaSetDevice(b->device);
+  drop_cache(b);
+  for (auto& ch : b->chains) {
+    if (ch.ws) cudaFree(ch.ws);
+    if (ch.ctr) cudaFree(ch.ctr);
+    if (ch.hpar) cudaFree(ch.hpar);
+    if (ch.stage) cudaFree(ch.stage);
+    for (cudaEvent_t e : {ch.ev_tab, ch.ev_free[0], ch.ev_free[1], ch.ev_join, ch.ev_join_cp})
+      if (e) cudaEventDestroy(e);
+    if (ch.cs) cudaStreamDestroy(ch.cs);
+    if (ch.cps) cudaStreamDestroy(ch.cps);
+  }
+  if (b->d_sums) cudaFree(b->d_sums);
+  if (b->h_sums) cudaFreeHost(b->h_sums);
+  if (b->d_src) cudaFree(b->d_src);
+  if (b->h_src) cudaFreeHost(b->h_src);
+  if (b->d_rows) cudaFree(b->d_rows);
+  if (b->h_rows) cudaFreeHost(b->h_rows);
+  if (b->ev_fork) cudaEventDestroy(b->ev_fork);
+  for (auto s : b->body)
+    if (s) cudaStreamDestroy(s);
+  if (b->origin) cudaStreamDestroy(b->origin);
+  delete b;
+}
+
+void batch_forget_graph(xb_ctx* c, const xb_graph* g) {
+  if (!c || !c->batch) return;
+  auto& cache = c->batch->cache;
+  for (size_t i = 0; i < cache.size();) {
+    bool uses = false;
+    for (const xb_graph* x : cache[i].graphs) uses |= x == g;
+    if (uses) {
+      if (cache[i].exec) cudaGraphExecDestroy(cache[i].exec);
+      cache.erase(cache.begin() + (ptrdiff_t)i);
+    } else {
+      i++;
+    }
+  }
+}
+
+}  // namespace xbe
+
+extern "C" xb_status xb_traverse_batched(xb_ctx* c, const xb_batch_item* items, int32_t nitems, xb_stats* stats) {
+  xbi::clear_error();
+  if (!c) return fail(XB_ERR_ARG, "null context");
+  if (nitems < 0 || (nitems > 0 && !items)) return fail(XB_ERR_ARG, "bad item list");
+  if (stats) std::memset(stats, 0, sizeof(*stats));
+  XB_CUDA(cudaSetDevice(c->device));
+  std::vector<xb_batch_item> its(items, items + nitems);
+  std::vector<std::vector<int32_t>> hsrc((size_t)nitems);
+  for (int32_t i = 0; i < nitems; i++) {
+    const xb_batch_item& it = its[(size_t)i];
+    const std::string at = "item " + std::to_string(i) + ": ";
+    if (!it.graph) return fail(XB_ERR_ARG, at + "null graph");
+    if (it.graph->ctx->device != c->device) return fail(XB_ERR_ARG, at + "graph lives on another device");
+    if (it.k < 0) return fail(XB_ERR_ARG, at + "negative source count");
+    if (it.k == 0) continue;
+    if (!it.sources || !it.level || !it.parent) return fail(XB_ERR_ARG, at + "null sources or output tables");
+    if (!(it.flags & XB_OUT_DEVICE)) {
+      for (const int32_t* ptr : {it.level, it.parent}) {
+        cudaPointerAttributes a{};
+        if (cudaPointerGetAttributes(&a, ptr) != cudaSuccess || a.type != cudaMemoryTypeHost) {
+          cudaGetLastError();
+          return fail(XB_ERR_ARG, at + "host tables must be page-locked (cudaHostAlloc / cudaHostRegister)");
+        }
+      }
+    }
+    auto& h = hsrc[(size_t)i];
+    h.resize((size_t)it.k);
+    if (it.flags & XB_SOURCES_DEVICE) {
+      XB_CUDA(cudaMemcpy(h.data(), it.sources, sizeof(int32_t) * (size_t)it.k, cudaMemcpyDeviceToHost));
+    } else {
+      std::memcpy(h.data(), it.sources, sizeof(int32_t) * (size_t)it.k);
+    }
+    for (int32_t s = 0; s < it.k; s++)
+      if (h[(size_t)s] < 0 || h[(size_t)s] >= it.graph->n)
+        return fail(XB_ERR_ARG, at + "source " + std::to_string(s) + " out of range");
+  }
+  xb_status s = XB_OK;
+  const int nw = c->tuning.words;
+  if (c->tuning.word_bits == 64) {
+    s = nw == 1 ? xbe::run_batched<unsigned long long, 1>(c, its, hsrc, stats)
+        : nw == 2 ? xbe::run_batched<unsigned long long, 2>(c, its, hsrc, stats)
+                  : xbe::run_batched<unsigned long long, 4>(c, its, hsrc, stats);
+  } else {
+    s = nw == 1 ? xbe::run_batched<unsigned int, 1>(c, its, hsrc, stats)
+        : nw == 2 ? xbe::run_batched<unsigned int, 2>(c, its, hsrc, stats)
+                  : xbe::run_batched<unsigned int, 4>(c, its, hsrc, stats);
+  }
+  if (s != XB_OK) {
+    cudaStreamSynchronize(c->stream);
+    cudaGetLastError();
+  }
+  return s;
+}

@@ -8,122 +8,14 @@
 // decides the next step.  Unlike the reference it reads one 200-byte counter
 // block per level (instead of four D2H scalars plus a device sync per queue
 // swap) and traverses B (32 or 64) sources per launch sequence.
-#include <cuda_runtime.h>
-
-#include <algorithm>
-#include <cstring>
 #include <memory>
 #include <new>
-#include <string>
-#include <vector>
 
-#include "xb_internal.h"
-#include "xb_kernels.cuh"
+#include "xb_engine_common.cuh"
 
 using xbi::fail;
 
-#define XB_CUDA(call)                                                                        \
-  do {                                                                                       \
-    cudaError_t e_ = (call);                                                                 \
-    if (e_ != cudaSuccess) return fail(XB_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
-  } while (0)
-
-#define XB_LAUNCH_CHECK(what)                                                                \
-  do {                                                                                       \
-    cudaError_t e_ = cudaGetLastError();                                                     \
-    if (e_ != cudaSuccess) return fail(XB_ERR_CUDA, std::string("launch ") + what + ": " + cudaGetErrorString(e_)); \
-  } while (0)
-
-struct xb_ctx {
-  int device = 0;
-  int num_sms = 148;
-  cudaStream_t stream = nullptr;
-  xb_tuning tuning{};
-  // workspace
-  void* ws = nullptr;
-  size_t ws_bytes = 0;
-  int64_t ws_key[3] = {-1, -1, -1};  // (n, word bytes, words) of the current layout
-  xbk::Ctrs* d_ctr = nullptr;
-  xbk::Ctrs* h_ctr = nullptr;  // pinned
-  int32_t* d_src = nullptr;
-  int64_t src_cap = 0;
-  int32_t* d_stage = nullptr;  // device staging for host-bound tables
-  size_t stage_bytes = 0;
-  int32_t epoch = 1;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr, evc0 = nullptr, evc1 = nullptr;
-};
-
-struct xb_graph {
-  xb_ctx* ctx = nullptr;
-  int64_t n = 0, m = 0, max_deg = 0;
-  bool off64 = false;
-  void* d_ro = nullptr;
-  int32_t* d_ci = nullptr;
-  std::vector<int64_t> h_ro;
-  int32_t* d_heavy = nullptr;  // vertices with degree > heavy_thr, ascending
-  int32_t* d_hpar = nullptr;   // per heavy vertex, 64 parent slots of the table pass
-  int2* d_hitems = nullptr;    // (heavy index, chunk) items of the table pass
-  int64_t n_hitems = 0;
-  int2* d_hub_items = nullptr;  // (heavy index, chunk) items of the hub pull
-  int64_t n_hub_items = 0;
-  int32_t* d_hidx_of = nullptr;  // vertex -> index in the heavy list (-1 for light)
-  int32_t n_heavy = 0;
-  int32_t heavy_thr = -1;
-};
-
-namespace {
-
-// Edges per work item of the heavy-vertex table scan.
-constexpr int kTableChunk = 4096;
-// Vertices above this degree (hubs) are pulled in chunks by many warps; the
-// other heavy vertices by one warp each.
-constexpr int kHubDegree = 4096;
-constexpr int kHubChunk = 2048;
-// Parent slots per heavy vertex: up to 64 sources x 4 words.
-constexpr int kHparRow = 256;
-
-struct WsLayout {
-  size_t seen, F, N, p01, ph, pushed, p8, touched, fl_light, fl_heavy, nl_light, nl_heavy, stamp, total;
-  int64_t plane_stride;  // in words
-  int nplanes_alloc;
-};
-
-int bitlen_levels(int64_t n) {
-  // levels are in [0, n-1]; number of bits to hold n-1, at least 3
-  int b = 0;
-  int64_t x = n > 1 ? n - 1 : 0;
-  while (x) {
-    b++;
-    x >>= 1;
-  }
-  return std::max(3, b);
-}
-
-size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
-
-WsLayout layout_for(int64_t n, int word_bytes, int nw) {
-  WsLayout L{};
-  const size_t sw = align_up((size_t)n * nw * word_bytes);
-  const size_t li = align_up((size_t)std::max<int64_t>(n, 1) * 4);
-  L.nplanes_alloc = bitlen_levels(n);
-  L.plane_stride = (int64_t)(sw / word_bytes);
-  size_t o = 0;
-  L.seen = o; o += sw;
-  L.F = o; o += sw;
-  L.N = o; o += sw;
-  L.p01 = o; o += 2 * sw;
-  L.ph = o; o += sw * (L.nplanes_alloc - 2);
-  L.pushed = o; o += sw;
-  L.p8 = o; o += align_up((size_t)n * nw * word_bytes * 8);  // 8 position planes per (vertex, word)
-  L.touched = o; o += li;
-  L.fl_light = o; o += li;
-  L.fl_heavy = o; o += li;
-  L.nl_light = o; o += li;
-  L.nl_heavy = o; o += li;
-  L.stamp = o; o += li;
-  L.total = o;
-  return L;
-}
+namespace xbe {
 
 // The F/N "all zero between calls" invariant and the epoch stamps hold per
 // layout; a call with another (n, word size, words) places the regions at
@@ -134,12 +26,10 @@ xb_status ensure_workspace(xb_ctx* c, const WsLayout& L, int64_t n, int wbytes, 
     if (std::memcmp(key, c->ws_key, sizeof(key)) != 0) {
       XB_CUDA(cudaMemsetAsync(c->ws, 0, L.total, c->stream));
       std::memcpy(c->ws_key, key, sizeof(key));
-      c->epoch = 1;
     }
     return XB_OK;
   }
   std::memcpy(c->ws_key, key, sizeof(key));
-  c->epoch = 1;
   if (c->ws) {
     cudaFree(c->ws);
     c->ws = nullptr;
@@ -179,6 +69,19 @@ xb_status ensure_stage(xb_ctx* c, size_t bytes) {
     return fail(XB_ERR_OOM, "table staging allocation failed");
   }
   c->stage_bytes = bytes;
+  return XB_OK;
+}
+
+xb_status ensure_rows(xb_ctx* c, int64_t count) {
+  if (c->rows_cap >= count) return XB_OK;
+  if (c->d_rows) cudaFree(c->d_rows);
+  c->d_rows = nullptr;
+  c->rows_cap = 0;
+  if (cudaMalloc(&c->d_rows, sizeof(int32_t*) * (size_t)std::max<int64_t>(count, 1)) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(XB_ERR_OOM, "row table allocation failed");
+  }
+  c->rows_cap = count;
   return XB_OK;
 }
 
@@ -245,258 +148,8 @@ xb_status ensure_heavy(xb_graph* g, int thr) {
   g->n_hub_items = (int64_t)hub_items.size();
   g->n_heavy = (int32_t)hv.size();
   g->heavy_thr = thr;
+  g->version++;
   return XB_OK;
-}
-
-struct ClassTimer {
-  xb_ctx* c;
-  xb_stats* st;
-  bool on;
-  void begin() {
-    if (on) cudaEventRecord(c->evc0, c->stream);
-  }
-  void end(int cls, int64_t launches) {
-    if (st) st->class_launches[cls] += launches;
-    if (!on) return;
-    cudaEventRecord(c->evc1, c->stream);
-    cudaEventSynchronize(c->evc1);
-    float ms = 0.f;
-    cudaEventElapsedTime(&ms, c->evc0, c->evc1);
-    if (st) st->class_ms[cls] += ms;
-  }
-};
-
-// Algorithmic bytes of a pass's level steps: the row-offset pair of every
-// scanned vertex, colIndices + the gathered frontier words of every scanned
-// edge, and a three-word sweep (seen read, seen and next-frontier write) of
-// every swept vertex.
-template <typename W, int NW, typename OffT>
-int64_t level_bytes(const xbk::BatchCtr& b) {
-  const int64_t R = (int64_t)sizeof(OffT) * 2;
-  const int64_t wbytes = (int64_t)sizeof(W) * NW;
-  return R * (int64_t)b.vertices_scanned + (4 + wbytes) * (int64_t)b.edges_scanned +
-         3 * wbytes * (int64_t)b.vertices_swept;
-}
-
-// Algorithmic bytes of a pass's table pass: per vertex its row offsets, seen,
-// level planes and parent-position planes (per word), the colIndices entry of
-// every recorded parent, colIndices + gathered plane pair of every searched
-// edge, and the two written tables.
-template <typename W, int NW, typename OffT>
-int64_t table_bytes(const xbk::BatchCtr& b, int64_t n, int kb) {
-  const int64_t R = (int64_t)sizeof(OffT) * 2;
-  return (int64_t)NW * n * (R + (int64_t)sizeof(W) * (1 + b.nplanes + 8)) + 4 * (int64_t)b.reached +
-         (4 + 2 * (int64_t)sizeof(W)) * (int64_t)b.parent_edges + 8 * (int64_t)kb * n;
-}
-
-// Pointers and constants of one traversal pass (a workspace + counters).
-template <typename W, int NW, typename OffT>
-struct PassRes {
-  int64_t n = 0;
-  const OffT* ro = nullptr;
-  const int32_t* ci = nullptr;
-  W* seen = nullptr;
-  W* buf[2] = {nullptr, nullptr};  // frontier words; buf[cur] = F, buf[cur ^ 1] = N
-  xbk::Planes<W, NW> pl{};
-  W* pushed = nullptr;
-  W* ppos = nullptr;
-  int32_t* touched = nullptr;
-  xbk::Lists lists[2] = {};  // lists[cur] = current frontier, lists[cur ^ 1] = next
-  int32_t* stamp = nullptr;
-  xbk::Ctrs* ctr = nullptr;
-  int32_t* hpar = nullptr;
-  int heavy = 256;
-  size_t state_bytes = 0, plane_bytes = 0, ppos_bytes = 0;
-  int nplanes_alloc = 3;
-};
-
-template <typename W, int NW, typename OffT>
-PassRes<W, NW, OffT> pass_res(const xb_graph* g, void* ws, const WsLayout& L, xbk::Ctrs* ctr, int32_t* hpar,
-                              int heavy) {
-  PassRes<W, NW, OffT> p;
-  char* base = (char*)ws;
-  p.n = g->n;
-  p.ro = (const OffT*)g->d_ro;
-  p.ci = g->d_ci;
-  p.seen = (W*)(base + L.seen);
-  p.buf[0] = (W*)(base + L.F);
-  p.buf[1] = (W*)(base + L.N);
-  p.pl = xbk::Planes<W, NW>{(W*)(base + L.p01), (W*)(base + L.ph), L.plane_stride};
-  p.pushed = (W*)(base + L.pushed);
-  p.ppos = (W*)(base + L.p8);
-  p.touched = (int32_t*)(base + L.touched);
-  p.lists[0] = xbk::Lists{(int32_t*)(base + L.fl_light), (int32_t*)(base + L.fl_heavy)};
-  p.lists[1] = xbk::Lists{(int32_t*)(base + L.nl_light), (int32_t*)(base + L.nl_heavy)};
-  p.stamp = (int32_t*)(base + L.stamp);
-  p.ctr = ctr;
-  p.hpar = hpar;
-  p.heavy = heavy;
-  p.state_bytes = (size_t)g->n * NW * sizeof(W);
-  p.plane_bytes = (size_t)L.plane_stride * sizeof(W);
-  p.ppos_bytes = p.state_bytes * 8;
-  p.nplanes_alloc = L.nplanes_alloc;
-  return p;
-}
-
-template <typename W, int NW>
-xbk::Masks<W, NW> active_mask(int kb) {
-  constexpr int B = xbk::WB<W>::bits;
-  xbk::Masks<W, NW> a{};
-  for (int i = 0; i < NW; i++) {
-    const int lo = i * B, hi = std::min(kb, (i + 1) * B);
-    W m = 0;
-    for (int b = lo; b < hi; b++) m |= (W)1 << (b - lo);
-    a.w[i] = m;
-  }
-  return a;
-}
-
-// Launch shapes of the level-step kernels.
-struct StepShape {
-  int push_light_grid;   // 0: skip
-  dim3 push_heavy_grid;  // .y == 0: skip
-  int finalize_grid;
-  int pull_grid;
-  int heavy_grid;
-  int hub_grid;
-  int commit_grid;
-  int clear_grid;
-};
-
-template <typename W, int NW>
-constexpr int pull_warps() {
-  // the pull tile keeps 8 position words per lane and word in shared memory
-  return (xbk::WB<W>::bits * NW * 32 * 8 > 40 * 1024) ? 4 : 8;
-}
-
-// Pass start: clear the per-pass state, reset counters, seed the sources.
-template <typename W, int NW, typename OffT>
-xb_status emit_pass_init(const PassRes<W, NW, OffT>& p, const xb_graph* g, const int32_t* src, int kb,
-                         cudaStream_t s, int sms) {
-  XB_CUDA(cudaMemsetAsync(p.seen, 0, p.state_bytes, s));
-  XB_CUDA(cudaMemsetAsync(p.pl.p01, 0, 2 * p.plane_bytes, s));
-  XB_CUDA(cudaMemsetAsync(p.pl.ph, 0, p.plane_bytes, s));
-  XB_CUDA(cudaMemsetAsync(p.pushed, 0, p.state_bytes, s));
-  XB_CUDA(cudaMemsetAsync(p.ppos, 0, p.ppos_bytes, s));
-  if (g->n_heavy > 0) {  // parent slots of the heavy vertices (hub pulls fold in with atomicMin)
-    const int64_t hcount = (int64_t)g->n_heavy * kHparRow;
-    xbk::k_fill<int32_t><<<(int)std::min<int64_t>((hcount + 255) / 256, (int64_t)sms * 8), 256, 0, s>>>(p.hpar, hcount,
-                                                                                                   INT32_MAX);
-  }
-  xbk::k_pass_init<<<1, 1, 0, s>>>(p.ctr, (long long)g->m);
-  xbk::k_init_batch<W, NW, OffT><<<1, 256, 0, s>>>(src, kb, p.ro, p.buf[0], p.seen, p.pl, active_mask<W, NW>(kb),
-                                                   p.heavy, p.lists[0], p.ctr);
-  XB_LAUNCH_CHECK("pass init");
-  return XB_OK;
-}
-
-template <typename W, int NW, typename OffT>
-xb_status emit_push(const PassRes<W, NW, OffT>& p, const xb_graph* g, int cur, const StepShape& sh, int kb,
-                    cudaStream_t s, int64_t* launches) {
-  constexpr int PUSH_CHUNK = 2048;
-  W* F = p.buf[cur];
-  W* N = p.buf[cur ^ 1];
-  const xbk::Lists fl = p.lists[cur], nl = p.lists[cur ^ 1];
-  if (sh.push_light_grid > 0) {
-    xbk::k_push_light<W, NW, OffT><<<sh.push_light_grid, 256, 0, s>>>(fl.light, &p.ctr->lv[cur].n_light, p.ro, p.ci, F,
-                                                                      p.seen, N, p.stamp, p.touched, p.ctr, cur);
-    (*launches)++;
-  }
-  if (sh.push_heavy_grid.y > 0) {
-    xbk::k_push_heavy<W, NW, OffT><<<sh.push_heavy_grid, 256, 0, s>>>(fl.heavy, &p.ctr->lv[cur].n_heavy, p.ro, p.ci, F,
-                                                                      p.seen, N, p.stamp, p.touched, p.ctr, cur,
-                                                                      PUSH_CHUNK);
-    xbk::k_clear_list<W, NW><<<sh.clear_grid, 256, 0, s>>>(fl.heavy, &p.ctr->lv[cur].n_heavy, F);
-    *launches += 2;
-  }
-  xbk::k_push_finalize<W, NW, OffT><<<sh.finalize_grid, 256, 0, s>>>(p.touched, p.ro, N, p.seen, p.pl,
-                                                                     active_mask<W, NW>(kb), p.heavy, nl, p.ctr, cur,
-                                                                     p.pushed);
-  (*launches)++;
-  XB_LAUNCH_CHECK("push step");
-  return XB_OK;
-}
-
-template <typename W, int NW, typename OffT>
-xb_status emit_pull(const PassRes<W, NW, OffT>& p, const xb_graph* g, int cur, const StepShape& sh, int kb,
-                    cudaStream_t s, int64_t* launches) {
-  constexpr int PW = pull_warps<W, NW>();
-  W* F = p.buf[cur];
-  W* N = p.buf[cur ^ 1];
-  const xbk::Lists fl = p.lists[cur], nl = p.lists[cur ^ 1];
-  const xbk::Masks<W, NW> active = active_mask<W, NW>(kb);
-  xbk::k_pull_tiles<W, NW, OffT, PW, 4><<<sh.pull_grid, PW * 32, 0, s>>>(p.n, p.ro, p.ci, F, p.seen, N, p.pl, active,
-                                                                         p.heavy, nl, p.ctr, cur, p.ppos);
-  (*launches)++;
-  if (g->n_heavy > 0) {
-    xbk::k_pull_heavy<W, NW, OffT, 4><<<sh.heavy_grid, 256, 0, s>>>(g->d_heavy, g->n_heavy, p.ro, p.ci, F, p.seen, N,
-                                                                    p.pl, active, p.heavy, kHubDegree, nl, p.ctr, cur,
-                                                                    p.hpar);
-    (*launches)++;
-    if (g->n_hub_items > 0) {
-      xbk::k_pull_hubs<W, NW, OffT, 4><<<sh.hub_grid, 256, 0, s>>>(g->d_heavy, g->d_hub_items, g->n_hub_items, p.ro,
-                                                                   p.ci, F, p.seen, N, active, p.ctr, cur, kHubChunk,
-                                                                   p.hpar);
-      xbk::k_pull_hub_commit<W, NW, OffT><<<sh.commit_grid, 256, 0, s>>>(g->d_heavy, g->n_heavy, p.ro, p.seen, N, p.pl,
-                                                                        active, p.heavy, kHubDegree, nl, p.ctr, cur);
-      *launches += 2;
-    }
-  }
-  xbk::k_clear_frontier<W, NW><<<sh.clear_grid, 256, 0, s>>>(F, p.n, fl, p.ctr, cur);
-  (*launches)++;
-  XB_LAUNCH_CHECK("pull step");
-  return XB_OK;
-}
-
-// Table pass of one pass (all its words).  Row s of a word's tables starts at
-// lv_base + (wi*B + s) * row_stride.
-template <typename W, int NW, typename OffT>
-xb_status emit_tables(const PassRes<W, NW, OffT>& p, const xb_graph* g, const int32_t* src, int kb, int32_t* lv_base,
-                      int32_t* pr_base, bool search_heavy, cudaStream_t s, int sms, int64_t* launches) {
-  constexpr int B = xbk::WB<W>::bits;
-  constexpr int TAB_WARPS = (B == 64) ? 4 : 8;
-  const int64_t ntiles = (p.n + 31) / 32;
-  const int tab_grid = (int)std::max<int64_t>(1, std::min<int64_t>((ntiles + TAB_WARPS - 1) / TAB_WARPS, (int64_t)sms * 16));
-  for (int wi = 0; wi < NW; wi++) {
-    const int kbw = std::min(B, kb - wi * B);
-    if (kbw <= 0) break;
-    int32_t* lv_out = lv_base + (int64_t)wi * B * p.n;
-    int32_t* pr_out = pr_base + (int64_t)wi * B * p.n;
-    const int32_t* wsrc = src + wi * B;
-    if (g->n_heavy > 0 && search_heavy) {
-      // heavy vertices reached by a push step at level >= 2: search their parents
-      const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(g->n_hitems, (int64_t)sms * 8));
-      xbk::k_tables_heavy_scan<W, NW, OffT><<<grid, 256, 0, s>>>(g->d_heavy, g->d_hitems, g->n_hitems, p.ro, p.ci,
-                                                                 p.seen, p.pl, wi, kTableChunk, p.hpar, p.ctr,
-                                                                 p.pushed);
-      (*launches)++;
-    }
-    xbk::k_tables<W, NW, OffT, TAB_WARPS, 4><<<tab_grid, TAB_WARPS * 32, 0, s>>>(
-        p.n, p.ro, p.ci, p.seen, p.pl, wi, kbw, p.heavy, lv_out, pr_out, p.ctr, p.ppos, p.pushed, wsrc, g->d_hidx_of,
-        p.hpar);
-    (*launches)++;
-  }
-  XB_LAUNCH_CHECK("tables");
-  return XB_OK;
-}
-
-template <typename W, int NW, typename OffT>
-StepShape max_shape(const xb_graph* g, int sms) {
-  constexpr int PW = pull_warps<W, NW>();
-  StepShape sh{};
-  const int64_t n = g->n;
-  const int64_t ntiles = (n + 31) / 32;
-  sh.push_light_grid = sms * 16;
-  sh.push_heavy_grid = dim3((unsigned)std::max<int64_t>(1, std::min<int64_t>((g->max_deg + 2047) / 2048, 64)),
-                            (unsigned)std::max<int64_t>(1, std::min<int64_t>(g->n_heavy, 65535)));
-  if (g->n_heavy == 0) sh.push_heavy_grid.y = 0;
-  sh.finalize_grid = (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)sms * 8));
-  sh.pull_grid = (int)std::max<int64_t>(1, std::min<int64_t>((ntiles + PW - 1) / PW, (int64_t)sms * 8));
-  sh.heavy_grid = (int)std::max<int64_t>(1, std::min<int64_t>((g->n_heavy + 7) / 8, (int64_t)sms * 16));
-  sh.hub_grid = (int)std::max<int64_t>(1, std::min<int64_t>((g->n_hub_items + 7) / 8, (int64_t)sms * 16));
-  sh.commit_grid = (int)std::max<int64_t>(1, std::min<int64_t>((g->n_heavy + 255) / 256, (int64_t)sms * 4));
-  sh.clear_grid = sms * 8;
-  return sh;
 }
 
 template <typename W, int NW, typename OffT>
@@ -514,6 +167,23 @@ xb_status run_plain(xb_ctx* c, xb_graph* g, const int32_t* d_sources, int32_t k,
   if (!out_dev) {
     s = ensure_stage(c, sizeof(int32_t) * 2 * (size_t)SPP * (size_t)n);
     if (s != XB_OK) return s;
+  }
+  // row-pointer tables of every pass of the call, uploaded once
+  const int64_t npass = (k + SPP - 1) / SPP;
+  s = ensure_rows(c, npass * 2 * SPP);
+  if (s != XB_OK) return s;
+  {
+    std::vector<int32_t*> rows((size_t)(npass * 2 * SPP));
+    for (int64_t j = 0; j < npass; j++) {
+      const int kb = (int)std::min<int64_t>(SPP, k - j * SPP);
+      if (out_dev)
+        fill_rows<W, NW>(rows.data() + j * 2 * SPP, kb, level_out + j * SPP * n, parent_out + j * SPP * n, n);
+      else
+        fill_rows<W, NW>(rows.data() + j * 2 * SPP, kb, c->d_stage, c->d_stage + (size_t)SPP * n, n);
+    }
+    XB_CUDA(cudaMemcpyAsync(c->d_rows, rows.data(), sizeof(int32_t*) * rows.size(), cudaMemcpyHostToDevice,
+                            c->stream));
+    XB_CUDA(cudaStreamSynchronize(c->stream));
   }
   PassRes<W, NW, OffT> p = pass_res<W, NW, OffT>(g, c->ws, L, c->d_ctr, g->d_hpar, heavy);
   const int sms = c->num_sms;
@@ -559,13 +229,15 @@ xb_status run_plain(xb_ctx* c, xb_graph* g, const int32_t* d_sources, int32_t k,
       timer.end(0, launches);
       cur ^= 1;
     }
+    if (c->h_ctr->b.err)
+      return fail(XB_ERR_STATE, "the level loop ran past the level bound (corrupted traversal state)");
     max_levels = std::max(max_levels, c->h_ctr->b.level);
     timer.begin();
     int64_t launches = 0;
-    int32_t* lv_base = out_dev ? level_out + k0 * n : c->d_stage;
-    int32_t* pr_base = out_dev ? parent_out + k0 * n : c->d_stage + (size_t)SPP * n;
-    s = emit_tables<W, NW, OffT>(p, g, d_sources + k0, kb, lv_base, pr_base, c->h_ctr->b.pushed_deep != 0, c->stream,
-                                 sms, &launches);
+    int32_t* lv_base = c->d_stage;
+    int32_t* pr_base = c->d_stage + (size_t)SPP * n;
+    s = emit_tables<W, NW, OffT>(p, g, d_sources + k0, kb, c->d_rows + (k0 / SPP) * 2 * SPP,
+                                 c->h_ctr->b.pushed_deep != 0, c->stream, sms, &launches);
     if (s != XB_OK) return s;
     timer.end(1, launches);
     if (!out_dev) {
@@ -607,7 +279,7 @@ xb_status dispatch_nw(xb_ctx* c, xb_graph* g, const int32_t* d_src, int32_t k, i
   }
 }
 
-}  // namespace
+}  // namespace xbe
 
 extern "C" {
 
@@ -640,6 +312,7 @@ xb_status xb_ctx_create(int32_t device, xb_ctx** out) {
   c->tuning.pull_alpha = 64.0f;
   c->tuning.heavy_degree = 256;
   c->tuning.timing = 0;
+  c->tuning.chains = 2;
   *out = c.release();
   return XB_OK;
 }
@@ -649,9 +322,11 @@ xb_status xb_ctx_destroy(xb_ctx* c) {
   if (!c) return XB_OK;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  xbe::batch_state_free(c->batch);
   if (c->ws) cudaFree(c->ws);
   if (c->d_src) cudaFree(c->d_src);
   if (c->d_stage) cudaFree(c->d_stage);
+  if (c->d_rows) cudaFree(c->d_rows);
   if (c->d_ctr) cudaFree(c->d_ctr);
   if (c->h_ctr) cudaFreeHost(c->h_ctr);
   for (cudaEvent_t ev : {c->ev0, c->ev1, c->evc0, c->evc1})
@@ -669,7 +344,9 @@ xb_status xb_ctx_set_tuning(xb_ctx* c, const xb_tuning* t) {
   if (!(t->pull_alpha > 0)) return fail(XB_ERR_ARG, "pull_alpha must be positive");
   if (t->heavy_degree < 32 || t->heavy_degree > (1 << 20))
     return fail(XB_ERR_ARG, "heavy_degree must be in [32, 2^20]");
+  if (t->chains < 0 || t->chains > 16) return fail(XB_ERR_ARG, "chains must be in [0, 16]");
   c->tuning = *t;
+  if (c->tuning.chains == 0) c->tuning.chains = 2;
   return XB_OK;
 }
 
@@ -683,7 +360,7 @@ xb_status xb_ctx_get_tuning(const xb_ctx* c, xb_tuning* t) {
 xb_status xb_ctx_workspace_bytes(const xb_ctx* c, int64_t* bytes) {
   xbi::clear_error();
   if (!c || !bytes) return fail(XB_ERR_ARG, "null argument");
-  *bytes = (int64_t)(c->ws_bytes + c->stage_bytes + sizeof(int32_t) * c->src_cap);
+  *bytes = (int64_t)(c->ws_bytes + c->stage_bytes + sizeof(int32_t) * c->src_cap + sizeof(int32_t*) * c->rows_cap);
   return XB_OK;
 }
 
@@ -756,6 +433,7 @@ xb_status xb_graph_free(xb_graph* g) {
   xbi::clear_error();
   if (!g) return XB_OK;
   cudaSetDevice(g->ctx->device);
+  xbe::batch_forget_graph(g->ctx, g);
   if (g->d_ro) cudaFree(g->d_ro);
   if (g->d_ci) cudaFree(g->d_ci);
   if (g->d_heavy) cudaFree(g->d_heavy);
@@ -807,16 +485,16 @@ xb_status xb_traverse(xb_ctx* c, const xb_graph* gc, const int32_t* sources, int
   }
   for (int32_t i = 0; i < k; i++)
     if (hs[i] < 0 || hs[i] >= g->n) return fail(XB_ERR_ARG, "source " + std::to_string(i) + " out of range");
-  xb_status s = ensure_sources(c, k);
+  xb_status s = xbe::ensure_sources(c, k);
   if (s != XB_OK) return s;
   XB_CUDA(cudaMemcpyAsync(c->d_src, hs.data(), sizeof(int32_t) * k, cudaMemcpyHostToDevice, c->stream));
   XB_CUDA(cudaEventRecord(c->ev0, c->stream));
   if (c->tuning.word_bits == 64) {
-    s = g->off64 ? dispatch_nw<unsigned long long, int64_t>(c, g, c->d_src, k, level, parent, out_dev, st)
-                 : dispatch_nw<unsigned long long, int32_t>(c, g, c->d_src, k, level, parent, out_dev, st);
+    s = g->off64 ? xbe::dispatch_nw<unsigned long long, int64_t>(c, g, c->d_src, k, level, parent, out_dev, st)
+                 : xbe::dispatch_nw<unsigned long long, int32_t>(c, g, c->d_src, k, level, parent, out_dev, st);
   } else {
-    s = g->off64 ? dispatch_nw<unsigned int, int64_t>(c, g, c->d_src, k, level, parent, out_dev, st)
-                 : dispatch_nw<unsigned int, int32_t>(c, g, c->d_src, k, level, parent, out_dev, st);
+    s = g->off64 ? xbe::dispatch_nw<unsigned int, int64_t>(c, g, c->d_src, k, level, parent, out_dev, st)
+                 : xbe::dispatch_nw<unsigned int, int32_t>(c, g, c->d_src, k, level, parent, out_dev, st);
   }
   if (s != XB_OK) {
     cudaStreamSynchronize(c->stream);

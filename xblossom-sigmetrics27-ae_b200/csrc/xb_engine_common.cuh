@@ -1,0 +1,408 @@
+// xb_engine_common.cuh -- definitions shared by the plain path (xb_engine.cu)
+// and the batched path (xb_batched.cu) of libxbtrav.so: the context and
+// graph objects, the workspace layout of one traversal pass and the functions
+// that enqueue a pass's kernels on a stream.  Not part of the public ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "xb_internal.h"
+#include "xb_kernels.cuh"
+
+namespace xbe {
+struct BatchState;
+}
+
+#define XB_CUDA(call)                                                                        \
+  do {                                                                                       \
+    cudaError_t e_ = (call);                                                                 \
+    if (e_ != cudaSuccess) return fail(XB_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+#define XB_LAUNCH_CHECK(what)                                                                \
+  do {                                                                                       \
+    cudaError_t e_ = cudaGetLastError();                                                     \
+    if (e_ != cudaSuccess) return fail(XB_ERR_CUDA, std::string("launch ") + what + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+struct xb_ctx {
+  int device = 0;
+  int num_sms = 148;
+  cudaStream_t stream = nullptr;
+  xb_tuning tuning{};
+  // workspace
+  void* ws = nullptr;
+  size_t ws_bytes = 0;
+  int64_t ws_key[3] = {-1, -1, -1};  // (n, word bytes, words) of the current layout
+  xbk::Ctrs* d_ctr = nullptr;
+  xbk::Ctrs* h_ctr = nullptr;  // pinned
+  int32_t* d_src = nullptr;
+  int64_t src_cap = 0;
+  int32_t* d_stage = nullptr;  // device staging for host-bound tables
+  size_t stage_bytes = 0;
+  int32_t** d_rows = nullptr;  // row-pointer tables of the table pass (2*B per word)
+  int64_t rows_cap = 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, evc0 = nullptr, evc1 = nullptr;
+  xbe::BatchState* batch = nullptr;  // resources of xb_traverse_batched (created on first use)
+};
+
+struct xb_graph {
+  xb_ctx* ctx = nullptr;
+  int64_t n = 0, m = 0, max_deg = 0;
+  bool off64 = false;
+  void* d_ro = nullptr;
+  int32_t* d_ci = nullptr;
+  std::vector<int64_t> h_ro;
+  int32_t* d_heavy = nullptr;  // vertices with degree > heavy_thr, ascending
+  int32_t* d_hpar = nullptr;   // per heavy vertex, 64 parent slots of the table pass
+  int2* d_hitems = nullptr;    // (heavy index, chunk) items of the table pass
+  int64_t n_hitems = 0;
+  int2* d_hub_items = nullptr;  // (heavy index, chunk) items of the hub pull
+  int64_t n_hub_items = 0;
+  int32_t* d_hidx_of = nullptr;  // vertex -> index in the heavy list (-1 for light)
+  int32_t n_heavy = 0;
+  int32_t heavy_thr = -1;
+  uint64_t version = 0;  // bumped whenever the heavy-vertex arrays are rebuilt
+};
+
+namespace xbe {
+
+using xbi::fail;
+
+// Edges per work item of the heavy-vertex table scan.
+constexpr int kTableChunk = 4096;
+// Vertices above this degree (hubs) are pulled in chunks by many warps; the
+// other heavy vertices by one warp each.
+constexpr int kHubDegree = 4096;
+constexpr int kHubChunk = 2048;
+// Parent slots per heavy vertex: up to 64 sources x 4 words.
+constexpr int kHparRow = 256;
+
+struct WsLayout {
+  size_t seen, F, N, p01, ph, pushed, p8, touched, fl_light, fl_heavy, nl_light, nl_heavy, stamp, total;
+  int64_t plane_stride;  // in words
+  int nplanes_alloc;
+};
+
+inline int bitlen_levels(int64_t n) {
+  // levels are in [0, n-1]; number of bits to hold n-1, at least 3
+  int b = 0;
+  int64_t x = n > 1 ? n - 1 : 0;
+  while (x) {
+    b++;
+    x >>= 1;
+  }
+  return std::max(3, b);
+}
+
+inline size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
+
+inline WsLayout layout_for(int64_t n, int word_bytes, int nw) {
+  WsLayout L{};
+  const size_t sw = align_up((size_t)n * nw * word_bytes);
+  const size_t li = align_up((size_t)std::max<int64_t>(n, 1) * 4);
+  L.nplanes_alloc = bitlen_levels(n);
+  L.plane_stride = (int64_t)(sw / word_bytes);
+  size_t o = 0;
+  L.seen = o; o += sw;
+  L.F = o; o += sw;
+  L.N = o; o += sw;
+  L.p01 = o; o += 2 * sw;
+  L.ph = o; o += sw * (L.nplanes_alloc - 2);
+  L.pushed = o; o += sw;
+  L.p8 = o; o += align_up((size_t)n * nw * word_bytes * 8);  // 8 position planes per (vertex, word)
+  L.touched = o; o += li;
+  L.fl_light = o; o += li;
+  L.fl_heavy = o; o += li;
+  L.nl_light = o; o += li;
+  L.nl_heavy = o; o += li;
+  L.stamp = o; o += li;
+  L.total = o;
+  return L;
+}
+
+// Builds (or keeps) the graph's heavy-vertex arrays for cutoff thr.
+xb_status ensure_heavy(xb_graph* g, int thr);
+
+// Releases the batched path's resources of a context.
+void batch_state_free(BatchState* b);
+// Drops the batched path's cached graphs that reference g.
+void batch_forget_graph(xb_ctx* c, const xb_graph* g);
+
+struct ClassTimer {
+  xb_ctx* c;
+  xb_stats* st;
+  bool on;
+  void begin() {
+    if (on) cudaEventRecord(c->evc0, c->stream);
+  }
+  void end(int cls, int64_t launches) {
+    if (st) st->class_launches[cls] += launches;
+    if (!on) return;
+    cudaEventRecord(c->evc1, c->stream);
+    cudaEventSynchronize(c->evc1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->evc0, c->evc1);
+    if (st) st->class_ms[cls] += ms;
+  }
+};
+
+template <typename W, int NW, typename OffT>
+int64_t level_bytes(const xbk::BatchCtr& b) {
+  return xbk::level_bytes_of(b, (int)sizeof(OffT) * 2, (int)sizeof(W), NW);
+}
+
+template <typename W, int NW, typename OffT>
+int64_t table_bytes(const xbk::BatchCtr& b, int64_t n, int kb) {
+  return xbk::table_bytes_of(b, n, kb, (int)sizeof(OffT) * 2, (int)sizeof(W), NW);
+}
+
+// Pointers and constants of one traversal pass (a workspace + counters).
+template <typename W, int NW, typename OffT>
+struct PassRes {
+  int64_t n = 0;
+  const OffT* ro = nullptr;
+  const int32_t* ci = nullptr;
+  W* seen = nullptr;
+  W* buf[2] = {nullptr, nullptr};  // frontier words; buf[cur] = F, buf[cur ^ 1] = N
+  xbk::Planes<W, NW> pl{};
+  W* pushed = nullptr;
+  W* ppos = nullptr;
+  int32_t* touched = nullptr;
+  xbk::Lists lists[2] = {};  // lists[cur] = current frontier, lists[cur ^ 1] = next
+  int32_t* stamp = nullptr;
+  xbk::Ctrs* ctr = nullptr;
+  int32_t* hpar = nullptr;
+  int heavy = 256;
+  size_t state_bytes = 0, plane_bytes = 0, ppos_bytes = 0;
+  int nplanes_alloc = 3;
+};
+
+template <typename W, int NW, typename OffT>
+PassRes<W, NW, OffT> pass_res(const xb_graph* g, void* ws, const WsLayout& L, xbk::Ctrs* ctr, int32_t* hpar,
+                              int heavy) {
+  PassRes<W, NW, OffT> p;
+  char* base = (char*)ws;
+  p.n = g->n;
+  p.ro = (const OffT*)g->d_ro;
+  p.ci = g->d_ci;
+  p.seen = (W*)(base + L.seen);
+  p.buf[0] = (W*)(base + L.F);
+  p.buf[1] = (W*)(base + L.N);
+  p.pl = xbk::Planes<W, NW>{(W*)(base + L.p01), (W*)(base + L.ph), L.plane_stride};
+  p.pushed = (W*)(base + L.pushed);
+  p.ppos = (W*)(base + L.p8);
+  p.touched = (int32_t*)(base + L.touched);
+  p.lists[0] = xbk::Lists{(int32_t*)(base + L.fl_light), (int32_t*)(base + L.fl_heavy)};
+  p.lists[1] = xbk::Lists{(int32_t*)(base + L.nl_light), (int32_t*)(base + L.nl_heavy)};
+  p.stamp = (int32_t*)(base + L.stamp);
+  p.ctr = ctr;
+  p.hpar = hpar;
+  p.heavy = heavy;
+  p.state_bytes = (size_t)g->n * NW * sizeof(W);
+  p.plane_bytes = (size_t)L.plane_stride * sizeof(W);
+  p.ppos_bytes = p.state_bytes * 8;
+  p.nplanes_alloc = L.nplanes_alloc;
+  return p;
+}
+
+template <typename W, int NW>
+xbk::Masks<W, NW> active_mask(int kb) {
+  constexpr int B = xbk::WB<W>::bits;
+  xbk::Masks<W, NW> a{};
+  for (int i = 0; i < NW; i++) {
+    const int lo = i * B, hi = std::min(kb, (i + 1) * B);
+    W m = 0;
+    for (int b = lo; b < hi; b++) m |= (W)1 << (b - lo);
+    a.w[i] = m;
+  }
+  return a;
+}
+
+// Launch shapes of the level-step kernels.
+struct StepShape {
+  int push_light_grid;   // 0: skip
+  dim3 push_heavy_grid;  // .y == 0: skip
+  int finalize_grid;
+  int pull_grid;
+  int heavy_grid;
+  int hub_grid;
+  int commit_grid;
+  int clear_grid;
+};
+
+template <typename W, int NW>
+constexpr int pull_warps() {
+  // the pull tile keeps 8 position words per lane and word in shared memory
+  return (xbk::WB<W>::bits * NW * 32 * 8 > 40 * 1024) ? 4 : 8;
+}
+
+// Pass start: clear the per-pass state, reset counters, seed the sources.
+template <typename W, int NW, typename OffT>
+xb_status emit_pass_init(const PassRes<W, NW, OffT>& p, const xb_graph* g, const int32_t* src, int kb,
+                         cudaStream_t s, int sms, bool clear_frontiers = false) {
+  if (clear_frontiers) {  // a workspace shared by passes of other layouts: F, N and the stamps start zero
+    XB_CUDA(cudaMemsetAsync(p.buf[0], 0, p.state_bytes, s));
+    XB_CUDA(cudaMemsetAsync(p.buf[1], 0, p.state_bytes, s));
+    XB_CUDA(cudaMemsetAsync(p.stamp, 0, sizeof(int32_t) * (size_t)p.n, s));
+  }
+  XB_CUDA(cudaMemsetAsync(p.seen, 0, p.state_bytes, s));
+  XB_CUDA(cudaMemsetAsync(p.pl.p01, 0, 2 * p.plane_bytes, s));
+  XB_CUDA(cudaMemsetAsync(p.pl.ph, 0, p.plane_bytes, s));
+  XB_CUDA(cudaMemsetAsync(p.pushed, 0, p.state_bytes, s));
+  XB_CUDA(cudaMemsetAsync(p.ppos, 0, p.ppos_bytes, s));
+  if (g->n_heavy > 0) {  // parent slots of the heavy vertices (hub pulls fold in with atomicMin)
+    const int64_t hcount = (int64_t)g->n_heavy * kHparRow;
+    xbk::k_fill<int32_t><<<(int)std::min<int64_t>((hcount + 255) / 256, (int64_t)sms * 8), 256, 0, s>>>(p.hpar, hcount,
+                                                                                                   INT32_MAX);
+  }
+  xbk::k_pass_init<<<1, 1, 0, s>>>(p.ctr, (long long)g->m);
+  xbk::k_init_batch<W, NW, OffT><<<1, 256, 0, s>>>(src, kb, p.ro, p.buf[0], p.seen, p.pl, active_mask<W, NW>(kb),
+                                                   p.heavy, p.lists[0], p.ctr);
+  XB_LAUNCH_CHECK("pass init");
+  return XB_OK;
+}
+
+template <typename W, int NW, typename OffT>
+xb_status emit_push(const PassRes<W, NW, OffT>& p, const xb_graph* g, int cur, const StepShape& sh, int kb,
+                    cudaStream_t s, int64_t* launches) {
+  constexpr int PUSH_CHUNK = 2048;
+  W* F = p.buf[cur];
+  W* N = p.buf[cur ^ 1];
+  const xbk::Lists fl = p.lists[cur], nl = p.lists[cur ^ 1];
+  if (sh.push_light_grid > 0) {
+    xbk::k_push_light<W, NW, OffT><<<sh.push_light_grid, 256, 0, s>>>(fl.light, &p.ctr->lv[cur].n_light, p.ro, p.ci, F,
+                                                                      p.seen, N, p.stamp, p.touched, p.ctr, cur);
+    (*launches)++;
+  }
+  if (sh.push_heavy_grid.y > 0) {
+    xbk::k_push_heavy<W, NW, OffT><<<sh.push_heavy_grid, 256, 0, s>>>(fl.heavy, &p.ctr->lv[cur].n_heavy, p.ro, p.ci, F,
+                                                                      p.seen, N, p.stamp, p.touched, p.ctr, cur,
+                                                                      PUSH_CHUNK);
+    xbk::k_clear_list<W, NW><<<sh.clear_grid, 256, 0, s>>>(fl.heavy, &p.ctr->lv[cur].n_heavy, F);
+    *launches += 2;
+  }
+  xbk::k_push_finalize<W, NW, OffT><<<sh.finalize_grid, 256, 0, s>>>(p.touched, p.ro, N, p.seen, p.pl,
+                                                                     active_mask<W, NW>(kb), p.heavy, nl, p.ctr, cur,
+                                                                     p.pushed);
+  (*launches)++;
+  XB_LAUNCH_CHECK("push step");
+  return XB_OK;
+}
+
+template <typename W, int NW, typename OffT>
+xb_status emit_pull(const PassRes<W, NW, OffT>& p, const xb_graph* g, int cur, const StepShape& sh, int kb,
+                    cudaStream_t s, int64_t* launches) {
+  constexpr int PW = pull_warps<W, NW>();
+  W* F = p.buf[cur];
+  W* N = p.buf[cur ^ 1];
+  const xbk::Lists fl = p.lists[cur], nl = p.lists[cur ^ 1];
+  const xbk::Masks<W, NW> active = active_mask<W, NW>(kb);
+  xbk::k_pull_tiles<W, NW, OffT, PW, 4><<<sh.pull_grid, PW * 32, 0, s>>>(p.n, p.ro, p.ci, F, p.seen, N, p.pl, active,
+                                                                         p.heavy, nl, p.ctr, cur, p.ppos);
+  (*launches)++;
+  if (g->n_heavy > 0) {
+    xbk::k_pull_heavy<W, NW, OffT, 4><<<sh.heavy_grid, 256, 0, s>>>(g->d_heavy, g->n_heavy, p.ro, p.ci, F, p.seen, N,
+                                                                    p.pl, active, p.heavy, kHubDegree, nl, p.ctr, cur,
+                                                                    p.hpar);
+    (*launches)++;
+    if (g->n_hub_items > 0) {
+      xbk::k_pull_hubs<W, NW, OffT, 4><<<sh.hub_grid, 256, 0, s>>>(g->d_heavy, g->d_hub_items, g->n_hub_items, p.ro,
+                                                                   p.ci, F, p.seen, N, active, p.ctr, cur, kHubChunk,
+                                                                   p.hpar);
+      xbk::k_pull_hub_commit<W, NW, OffT><<<sh.commit_grid, 256, 0, s>>>(g->d_heavy, g->n_heavy, p.ro, p.seen, N, p.pl,
+                                                                        active, p.heavy, kHubDegree, nl, p.ctr, cur);
+      *launches += 2;
+    }
+  }
+  xbk::k_clear_frontier<W, NW><<<sh.clear_grid, 256, 0, s>>>(F, p.n, fl, p.ctr, cur);
+  (*launches)++;
+  XB_LAUNCH_CHECK("pull step");
+  return XB_OK;
+}
+
+// Table pass of one pass (all its words).  rows (device) holds 2*B row
+// pointers per word: rows[wi*2B + s] is the level row and rows[wi*2B + B + s]
+// the parent row of the word's source s.
+template <typename W, int NW, typename OffT>
+xb_status emit_tables(const PassRes<W, NW, OffT>& p, const xb_graph* g, const int32_t* src, int kb,
+                      int32_t* const* rows, bool search_heavy, cudaStream_t s, int sms, int64_t* launches) {
+  constexpr int B = xbk::WB<W>::bits;
+  constexpr int TAB_WARPS = (B == 64) ? 4 : 8;
+  const int64_t ntiles = (p.n + 31) / 32;
+  const int tab_grid = (int)std::max<int64_t>(1, std::min<int64_t>((ntiles + TAB_WARPS - 1) / TAB_WARPS, (int64_t)sms * 16));
+  for (int wi = 0; wi < NW; wi++) {
+    const int kbw = std::min(B, kb - wi * B);
+    if (kbw <= 0) break;
+    const int32_t* wsrc = src + wi * B;
+    if (g->n_heavy > 0 && search_heavy) {
+      // heavy vertices reached by a push step at level >= 2: search their parents
+      const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(g->n_hitems, (int64_t)sms * 8));
+      xbk::k_tables_heavy_scan<W, NW, OffT><<<grid, 256, 0, s>>>(g->d_heavy, g->d_hitems, g->n_hitems, p.ro, p.ci,
+                                                                 p.seen, p.pl, wi, kTableChunk, p.hpar, p.ctr,
+                                                                 p.pushed);
+      (*launches)++;
+    }
+    xbk::k_tables<W, NW, OffT, TAB_WARPS, 4><<<tab_grid, TAB_WARPS * 32, 0, s>>>(
+        p.n, p.ro, p.ci, p.seen, p.pl, wi, kbw, p.heavy, rows + (int64_t)wi * 2 * B, p.ctr, p.ppos, p.pushed, wsrc,
+        g->d_hidx_of, p.hpar);
+    (*launches)++;
+  }
+  XB_LAUNCH_CHECK("tables");
+  return XB_OK;
+}
+
+// Fills a pass's row-pointer table (host side, 2*B per word) for kb sources
+// whose level / parent rows start at lv0 / pr0 and follow each other every n
+// int32.
+template <typename W, int NW>
+void fill_rows(int32_t** rows, int kb, int32_t* lv0, int32_t* pr0, int64_t n) {
+  constexpr int B = xbk::WB<W>::bits;
+  for (int wi = 0; wi < NW; wi++)
+    for (int s = 0; s < B; s++) {
+      const int j = wi * B + s;
+      rows[wi * 2 * B + s] = j < kb ? lv0 + (int64_t)j * n : nullptr;
+      rows[wi * 2 * B + B + s] = j < kb ? pr0 + (int64_t)j * n : nullptr;
+    }
+}
+
+template <typename W, int NW, typename OffT>
+StepShape max_shape(const xb_graph* g, int sms) {
+  constexpr int PW = pull_warps<W, NW>();
+  StepShape sh{};
+  const int64_t n = g->n;
+  const int64_t ntiles = (n + 31) / 32;
+  sh.push_light_grid = sms * 16;
+  sh.push_heavy_grid = dim3((unsigned)std::max<int64_t>(1, std::min<int64_t>((g->max_deg + 2047) / 2048, 64)),
+                            (unsigned)std::max<int64_t>(1, std::min<int64_t>(g->n_heavy, 65535)));
+  if (g->n_heavy == 0) sh.push_heavy_grid.y = 0;
+  sh.finalize_grid = (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)sms * 8));
+  sh.pull_grid = (int)std::max<int64_t>(1, std::min<int64_t>((ntiles + PW - 1) / PW, (int64_t)sms * 8));
+  sh.heavy_grid = (int)std::max<int64_t>(1, std::min<int64_t>((g->n_heavy + 7) / 8, (int64_t)sms * 16));
+  sh.hub_grid = (int)std::max<int64_t>(1, std::min<int64_t>((g->n_hub_items + 7) / 8, (int64_t)sms * 16));
+  sh.commit_grid = (int)std::max<int64_t>(1, std::min<int64_t>((g->n_heavy + 255) / 256, (int64_t)sms * 4));
+  sh.clear_grid = sms * 8;
+  return sh;
+}
+
+// Launch shapes for steps the device decides (a captured graph): the count-
+// driven kernels stride over whatever the frontier holds, so their grids are
+// fixed, bounded by the graph's size and by a few waves of the GPU.
+template <typename W, int NW, typename OffT>
+StepShape graph_shape(const xb_graph* g, int sms) {
+  StepShape sh = max_shape<W, NW, OffT>(g, sms);
+  const int64_t n = g->n;
+  sh.push_light_grid = (int)std::max<int64_t>(1, std::min<int64_t>((n + 7) / 8, (int64_t)sms * 16));
+  if (g->n_heavy > 0)
+    sh.push_heavy_grid = dim3((unsigned)std::max<int64_t>(1, std::min<int64_t>((g->max_deg + 2047) / 2048, 16)),
+                              (unsigned)std::min<int64_t>(g->n_heavy, sms));
+  sh.clear_grid = (int)std::max<int64_t>(1, std::min<int64_t>((n * NW + 255) / 256, (int64_t)sms * 8));
+  return sh;
+}
+
+}  // namespace xbe

@@ -104,6 +104,7 @@ struct BatchCtr {
   int32_t pushed_deep;  // a push step reached level >= 2
   int32_t push_levels;
   int32_t pull_levels;
+  int32_t step_calls;  // k_step_begin calls of the pass ("done" included)
 };
 
 struct Ctrs {
@@ -946,8 +947,9 @@ __global__ void k_fill(T* p, int64_t count, T value) {
 }
 
 // ---------------------------------------------------------------------------
-// Table pass, word wi of the pass (sources word_base .. word_base+kbw-1; the
-// output pointers are already offset to row word_base).
+// Table pass, word wi of the pass (its sources wsrc[0..kbw)).  rows[s] and
+// rows[B + s] are the level and parent rows (n int32 each) of source s, so the
+// sources of one word may belong to different queries and output buffers.
 //
 // The vertex's own level classes: root = the vertex is the source (level 0 is
 // the only level with every plane bit clear); lvl1 = level exactly 1, whose
@@ -977,8 +979,7 @@ template <typename W, int NW, typename OffT, int WARPS, int U>
 __global__ void __launch_bounds__(WARPS * 32) k_tables(int64_t n, const OffT* __restrict__ ro,
                                                        const int32_t* __restrict__ ci, const W* __restrict__ seen,
                                                        Planes<W, NW> pl, int wi, int kbw, int heavy,
-                                                       int32_t* __restrict__ level_out,
-                                                       int32_t* __restrict__ parent_out, Ctrs* ctr,
+                                                       int32_t* const* __restrict__ rows, Ctrs* ctr,
                                                        const W* __restrict__ ppos, const W* __restrict__ pushed,
                                                        const int32_t* __restrict__ wsrc,
                                                        const int32_t* __restrict__ hidx_of,
@@ -988,7 +989,12 @@ __global__ void __launch_bounds__(WARPS * 32) k_tables(int64_t n, const OffT* __
   const int nplanes = ctr->b.nplanes;
   __shared__ int32_t s_par[WARPS][B][32];
   __shared__ int32_t s_src[B];
-  for (int s = threadIdx.x; s < B; s += blockDim.x) s_src[s] = s < kbw ? wsrc[s] : -1;
+  __shared__ int32_t* s_row[2][B];
+  for (int s = threadIdx.x; s < B; s += blockDim.x) {
+    s_src[s] = s < kbw ? wsrc[s] : -1;
+    s_row[0][s] = s < kbw ? rows[s] : nullptr;
+    s_row[1][s] = s < kbw ? rows[B + s] : nullptr;
+  }
   __syncthreads();
   __shared__ int32_t s_off[WARPS][33];
   __shared__ int64_t s_pos[WARPS][32];
@@ -1151,8 +1157,8 @@ __global__ void __launch_bounds__(WARPS * 32) k_tables(int64_t n, const OffT* __
                 pr = __ldg(&ci[beg + idx]);
               }
             }
-            __stcs(&level_out[(int64_t)s * n + v], lv);
-            __stcs(&parent_out[(int64_t)s * n + v], pr);
+            __stcs(&s_row[0][s][v], lv);
+            __stcs(&s_row[1][s][v], pr);
           }
         }
       }
@@ -1289,10 +1295,14 @@ static __global__ void k_step_begin(Ctrs* ctr, int cur, float alpha, int nplanes
   BatchCtr& b = ctr->b;
   const LevelCtr& lc = ctr->lv[cur];
   int dir = 2;
+  b.step_calls += 1;
+  b.zero_plane = -1;  // k_zero_plane runs after every decision in a graph, "done" included
+  // a traversal has at most n <= 2^nplanes_alloc levels; a frontier still alive
+  // beyond that means corrupted state: stop the loop and flag it
+  if (b.dir != 2 && b.err == 0 && b.level >= (1 << nplanes_alloc)) b.err = 2;
   if (b.dir != 2 && b.err == 0 && (long long)lc.n_light + lc.n_heavy > 0) {
     dir = ((double)lc.edges * (double)alpha > (double)b.m_unfinished) ? 1 : 0;
     b.level += 1;
-    b.zero_plane = -1;
     if (b.nplanes < nplanes_alloc && (1 << b.nplanes) <= b.level) {
       b.zero_plane = b.nplanes;
       b.nplanes += 1;
@@ -1348,15 +1358,48 @@ static __global__ void k_loop_end(const Ctrs* ctr, int cur_next, cudaGraphCondit
   cudaGraphSetConditional(hwhile, more ? 1u : 0u);
 }
 
+// Algorithmic bytes of a pass's level steps: the row-offset pair (R bytes) of
+// every scanned vertex, colIndices + the gathered frontier words of every
+// scanned edge, and a three-word sweep (seen read, seen and next-frontier
+// write) of every swept vertex.  wsz = bytes per word, nw = words per vertex.
+__host__ __device__ inline long long level_bytes_of(const BatchCtr& b, int R, int wsz, int nw) {
+  const long long wb = (long long)wsz * nw;
+  return (long long)R * (long long)b.vertices_scanned + (4 + wb) * (long long)b.edges_scanned +
+         3 * wb * (long long)b.vertices_swept;
+}
+
+// Algorithmic bytes of a pass's table pass: per vertex its row offsets, seen,
+// level planes and parent-position planes (per word), the colIndices entry of
+// every recorded parent, colIndices + gathered plane pair of every searched
+// edge, and the two written tables (kb rows of n int32 each).
+__host__ __device__ inline long long table_bytes_of(const BatchCtr& b, long long n, int kb, int R, int wsz, int nw) {
+  return (long long)nw * n * (R + (long long)wsz * (1 + b.nplanes + 8)) + 4 * (long long)b.reached +
+         (4 + 2 * (long long)wsz) * (long long)b.parent_edges + 8 * (long long)kb * n;
+}
+
 // Per-call totals over passes (device).
 struct PassSum {
   unsigned long long edges_traversed, reached, edges_scanned, vertices_scanned, vertices_swept, parent_edges;
+  unsigned long long level_bytes, table_bytes;
+  unsigned long long launches;  // kernels the passes ran (graph mode)
   int32_t max_level, push_levels, pull_levels, passes;
+  int32_t errors;  // passes that ended with BatchCtr::err set
+  int32_t pad;
 };
 
-static __global__ void k_pass_accum(const Ctrs* ctr, PassSum* sum) {
+// Folds a finished pass (n vertices, kb sources; R, wsz, nw as in
+// level_bytes_of) into the totals.  Kernel count of a pass run by a graph:
+// fixed_k outside the level loop (this one included), two per step decision
+// (k_step_begin, k_zero_plane), one k_loop_end per two decisions, and push_k /
+// pull_k per push / pull step.
+static __global__ void k_pass_accum(const Ctrs* ctr, PassSum* sum, long long n, int kb, int R, int wsz, int nw,
+                                    int fixed_k, int push_k, int pull_k) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   const BatchCtr& b = ctr->b;
+  sum->launches += (unsigned long long)(fixed_k + 2 * b.step_calls + b.step_calls / 2 + push_k * b.push_levels +
+                                        pull_k * b.pull_levels);
+  sum->level_bytes += (unsigned long long)level_bytes_of(b, R, wsz, nw);
+  sum->table_bytes += (unsigned long long)table_bytes_of(b, n, kb, R, wsz, nw);
   sum->edges_traversed += b.edges_traversed;
   sum->reached += b.reached;
   sum->edges_scanned += b.edges_scanned;
@@ -1367,6 +1410,7 @@ static __global__ void k_pass_accum(const Ctrs* ctr, PassSum* sum) {
   sum->push_levels += b.push_levels;
   sum->pull_levels += b.pull_levels;
   sum->passes += 1;
+  if (b.err) sum->errors += 1;
 }
 
 }  // namespace xbk

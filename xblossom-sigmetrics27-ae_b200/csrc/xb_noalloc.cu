@@ -53,7 +53,8 @@ constexpr size_t kListsOff = kP8Off + 8 * kW;                     // 6 int32 lis
 constexpr size_t kCtrOff = kListsOff + 3 * kW;
 constexpr size_t kCtrWords = (sizeof(xbk::Ctrs) + 7) / 8;
 constexpr size_t kMiscOff = kCtrOff + kCtrWords;  // int32 heavy count, int32 error flag
-constexpr size_t kTotalWords = kMiscOff + 4;
+constexpr size_t kRowsOff = kMiscOff + 4;          // 2 x 64 row pointers of the table pass
+constexpr size_t kTotalWords = kRowsOff + 128;
 
 constexpr int kHeavy = 2048;
 constexpr float kAlpha = 4.0f;
@@ -159,6 +160,7 @@ extern "C" xb_status xb_traverse_noalloc(int64_t n, const int32_t* row_offsets, 
   int32_t* heavy_list = lists + 5 * kW;
   xbk::Ctrs* ctr = (xbk::Ctrs*)(scratch + kCtrOff);
   int32_t* misc = (int32_t*)(scratch + kMiscOff);  // [0] heavy count, [1] validation error
+  int32_t** rows = (int32_t**)(scratch + kRowsOff);
   const size_t plane_bytes = sizeof(W) * kW;
   const size_t state_bytes = sizeof(W) * (size_t)n;
 
@@ -251,11 +253,19 @@ extern "C" xb_status xb_traverse_noalloc(int64_t n, const int32_t* row_offsets, 
       std::swap(fl, nl);
       cur ^= 1;
     }
+    if (h.b.err) return fail(XB_ERR_STATE, "the level loop ran past the level bound (corrupted traversal state)");
     max_levels = std::max(max_levels, h.b.level);
     // every vertex takes the edge-flat table path here (no heavy-vertex staging)
+    int32_t* hrows[2 * B];
+    for (int j = 0; j < B; j++) {
+      hrows[j] = j < kb ? level + (k0 + j) * n : nullptr;
+      hrows[B + j] = j < kb ? parent + (k0 + j) * n : nullptr;
+    }
+    // pageable source: the copy has taken hrows by the time the call returns
+    NA_CUDA(cudaMemcpyAsync(rows, hrows, sizeof(hrows), cudaMemcpyHostToDevice, sm));
     xbk::k_tables<W, 1, int32_t, TAB_WARPS, U><<<tab_grid, TAB_WARPS * 32, 0, sm>>>(
-        n, row_offsets, col_indices, seen, pl, 0, kb, INT32_MAX, level + k0 * n, parent + k0 * n, ctr, ppos, pushed,
-        sources + k0, nullptr, nullptr);
+        n, row_offsets, col_indices, seen, pl, 0, kb, INT32_MAX, rows, ctr, ppos, pushed, sources + k0, nullptr,
+        nullptr);
     NA_CUDA(cudaGetLastError());
     NA_CUDA(cudaMemcpyAsync(&h, ctr, sizeof(h), cudaMemcpyDeviceToHost, sm));
     NA_CUDA(cudaStreamSynchronize(sm));

@@ -10,6 +10,7 @@ Reference-facing names (paths relative to the X-Blossom project):
                                    apps/xb/src/include/graph/hgraph.h:37-48
   Context.upload(csr)           <- zblossom::DGraph(const HGraph&)
                                    apps/xb/src/include/graph/dgraph.h:50-63
+  Context.traverse_batched(...) <- (no counterpart: many queries per launch)
   Context.traverse(...)         <- the expand phase of
                                    apps/xb/src/xblsm_gpu/xblossom_gpu_engine_10.cu:270-359
                                    returning level (root_distance_) and parent
@@ -82,6 +83,18 @@ class XbTuning(C.Structure):
         ("pull_alpha", C.c_float),
         ("heavy_degree", C.c_int32),
         ("timing", C.c_int32),
+        ("chains", C.c_int32),
+    ]
+
+
+class XbBatchItem(C.Structure):
+    _fields_ = [
+        ("graph", C.c_void_p),
+        ("sources", C.c_void_p),
+        ("k", C.c_int32),
+        ("flags", C.c_uint32),
+        ("level", C.c_void_p),
+        ("parent", C.c_void_p),
     ]
 
 
@@ -124,6 +137,7 @@ def lib() -> C.CDLL:
         "xb_graph_info": (i32, [vp, P(i64), P(i64), P(i64)]),
         "xb_select_sources": (i32, [vp, u64, i32, vp]),
         "xb_traverse": (i32, [vp, vp, vp, i32, i32, vp, vp, vp, vp, u32, P(XbStats)]),
+        "xb_traverse_batched": (i32, [vp, P(XbBatchItem), i32, P(XbStats)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -353,6 +367,61 @@ class Context:
         _check(lib().xb_traverse(self._h, graph._h, sptr, k, XB_MODE_PLAIN, None, lp, pp, None, flags,
                                  C.byref(st)))
         return TraversalResult(level, parent, st.as_dict())
+
+    def traverse_batched(self, queries, out: str = "device", outputs=None) -> tuple[list, dict]:
+        """All queries in one launch through xb_traverse_batched.
+
+        queries: list of (graph, sources) pairs (sources as in traverse).
+        out="device": torch int32 CUDA tensors (k, n) per query; out="host":
+        numpy views of page-locked torch tensors (the launch copies into
+        them).  outputs: optional list of (level, parent) to fill instead
+        (device tensors, or page-locked host tensors / arrays for "host").
+        Returns ([TraversalResult per query], batch stats).
+        """
+        import torch
+
+        items = (XbBatchItem * max(len(queries), 1))()
+        keep, results = [], []
+        dev = torch.device("cuda", self.device)
+        for i, (graph, sources) in enumerate(queries):
+            flags = 0
+            if hasattr(sources, "data_ptr"):
+                flags |= XB_SOURCES_DEVICE
+                k = int(sources.numel())
+                sptr = sources.data_ptr()
+                keep.append(sources)
+            else:
+                arr = np.ascontiguousarray(sources, dtype=np.int32)
+                keep.append(arr)
+                k = len(arr)
+                sptr = arr.ctypes.data
+            n = graph.n
+            if outputs is not None:
+                level, parent = outputs[i]
+            elif out == "device":
+                level = torch.empty((k, n), dtype=torch.int32, device=dev)
+                parent = torch.empty((k, n), dtype=torch.int32, device=dev)
+            else:
+                level = torch.empty((k, n), dtype=torch.int32, pin_memory=True)
+                parent = torch.empty((k, n), dtype=torch.int32, pin_memory=True)
+            if out == "device":
+                flags |= XB_OUT_DEVICE
+            keep.extend([level, parent])
+
+            def ptr(t):
+                return t.data_ptr() if hasattr(t, "data_ptr") else t.ctypes.data
+
+            items[i] = XbBatchItem(graph._h.value, sptr if k else None, k, flags, ptr(level) if k else None,
+                                   ptr(parent) if k else None)
+            if out == "host" and hasattr(level, "numpy"):
+                level, parent = level.numpy(), parent.numpy()
+            results.append([level, parent])
+        if out == "device":
+            torch.cuda.synchronize(dev)
+        st = XbStats()
+        _check(lib().xb_traverse_batched(self._h, items, len(queries), C.byref(st)))
+        stats = st.as_dict()
+        return [TraversalResult(lv, pr, {}) for lv, pr in results], stats
 
     def close(self) -> None:
         if self._h and self._h.value:
