@@ -217,6 +217,8 @@ def main() -> None:
     ap.add_argument("--path", default="batched", choices=["batched", "plain"],
                     help="path the headline value measures (both are timed)")
     ap.add_argument("--chains", type=int, default=0, help="batched chains (0: tuned default)")
+    ap.add_argument("--plain-only", action="store_true",
+                    help="time the plain path only (short runs for kernel profiles)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
@@ -327,10 +329,14 @@ def main() -> None:
     ctx.set_tuning(timing=0)
 
     # batched path: the whole step is one CUDA-graph launch
-    for _ in range(args.warmup):
-        batched_step()
     clocks = ClockSampler(local)
-    b_ms, b_agg, clk = timed(batched_step, args.steps, clocks)
+    if args.plain_only:
+        args.path = "plain"
+        b_ms, b_agg, clk = plain_ms, plain_agg, {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["not sampled"]}
+    else:
+        for _ in range(args.warmup):
+            batched_step()
+        b_ms, b_agg, clk = timed(batched_step, args.steps, clocks)
     edges_total = sum_over_ranks(b_agg["edges_traversed"])
     value = edges_total / (b_ms / 1e3) / 1e9
     headline = value if args.path == "batched" else plain_gteps

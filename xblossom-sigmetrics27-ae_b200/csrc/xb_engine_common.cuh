@@ -333,7 +333,7 @@ template <typename W, int NW, typename OffT>
 xb_status emit_tables(const PassRes<W, NW, OffT>& p, const xb_graph* g, const int32_t* src, int kb,
                       int32_t* const* rows, bool search_heavy, cudaStream_t s, int sms, int64_t* launches) {
   constexpr int B = xbk::WB<W>::bits;
-  constexpr int TAB_WARPS = (B == 64) ? 4 : 8;
+  constexpr int TAB_WARPS = 4;
   const int64_t ntiles = (p.n + 31) / 32;
   const int tab_grid = (int)std::max<int64_t>(1, std::min<int64_t>((ntiles + TAB_WARPS - 1) / TAB_WARPS, (int64_t)sms * 16));
   for (int wi = 0; wi < NW; wi++) {

@@ -541,7 +541,7 @@ __device__ __forceinline__ WinOwner window_owner(int32_t off, int32_t d, int32_t
 // of sources costs at most 8 ORs and the table pass reads parents instead of
 // searching for them.  ppos must be zero at the start of the pass.
 template <typename W, int NW, typename OffT, int WARPS, int U>
-__global__ void __launch_bounds__(WARPS * 32) k_pull_tiles(int64_t n, const OffT* __restrict__ ro,
+__global__ void __launch_bounds__(WARPS * 32, 32 / WARPS) k_pull_tiles(int64_t n, const OffT* __restrict__ ro,
                                                            const int32_t* __restrict__ ci, const W* __restrict__ F,
                                                            W* seen, W* N, Planes<W, NW> pl, Masks<W, NW> active,
                                                            int heavy, Lists nl, Ctrs* ctr, int cur,
@@ -638,7 +638,11 @@ __global__ void __launch_bounds__(WARPS * 32) k_pull_tiles(int64_t n, const OffT
         const int32_t pos = o >= 0 ? e - s_off[wib][o] : 0;  // position in the owner's adjacency
 #pragma unroll
         for (int i = 0; i < NW; i++) {
-          W x = f[u][i];
+          // candidates: wanted bits of the owner this edge brings that no
+          // earlier window had; a window without any changes nothing
+          const W c = o >= 0 ? (f[u][i] & s_want[wib][o][i] & ~s_acc[wib][o][i]) : (W)0;
+          if (!__any_sync(0xffffffffu, c != 0)) continue;
+          W x = c;
 #pragma unroll
           for (int s = 1; s < 32; s <<= 1) {
             const W y = shfl_up<W>(x, s);
@@ -647,7 +651,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_pull_tiles(int64_t n, const OffT
           W ex = shfl_up<W>(x, 1);
           if (!(lane >= 1 && lane - 1 >= h)) ex = 0;
           if (o >= 0) {
-            const W claim = f[u][i] & s_want[wib][o][i] & ~ex & ~s_acc[wib][o][i];
+            const W claim = c & ~ex;
             if (claim && pos < kP8MaxDegree) {
               // bit k of this position goes to plane k of every claimed source
 #pragma unroll
@@ -778,8 +782,12 @@ __global__ void k_pull_heavy(const int32_t* __restrict__ hlist, int32_t nh, cons
       for (int u = 0; u < U; u++) {
 #pragma unroll
         for (int i = 0; i < NW; i++) {
+          // candidates: wanted bits this edge brings that no earlier round had;
+          // most rounds have none, and then nothing changes
+          const W c = f[u][i] & want[i] & ~acc[i];
+          if (!__any_sync(0xffffffffu, c != 0)) continue;
           W grp;
-          W claim = first_bits<W>(f[u][i], acc[i], &grp) & want[i];
+          W claim = first_bits<W>(c, 0, &grp);
           if (hpar == nullptr) claim = 0;  // caller searches these parents later
           while (claim) {
             const int b = ffs0(claim);
@@ -874,8 +882,10 @@ __global__ void k_pull_hubs(const int32_t* __restrict__ hlist, const int2* __res
       for (int u = 0; u < U; u++) {
 #pragma unroll
         for (int i = 0; i < NW; i++) {
+          const W c = f[u][i] & want[i] & ~acc[i];
+          if (!__any_sync(0xffffffffu, c != 0)) continue;
           W grp;
-          W claim = first_bits<W>(f[u][i], acc[i], &grp) & want[i];
+          W claim = first_bits<W>(c, 0, &grp);
           while (claim) {
             const int b = ffs0(claim);
             atomicMin(&hpar[idx * ROW + i * B + b], col[u]);
@@ -954,6 +964,32 @@ __global__ void k_fill(T* p, int64_t count, T value) {
 // The vertex's own level classes: root = the vertex is the source (level 0 is
 // the only level with every plane bit clear); lvl1 = level exactly 1, whose
 // only possible parent is the source itself.
+// Neighbours per vertex the table pass keeps in shared memory for the
+// recorded-position lookups.
+constexpr int kCiCache = 8;
+
+// 8x8 bit-matrix transpose (Hacker's Delight, 2nd ed., section 7-3): bit
+// 8r + c moves to bit 8c + r.
+__device__ __forceinline__ unsigned long long transpose8(unsigned long long x) {
+  unsigned long long t;
+  t = (x ^ (x >> 7)) & 0x00AA00AA00AA00AAull;
+  x ^= t ^ (t << 7);
+  t = (x ^ (x >> 14)) & 0x0000CCCC0000CCCCull;
+  x ^= t ^ (t << 14);
+  t = (x ^ (x >> 28)) & 0x00000000F0F0F0F0ull;
+  x ^= t ^ (t << 28);
+  return x;
+}
+
+// Byte b of each of 8 words, word r landing in byte r.
+template <typename W>
+__device__ __forceinline__ unsigned long long gather_bytes8(const W (&p)[8], int b) {
+  unsigned long long x = 0;
+#pragma unroll
+  for (int r = 0; r < 8; r++) x |= (unsigned long long)((p[r] >> (8 * b)) & 0xFF) << (8 * r);
+  return x;
+}
+
 template <typename W, int NW>
 __device__ __forceinline__ void vertex_levels(const W* __restrict__ seen, const Planes<W, NW>& pl, int nplanes,
                                               int64_t v, int wi, W& sv, W& p0, W& p1, W& root, W& lvl1) {
@@ -976,7 +1012,7 @@ __device__ __forceinline__ void vertex_levels(const W* __restrict__ seen, const 
 // exclusive prefix OR in edge order hands each needed bit to its first
 // (= smallest-id) matching neighbour.
 template <typename W, int NW, typename OffT, int WARPS, int U>
-__global__ void __launch_bounds__(WARPS * 32) k_tables(int64_t n, const OffT* __restrict__ ro,
+__global__ void __launch_bounds__(WARPS * 32, 32 / WARPS) k_tables(int64_t n, const OffT* __restrict__ ro,
                                                        const int32_t* __restrict__ ci, const W* __restrict__ seen,
                                                        Planes<W, NW> pl, int wi, int kbw, int heavy,
                                                        int32_t* const* __restrict__ rows, Ctrs* ctr,
@@ -987,7 +1023,6 @@ __global__ void __launch_bounds__(WARPS * 32) k_tables(int64_t n, const OffT* __
   constexpr int B = WB<W>::bits;
   constexpr int ROW = B * NW;
   const int nplanes = ctr->b.nplanes;
-  __shared__ int32_t s_par[WARPS][B][32];
   __shared__ int32_t s_src[B];
   __shared__ int32_t* s_row[2][B];
   for (int s = threadIdx.x; s < B; s += blockDim.x) {
@@ -1002,6 +1037,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_tables(int64_t n, const OffT* __
   __shared__ W s_t0[WARPS][32];
   __shared__ W s_t1[WARPS][32];
   __shared__ W s_found[WARPS][32];
+  __shared__ int32_t s_ci[WARPS][32][kCiCache + 1];
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
   const int64_t ntiles = (n + 31) >> 5;
@@ -1091,10 +1127,12 @@ __global__ void __launch_bounds__(WARPS * 32) k_tables(int64_t n, const OffT* __
         const int knext = __shfl_down_sync(0xffffffffu, k, 1);
         const bool tail = (lane == 31) || (knext != k);
         if (act) {
+          // first match of each needed bit: the parent goes straight to its
+          // row (the row pass below leaves these entries alone)
           W mine = eq & ~excl & ~s_found[wib][k];
           while (mine) {
             const int b = ffs0(mine);
-            s_par[wib][b][k] = col[u];
+            __stcs(&s_row[1][b][tile * 32 + k], col[u]);
             mine &= mine - 1;
           }
         }
@@ -1130,36 +1168,48 @@ __global__ void __launch_bounds__(WARPS * 32) k_tables(int64_t n, const OffT* __
         pp[k2 + 1] = t2[1];
       }
       const int32_t* hrow = is_heavy ? hpar + (int64_t)hidx_of[v] * ROW + wi * B : nullptr;
-      const W searched = need;
-      for (int s4 = 0; s4 < kbw; s4 += 4) {
+      // the first kCiCache neighbours of the vertex: most recorded positions
+      // point there (the first frontier neighbour of a large frontier)
+      int32_t* cic = s_ci[wib][lane];
+      if (use_pp) {
 #pragma unroll
-        for (int j4 = 0; j4 < 4; j4++) {
-          const int s = s4 + j4;
-          if (s < kbw) {
-            int32_t lv = -1, pr = -1;
-            if ((sv >> s) & 1) {
-              lv = 0;
+        for (int j = 0; j < kCiCache; j++) cic[j] = j < dg ? __ldg(&ci[beg + j]) : -1;
+      }
+      // eight sources at a time: level bytes and position bytes by 8x8 bit
+      // transposes of the planes (byte c of the result = source 8b + c); the
+      // per-source class bits come from one byte of each mask, and the parent
+      // is picked by selects (lanes of a warp rarely share a class).  Searched
+      // bits (need) already hold their parent.
+      const bool deep = nplanes > RP;
+#pragma unroll 1
+      for (int b8 = 0; b8 < B / 8; b8++) {
+        if (b8 * 8 >= kbw) break;
+        const unsigned long long lvx = transpose8(gather_bytes8<W>(plr, b8));
+        const unsigned long long ppx = use_pp ? transpose8(gather_bytes8<W>(pp, b8)) : 0ull;
+        const uint32_t svb = (uint32_t)(sv >> (8 * b8)) & 0xFFu;
+        const uint32_t rtb = (uint32_t)(root >> (8 * b8)) & 0xFFu;
+        const uint32_t l1b = (uint32_t)(lvl1 >> (8 * b8)) & 0xFFu;
+        const uint32_t ndb = (uint32_t)(need >> (8 * b8)) & 0xFFu;
+        const uint32_t far = svb & ~(ndb | rtb | l1b);  // recorded positions, possibly beyond the cache
 #pragma unroll
-              for (int j = 0; j < RP; j++) lv |= (int32_t)((plr[j] >> s) & 1) << j;
-              for (int j = RP; j < nplanes; j++) lv |= (int32_t)((pl.get(j, v, wi) >> s) & 1) << j;
-              if ((root >> s) & 1) {
-                pr = (int32_t)v;
-              } else if ((lvl1 >> s) & 1) {
-                pr = s_src[s];
-              } else if (hrow) {
-                pr = hrow[s];
-              } else if ((searched >> s) & 1 || !use_pp) {
-                pr = s_par[wib][s][lane];
-              } else {
-                int32_t idx = 0;
-#pragma unroll
-                for (int k = 0; k < 8; k++) idx |= (int32_t)((pp[k] >> s) & 1) << k;
-                pr = __ldg(&ci[beg + idx]);
-              }
-            }
-            __stcs(&s_row[0][s][v], lv);
-            __stcs(&s_row[1][s][v], pr);
+        for (int i = 0; i < 8; i++) {
+          const int s = b8 * 8 + i;
+          if (s >= kbw) break;
+          int32_t lv = (int32_t)((lvx >> (8 * i)) & 0xFF);
+          if (deep && ((svb >> i) & 1))
+            for (int j = RP; j < nplanes; j++) lv |= (int32_t)((pl.get(j, v, wi) >> s) & 1) << j;
+          const int idx = (int)((ppx >> (8 * i)) & 0xFF);
+          int32_t pr = cic[idx & (kCiCache - 1)];
+          if (idx >= kCiCache && ((far >> i) & 1) && !hrow) pr = __ldg(&ci[beg + idx]);
+          if (hrow) pr = hrow[s];
+          pr = ((l1b >> i) & 1) ? s_src[s] : pr;
+          pr = ((rtb >> i) & 1) ? (int32_t)v : pr;
+          if (!((svb >> i) & 1)) {
+            lv = -1;
+            pr = -1;
           }
+          __stcs(&s_row[0][s][v], lv);
+          if (!((ndb >> i) & 1)) __stcs(&s_row[1][s][v], pr);
         }
       }
     }
