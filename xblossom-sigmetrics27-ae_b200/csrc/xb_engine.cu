@@ -113,6 +113,33 @@ xb_status ensure_heavy(xb_graph* g, int thr) {
     }
     XB_CUDA(cudaMemcpy(g->d_hidx_of, hidx_of.data(), sizeof(int32_t) * (size_t)g->n, cudaMemcpyHostToDevice));
   }
+  {  // light vertices by falling degree (counting sort; ties by ascending id)
+    std::vector<int64_t> cnt((size_t)thr + 2, 0);
+    for (int64_t v = 0; v < g->n; v++) {
+      const int64_t d = g->h_ro[v + 1] - g->h_ro[v];
+      if (d >= 1 && d <= thr) cnt[(size_t)(thr - d)]++;
+    }
+    int64_t acc = 0;
+    for (auto& x : cnt) {
+      const int64_t c = x;
+      x = acc;
+      acc += c;
+    }
+    std::vector<int32_t> lorder((size_t)acc);
+    for (int64_t v = 0; v < g->n; v++) {
+      const int64_t d = g->h_ro[v + 1] - g->h_ro[v];
+      if (d >= 1 && d <= thr) lorder[(size_t)cnt[(size_t)(thr - d)]++] = (int32_t)v;
+    }
+    if (g->d_lorder) cudaFree(g->d_lorder);
+    g->d_lorder = nullptr;
+    if (cudaMalloc(&g->d_lorder, sizeof(int32_t) * std::max<size_t>(lorder.size(), 1)) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(XB_ERR_OOM, "light vertex list allocation failed");
+    }
+    if (!lorder.empty())
+      XB_CUDA(cudaMemcpy(g->d_lorder, lorder.data(), sizeof(int32_t) * lorder.size(), cudaMemcpyHostToDevice));
+    g->n_lorder = (int64_t)lorder.size();
+  }
   // (heavy index, chunk) work items of the table pass, heaviest vertices first
   // (ids ascend roughly with falling degree in R-MAT-like graphs, so this is
   // the list order)
@@ -394,8 +421,10 @@ xb_status xb_graph_upload(xb_ctx* c, int64_t n, const void* row_offsets, int32_t
   g->off64 = m >= (int64_t)INT32_MAX;
   for (int64_t v = 0; v < n; v++) g->max_deg = std::max(g->max_deg, ro[v + 1] - ro[v]);
   const size_t ro_bytes = (g->off64 ? 8 : 4) * (size_t)(n + 1);
+  // colIndices carries kCiPad zero entries past the end: the 16-byte loads of
+  // the per-lane pull read whole aligned groups of 4 entries
   if (cudaMalloc(&g->d_ro, ro_bytes) != cudaSuccess ||
-      cudaMalloc(&g->d_ci, sizeof(int32_t) * (size_t)std::max<int64_t>(m, 1)) != cudaSuccess) {
+      cudaMalloc(&g->d_ci, sizeof(int32_t) * (size_t)(m + xbe::kCiPad)) != cudaSuccess) {
     cudaGetLastError();
     if (g->d_ro) cudaFree(g->d_ro);
     if (g->d_ci) cudaFree(g->d_ci);
@@ -408,6 +437,7 @@ xb_status xb_graph_upload(xb_ctx* c, int64_t n, const void* row_offsets, int32_t
     for (int64_t i = 0; i <= n; i++) r32[i] = (int32_t)ro[i];
     XB_CUDA(cudaMemcpy(g->d_ro, r32.data(), ro_bytes, cudaMemcpyHostToDevice));
   }
+  XB_CUDA(cudaMemset(g->d_ci + m, 0, sizeof(int32_t) * xbe::kCiPad));
   if (m > 0) XB_CUDA(cudaMemcpy(g->d_ci, col_indices, sizeof(int32_t) * (size_t)m, cudaMemcpyHostToDevice));
   g->h_ro = std::move(ro);
   *out = g.release();
@@ -441,6 +471,7 @@ xb_status xb_graph_free(xb_graph* g) {
   if (g->d_hitems) cudaFree(g->d_hitems);
   if (g->d_hub_items) cudaFree(g->d_hub_items);
   if (g->d_hidx_of) cudaFree(g->d_hidx_of);
+  if (g->d_lorder) cudaFree(g->d_lorder);
   delete g;
   return XB_OK;
 }

@@ -65,6 +65,8 @@ struct xb_graph {
   int2* d_hub_items = nullptr;  // (heavy index, chunk) items of the hub pull
   int64_t n_hub_items = 0;
   int32_t* d_hidx_of = nullptr;  // vertex -> index in the heavy list (-1 for light)
+  int32_t* d_lorder = nullptr;   // light vertices (degree 1..heavy_thr) by falling degree
+  int64_t n_lorder = 0;
   int32_t n_heavy = 0;
   int32_t heavy_thr = -1;
   uint64_t version = 0;  // bumped whenever the heavy-vertex arrays are rebuilt
@@ -82,6 +84,8 @@ constexpr int kHubDegree = 4096;
 constexpr int kHubChunk = 2048;
 // Parent slots per heavy vertex: up to 64 sources x 4 words.
 constexpr int kHparRow = 256;
+// Zero entries allocated past the end of a resident colIndices array.
+constexpr int64_t kCiPad = 16;
 
 struct WsLayout {
   size_t seen, F, N, p01, ph, pushed, p8, touched, fl_light, fl_heavy, nl_light, nl_heavy, stamp, total;
@@ -295,6 +299,25 @@ xb_status emit_push(const PassRes<W, NW, OffT>& p, const xb_graph* g, int cur, c
   return XB_OK;
 }
 
+// Blocks of `threads` threads of `kernel` resident per SM (occupancy query).
+template <typename K>
+int resident_blocks(K kernel, int threads) {
+  int b = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernel, threads, 0) != cudaSuccess) {
+    cudaGetLastError();
+    b = 1;
+  }
+  return std::max(1, b);
+}
+
+// Light vertices pulled one per lane (k_pull_lanes) for up to two words per
+// vertex; wider layouts keep the edge-flat tiles (k_pull_tiles).
+template <int NW>
+constexpr bool pull_by_lanes() {
+  return NW <= 2;
+}
+constexpr int kLaneWarps = 8;
+
 template <typename W, int NW, typename OffT>
 xb_status emit_pull(const PassRes<W, NW, OffT>& p, const xb_graph* g, int cur, const StepShape& sh, int kb,
                     cudaStream_t s, int64_t* launches) {
@@ -303,9 +326,17 @@ xb_status emit_pull(const PassRes<W, NW, OffT>& p, const xb_graph* g, int cur, c
   W* N = p.buf[cur ^ 1];
   const xbk::Lists fl = p.lists[cur], nl = p.lists[cur ^ 1];
   const xbk::Masks<W, NW> active = active_mask<W, NW>(kb);
-  xbk::k_pull_tiles<W, NW, OffT, PW, 4><<<sh.pull_grid, PW * 32, 0, s>>>(p.n, p.ro, p.ci, F, p.seen, N, p.pl, active,
-                                                                         p.heavy, nl, p.ctr, cur, p.ppos);
-  (*launches)++;
+  if constexpr (pull_by_lanes<NW>()) {
+    if (g->n_lorder > 0) {
+      xbk::k_pull_lanes<W, NW, OffT, kLaneWarps><<<sh.pull_grid, kLaneWarps * 32, 0, s>>>(
+          g->n_lorder, g->d_lorder, p.ro, p.ci, F, p.seen, N, p.pl, active, p.heavy, nl, p.ctr, cur, p.ppos);
+      (*launches)++;
+    }
+  } else {
+    xbk::k_pull_tiles<W, NW, OffT, PW, 4><<<sh.pull_grid, PW * 32, 0, s>>>(p.n, p.ro, p.ci, F, p.seen, N, p.pl,
+                                                                           active, p.heavy, nl, p.ctr, cur, p.ppos);
+    (*launches)++;
+  }
   if (g->n_heavy > 0) {
     xbk::k_pull_heavy<W, NW, OffT, 4><<<sh.heavy_grid, 256, 0, s>>>(g->d_heavy, g->n_heavy, p.ro, p.ci, F, p.seen, N,
                                                                     p.pl, active, p.heavy, kHubDegree, nl, p.ctr, cur,
@@ -382,7 +413,15 @@ StepShape max_shape(const xb_graph* g, int sms) {
                             (unsigned)std::max<int64_t>(1, std::min<int64_t>(g->n_heavy, 65535)));
   if (g->n_heavy == 0) sh.push_heavy_grid.y = 0;
   sh.finalize_grid = (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)sms * 8));
-  sh.pull_grid = (int)std::max<int64_t>(1, std::min<int64_t>((ntiles + PW - 1) / PW, (int64_t)sms * 8));
+  if constexpr (pull_by_lanes<NW>()) {
+    // persistent: warps take chunks of the light list from a counter
+    static const int lane_res = resident_blocks(xbk::k_pull_lanes<W, NW, OffT, kLaneWarps>, kLaneWarps * 32);
+    const int64_t chunks = (g->n_lorder + xbk::kLaneChunk - 1) / xbk::kLaneChunk;
+    sh.pull_grid = (int)std::max<int64_t>(
+        1, std::min<int64_t>((chunks + kLaneWarps - 1) / kLaneWarps, (int64_t)sms * lane_res));
+  } else {
+    sh.pull_grid = (int)std::max<int64_t>(1, std::min<int64_t>((ntiles + PW - 1) / PW, (int64_t)sms * 8));
+  }
   sh.heavy_grid = (int)std::max<int64_t>(1, std::min<int64_t>((g->n_heavy + 7) / 8, (int64_t)sms * 16));
   sh.hub_grid = (int)std::max<int64_t>(1, std::min<int64_t>((g->n_hub_items + 7) / 8, (int64_t)sms * 16));
   sh.commit_grid = (int)std::max<int64_t>(1, std::min<int64_t>((g->n_heavy + 255) / 256, (int64_t)sms * 4));

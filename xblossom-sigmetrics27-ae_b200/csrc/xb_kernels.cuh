@@ -82,7 +82,7 @@ struct LevelCtr {
   int32_t n_light;
   int32_t n_heavy;
   int32_t n_touched;
-  int32_t pad;
+  int32_t work;  // chunks handed out by the step that builds this frontier (k_pull_lanes)
   unsigned long long edges;  // sum of degrees of the frontier
   unsigned long long live[4];
 };
@@ -693,6 +693,204 @@ __global__ void __launch_bounds__(WARPS * 32, 32 / WARPS) k_pull_tiles(int64_t n
     __syncwarp();
   }
   flush_stats<W, NW>(acc, nctr, &ctr->b);
+  e_scan = warp_sum_u64(e_scan);
+  v_scan = warp_sum_u64(v_scan);
+  v_sweep = warp_sum_u64(v_sweep);
+  if (lane == 0) {
+    if (e_scan) atomicAdd(&ctr->b.edges_scanned, e_scan);
+    if (v_scan) atomicAdd(&ctr->b.vertices_scanned, v_scan);
+    if (v_sweep) atomicAdd(&ctr->b.vertices_swept, v_sweep);
+  }
+}
+
+// Pull, light vertices (degree 1..heavy), one vertex per lane.  The graph's
+// light vertices are listed by falling degree (lorder), so the 32 lanes of a
+// warp walk adjacencies of nearly equal length; warps take chunks of kLaneChunk
+// list entries from a counter (longest first) and queue the chunk's wanted
+// vertices in shared memory, so every processed group of 32 is full.  Each
+// lane scans its adjacency in ascending order with 16-byte colIndices loads and
+// one frontier-word gather per edge, and stops once every wanted bit is found:
+// the edge where a bit first appears is its smallest-id parent, recorded
+// bit-sliced in ppos (position < kP8MaxDegree) as in k_pull_tiles.  nctr->work
+// must be zero at launch (k_step_begin clears the next level's counters).
+constexpr int kLaneChunk = 256;
+
+template <typename W, int NW, typename OffT>
+__device__ __forceinline__ void pull_lane_vertex(bool act, int32_t v, const W (&sw)[NW], const W (&live)[NW],
+                                                 const OffT* __restrict__ ro, const int32_t* __restrict__ ci,
+                                                 const W* __restrict__ F, W* seen, W* N, const Planes<W, NW>& pl,
+                                                 const Masks<W, NW>& active, int heavy, int level, Lists nl,
+                                                 LevelCtr* nctr, W* __restrict__ ppos, StatAcc<W, NW>& sacc,
+                                                 unsigned long long& e_scan) {
+  W want[NW], acc[NW], pp[NW][8];
+  int64_t beg = 0, end = 0;
+  if (act) {
+    beg = ro[v];
+    end = ro[v + 1];
+  }
+#pragma unroll
+  for (int i = 0; i < NW; i++) {
+    want[i] = act ? (live[i] & ~sw[i]) : (W)0;
+    acc[i] = 0;
+#pragma unroll
+    for (int k = 0; k < 8; k++) pp[i][k] = 0;
+  }
+  const bool rec = end - beg <= kP8MaxDegree;
+  // aligned groups of 4 entries; entries outside [beg, end) are masked off
+  int64_t j0 = beg & ~(int64_t)3;
+  for (; j0 < end; j0 += 4) {
+    const int4 q = __ldg(reinterpret_cast<const int4*>(ci + j0));
+    const int32_t cols[4] = {q.x, q.y, q.z, q.w};
+    W f[4][NW];
+#pragma unroll
+    for (int t = 0; t < 4; t++) {
+      const int64_t j = j0 + t;
+      if (j >= beg && j < end) {
+        load_words<W, NW>(F + (int64_t)cols[t] * NW, f[t]);
+      } else {
+#pragma unroll
+        for (int i = 0; i < NW; i++) f[t][i] = 0;
+      }
+    }
+    bool done = true;
+#pragma unroll
+    for (int t = 0; t < 4; t++) {
+      const int pos = (int)(j0 + t - beg);
+#pragma unroll
+      for (int i = 0; i < NW; i++) {
+        const W c = f[t][i] & want[i] & ~acc[i];
+        if (c) {
+          acc[i] |= c;
+          if (rec) {
+#pragma unroll
+            for (int k = 0; k < 8; k++)
+              if ((pos >> k) & 1) pp[i][k] |= c;
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < NW; i++) done = done && acc[i] == want[i];
+    if (done) {
+      j0 += 4;
+      break;
+    }
+  }
+  if (act) e_scan += (unsigned long long)(imin64(j0, end) - beg);
+  bool has = false;
+#pragma unroll
+  for (int i = 0; i < NW; i++) has = has || acc[i] != 0;
+  if (has) {
+#pragma unroll
+    for (int i = 0; i < NW; i++) {
+      N[(int64_t)v * NW + i] = acc[i];
+      if (rec && acc[i]) {
+        W* prow = ppos + ((int64_t)v * NW + i) * 8;
+#pragma unroll
+        for (int k = 0; k < 8; k++)
+          if (pp[i][k]) prow[k] |= pp[i][k];
+      }
+    }
+  }
+  commit_new<W, NW, OffT>(has, v, acc, sw, end - beg, level, seen, pl, active, heavy, nl, nctr, sacc);
+}
+
+template <typename W, int NW, typename OffT, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32) k_pull_lanes(int64_t nlight, const int32_t* __restrict__ lorder,
+                                                           const OffT* __restrict__ ro,
+                                                           const int32_t* __restrict__ ci, const W* __restrict__ F,
+                                                           W* seen, W* N, Planes<W, NW> pl, Masks<W, NW> active,
+                                                           int heavy, Lists nl, Ctrs* ctr, int cur,
+                                                           W* __restrict__ ppos) {
+  const int level = ctr->b.level;
+  __shared__ int32_t s_qv[WARPS][64];
+  __shared__ W s_qs[WARPS][64][NW];
+  const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  LevelCtr* cctr = &ctr->lv[cur];
+  LevelCtr* nctr = &ctr->lv[cur ^ 1];
+  W live[NW];
+#pragma unroll
+  for (int i = 0; i < NW; i++) live[i] = (W)cctr->live[i] & active.w[i];
+  unsigned long long e_scan = 0, v_scan = 0, v_sweep = 0;
+  StatAcc<W, NW> sacc;
+  int qn = 0;  // queued vertices (warp-uniform)
+  for (;;) {
+    int chunk = 0;
+    if (lane == 0) chunk = atomicAdd(&nctr->work, 1);
+    chunk = __shfl_sync(0xffffffffu, chunk, 0);
+    const int64_t c0 = (int64_t)chunk * kLaneChunk;
+    const bool last = c0 >= nlight;
+    if (!last) {
+      const int64_t c1 = imin64(c0 + kLaneChunk, nlight);
+      for (int64_t t = c0; t < c1; t += 32) {
+        const int64_t idx = t + lane;
+        int32_t v = 0;
+        W sw[NW];
+        bool want = false;
+#pragma unroll
+        for (int i = 0; i < NW; i++) sw[i] = 0;
+        if (idx < c1) {
+          v = lorder[idx];
+          load_words<W, NW>(seen + (int64_t)v * NW, sw);
+#pragma unroll
+          for (int i = 0; i < NW; i++) want = want || (live[i] & ~sw[i]) != 0;
+          v_sweep++;
+        }
+        const unsigned wm = __ballot_sync(0xffffffffu, want);
+        if (want) {
+          const int slot = qn + __popc(wm & ((1u << lane) - 1u));
+          s_qv[wib][slot] = v;
+#pragma unroll
+          for (int i = 0; i < NW; i++) s_qs[wib][slot][i] = sw[i];
+        }
+        qn += __popc(wm);
+        __syncwarp();
+        if (qn >= 32) {
+          W qs[NW];
+#pragma unroll
+          for (int i = 0; i < NW; i++) qs[i] = s_qs[wib][lane][i];
+          const int32_t qv = s_qv[wib][lane];
+          // move the overflow (< 32 entries) to the front
+          const int rest = qn - 32;
+          int32_t mv = 0;
+          W ms[NW];
+          if (lane < rest) {
+            mv = s_qv[wib][32 + lane];
+#pragma unroll
+            for (int i = 0; i < NW; i++) ms[i] = s_qs[wib][32 + lane][i];
+          }
+          __syncwarp();
+          if (lane < rest) {
+            s_qv[wib][lane] = mv;
+#pragma unroll
+            for (int i = 0; i < NW; i++) s_qs[wib][lane][i] = ms[i];
+          }
+          qn = rest;
+          __syncwarp();
+          v_scan++;
+          pull_lane_vertex<W, NW, OffT>(true, qv, qs, live, ro, ci, F, seen, N, pl, active, heavy, level, nl, nctr,
+                                        ppos, sacc, e_scan);
+        }
+      }
+    }
+    if (last) {
+      // the list is exhausted: drain the partial queue
+      if (qn > 0) {
+        const bool act = lane < qn;
+        W qs[NW];
+        int32_t qv = 0;
+#pragma unroll
+        for (int i = 0; i < NW; i++) qs[i] = act ? s_qs[wib][lane][i] : (W)0;
+        if (act) qv = s_qv[wib][lane];
+        v_scan += act ? 1 : 0;
+        pull_lane_vertex<W, NW, OffT>(act, qv, qs, live, ro, ci, F, seen, N, pl, active, heavy, level, nl, nctr,
+                                      ppos, sacc, e_scan);
+      }
+      break;
+    }
+  }
+  flush_stats<W, NW>(sacc, nctr, &ctr->b);
   e_scan = warp_sum_u64(e_scan);
   v_scan = warp_sum_u64(v_scan);
   v_sweep = warp_sum_u64(v_sweep);
