@@ -228,7 +228,7 @@ xb_status capture_pass(xb_ctx* c, BatchState* bs, const PassPlan& pp, int64_t ro
   const xb_graph* g = pp.g;
   const int sms = c->num_sms;
   const int heavy = std::max(32, c->tuning.heavy_degree);
-  const float alpha = c->tuning.pull_alpha > 0 ? c->tuning.pull_alpha : 64.0f;
+  const float alpha = c->tuning.pull_alpha > 0 ? c->tuning.pull_alpha : 256.0f;
   const WsLayout L = layout_for(g->n, (int)sizeof(W), NW);
   const PassRes<W, NW, OffT> p = pass_res<W, NW, OffT>(g, ch.ws, L, ch.ctr, ch.hpar, heavy);
   const StepShape sh = graph_shape<W, NW, OffT>(g, sms);

@@ -87,9 +87,15 @@ xb_status ensure_rows(xb_ctx* c, int64_t count) {
 
 xb_status ensure_heavy(xb_graph* g, int thr) {
   if (g->heavy_thr == thr) return XB_OK;
+  // heavy vertices by falling degree (ties by ascending id): every heavy
+  // index (hpar rows, work items, hidx_of) follows this order, and the pull
+  // kernels hand the vertices out longest first
   std::vector<int32_t> hv;
   for (int64_t v = 0; v < g->n; v++)
     if (g->h_ro[v + 1] - g->h_ro[v] > thr) hv.push_back((int32_t)v);
+  std::stable_sort(hv.begin(), hv.end(), [&](int32_t a, int32_t b) {
+    return g->h_ro[a + 1] - g->h_ro[a] > g->h_ro[b + 1] - g->h_ro[b];
+  });
   if (g->d_heavy) cudaFree(g->d_heavy);
   if (g->d_hpar) cudaFree(g->d_hpar);
   g->d_heavy = nullptr;
@@ -139,10 +145,31 @@ xb_status ensure_heavy(xb_graph* g, int thr) {
     if (!lorder.empty())
       XB_CUDA(cudaMemcpy(g->d_lorder, lorder.data(), sizeof(int32_t) * lorder.size(), cudaMemcpyHostToDevice));
     g->n_lorder = (int64_t)lorder.size();
+    // chunks of the list: at most kLaneChunk vertices, and a new chunk once
+    // kLaneChunkEdges edges are reached
+    std::vector<int32_t> lchunk{0};
+    int64_t edges = 0;
+    for (size_t i = 0; i < lorder.size(); i++) {
+      const int64_t d = g->h_ro[lorder[i] + 1] - g->h_ro[lorder[i]];
+      if (i > (size_t)lchunk.back() &&
+          ((int64_t)i - lchunk.back() >= xbk::kLaneChunk || edges + d > xbk::kLaneChunkEdges)) {
+        lchunk.push_back((int32_t)i);
+        edges = 0;
+      }
+      edges += d;
+    }
+    lchunk.push_back((int32_t)lorder.size());
+    if (g->d_lchunk) cudaFree(g->d_lchunk);
+    g->d_lchunk = nullptr;
+    if (cudaMalloc(&g->d_lchunk, sizeof(int32_t) * lchunk.size()) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(XB_ERR_OOM, "light chunk table allocation failed");
+    }
+    XB_CUDA(cudaMemcpy(g->d_lchunk, lchunk.data(), sizeof(int32_t) * lchunk.size(), cudaMemcpyHostToDevice));
+    g->n_lchunks = lorder.empty() ? 0 : (int32_t)lchunk.size() - 1;
   }
   // (heavy index, chunk) work items of the table pass, heaviest vertices first
-  // (ids ascend roughly with falling degree in R-MAT-like graphs, so this is
-  // the list order)
+  // (the list order)
   std::vector<int2> items;
   for (size_t i = 0; i < hv.size(); i++) {
     const int64_t d = g->h_ro[hv[i] + 1] - g->h_ro[hv[i]];
@@ -214,7 +241,7 @@ xb_status run_plain(xb_ctx* c, xb_graph* g, const int32_t* d_sources, int32_t k,
   }
   PassRes<W, NW, OffT> p = pass_res<W, NW, OffT>(g, c->ws, L, c->d_ctr, g->d_hpar, heavy);
   const int sms = c->num_sms;
-  const float alpha = c->tuning.pull_alpha > 0 ? c->tuning.pull_alpha : 64.0f;
+  const float alpha = c->tuning.pull_alpha > 0 ? c->tuning.pull_alpha : 256.0f;
   ClassTimer timer{c, st, c->tuning.timing != 0};
   const StepShape mx = max_shape<W, NW, OffT>(g, sms);
   int max_levels = 0;
@@ -334,9 +361,9 @@ xb_status xb_ctx_create(int32_t device, xb_ctx** out) {
   XB_CUDA(cudaEventCreate(&c->evc1));
   c->tuning.word_bits = 64;
   c->tuning.words = 1;
-  // pull unless the frontier's edges are under 1/64 of the unfinished edges:
+  // pull unless the frontier's edges are under 1/256 of the unfinished edges:
   // pull steps record parents as they go, push steps leave them to a search
-  c->tuning.pull_alpha = 64.0f;
+  c->tuning.pull_alpha = 256.0f;
   c->tuning.heavy_degree = 256;
   c->tuning.timing = 0;
   c->tuning.chains = 2;
@@ -472,6 +499,7 @@ xb_status xb_graph_free(xb_graph* g) {
   if (g->d_hub_items) cudaFree(g->d_hub_items);
   if (g->d_hidx_of) cudaFree(g->d_hidx_of);
   if (g->d_lorder) cudaFree(g->d_lorder);
+  if (g->d_lchunk) cudaFree(g->d_lchunk);
   delete g;
   return XB_OK;
 }

@@ -67,6 +67,8 @@ struct xb_graph {
   int32_t* d_hidx_of = nullptr;  // vertex -> index in the heavy list (-1 for light)
   int32_t* d_lorder = nullptr;   // light vertices (degree 1..heavy_thr) by falling degree
   int64_t n_lorder = 0;
+  int32_t* d_lchunk = nullptr;   // chunk starts in d_lorder (n_lchunks + 1 entries)
+  int32_t n_lchunks = 0;
   int32_t n_heavy = 0;
   int32_t heavy_thr = -1;
   uint64_t version = 0;  // bumped whenever the heavy-vertex arrays are rebuilt
@@ -329,7 +331,8 @@ xb_status emit_pull(const PassRes<W, NW, OffT>& p, const xb_graph* g, int cur, c
   if constexpr (pull_by_lanes<NW>()) {
     if (g->n_lorder > 0) {
       xbk::k_pull_lanes<W, NW, OffT, kLaneWarps><<<sh.pull_grid, kLaneWarps * 32, 0, s>>>(
-          g->n_lorder, g->d_lorder, p.ro, p.ci, F, p.seen, N, p.pl, active, p.heavy, nl, p.ctr, cur, p.ppos);
+          g->n_lchunks, g->d_lchunk, g->d_lorder, p.ro, p.ci, F, p.seen, N, p.pl, active, p.heavy, nl, p.ctr, cur,
+          p.ppos);
       (*launches)++;
     }
   } else {
@@ -416,13 +419,13 @@ StepShape max_shape(const xb_graph* g, int sms) {
   if constexpr (pull_by_lanes<NW>()) {
     // persistent: warps take chunks of the light list from a counter
     static const int lane_res = resident_blocks(xbk::k_pull_lanes<W, NW, OffT, kLaneWarps>, kLaneWarps * 32);
-    const int64_t chunks = (g->n_lorder + xbk::kLaneChunk - 1) / xbk::kLaneChunk;
     sh.pull_grid = (int)std::max<int64_t>(
-        1, std::min<int64_t>((chunks + kLaneWarps - 1) / kLaneWarps, (int64_t)sms * lane_res));
+        1, std::min<int64_t>(((int64_t)g->n_lchunks + kLaneWarps - 1) / kLaneWarps, (int64_t)sms * lane_res));
   } else {
     sh.pull_grid = (int)std::max<int64_t>(1, std::min<int64_t>((ntiles + PW - 1) / PW, (int64_t)sms * 8));
   }
-  sh.heavy_grid = (int)std::max<int64_t>(1, std::min<int64_t>((g->n_heavy + 7) / 8, (int64_t)sms * 16));
+  static const int heavy_res = resident_blocks(xbk::k_pull_heavy<W, NW, OffT, 4>, 256);
+  sh.heavy_grid = (int)std::max<int64_t>(1, std::min<int64_t>((g->n_heavy + 7) / 8, (int64_t)sms * heavy_res));
   sh.hub_grid = (int)std::max<int64_t>(1, std::min<int64_t>((g->n_hub_items + 7) / 8, (int64_t)sms * 16));
   sh.commit_grid = (int)std::max<int64_t>(1, std::min<int64_t>((g->n_heavy + 255) / 256, (int64_t)sms * 4));
   sh.clear_grid = sms * 8;

@@ -82,7 +82,9 @@ struct LevelCtr {
   int32_t n_light;
   int32_t n_heavy;
   int32_t n_touched;
-  int32_t work;  // chunks handed out by the step that builds this frontier (k_pull_lanes)
+  int32_t work;   // chunks handed out by the step that builds this frontier (k_pull_lanes)
+  int32_t work2;  // heavy vertices handed out by the same step (k_pull_heavy)
+  int32_t pad;
   unsigned long long edges;  // sum of degrees of the frontier
   unsigned long long live[4];
 };
@@ -705,15 +707,17 @@ __global__ void __launch_bounds__(WARPS * 32, 32 / WARPS) k_pull_tiles(int64_t n
 
 // Pull, light vertices (degree 1..heavy), one vertex per lane.  The graph's
 // light vertices are listed by falling degree (lorder), so the 32 lanes of a
-// warp walk adjacencies of nearly equal length; warps take chunks of kLaneChunk
-// list entries from a counter (longest first) and queue the chunk's wanted
-// vertices in shared memory, so every processed group of 32 is full.  Each
+// warp walk adjacencies of nearly equal length; warps take chunks of the list
+// (lchunk: at most kLaneChunk vertices and about kLaneChunkEdges edges each)
+// from a counter, longest first, and queue the wanted vertices in shared
+// memory, so every processed group of 32 is full.  Each
 // lane scans its adjacency in ascending order with 16-byte colIndices loads and
 // one frontier-word gather per edge, and stops once every wanted bit is found:
 // the edge where a bit first appears is its smallest-id parent, recorded
 // bit-sliced in ppos (position < kP8MaxDegree) as in k_pull_tiles.  nctr->work
 // must be zero at launch (k_step_begin clears the next level's counters).
 constexpr int kLaneChunk = 256;
+constexpr int kLaneChunkEdges = 2048;
 
 template <typename W, int NW, typename OffT>
 __device__ __forceinline__ void pull_lane_vertex(bool act, int32_t v, const W (&sw)[NW], const W (&live)[NW],
@@ -736,14 +740,24 @@ __device__ __forceinline__ void pull_lane_vertex(bool act, int32_t v, const W (&
     for (int k = 0; k < 8; k++) pp[i][k] = 0;
   }
   const bool rec = end - beg <= kP8MaxDegree;
-  // aligned groups of 4 entries; entries outside [beg, end) are masked off
+  // aligned groups of 8 entries (two 16-byte loads); entries outside
+  // [beg, end) are masked off.  The next group's colIndices are loaded before
+  // this group's frontier words are gathered, so the two latencies overlap.
   int64_t j0 = beg & ~(int64_t)3;
-  for (; j0 < end; j0 += 4) {
-    const int4 q = __ldg(reinterpret_cast<const int4*>(ci + j0));
-    const int32_t cols[4] = {q.x, q.y, q.z, q.w};
-    W f[4][NW];
+  int4 qa = make_int4(0, 0, 0, 0), qb = make_int4(0, 0, 0, 0);
+  if (j0 < end) {
+    qa = __ldg(reinterpret_cast<const int4*>(ci + j0));
+    qb = __ldg(reinterpret_cast<const int4*>(ci + j0 + 4));
+  }
+  for (; j0 < end; j0 += 8) {
+    const int32_t cols[8] = {qa.x, qa.y, qa.z, qa.w, qb.x, qb.y, qb.z, qb.w};
+    if (j0 + 8 < end) {
+      qa = __ldg(reinterpret_cast<const int4*>(ci + j0 + 8));
+      qb = __ldg(reinterpret_cast<const int4*>(ci + j0 + 12));
+    }
+    W f[8][NW];
 #pragma unroll
-    for (int t = 0; t < 4; t++) {
+    for (int t = 0; t < 8; t++) {
       const int64_t j = j0 + t;
       if (j >= beg && j < end) {
         load_words<W, NW>(F + (int64_t)cols[t] * NW, f[t]);
@@ -754,7 +768,7 @@ __device__ __forceinline__ void pull_lane_vertex(bool act, int32_t v, const W (&
     }
     bool done = true;
 #pragma unroll
-    for (int t = 0; t < 4; t++) {
+    for (int t = 0; t < 8; t++) {
       const int pos = (int)(j0 + t - beg);
 #pragma unroll
       for (int i = 0; i < NW; i++) {
@@ -772,7 +786,7 @@ __device__ __forceinline__ void pull_lane_vertex(bool act, int32_t v, const W (&
 #pragma unroll
     for (int i = 0; i < NW; i++) done = done && acc[i] == want[i];
     if (done) {
-      j0 += 4;
+      j0 += 8;
       break;
     }
   }
@@ -796,7 +810,8 @@ __device__ __forceinline__ void pull_lane_vertex(bool act, int32_t v, const W (&
 }
 
 template <typename W, int NW, typename OffT, int WARPS>
-__global__ void __launch_bounds__(WARPS * 32) k_pull_lanes(int64_t nlight, const int32_t* __restrict__ lorder,
+__global__ void __launch_bounds__(WARPS * 32, 3) k_pull_lanes(int32_t nchunks, const int32_t* __restrict__ lchunk,
+                                                           const int32_t* __restrict__ lorder,
                                                            const OffT* __restrict__ ro,
                                                            const int32_t* __restrict__ ci, const W* __restrict__ F,
                                                            W* seen, W* N, Planes<W, NW> pl, Masks<W, NW> active,
@@ -819,10 +834,9 @@ __global__ void __launch_bounds__(WARPS * 32) k_pull_lanes(int64_t nlight, const
     int chunk = 0;
     if (lane == 0) chunk = atomicAdd(&nctr->work, 1);
     chunk = __shfl_sync(0xffffffffu, chunk, 0);
-    const int64_t c0 = (int64_t)chunk * kLaneChunk;
-    const bool last = c0 >= nlight;
+    const bool last = chunk >= nchunks;
     if (!last) {
-      const int64_t c1 = imin64(c0 + kLaneChunk, nlight);
+      const int64_t c0 = lchunk[chunk], c1 = lchunk[chunk + 1];
       for (int64_t t = c0; t < c1; t += 32) {
         const int64_t idx = t + lane;
         int32_t v = 0;
@@ -942,7 +956,15 @@ __global__ void k_pull_heavy(const int32_t* __restrict__ hlist, int32_t nh, cons
   for (int i = 0; i < NW; i++) live[i] = (W)cctr->live[i] & active.w[i];
   StatAcc<W, NW> sacc;
   unsigned long long scanned = 0, vcount = 0;
-  for (int64_t idx = warp; idx < nh; idx += nwarps) {
+  (void)warp;
+  (void)nwarps;
+  for (;;) {
+    // the heavy list runs by falling degree: warps take vertices from a
+    // counter, the longest adjacencies first
+    int32_t idx = 0;
+    if (lane == 0) idx = atomicAdd(&nctr->work2, 1);
+    idx = __shfl_sync(0xffffffffu, idx, 0);
+    if (idx >= nh) break;
     const int32_t v = hlist[idx];
     const int64_t beg = ro[v], end = ro[v + 1];
     if (end - beg > hub) continue;  // warp-uniform
@@ -959,12 +981,20 @@ __global__ void k_pull_heavy(const int32_t* __restrict__ hlist, int32_t nh, cons
     W acc[NW];
 #pragma unroll
     for (int i = 0; i < NW; i++) acc[i] = 0;
+    // colIndices of the next round are loaded before this round's gathers
+    int32_t coln[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const int64_t e = beg + u * 32 + lane;
+      coln[u] = e < end ? __ldg(&ci[e]) : -1;
+    }
     for (int64_t base = beg; base < end; base += 32 * U) {
       int32_t col[U];
 #pragma unroll
       for (int u = 0; u < U; u++) {
-        const int64_t e = base + u * 32 + lane;
-        col[u] = e < end ? __ldg(&ci[e]) : -1;
+        col[u] = coln[u];
+        const int64_t e = base + 32 * U + u * 32 + lane;
+        coln[u] = e < end ? __ldg(&ci[e]) : -1;
       }
       W f[U][NW];
 #pragma unroll
