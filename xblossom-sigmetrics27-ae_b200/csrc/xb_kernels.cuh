@@ -1209,6 +1209,37 @@ __device__ __forceinline__ unsigned long long transpose8(unsigned long long x) {
   return x;
 }
 
+// Half h (0 = low) of a word, as 32 bits.
+template <typename W>
+__device__ __forceinline__ uint32_t half32(W x, int h) {
+  if constexpr (sizeof(W) == 4) {
+    return (uint32_t)x;
+  } else {
+    return (uint32_t)(h ? (x >> 32) : x);
+  }
+}
+
+// Byte bb of each of a, b, c, d in bytes 0..3; sel = bb | (bb + 4) << 4.
+__device__ __forceinline__ uint32_t gather4(uint32_t a, uint32_t b, uint32_t c, uint32_t d, uint32_t sel) {
+  return __byte_perm(__byte_perm(a, b, sel), __byte_perm(c, d, sel), 0x5410);
+}
+
+// transpose8 on the 64-bit value hi:lo, in 32-bit operations.
+__device__ __forceinline__ void transpose8x8(uint32_t& lo, uint32_t& hi) {
+  uint32_t t;
+  t = (lo ^ (lo >> 7)) & 0x00AA00AAu;
+  lo ^= t ^ (t << 7);
+  t = (hi ^ (hi >> 7)) & 0x00AA00AAu;
+  hi ^= t ^ (t << 7);
+  t = (lo ^ (lo >> 14)) & 0x0000CCCCu;
+  lo ^= t ^ (t << 14);
+  t = (hi ^ (hi >> 14)) & 0x0000CCCCu;
+  hi ^= t ^ (t << 14);
+  t = (lo ^ ((lo >> 28) | (hi << 4))) & 0xF0F0F0F0u;
+  lo ^= t ^ (t << 28);
+  hi ^= t >> 4;
+}
+
 // Byte b of each of 8 words, word r landing in byte r.
 template <typename W>
 __device__ __forceinline__ unsigned long long gather_bytes8(const W (&p)[8], int b) {
@@ -1375,26 +1406,16 @@ __global__ void __launch_bounds__(WARPS * 32, 32 / WARPS) k_tables(int64_t n, co
       if (lane == 0) pe += (unsigned long long)take;
       __syncwarp();
     }
-    // write rows: level and parent of sources 0..kbw-1 at vertices tile*32 + lane
-    if (valid) {
-      constexpr int RP = 8;  // planes held in registers; deeper levels read on demand
-      W plr[RP];
-      plr[0] = p0;
-      plr[1] = p1;
-#pragma unroll
-      for (int j = 2; j < RP; j++) plr[j] = j < nplanes ? pl.get(j, v, wi) : (W)0;
+    // write rows: level and parent of sources 0..kbw-1 at vertices tile*32 + lane.
+    // Every lane runs the decode (it holds a warp vote); lanes past n load and
+    // store nothing.
+    {
+      constexpr int RP = 8;  // planes decoded by transposes; deeper levels read on demand
       // parent sources: recorded position (light, pulled; bit-sliced in 8
-      // planes), recorded id (heavy), searched (s_par), the source itself
-      // (levels 0 and 1)
-      W pp[8];
-      const bool use_pp = !is_heavy && has_p8;
-#pragma unroll
-      for (int k2 = 0; k2 < 8; k2 += 2) {
-        W t2[2] = {0, 0};
-        if (use_pp) load_words<W, 2>(ppos + (v * NW + wi) * 8 + k2, t2);
-        pp[k2] = t2[0];
-        pp[k2 + 1] = t2[1];
-      }
+      // planes), recorded id (heavy), searched (written above), the source
+      // itself (levels 0 and 1)
+      const bool use_pp = valid && !is_heavy && has_p8;
+      const W* prow = ppos + (v * NW + wi) * 8;
       const int32_t* hrow = is_heavy ? hpar + (int64_t)hidx_of[v] * ROW + wi * B : nullptr;
       // the first kCiCache neighbours of the vertex: most recorded positions
       // point there (the first frontier neighbour of a large frontier)
@@ -1403,41 +1424,82 @@ __global__ void __launch_bounds__(WARPS * 32, 32 / WARPS) k_tables(int64_t n, co
 #pragma unroll
         for (int j = 0; j < kCiCache; j++) cic[j] = j < dg ? __ldg(&ci[beg + j]) : -1;
       }
-      // eight sources at a time: level bytes and position bytes by 8x8 bit
-      // transposes of the planes (byte c of the result = source 8b + c); the
-      // per-source class bits come from one byte of each mask, and the parent
-      // is picked by selects (lanes of a warp rarely share a class).  Searched
-      // bits (need) already hold their parent.
+      // Eight sources at a time, per 32-bit half of the words: the level bytes
+      // and position bytes of sources 8b..8b+7 come from byte permutes of the
+      // 8 plane halves and an 8x8 bit transpose; the parent is the cached
+      // neighbour at the recorded position.  Rarer classes (the source itself,
+      // level 1, heavy rows, positions beyond the cache) are patched only when
+      // some lane of the warp has one.  Searched bits (need) already hold
+      // their parent.
       const bool deep = nplanes > RP;
+      constexpr int HALVES = (int)sizeof(W) / 4;
 #pragma unroll 1
-      for (int b8 = 0; b8 < B / 8; b8++) {
-        if (b8 * 8 >= kbw) break;
-        const unsigned long long lvx = transpose8(gather_bytes8<W>(plr, b8));
-        const unsigned long long ppx = use_pp ? transpose8(gather_bytes8<W>(pp, b8)) : 0ull;
-        const uint32_t svb = (uint32_t)(sv >> (8 * b8)) & 0xFFu;
-        const uint32_t rtb = (uint32_t)(root >> (8 * b8)) & 0xFFu;
-        const uint32_t l1b = (uint32_t)(lvl1 >> (8 * b8)) & 0xFFu;
-        const uint32_t ndb = (uint32_t)(need >> (8 * b8)) & 0xFFu;
-        const uint32_t far = svb & ~(ndb | rtb | l1b);  // recorded positions, possibly beyond the cache
+      for (int h = 0; h < HALVES; h++) {
+        if (h * 32 >= kbw) break;
+        // 32-bit halves of the level planes and position planes
+        uint32_t L[8], P[8];
+        L[0] = half32<W>(p0, h);
+        L[1] = half32<W>(p1, h);
 #pragma unroll
-        for (int i = 0; i < 8; i++) {
-          const int s = b8 * 8 + i;
-          if (s >= kbw) break;
-          int32_t lv = (int32_t)((lvx >> (8 * i)) & 0xFF);
-          if (deep && ((svb >> i) & 1))
-            for (int j = RP; j < nplanes; j++) lv |= (int32_t)((pl.get(j, v, wi) >> s) & 1) << j;
-          const int idx = (int)((ppx >> (8 * i)) & 0xFF);
-          int32_t pr = cic[idx & (kCiCache - 1)];
-          if (idx >= kCiCache && ((far >> i) & 1) && !hrow) pr = __ldg(&ci[beg + idx]);
-          if (hrow) pr = hrow[s];
-          pr = ((l1b >> i) & 1) ? s_src[s] : pr;
-          pr = ((rtb >> i) & 1) ? (int32_t)v : pr;
-          if (!((svb >> i) & 1)) {
-            lv = -1;
-            pr = -1;
+        for (int j = 2; j < RP; j++)
+          L[j] = (valid && j < nplanes)
+                     ? reinterpret_cast<const uint32_t*>(pl.ph + (int64_t)(j - 2) * pl.stride + v * NW + wi)[h]
+                     : 0u;
+#pragma unroll
+        for (int r = 0; r < 8; r++) P[r] = use_pp ? reinterpret_cast<const uint32_t*>(prow + r)[h] : 0u;
+        const uint32_t sv32 = half32<W>(sv, h), rt32 = half32<W>(root, h), l132 = half32<W>(lvl1, h);
+        const uint32_t nd32 = half32<W>(need, h);
+        // recorded positions >= kCiCache (a bit in position planes 3..7)
+        const uint32_t far32 = (P[3] | P[4] | P[5] | P[6] | P[7]) & sv32 & ~(nd32 | rt32 | l132);
+        const bool rare = __any_sync(0xffffffffu, (rt32 | l132 | far32) != 0 || hrow != nullptr);
+#pragma unroll 1
+        for (int bb = 0; bb < 4; bb++) {
+          const int sb = h * 32 + bb * 8;
+          if (sb >= kbw) break;
+          const uint32_t sel = (uint32_t)bb | ((uint32_t)(bb + 4) << 4);
+          uint32_t llo = gather4(L[0], L[1], L[2], L[3], sel), lhi = gather4(L[4], L[5], L[6], L[7], sel);
+          transpose8x8(llo, lhi);
+          uint32_t plo = 0, phi = 0;
+          if (use_pp) {
+            plo = gather4(P[0], P[1], P[2], P[3], sel);
+            phi = gather4(P[4], P[5], P[6], P[7], sel);
+            transpose8x8(plo, phi);
           }
-          __stcs(&s_row[0][s][v], lv);
-          if (!((ndb >> i) & 1)) __stcs(&s_row[1][s][v], pr);
+          const uint32_t svb = (sv32 >> (8 * bb)) & 0xFFu, ndb = (nd32 >> (8 * bb)) & 0xFFu;
+          int32_t lv[8], pr[8];
+#pragma unroll
+          for (int i = 0; i < 8; i++) {
+            const uint32_t lw = i < 4 ? llo : lhi, pw = i < 4 ? plo : phi;
+            lv[i] = (int32_t)((lw >> (8 * (i & 3))) & 0xFFu);
+            pr[i] = cic[(pw >> (8 * (i & 3))) & (kCiCache - 1)];
+          }
+          if (rare) {
+            const uint32_t rtb = (rt32 >> (8 * bb)) & 0xFFu, l1b = (l132 >> (8 * bb)) & 0xFFu;
+            const uint32_t farb = (far32 >> (8 * bb)) & 0xFFu;
+#pragma unroll
+            for (int i = 0; i < 8; i++) {
+              const uint32_t pw = i < 4 ? plo : phi;
+              if (((farb >> i) & 1) && !hrow) pr[i] = __ldg(&ci[beg + ((pw >> (8 * (i & 3))) & 0xFFu)]);
+              if (hrow && sb + i < kbw) pr[i] = hrow[sb + i];
+              if ((l1b >> i) & 1) pr[i] = s_src[sb + i];
+              if ((rtb >> i) & 1) pr[i] = (int32_t)v;
+            }
+          }
+          if (deep) {
+#pragma unroll
+            for (int i = 0; i < 8; i++)
+              if ((svb >> i) & 1)
+                for (int j = RP; j < nplanes; j++) lv[i] |= (int32_t)((pl.get(j, v, wi) >> (sb + i)) & 1) << j;
+          }
+#pragma unroll
+          for (int i = 0; i < 8; i++) {
+            const int s = sb + i;
+            if (s < kbw && valid) {
+              const bool hit = (svb >> i) & 1;
+              __stcs(&s_row[0][s][v], hit ? lv[i] : -1);
+              if (!((ndb >> i) & 1)) __stcs(&s_row[1][s][v], hit ? pr[i] : -1);
+            }
+          }
         }
       }
     }
