@@ -46,6 +46,11 @@ WORKLOADS = {
     "rmat22_k1024": dict(kind="rmat", scale=22, ef=16, k=1024),
     "er335k_k256": dict(kind="er", n=335_000, pairs=1_850_000, k=256),
     "rmat16_k64": dict(kind="rmat", scale=16, ef=16, k=64),
+    # 128 independent R-MAT graphs (scale U[10,20], edge factor in {4,8,16,32}), 1..512 sources each
+    # (log-uniform), uploaded as one concatenated CSR; all queries in one batched launch
+    "multi128": dict(kind="multi", instances=128, k=0),
+    # the default graph with one word of sources: ncu DRAM-traffic captures (about 4 GB on the device)
+    "rmat22_k64": dict(kind="rmat", scale=22, ef=16, k=64),
     # smaller case for kernel profiles (graph > L2, a few hundred MB on the device)
     "rmat20_k64": dict(kind="rmat", scale=20, ef=16, k=64),
 }
@@ -207,6 +212,87 @@ def run_reference(args, w, name) -> None:
     print(json.dumps(line), flush=True)
 
 
+def multi_instances(count: int, seed: int):
+    """Seeded instance specs of the uneven workload: (scale, edge factor, k, graph seed)."""
+    rng = np.random.default_rng(seed)
+    specs = []
+    for i in range(count):
+        scale = int(rng.integers(10, 21))
+        ef = int(rng.choice([4, 8, 16, 32]))
+        k = int(np.floor(np.exp(rng.uniform(0.0, np.log(513.0)))))
+        specs.append((scale, ef, max(1, min(512, k)), seed + 1000 + i))
+    return specs
+
+
+def run_multi(args, w, name) -> None:
+    """Config of many uneven graphs: batched (one launch) vs plain (one call per query)."""
+    import torch
+
+    import xbtrav
+
+    dev = torch.device("cuda", 0)
+    t0 = time.perf_counter()
+    specs = multi_instances(w["instances"], SEED)
+    hosts = [xbtrav.HostCSR.rmat(sc, ef, 0.57, 0.19, 0.19, seed=gs) for sc, ef, _, gs in specs]
+    ctx = xbtrav.Context(0)
+    if args.chains:
+        ctx.set_tuning(chains=args.chains)
+    graphs = ctx.upload_batch(hosts)
+    queries = []
+    for (sc, ef, k, gs), g in zip(specs, graphs):
+        queries.append((g, torch.from_numpy(g.select_sources(gs + 1, k)).to(dev)))
+    outs = [(torch.empty((int(q.numel()), g.n), dtype=torch.int32, device=dev),
+             torch.empty((int(q.numel()), g.n), dtype=torch.int32, device=dev)) for g, q in queries]
+    setup_s = time.perf_counter() - t0
+    stream = torch.cuda.ExternalStream(ctx.stream_handle(), device=dev)
+
+    def batched():
+        return ctx.traverse_batched(queries, outputs=outs)[1]["edges_traversed"]
+
+    def plain():
+        e = 0
+        for (g, q), (lv, pr) in zip(queries, outs):
+            e += ctx.traverse(g, q, out="device", level=lv, parent=pr).stats["edges_traversed"]
+        return e
+
+    def timed(fn, steps):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize(dev)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            ev0.record(stream)
+        e = sum(fn() for _ in range(steps))
+        with torch.cuda.stream(stream):
+            ev1.record(stream)
+        torch.cuda.synchronize(dev)
+        return ev0.elapsed_time(ev1), e
+
+    clocks = ClockSampler(0)
+    clocks.start()
+    b_ms, b_e = timed(batched, args.steps)
+    clk = clocks.stop()
+    p_ms, p_e = timed(plain, args.steps)
+    value = b_e / (b_ms / 1e3) / 1e9
+    plain_v = p_e / (p_ms / 1e3) / 1e9
+    tun = ctx.tuning()
+    line = {
+        "metric": METRIC, "value": value, "unit": "GTEPS", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": b_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u64", "data": "synthetic (seeded R-MAT generator)",
+        "config": {"workload": name, "instances": len(specs), "sources": int(sum(s[2] for s in specs)),
+                   "vertices": int(sum(g.n for g in graphs)), "m_directed": int(sum(g.m for g in graphs)),
+                   "seed": SEED, "layout": "one concatenated CSR, per-instance offsets (xb_graph_upload_batch)",
+                   "path": f"xb_traverse_batched, {tun['chains']} chains"},
+        "batched_gteps": value, "plain_gteps": plain_v, "batched_over_plain": value / plain_v,
+        "plain_ms_per_step": p_ms / args.steps, "clocks": clk, "setup_s": setup_s,
+    }
+    print(json.dumps(line), flush=True)
+    for g in graphs:
+        g.close()
+    ctx.close()
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -225,7 +311,14 @@ def main() -> None:
     args.warmup = max(args.warmup, 3)
     w = WORKLOADS[args.workload]
     if args.impl == "reference":
+        if w["kind"] == "multi":
+            print(json.dumps({"impl": "reference", "unavailable": "the uneven multi-graph workload is timed on the GPU "
+                              "paths only; the reference arm runs the single-graph workloads"}))
+            return
         run_reference(args, w, args.workload)
+        return
+    if w["kind"] == "multi":
+        run_multi(args, w, args.workload)
         return
 
     import torch

@@ -143,6 +143,17 @@ xb_status xb_graph_upload(xb_ctx* ctx, int64_t n, const void* row_offsets,
                           int32_t offsets_are_64bit, int64_t m, const int32_t* col_indices,
                           xb_graph** out);
 xb_status xb_graph_from_host_csr(xb_ctx* ctx, const xb_host_csr* g, xb_graph** out);
+/* Uploads ninst independent graphs stored back to back as ONE device CSR with
+ * per-instance offsets: instance i has inst_n[i] vertices; its row offsets
+ * (inst_n[i] + 1 entries, local, starting at 0) follow those of instance i-1
+ * in row_offsets, and its column indices (local ids, row_offsets[..][n]
+ * entries) follow those of instance i-1 in col_indices.  out[i] receives a
+ * graph handle per instance (views of the shared arrays; each is freed with
+ * xb_graph_free, the arrays with the last of them).  Offsets are stored as
+ * int32 unless an instance has 2^31-1 or more entries. */
+xb_status xb_graph_upload_batch(xb_ctx* ctx, int32_t ninst, const int64_t* inst_n,
+                                const int64_t* row_offsets, const int32_t* col_indices,
+                                xb_graph** out);
 xb_status xb_graph_load_csr_text(xb_ctx* ctx, const char* row_path, const char* col_path,
                                  xb_graph** out);
 xb_status xb_graph_free(xb_graph* g);

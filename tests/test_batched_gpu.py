@@ -112,6 +112,30 @@ def test_uneven_multi_graph_batch(ctx, out, chains):
         g.close()
 
 
+@pytest.mark.parametrize("chains", [2, 8])
+def test_concatenated_csr_instances(ctx, chains):
+    """Instances uploaded as one concatenated CSR (xb_graph_upload_batch)
+    traverse exactly like separately uploaded graphs, on both paths."""
+    gs, queries = _uneven_graphs()
+    _tune(ctx, chains=chains)
+    views = ctx.upload_batch(gs)
+    assert [v.n for v in views] == [len(ro) - 1 for ro, _ in gs]
+    res, st = ctx.traverse_batched([(views[gi], src) for gi, src in queries])
+    for (gi, src), r in zip(queries, res):
+        _check(*gs[gi], src, r)
+        plain = ctx.traverse(views[gi], src)
+        np.testing.assert_array_equal(plain.level, _host(r.level))
+        np.testing.assert_array_equal(plain.parent, _host(r.parent))
+    # freeing some views leaves the others usable
+    for v in views[::2]:
+        v.close()
+    gi, src = next((q for q in queries if q[0] % 2 == 1))
+    r = ctx.traverse(views[gi], src)
+    _check(*gs[gi], src, r)
+    for v in views[1::2]:
+        v.close()
+
+
 def test_same_results_as_plain_path(ctx):
     h = xbtrav.HostCSR.rmat(14, 16, seed=9)
     ro, ci = h.arrays()

@@ -450,13 +450,15 @@ xb_status xb_graph_upload(xb_ctx* c, int64_t n, const void* row_offsets, int32_t
   const size_t ro_bytes = (g->off64 ? 8 : 4) * (size_t)(n + 1);
   // colIndices carries kCiPad zero entries past the end: the 16-byte loads of
   // the per-lane pull read whole aligned groups of 4 entries
-  if (cudaMalloc(&g->d_ro, ro_bytes) != cudaSuccess ||
-      cudaMalloc(&g->d_ci, sizeof(int32_t) * (size_t)(m + xbe::kCiPad)) != cudaSuccess) {
+  g->store = std::make_shared<xb_csr_store>();
+  g->store->device = c->device;
+  if (cudaMalloc(&g->store->ro, ro_bytes) != cudaSuccess ||
+      cudaMalloc(&g->store->ci, sizeof(int32_t) * (size_t)(m + xbe::kCiPad)) != cudaSuccess) {
     cudaGetLastError();
-    if (g->d_ro) cudaFree(g->d_ro);
-    if (g->d_ci) cudaFree(g->d_ci);
     return fail(XB_ERR_OOM, "graph allocation failed");
   }
+  g->d_ro = g->store->ro;
+  g->d_ci = g->store->ci;
   if (g->off64) {
     XB_CUDA(cudaMemcpy(g->d_ro, ro.data(), ro_bytes, cudaMemcpyHostToDevice));
   } else {
@@ -468,6 +470,69 @@ xb_status xb_graph_upload(xb_ctx* c, int64_t n, const void* row_offsets, int32_t
   if (m > 0) XB_CUDA(cudaMemcpy(g->d_ci, col_indices, sizeof(int32_t) * (size_t)m, cudaMemcpyHostToDevice));
   g->h_ro = std::move(ro);
   *out = g.release();
+  return XB_OK;
+}
+
+xb_status xb_graph_upload_batch(xb_ctx* c, int32_t ninst, const int64_t* inst_n, const int64_t* row_offsets,
+                                const int32_t* col_indices, xb_graph** out) {
+  xbi::clear_error();
+  if (!c || !out || !inst_n || ninst < 1) return fail(XB_ERR_ARG, "bad arguments");
+  if (!row_offsets) return fail(XB_ERR_ARG, "null row offsets");
+  for (int32_t i = 0; i < ninst; i++) out[i] = nullptr;
+  // host-side offsets of every instance; validation per instance
+  std::vector<int64_t> vtx_off((size_t)ninst + 1, 0), edge_src((size_t)ninst + 1, 0), edge_dev((size_t)ninst + 1, 0);
+  bool off64 = false;
+  for (int32_t i = 0; i < ninst; i++) {
+    const int64_t n = inst_n[i];
+    if (n < 1 || n >= INT32_MAX) return fail(XB_ERR_ARG, "instance " + std::to_string(i) + ": n out of range");
+    const int64_t* ro = row_offsets + vtx_off[(size_t)i];
+    const int64_t m = ro[n];
+    xb_status s = xbi::validate_csr(n, ro, col_indices ? col_indices + edge_src[(size_t)i] : nullptr);
+    if (s != XB_OK) return fail(s, "instance " + std::to_string(i) + ": " + xb_last_error());
+    off64 = off64 || m >= (int64_t)INT32_MAX;
+    vtx_off[(size_t)i + 1] = vtx_off[(size_t)i] + n + 1;
+    edge_src[(size_t)i + 1] = edge_src[(size_t)i] + m;
+    edge_dev[(size_t)i + 1] = edge_dev[(size_t)i] + ((m + 3) & ~(int64_t)3);  // instances start 16-byte aligned
+  }
+  XB_CUDA(cudaSetDevice(c->device));
+  auto store = std::make_shared<xb_csr_store>();
+  store->device = c->device;
+  const size_t nro = (size_t)vtx_off[(size_t)ninst];
+  const size_t ro_bytes = (off64 ? 8 : 4) * nro;
+  const size_t nci = (size_t)edge_dev[(size_t)ninst] + (size_t)xbe::kCiPad;
+  if (cudaMalloc(&store->ro, ro_bytes) != cudaSuccess || cudaMalloc(&store->ci, sizeof(int32_t) * nci) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(XB_ERR_OOM, "batch graph allocation failed");
+  }
+  if (off64) {
+    XB_CUDA(cudaMemcpy(store->ro, row_offsets, ro_bytes, cudaMemcpyHostToDevice));
+  } else {
+    std::vector<int32_t> r32(nro);
+    for (size_t i = 0; i < nro; i++) r32[i] = (int32_t)row_offsets[i];
+    XB_CUDA(cudaMemcpy(store->ro, r32.data(), ro_bytes, cudaMemcpyHostToDevice));
+  }
+  XB_CUDA(cudaMemset(store->ci, 0, sizeof(int32_t) * nci));
+  std::vector<std::unique_ptr<xb_graph>> gs;
+  for (int32_t i = 0; i < ninst; i++) {
+    const int64_t n = inst_n[i];
+    const int64_t* ro = row_offsets + vtx_off[(size_t)i];
+    const int64_t m = ro[n];
+    if (m > 0)
+      XB_CUDA(cudaMemcpy(store->ci + edge_dev[(size_t)i], col_indices + edge_src[(size_t)i], sizeof(int32_t) * (size_t)m,
+                         cudaMemcpyHostToDevice));
+    std::unique_ptr<xb_graph> g(new xb_graph());
+    g->ctx = c;
+    g->n = n;
+    g->m = m;
+    g->off64 = off64;
+    g->store = store;
+    g->d_ro = (char*)store->ro + (off64 ? 8 : 4) * (size_t)vtx_off[(size_t)i];
+    g->d_ci = store->ci + edge_dev[(size_t)i];
+    g->h_ro.assign(ro, ro + n + 1);
+    for (int64_t v = 0; v < n; v++) g->max_deg = std::max(g->max_deg, ro[v + 1] - ro[v]);
+    gs.push_back(std::move(g));
+  }
+  for (int32_t i = 0; i < ninst; i++) out[i] = gs[(size_t)i].release();
   return XB_OK;
 }
 
@@ -491,8 +556,7 @@ xb_status xb_graph_free(xb_graph* g) {
   if (!g) return XB_OK;
   cudaSetDevice(g->ctx->device);
   xbe::batch_forget_graph(g->ctx, g);
-  if (g->d_ro) cudaFree(g->d_ro);
-  if (g->d_ci) cudaFree(g->d_ci);
+  g->store.reset();  // frees the CSR arrays with the last graph viewing them
   if (g->d_heavy) cudaFree(g->d_heavy);
   if (g->d_hpar) cudaFree(g->d_hpar);
   if (g->d_hitems) cudaFree(g->d_hitems);

@@ -8,6 +8,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -51,12 +52,28 @@ struct xb_ctx {
   xbe::BatchState* batch = nullptr;  // resources of xb_traverse_batched (created on first use)
 };
 
+// Device CSR arrays, shared by the graphs that view them (one upload, or all
+// instances of a batch upload); freed with the last view.
+struct xb_csr_store {
+  int device = 0;
+  void* ro = nullptr;
+  int32_t* ci = nullptr;
+  ~xb_csr_store() {
+    if (ro || ci) {
+      cudaSetDevice(device);
+      if (ro) cudaFree(ro);
+      if (ci) cudaFree(ci);
+    }
+  }
+};
+
 struct xb_graph {
   xb_ctx* ctx = nullptr;
   int64_t n = 0, m = 0, max_deg = 0;
   bool off64 = false;
-  void* d_ro = nullptr;
-  int32_t* d_ci = nullptr;
+  std::shared_ptr<xb_csr_store> store;
+  void* d_ro = nullptr;     // this graph's row offsets inside store->ro
+  int32_t* d_ci = nullptr;  // this graph's colIndices inside store->ci (16-byte aligned)
   std::vector<int64_t> h_ro;
   int32_t* d_heavy = nullptr;  // vertices with degree > heavy_thr, ascending
   int32_t* d_hpar = nullptr;   // per heavy vertex, 64 parent slots of the table pass

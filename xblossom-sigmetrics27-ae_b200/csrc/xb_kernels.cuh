@@ -396,7 +396,7 @@ __global__ void k_push_light(const int32_t* __restrict__ list, const int32_t* __
       bool app = false;
       int32_t w = 0;
       if (e < end) {
-        w = __ldg(&ci[e]);
+        w = __ldcs(&ci[e]);
         app = push_edge<W, NW>(w, f, seen, N, stamp, epoch);
       }
       warp_append(app, w, touched, &nctr->n_touched);
@@ -436,7 +436,7 @@ __global__ void k_push_heavy(const int32_t* __restrict__ list, const int32_t* __
         bool app = false;
         int32_t w = 0;
         if (e < ce) {
-          w = __ldg(&ci[e]);
+          w = __ldcs(&ci[e]);
           app = push_edge<W, NW>(w, f, seen, N, stamp, epoch);
         }
         warp_append(app, w, touched, &nctr->n_touched);
@@ -618,7 +618,7 @@ __global__ void __launch_bounds__(WARPS * 32, 32 / WARPS) k_pull_tiles(int64_t n
       for (int u = 0; u < U; u++) {
         const int32_t wb = base + u * 32;
         wo[u] = window_owner(off, d, wb, total, s_r2l[wib]);
-        col[u] = wo[u].owner >= 0 ? __ldg(&ci[s_base[wib][wo[u].owner] + wb + lane]) : -1;
+        col[u] = wo[u].owner >= 0 ? __ldcs(&ci[s_base[wib][wo[u].owner] + wb + lane]) : -1;
       }
       W f[U][NW];
 #pragma unroll
@@ -705,6 +705,10 @@ __global__ void __launch_bounds__(WARPS * 32, 32 / WARPS) k_pull_tiles(int64_t n
   }
 }
 
+// colIndices are read once per step and are larger than L2: their loads use
+// the streaming (evict-first) path so the frontier and seen words the edges
+// gather stay resident in L2.
+//
 // Pull, light vertices (degree 1..heavy), one vertex per lane.  The graph's
 // light vertices are listed by falling degree (lorder), so the 32 lanes of a
 // warp walk adjacencies of nearly equal length; warps take chunks of the list
@@ -746,14 +750,14 @@ __device__ __forceinline__ void pull_lane_vertex(bool act, int32_t v, const W (&
   int64_t j0 = beg & ~(int64_t)3;
   int4 qa = make_int4(0, 0, 0, 0), qb = make_int4(0, 0, 0, 0);
   if (j0 < end) {
-    qa = __ldg(reinterpret_cast<const int4*>(ci + j0));
-    qb = __ldg(reinterpret_cast<const int4*>(ci + j0 + 4));
+    qa = __ldcs(reinterpret_cast<const int4*>(ci + j0));
+    qb = __ldcs(reinterpret_cast<const int4*>(ci + j0 + 4));
   }
   for (; j0 < end; j0 += 8) {
     const int32_t cols[8] = {qa.x, qa.y, qa.z, qa.w, qb.x, qb.y, qb.z, qb.w};
     if (j0 + 8 < end) {
-      qa = __ldg(reinterpret_cast<const int4*>(ci + j0 + 8));
-      qb = __ldg(reinterpret_cast<const int4*>(ci + j0 + 12));
+      qa = __ldcs(reinterpret_cast<const int4*>(ci + j0 + 8));
+      qb = __ldcs(reinterpret_cast<const int4*>(ci + j0 + 12));
     }
     W f[8][NW];
 #pragma unroll
@@ -986,7 +990,7 @@ __global__ void k_pull_heavy(const int32_t* __restrict__ hlist, int32_t nh, cons
 #pragma unroll
     for (int u = 0; u < U; u++) {
       const int64_t e = beg + u * 32 + lane;
-      coln[u] = e < end ? __ldg(&ci[e]) : -1;
+      coln[u] = e < end ? __ldcs(&ci[e]) : -1;
     }
     for (int64_t base = beg; base < end; base += 32 * U) {
       int32_t col[U];
@@ -994,7 +998,7 @@ __global__ void k_pull_heavy(const int32_t* __restrict__ hlist, int32_t nh, cons
       for (int u = 0; u < U; u++) {
         col[u] = coln[u];
         const int64_t e = base + 32 * U + u * 32 + lane;
-        coln[u] = e < end ? __ldg(&ci[e]) : -1;
+        coln[u] = e < end ? __ldcs(&ci[e]) : -1;
       }
       W f[U][NW];
 #pragma unroll
@@ -1094,7 +1098,7 @@ __global__ void k_pull_hubs(const int32_t* __restrict__ hlist, const int2* __res
 #pragma unroll
       for (int u = 0; u < U; u++) {
         const int64_t e = base + u * 32 + lane;
-        col[u] = e < ce ? __ldg(&ci[e]) : -1;
+        col[u] = e < ce ? __ldcs(&ci[e]) : -1;
       }
       W f[U][NW];
 #pragma unroll
@@ -1354,7 +1358,7 @@ __global__ void __launch_bounds__(WARPS * 32, 32 / WARPS) k_tables(int64_t n, co
         if (e < take) {
           const int o = flat_owner(s_off[wib], e);
           key[u] = o;
-          col[u] = __ldg(&ci[s_pos[wib][o] + (e - s_off[wib][o])]);
+          col[u] = __ldcs(&ci[s_pos[wib][o] + (e - s_off[wib][o])]);
         }
       }
 #pragma unroll
@@ -1553,7 +1557,7 @@ __global__ void __launch_bounds__(256) k_tables_heavy_scan(const int32_t* __rest
 #pragma unroll
         for (int u = 0; u < 4; u++) {
           const int64_t e = base + u * 256 + threadIdx.x;
-          col[u] = e < ce ? __ldg(&ci[e]) : -1;
+          col[u] = e < ce ? __ldcs(&ci[e]) : -1;
         }
 #pragma unroll
         for (int u = 0; u < 4; u++) {

@@ -132,6 +132,7 @@ def lib() -> C.CDLL:
         "xb_ctx_get_stream": (i32, [vp, P(vp)]),
         "xb_graph_upload": (i32, [vp, i64, vp, i32, i64, vp, P(vp)]),
         "xb_graph_from_host_csr": (i32, [vp, vp, P(vp)]),
+        "xb_graph_upload_batch": (i32, [vp, i32, vp, vp, vp, P(vp)]),
         "xb_graph_load_csr_text": (i32, [vp, C.c_char_p, C.c_char_p, P(vp)]),
         "xb_graph_free": (i32, [vp]),
         "xb_graph_info": (i32, [vp, P(i64), P(i64), P(i64)]),
@@ -321,6 +322,24 @@ class Context:
         _check(lib().xb_graph_upload(self._h, len(ro) - 1, ro.ctypes.data, 1, int(ro[-1]),
                                      ci.ctypes.data if len(ci) else None, C.byref(h)))
         return Graph(self, h.value)
+
+    def upload_batch(self, graphs) -> list:
+        """Uploads several graphs as ONE device CSR with per-instance offsets
+        (xb_graph_upload_batch); graphs: list of HostCSR or (row_offsets,
+        col_indices) pairs.  Returns one Graph per instance."""
+        ros, cis, ns = [], [], []
+        for gr in graphs:
+            ro, ci = gr.arrays() if isinstance(gr, HostCSR) else gr
+            ros.append(np.ascontiguousarray(ro, dtype=np.int64))
+            cis.append(np.ascontiguousarray(ci, dtype=np.int32))
+            ns.append(len(ros[-1]) - 1)
+        ro_all = np.concatenate(ros)
+        ci_all = np.concatenate(cis) if sum(len(c) for c in cis) else np.zeros(1, np.int32)
+        n_arr = np.array(ns, dtype=np.int64)
+        hs = (C.c_void_p * len(ns))()
+        _check(lib().xb_graph_upload_batch(self._h, len(ns), n_arr.ctypes.data, ro_all.ctypes.data,
+                                           ci_all.ctypes.data, hs))
+        return [Graph(self, h) for h in hs]
 
     def load_text(self, row_path: str, col_path: str) -> Graph:
         h = C.c_void_p()
