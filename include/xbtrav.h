@@ -202,6 +202,41 @@ typedef struct xb_batch_item {
 xb_status xb_traverse_batched(xb_ctx* ctx, const xb_batch_item* items, int32_t nitems,
                               xb_stats* stats);
 
+/* ---- serving slots ------------------------------------------------------ */
+/* Summary of one source's tables, for serving clients that need no full
+ * tables: reached = vertices with level >= 0, level_sum and parent_sum over
+ * them, depth = the largest level. */
+typedef struct xb_row_digest {
+  int64_t reached;
+  int64_t level_sum;
+  int64_t parent_sum;
+  int32_t depth; /* -1 for a row written to a caller buffer (no digest taken) */
+  int32_t pad;
+} xb_row_digest;
+
+#define XB_MAX_SLOTS 16
+/* Asynchronous passes for a serving loop (no counterpart in the reference,
+ * which has no serving path).  A slot (0..XB_MAX_SLOTS-1) runs one pass of up
+ * to word_bits*words sources of ONE graph at a time, on its own stream and
+ * workspace, so passes on different slots overlap on the device; a host
+ * scheduler packs the sources of whatever queries are waiting into each pass.
+ * level_rows[j] / parent_rows[j] are device pointers to the n-entry rows of
+ * source j (sources is a host array); a NULL pair sends both rows to the
+ * slot's scratch and only their digest comes back.  The slot must be idle
+ * (XB_ERR_STATE otherwise); the call returns once the pass is queued.
+ * Results match xb_traverse's for the same sources. */
+xb_status xb_slot_launch(xb_ctx* ctx, int32_t slot, const xb_graph* g, const int32_t* sources,
+                         int32_t kb, int32_t* const* level_rows, int32_t* const* parent_rows);
+/* Non-blocking: *done = 0 while the slot's pass runs; *done = 1 once it has
+ * finished, with its counters in stats and kb digests in digests (either may
+ * be NULL); the slot is then idle.  XB_ERR_STATE for an idle slot. */
+xb_status xb_slot_poll(xb_ctx* ctx, int32_t slot, int32_t* done, xb_stats* stats,
+                       xb_row_digest* digests);
+/* Blocking form of xb_slot_poll. */
+xb_status xb_slot_wait(xb_ctx* ctx, int32_t slot, xb_stats* stats, xb_row_digest* digests);
+/* Frees every slot's device memory (all slots must be idle). */
+xb_status xb_slots_release(xb_ctx* ctx);
+
 /* ---- traversal without device allocation -------------------------------- */
 /* No counterpart in the reference (whose engine allocates all its device
  * buffers itself): an entry point for callers that may not allocate device

@@ -34,6 +34,8 @@ namespace xbe {
 
 constexpr int kMaxChains = 16;
 constexpr size_t kMaxCached = 8;
+// One-pass graphs a serving slot keeps (one per source count seen, at most 64 x 4 words).
+constexpr size_t kSlotMaxCached = 80;
 
 struct Chain {
   void* ws = nullptr;
@@ -54,8 +56,37 @@ struct CachedGraph {
   uint64_t last_use = 0;
 };
 
+// A serving slot: one pass in flight at a time on its own stream, with its
+// own workspace (so slots run concurrently), staging, scratch rows for
+// digest-only sources, and cached one-pass graphs.
+constexpr int kMaxSlots = 16;
+constexpr int kSlotMaxRows = 256;  // 64 sources x 4 words
+
+struct SlotState {
+  bool init = false, busy = false;
+  int kb = 0;
+  void* ws = nullptr;
+  size_t ws_bytes = 0;
+  xbk::Ctrs* ctr = nullptr;
+  int32_t* hpar = nullptr;
+  size_t hpar_bytes = 0;
+  int32_t* scratch = nullptr;  // level rows then parent rows, kSlotMaxRows each, n_scratch apart
+  size_t scratch_bytes = 0;
+  int64_t n_scratch = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t done = nullptr;
+  int32_t *d_src = nullptr, *h_src = nullptr;
+  int32_t **d_rows = nullptr, **h_rows = nullptr;
+  int32_t *d_flags = nullptr, *h_flags = nullptr;
+  xbk::PassSum *d_sum = nullptr, *h_sum = nullptr;
+  xbk::RowDigest *d_dig = nullptr, *h_dig = nullptr;
+  std::vector<CachedGraph> cache;
+  uint64_t gen = 1, tick = 0;
+};
+
 struct BatchState {
   int device = 0;
+  SlotState slots[kMaxSlots];
   Chain chains[kMaxChains];
   xbk::PassSum* d_sums = nullptr;  // one per chain
   xbk::PassSum* h_sums = nullptr;  // pinned
@@ -218,6 +249,44 @@ xb_status capture_level_loop(BatchState* bs, const PassRes<W, NW, OffT>& p, cons
   return end_body(b0, st);
 }
 
+// A pass's resources for capture: workspace, counters, heavy-parent slots.
+template <typename W, int NW, typename OffT>
+PassRes<W, NW, OffT> capture_res(xb_ctx* c, const xb_graph* g, void* ws, xbk::Ctrs* ctr, int32_t* hpar) {
+  const int heavy = std::max(32, c->tuning.heavy_degree);
+  return pass_res<W, NW, OffT>(g, ws, layout_for(g->n, (int)sizeof(W), NW), ctr, hpar, heavy);
+}
+
+// First half of a captured pass on stream s: init and the device level loop.
+template <typename W, int NW, typename OffT>
+xb_status capture_pass_levels(xb_ctx* c, BatchState* bs, const PassRes<W, NW, OffT>& p, const xb_graph* g,
+                              const int32_t* src, int kb, cudaStream_t s) {
+  const int sms = c->num_sms;
+  const float alpha = c->tuning.pull_alpha > 0 ? c->tuning.pull_alpha : 256.0f;
+  const StepShape sh = graph_shape<W, NW, OffT>(g, sms);
+  xb_status st = emit_pass_init<W, NW, OffT>(p, g, src, kb, s, sms, true);
+  if (st != XB_OK) return st;
+  return capture_level_loop<W, NW, OffT>(bs, p, g, kb, alpha, sh, s, sms);
+}
+
+// Second half: the table pass through the row table and the fold into *sum.
+template <typename W, int NW, typename OffT>
+xb_status capture_pass_tables(xb_ctx* c, const PassRes<W, NW, OffT>& p, const xb_graph* g, const int32_t* src,
+                              int kb, int32_t* const* rows, xbk::PassSum* sum, cudaStream_t s) {
+  constexpr int B = xbk::WB<W>::bits;
+  int64_t launches = 0;
+  xb_status st = emit_tables<W, NW, OffT>(p, g, src, kb, rows, true, s, c->num_sms, &launches);
+  if (st != XB_OK) return st;
+  const int hv = g->n_heavy > 0 ? 1 : 0;
+  const int words = (kb + B - 1) / B;
+  const int fixed_k = hv + 2 + words * (1 + hv) + 1;
+  const int push_k = 2 + 2 * hv;
+  const int pull_k = 2 + hv + (g->n_hub_items > 0 ? 2 : 0);
+  xbk::k_pass_accum<<<1, 1, 0, s>>>(p.ctr, sum, (long long)g->n, kb, (int)sizeof(OffT) * 2, (int)sizeof(W), NW,
+                                    fixed_k, push_k, pull_k);
+  XB_LAUNCH_CHECK("pass accumulate");
+  return XB_OK;
+}
+
 // One pass on its chain's compute stream (and copy stream for host rows).
 template <typename W, int NW, typename OffT>
 xb_status capture_pass(xb_ctx* c, BatchState* bs, const PassPlan& pp, int64_t rows_off, int64_t n_stage,
@@ -226,29 +295,13 @@ xb_status capture_pass(xb_ctx* c, BatchState* bs, const PassPlan& pp, int64_t ro
   constexpr int SPP = B * NW;
   Chain& ch = bs->chains[pp.chain];
   const xb_graph* g = pp.g;
-  const int sms = c->num_sms;
-  const int heavy = std::max(32, c->tuning.heavy_degree);
-  const float alpha = c->tuning.pull_alpha > 0 ? c->tuning.pull_alpha : 256.0f;
-  const WsLayout L = layout_for(g->n, (int)sizeof(W), NW);
-  const PassRes<W, NW, OffT> p = pass_res<W, NW, OffT>(g, ch.ws, L, ch.ctr, ch.hpar, heavy);
-  const StepShape sh = graph_shape<W, NW, OffT>(g, sms);
+  const PassRes<W, NW, OffT> p = capture_res<W, NW, OffT>(c, g, ch.ws, ch.ctr, ch.hpar);
   const int32_t* src = bs->d_src + pp.src_off;
-  xb_status st = emit_pass_init<W, NW, OffT>(p, g, src, pp.kb, ch.cs, sms, true);
-  if (st != XB_OK) return st;
-  st = capture_level_loop<W, NW, OffT>(bs, p, g, pp.kb, alpha, sh, ch.cs, sms);
+  xb_status st = capture_pass_levels<W, NW, OffT>(c, bs, p, g, src, pp.kb, ch.cs);
   if (st != XB_OK) return st;
   if (pp.host && slot_used[pp.chain][pp.slot]) XB_CUDA(cudaStreamWaitEvent(ch.cs, ch.ev_free[pp.slot], 0));
-  int64_t launches = 0;
-  st = emit_tables<W, NW, OffT>(p, g, src, pp.kb, bs->d_rows + rows_off, true, ch.cs, sms, &launches);
+  st = capture_pass_tables<W, NW, OffT>(c, p, g, src, pp.kb, bs->d_rows + rows_off, bs->d_sums + pp.chain, ch.cs);
   if (st != XB_OK) return st;
-  const int hv = g->n_heavy > 0 ? 1 : 0;
-  const int words = (pp.kb + B - 1) / B;
-  const int fixed_k = hv + 2 + words * (1 + hv) + 1;
-  const int push_k = 2 + 2 * hv;
-  const int pull_k = 2 + hv + (g->n_hub_items > 0 ? 2 : 0);
-  xbk::k_pass_accum<<<1, 1, 0, ch.cs>>>(p.ctr, bs->d_sums + pp.chain, (long long)g->n, pp.kb,
-                                        (int)sizeof(OffT) * 2, (int)sizeof(W), NW, fixed_k, push_k, pull_k);
-  XB_LAUNCH_CHECK("pass accumulate");
   if (pp.host) {
     XB_CUDA(cudaEventRecord(ch.ev_tab, ch.cs));
     XB_CUDA(cudaStreamWaitEvent(ch.cps, ch.ev_tab, 0));
@@ -592,9 +645,220 @@ xb_status run_batched(xb_ctx* c, const std::vector<xb_batch_item>& items, const 
 
 }  // namespace
 
+namespace {
+
+void slot_free(SlotState& sl) {
+  if (sl.stream) cudaStreamSynchronize(sl.stream);
+  for (auto& e : sl.cache)
+    if (e.exec) cudaGraphExecDestroy(e.exec);
+  sl.cache.clear();
+  for (void* p : {(void*)sl.ws, (void*)sl.ctr, (void*)sl.hpar, (void*)sl.scratch, (void*)sl.d_src, (void*)sl.d_rows,
+                  (void*)sl.d_flags, (void*)sl.d_sum, (void*)sl.d_dig})
+    if (p) cudaFree(p);
+  for (void* p : {(void*)sl.h_src, (void*)sl.h_rows, (void*)sl.h_flags, (void*)sl.h_sum, (void*)sl.h_dig})
+    if (p) cudaFreeHost(p);
+  if (sl.done) cudaEventDestroy(sl.done);
+  if (sl.stream) cudaStreamDestroy(sl.stream);
+  sl = SlotState();
+}
+
+xb_status slot_init(SlotState& sl) {
+  if (sl.init) return XB_OK;
+  XB_CUDA(cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking));
+  XB_CUDA(cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming));
+  XB_CUDA(cudaMalloc(&sl.d_src, sizeof(int32_t) * kSlotMaxRows));
+  XB_CUDA(cudaMallocHost(&sl.h_src, sizeof(int32_t) * kSlotMaxRows));
+  XB_CUDA(cudaMalloc(&sl.d_rows, sizeof(int32_t*) * 2 * kSlotMaxRows));
+  XB_CUDA(cudaMallocHost(&sl.h_rows, sizeof(int32_t*) * 2 * kSlotMaxRows));
+  XB_CUDA(cudaMalloc(&sl.d_flags, sizeof(int32_t) * kSlotMaxRows));
+  XB_CUDA(cudaMallocHost(&sl.h_flags, sizeof(int32_t) * kSlotMaxRows));
+  XB_CUDA(cudaMalloc(&sl.d_sum, sizeof(xbk::PassSum)));
+  XB_CUDA(cudaMallocHost(&sl.h_sum, sizeof(xbk::PassSum)));
+  XB_CUDA(cudaMalloc(&sl.d_dig, sizeof(xbk::RowDigest) * kSlotMaxRows));
+  XB_CUDA(cudaMallocHost(&sl.h_dig, sizeof(xbk::RowDigest) * kSlotMaxRows));
+  XB_CUDA(cudaMalloc(&sl.ctr, sizeof(xbk::Ctrs)));
+  XB_CUDA(cudaMemset(sl.ctr, 0, sizeof(xbk::Ctrs)));
+  sl.init = true;
+  return XB_OK;
+}
+
+// Captures the one-pass graph of a slot: clear the totals, the pass, the
+// digests of the flagged rows, and the copies of totals and digests to the
+// slot's pinned mirrors.
+template <typename W, int NW, typename OffT>
+xb_status capture_slot_pass(xb_ctx* c, BatchState* bs, SlotState& sl, const xb_graph* g, int kb,
+                            cudaGraphExec_t* exec) {
+  constexpr int B = xbk::WB<W>::bits;
+  cudaStream_t s = sl.stream;
+  XB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
+  auto body = [&]() -> xb_status {
+    XB_CUDA(cudaMemsetAsync(sl.d_sum, 0, sizeof(xbk::PassSum), s));
+    XB_CUDA(cudaMemsetAsync(sl.d_dig, 0, sizeof(xbk::RowDigest) * kSlotMaxRows, s));
+    const PassRes<W, NW, OffT> p = capture_res<W, NW, OffT>(c, g, sl.ws, sl.ctr, sl.hpar);
+    xb_status st = capture_pass_levels<W, NW, OffT>(c, bs, p, g, sl.d_src, kb, s);
+    if (st != XB_OK) return st;
+    st = capture_pass_tables<W, NW, OffT>(c, p, g, sl.d_src, kb, sl.d_rows, sl.d_sum, s);
+    if (st != XB_OK) return st;
+    const int gx = (int)std::max<int64_t>(1, std::min<int64_t>((g->n + 2047) / 2048, 64));
+    xbk::k_row_digest<<<dim3((unsigned)gx, (unsigned)kb), 256, 0, s>>>(sl.d_rows, sl.d_flags, kb, B, g->n, sl.d_dig);
+    XB_LAUNCH_CHECK("row digest");
+    XB_CUDA(cudaMemcpyAsync(sl.h_sum, sl.d_sum, sizeof(xbk::PassSum), cudaMemcpyDeviceToHost, s));
+    XB_CUDA(cudaMemcpyAsync(sl.h_dig, sl.d_dig, sizeof(xbk::RowDigest) * kb, cudaMemcpyDeviceToHost, s));
+    return XB_OK;
+  };
+  xb_status st = body();
+  cudaGraph_t graph = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(s, &graph);
+  if (st == XB_OK && e != cudaSuccess) st = fail(XB_ERR_CUDA, std::string("slot capture: ") + cudaGetErrorString(e));
+  if (st == XB_OK) {
+    const cudaError_t ei = cudaGraphInstantiate(exec, graph, 0);
+    if (ei != cudaSuccess) st = fail(XB_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ei));
+  }
+  if (graph) cudaGraphDestroy(graph);
+  cudaGetLastError();
+  return st;
+}
+
+template <typename W, int NW>
+xb_status slot_launch(xb_ctx* c, int slot, xb_graph* g, const int32_t* sources, int kb,
+                      int32_t* const* level_rows, int32_t* const* parent_rows) {
+  constexpr int B = xbk::WB<W>::bits;
+  constexpr int SPP = B * NW;
+  if (kb < 1 || kb > SPP) return fail(XB_ERR_ARG, "a slot pass takes 1.." + std::to_string(SPP) + " sources");
+  xb_status st = make_state(c);
+  if (st != XB_OK) return st;
+  BatchState* bs = c->batch;
+  SlotState& sl = bs->slots[slot];
+  if (sl.busy) return fail(XB_ERR_STATE, "slot " + std::to_string(slot) + " has a pass in flight");
+  st = slot_init(sl);
+  if (st != XB_OK) return st;
+  const int heavy = std::max(32, c->tuning.heavy_degree);
+  st = ensure_heavy(g, heavy);
+  if (st != XB_OK) return st;
+  // resources for this graph
+  size_t cap = sl.ws_bytes;
+  st = grow(&sl.ws, &cap, layout_for(g->n, (int)sizeof(W), NW).total, &sl.gen, "slot workspace");
+  sl.ws_bytes = cap;
+  if (st != XB_OK) return st;
+  cap = sl.hpar_bytes;
+  st = grow(&sl.hpar, &cap, sizeof(int32_t) * (size_t)std::max(g->n_heavy, 1) * kHparRow, &sl.gen, "slot heavy slots");
+  sl.hpar_bytes = cap;
+  if (st != XB_OK) return st;
+  bool any_digest = false;
+  for (int j = 0; j < kb; j++) {
+    if (!level_rows[j] != !parent_rows[j]) return fail(XB_ERR_ARG, "row " + std::to_string(j) + ": one of level/parent is NULL");
+    any_digest |= level_rows[j] == nullptr;
+  }
+  if (any_digest) {
+    cap = sl.scratch_bytes;
+    st = grow(&sl.scratch, &cap, sizeof(int32_t) * 2 * kSlotMaxRows * (size_t)g->n, &sl.gen, "slot scratch rows");
+    sl.scratch_bytes = cap;
+    if (st != XB_OK) return st;
+    sl.n_scratch = (int64_t)(sl.scratch_bytes / (sizeof(int32_t) * 2 * kSlotMaxRows));
+  }
+  // staging (the slot is idle: its previous pass has been collected)
+  for (int j = 0; j < SPP; j++) {
+    const int wi = j / B, b = j % B;
+    int32_t* lv = nullptr;
+    int32_t* pr = nullptr;
+    int flag = 0;
+    if (j < kb) {
+      sl.h_src[j] = sources[j];
+      lv = level_rows[j];
+      pr = parent_rows[j];
+      if (!lv) {
+        lv = sl.scratch + (size_t)j * sl.n_scratch;
+        pr = sl.scratch + (size_t)(kSlotMaxRows + j) * sl.n_scratch;
+        flag = 1;
+      }
+    }
+    sl.h_rows[wi * 2 * B + b] = lv;
+    sl.h_rows[wi * 2 * B + B + b] = pr;
+    sl.h_flags[j] = flag;
+  }
+  // cached one-pass graph
+  uint32_t abits = 0;
+  std::memcpy(&abits, &c->tuning.pull_alpha, sizeof(abits));
+  const std::vector<uint64_t> key = {sl.gen, (uint64_t)(uintptr_t)g, g->version, (uint64_t)kb, sizeof(W), NW,
+                                     (uint64_t)heavy, abits};
+  CachedGraph* hit = nullptr;
+  for (auto& e : sl.cache)
+    if (e.key == key) hit = &e;
+  if (!hit) {
+    for (size_t i = 0; i < sl.cache.size();) {  // entries made before a reallocation
+      if (sl.cache[i].key[0] != sl.gen) {
+        cudaGraphExecDestroy(sl.cache[i].exec);
+        sl.cache.erase(sl.cache.begin() + (ptrdiff_t)i);
+      } else {
+        i++;
+      }
+    }
+    if (sl.cache.size() >= kSlotMaxCached) {
+      auto lru = std::min_element(sl.cache.begin(), sl.cache.end(),
+                                  [](const CachedGraph& a, const CachedGraph& b) { return a.last_use < b.last_use; });
+      cudaGraphExecDestroy(lru->exec);
+      sl.cache.erase(lru);
+    }
+    CachedGraph e;
+    e.key = key;
+    e.graphs = {g};
+    st = g->off64 ? capture_slot_pass<W, NW, int64_t>(c, bs, sl, g, kb, &e.exec)
+                  : capture_slot_pass<W, NW, int32_t>(c, bs, sl, g, kb, &e.exec);
+    if (st != XB_OK) return st;
+    sl.cache.push_back(std::move(e));
+    hit = &sl.cache.back();
+  }
+  hit->last_use = ++sl.tick;
+  XB_CUDA(cudaMemcpyAsync(sl.d_src, sl.h_src, sizeof(int32_t) * kb, cudaMemcpyHostToDevice, sl.stream));
+  XB_CUDA(cudaMemcpyAsync(sl.d_rows, sl.h_rows, sizeof(int32_t*) * 2 * SPP, cudaMemcpyHostToDevice, sl.stream));
+  XB_CUDA(cudaMemcpyAsync(sl.d_flags, sl.h_flags, sizeof(int32_t) * SPP, cudaMemcpyHostToDevice, sl.stream));
+  XB_CUDA(cudaGraphLaunch(hit->exec, sl.stream));
+  XB_CUDA(cudaEventRecord(sl.done, sl.stream));
+  sl.busy = true;
+  sl.kb = kb;
+  return XB_OK;
+}
+
+// Collects a finished slot pass.
+xb_status slot_collect(SlotState& sl, xb_stats* stats, xb_row_digest* digests) {
+  sl.busy = false;
+  const xbk::PassSum& s = *sl.h_sum;
+  if (stats) {
+    std::memset(stats, 0, sizeof(*stats));
+    stats->edges_traversed = (int64_t)s.edges_traversed;
+    stats->reached = (int64_t)s.reached;
+    stats->edges_scanned = (int64_t)s.edges_scanned;
+    stats->vertices_scanned = (int64_t)s.vertices_scanned;
+    stats->vertices_swept = (int64_t)s.vertices_swept;
+    stats->parent_edges_scanned = (int64_t)s.parent_edges;
+    stats->class_bytes[0] = (int64_t)s.level_bytes;
+    stats->class_bytes[1] = (int64_t)s.table_bytes;
+    stats->algo_bytes = (int64_t)(s.level_bytes + s.table_bytes);
+    stats->levels = s.max_level;
+    stats->push_levels = s.push_levels;
+    stats->pull_levels = s.pull_levels;
+    stats->batches = s.passes;
+    stats->class_launches[2] = (int64_t)s.launches;
+  }
+  if (digests)
+    for (int j = 0; j < sl.kb; j++) {
+      const xbk::RowDigest& d = sl.h_dig[j];
+      digests[j].reached = (int64_t)d.reached;
+      digests[j].level_sum = (int64_t)d.level_sum;
+      digests[j].parent_sum = (int64_t)d.parent_sum;
+      digests[j].depth = sl.h_flags[j] ? (int32_t)d.depth : -1;
+      digests[j].pad = 0;
+    }
+  if (s.errors) return fail(XB_ERR_STATE, "the pass's level loop ran past the level bound (corrupted state)");
+  return XB_OK;
+}
+
+}  // namespace
+
 void batch_state_free(BatchState* b) {
   if (!b) return;
   cudaSetDevice(b->device);
+  for (auto& sl : b->slots) slot_free(sl);
   drop_cache(b);
   for (auto& ch : b->chains) {
     if (ch.ws) cudaFree(ch.ws);
@@ -621,6 +885,16 @@ void batch_state_free(BatchState* b) {
 
 void batch_forget_graph(xb_ctx* c, const xb_graph* g) {
   if (!c || !c->batch) return;
+  for (auto& sl : c->batch->slots)
+    for (size_t i = 0; i < sl.cache.size();) {
+      if (sl.cache[i].graphs.size() == 1 && sl.cache[i].graphs[0] == g) {
+        if (sl.busy && sl.stream) cudaStreamSynchronize(sl.stream);
+        cudaGraphExecDestroy(sl.cache[i].exec);
+        sl.cache.erase(sl.cache.begin() + (ptrdiff_t)i);
+      } else {
+        i++;
+      }
+    }
   auto& cache = c->batch->cache;
   for (size_t i = 0; i < cache.size();) {
     bool uses = false;
@@ -688,4 +962,72 @@ extern "C" xb_status xb_traverse_batched(xb_ctx* c, const xb_batch_item* items, 
     cudaGetLastError();
   }
   return s;
+}
+
+extern "C" xb_status xb_slot_launch(xb_ctx* c, int32_t slot, const xb_graph* gc, const int32_t* sources, int32_t kb,
+                                    int32_t* const* level_rows, int32_t* const* parent_rows) {
+  xbi::clear_error();
+  xb_graph* g = const_cast<xb_graph*>(gc);
+  if (!c || !g || !sources || !level_rows || !parent_rows) return fail(XB_ERR_ARG, "null argument");
+  if (slot < 0 || slot >= xbe::kMaxSlots) return fail(XB_ERR_ARG, "slot out of range");
+  if (g->ctx->device != c->device) return fail(XB_ERR_ARG, "graph lives on another device");
+  for (int32_t j = 0; j < kb; j++)
+    if (sources[j] < 0 || sources[j] >= g->n) return fail(XB_ERR_ARG, "source " + std::to_string(j) + " out of range");
+  XB_CUDA(cudaSetDevice(c->device));
+  const int nw = c->tuning.words;
+  xb_status s;
+  if (c->tuning.word_bits == 64) {
+    s = nw == 1 ? xbe::slot_launch<unsigned long long, 1>(c, slot, g, sources, kb, level_rows, parent_rows)
+        : nw == 2 ? xbe::slot_launch<unsigned long long, 2>(c, slot, g, sources, kb, level_rows, parent_rows)
+                  : xbe::slot_launch<unsigned long long, 4>(c, slot, g, sources, kb, level_rows, parent_rows);
+  } else {
+    s = nw == 1 ? xbe::slot_launch<unsigned int, 1>(c, slot, g, sources, kb, level_rows, parent_rows)
+        : nw == 2 ? xbe::slot_launch<unsigned int, 2>(c, slot, g, sources, kb, level_rows, parent_rows)
+                  : xbe::slot_launch<unsigned int, 4>(c, slot, g, sources, kb, level_rows, parent_rows);
+  }
+  return s;
+}
+
+extern "C" xb_status xb_slot_poll(xb_ctx* c, int32_t slot, int32_t* done, xb_stats* stats, xb_row_digest* digests) {
+  xbi::clear_error();
+  if (!c || !done) return fail(XB_ERR_ARG, "null argument");
+  if (slot < 0 || slot >= xbe::kMaxSlots) return fail(XB_ERR_ARG, "slot out of range");
+  if (!c->batch || !c->batch->slots[slot].busy) return fail(XB_ERR_STATE, "no pass in flight on this slot");
+  xbe::SlotState& sl = c->batch->slots[slot];
+  const cudaError_t q = cudaEventQuery(sl.done);
+  if (q == cudaErrorNotReady) {
+    *done = 0;
+    return XB_OK;
+  }
+  if (q != cudaSuccess) {
+    sl.busy = false;
+    return fail(XB_ERR_CUDA, std::string("slot pass: ") + cudaGetErrorString(q));
+  }
+  *done = 1;
+  return xbe::slot_collect(sl, stats, digests);
+}
+
+extern "C" xb_status xb_slot_wait(xb_ctx* c, int32_t slot, xb_stats* stats, xb_row_digest* digests) {
+  xbi::clear_error();
+  if (!c) return fail(XB_ERR_ARG, "null context");
+  if (slot < 0 || slot >= xbe::kMaxSlots) return fail(XB_ERR_ARG, "slot out of range");
+  if (!c->batch || !c->batch->slots[slot].busy) return fail(XB_ERR_STATE, "no pass in flight on this slot");
+  xbe::SlotState& sl = c->batch->slots[slot];
+  const cudaError_t e = cudaEventSynchronize(sl.done);
+  if (e != cudaSuccess) {
+    sl.busy = false;
+    return fail(XB_ERR_CUDA, std::string("slot pass: ") + cudaGetErrorString(e));
+  }
+  return xbe::slot_collect(sl, stats, digests);
+}
+
+extern "C" xb_status xb_slots_release(xb_ctx* c) {
+  xbi::clear_error();
+  if (!c) return fail(XB_ERR_ARG, "null context");
+  if (!c->batch) return XB_OK;
+  for (auto& sl : c->batch->slots)
+    if (sl.busy) return fail(XB_ERR_STATE, "a slot has a pass in flight");
+  cudaSetDevice(c->device);
+  for (auto& sl : c->batch->slots) xbe::slot_free(sl);
+  return XB_OK;
 }

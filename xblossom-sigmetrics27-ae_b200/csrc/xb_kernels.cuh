@@ -1757,4 +1757,48 @@ static __global__ void k_pass_accum(const Ctrs* ctr, PassSum* sum, long long n, 
   if (b.err) sum->errors += 1;
 }
 
+// Digest of one table row pair (level row, parent row of a source): the
+// summary a serving client gets instead of the full tables.
+struct RowDigest {
+  unsigned long long reached;     // vertices with level >= 0
+  unsigned long long level_sum;   // sum of their levels
+  unsigned long long parent_sum;  // sum of their parent ids
+  unsigned int depth;             // largest level
+  unsigned int pad;
+};
+
+// Digests of the pass rows the flags mark; rows are in the table pass layout
+// (word wi: level rows at rows[wi*2B + b], parent rows at rows[wi*2B + B + b]).
+// blockIdx.y = row within the pass; out[row] must be zero beforehand.
+static __global__ void __launch_bounds__(256) k_row_digest(int32_t* const* __restrict__ rows,
+                                                          const int32_t* __restrict__ flags, int kb, int B,
+                                                          int64_t n, RowDigest* out) {
+  const int r = blockIdx.y;
+  if (r >= kb || !flags[r]) return;
+  const int wi = r / B, b = r % B;
+  const int32_t* lv = rows[wi * 2 * B + b];
+  const int32_t* pr = rows[wi * 2 * B + B + b];
+  unsigned long long cnt = 0, ls = 0, ps = 0;
+  unsigned int dep = 0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t l = __ldcs(&lv[i]);
+    if (l >= 0) {
+      cnt++;
+      ls += (unsigned long long)l;
+      ps += (unsigned long long)(uint32_t)__ldcs(&pr[i]);
+      dep = max(dep, (unsigned int)l);
+    }
+  }
+  cnt = warp_sum_u64(cnt);
+  ls = warp_sum_u64(ls);
+  ps = warp_sum_u64(ps);
+  for (int o = 16; o > 0; o >>= 1) dep = max(dep, __shfl_xor_sync(0xffffffffu, dep, o));
+  if ((threadIdx.x & 31) == 0 && cnt) {
+    atomicAdd(&out[r].reached, cnt);
+    atomicAdd(&out[r].level_sum, ls);
+    atomicAdd(&out[r].parent_sum, ps);
+    atomicMax(&out[r].depth, dep);
+  }
+}
+
 }  // namespace xbk

@@ -41,6 +41,8 @@ XB_MODE_PLAIN = 0
 XB_MODE_ALTERNATING = 1
 XB_OUT_DEVICE = 1
 XB_SOURCES_DEVICE = 2
+XB_MAX_SLOTS = 16
+SLOT_MAX_ROWS = 256  # sources per slot pass at most (64 per word x 4 words)
 
 
 class XbError(RuntimeError):
@@ -84,6 +86,16 @@ class XbTuning(C.Structure):
         ("heavy_degree", C.c_int32),
         ("timing", C.c_int32),
         ("chains", C.c_int32),
+    ]
+
+
+class XbRowDigest(C.Structure):
+    _fields_ = [
+        ("reached", C.c_int64),
+        ("level_sum", C.c_int64),
+        ("parent_sum", C.c_int64),
+        ("depth", C.c_int32),
+        ("pad", C.c_int32),
     ]
 
 
@@ -139,6 +151,10 @@ def lib() -> C.CDLL:
         "xb_select_sources": (i32, [vp, u64, i32, vp]),
         "xb_traverse": (i32, [vp, vp, vp, i32, i32, vp, vp, vp, vp, u32, P(XbStats)]),
         "xb_traverse_batched": (i32, [vp, P(XbBatchItem), i32, P(XbStats)]),
+        "xb_slot_launch": (i32, [vp, i32, vp, vp, i32, vp, vp]),
+        "xb_slot_poll": (i32, [vp, i32, P(i32), P(XbStats), vp]),
+        "xb_slot_wait": (i32, [vp, i32, P(XbStats), vp]),
+        "xb_slots_release": (i32, [vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -441,6 +457,47 @@ class Context:
         _check(lib().xb_traverse_batched(self._h, items, len(queries), C.byref(st)))
         stats = st.as_dict()
         return [TraversalResult(lv, pr, {}) for lv, pr in results], stats
+
+    # serving slots ------------------------------------------------------------
+    def slot_launch(self, slot: int, graph: Graph, sources, rows=None) -> None:
+        """Queues one pass on a serving slot (xb_slot_launch).  rows: per source
+        a (level_row, parent_row) pair of device addresses, or None for a
+        digest-only source (default: all digest-only)."""
+        src = np.ascontiguousarray(sources, dtype=np.int32)
+        kb = len(src)
+        lv = (C.c_void_p * max(kb, 1))()
+        pr = (C.c_void_p * max(kb, 1))()
+        if rows is not None:
+            for j, r in enumerate(rows):
+                if r is not None:
+                    lv[j], pr[j] = r
+        _check(lib().xb_slot_launch(self._h, slot, graph._h, src.ctypes.data, kb, lv, pr))
+        # only a launch the library accepted replaces the slot's record
+        self._slot_keep = getattr(self, "_slot_keep", {})
+        self._slot_keep[slot] = (src, lv, pr)
+
+    def slot_poll(self, slot: int, wait: bool = False):
+        """(done, stats, digests) of a slot's pass; digests: int64 (kb, 4)
+        array of reached, level_sum, parent_sum, depth (depth -1 for rows
+        written to caller buffers)."""
+        keep = getattr(self, "_slot_keep", {}).get(slot)
+        kb = len(keep[0]) if keep is not None else 0
+        st = XbStats()
+        dig = (XbRowDigest * SLOT_MAX_ROWS)()  # the library writes one entry per row of the pass
+        if wait:
+            _check(lib().xb_slot_wait(self._h, slot, C.byref(st), dig))
+            done = 1
+        else:
+            d = C.c_int32(0)
+            _check(lib().xb_slot_poll(self._h, slot, C.byref(d), C.byref(st), dig))
+            done = d.value
+        if not done:
+            return False, None, None
+        arr = np.array([(x.reached, x.level_sum, x.parent_sum, x.depth) for x in dig[:kb]], dtype=np.int64)
+        return True, st.as_dict(), arr.reshape(kb, 4)
+
+    def slots_release(self) -> None:
+        _check(lib().xb_slots_release(self._h))
 
     def close(self) -> None:
         if self._h and self._h.value:
