@@ -70,7 +70,7 @@ struct SlotState {
   xbk::Ctrs* ctr = nullptr;
   int32_t* hpar = nullptr;
   size_t hpar_bytes = 0;
-  int32_t* scratch = nullptr;  // level rows then parent rows, kSlotMaxRows each, n_scratch apart
+  int32_t* scratch = nullptr;  // level rows then parent rows of a pass, n_scratch apart
   size_t scratch_bytes = 0;
   int64_t n_scratch = 0;
   cudaStream_t stream = nullptr;
@@ -749,12 +749,12 @@ xb_status slot_launch(xb_ctx* c, int slot, xb_graph* g, const int32_t* sources, 
     if (!level_rows[j] != !parent_rows[j]) return fail(XB_ERR_ARG, "row " + std::to_string(j) + ": one of level/parent is NULL");
     any_digest |= level_rows[j] == nullptr;
   }
-  if (any_digest) {
+  if (any_digest) {  // SPP level rows then SPP parent rows, n_scratch entries apart
     cap = sl.scratch_bytes;
-    st = grow(&sl.scratch, &cap, sizeof(int32_t) * 2 * kSlotMaxRows * (size_t)g->n, &sl.gen, "slot scratch rows");
+    st = grow(&sl.scratch, &cap, sizeof(int32_t) * 2 * SPP * (size_t)g->n, &sl.gen, "slot scratch rows");
     sl.scratch_bytes = cap;
     if (st != XB_OK) return st;
-    sl.n_scratch = (int64_t)(sl.scratch_bytes / (sizeof(int32_t) * 2 * kSlotMaxRows));
+    sl.n_scratch = (int64_t)(sl.scratch_bytes / (sizeof(int32_t) * 2 * SPP));
   }
   // staging (the slot is idle: its previous pass has been collected)
   for (int j = 0; j < SPP; j++) {
@@ -768,7 +768,7 @@ xb_status slot_launch(xb_ctx* c, int slot, xb_graph* g, const int32_t* sources, 
       pr = parent_rows[j];
       if (!lv) {
         lv = sl.scratch + (size_t)j * sl.n_scratch;
-        pr = sl.scratch + (size_t)(kSlotMaxRows + j) * sl.n_scratch;
+        pr = sl.scratch + (size_t)(SPP + j) * sl.n_scratch;
         flag = 1;
       }
     }
