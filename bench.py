@@ -139,12 +139,20 @@ class ClockSampler:
 
 
 def traffic_from_profile(workload: str):
-    """Per-launch DRAM bytes of the dominant kernel from the committed ncu summary, if any."""
-    p = os.path.join(ROOT, "profiles", f"traffic_{workload}.json")
+    """DRAM bytes per step of each kernel class ({"0": level steps, "1": table
+    pass}) from the committed ncu summary profiles/traffic_<workload>.txt."""
+    p = os.path.join(ROOT, "profiles", f"traffic_{workload}.txt")
+    out = {}
     try:
-        return json.load(open(p))
-    except Exception:
+        for line in open(p):
+            line = line.split("#", 1)[0].strip()
+            if "=" in line:
+                key, val = (x.strip() for x in line.split("=", 1))
+                if key.startswith("class"):
+                    out[key[5]] = float(val)
+    except OSError:
         return None
+    return out or None
 
 
 def cpu_baseline_port(ro, ci, sources, budget_s: float = 15.0) -> dict:
