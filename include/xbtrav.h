@@ -171,6 +171,10 @@ xb_status xb_traverse(xb_ctx* ctx, const xb_graph* g, const int32_t* sources, in
                       int32_t mode, const int32_t* matching, int32_t* level, int32_t* parent,
                       int32_t* owner, uint32_t flags, xb_stats* stats);
 
+/* Page-locked host memory (for host tables of the batched call). */
+xb_status xb_host_alloc(int64_t bytes, void** out);
+xb_status xb_host_free(void* p);
+
 /* ---- batched traversal ------------------------------------------------- */
 /* One query of a batch: k sources on a resident graph, tables k*n int32 each
  * (source-major), with the same meaning as xb_traverse's.  flags:

@@ -186,4 +186,33 @@ def test_cpp_host_api_matches_python_binding(ctx, tmp_path):
             h = (h ^ np.uint64(x)) * prime
     assert kv["checksum"] == f"{int(h):016x}"
     assert int(kv["edges_traversed"]) == r.stats["edges_traversed"]
+    # the same sources as three queries in one batched launch (BatchedEngine)
+    out_b = subprocess.run([exe, "--rmat", "12", "16", "64", "0x77", "--batched"], capture_output=True, text=True,
+                           check=True).stdout
+    kvb = dict(x.split("=") for x in out_b.split())
+    assert kvb["checksum"] == kv["checksum"]
+    assert kvb["edges_traversed"] == kv["edges_traversed"]
+    g.close()
+
+
+def test_autotuner_picks_a_config_that_keeps_parity(ctx, tmp_path):
+    from xbtrav import autotune
+
+    csr = xbtrav.HostCSR.rmat(12, 16, seed=31)
+    ro, ci = csr.arrays()
+    src = xbtrav.select_sources_csr(ro, 32, 96)
+    g = ctx.upload(csr)
+    space = {"word_bits": [64, 32], "words": [1, 2], "heavy_degree": [128, 256], "pull_alpha": [64.0, 256.0],
+             "chains": [1, 2]}
+    for path in ("plain", "batched"):
+        best, table = autotune.autotune(ctx, g, src, space=space, reps=1, path=path)
+        assert all(best[k] in space[k] for k in space if path == "batched" or k != "chains")
+        assert best == {k: ctx.tuning()[k] for k in best}
+        assert len(table) >= 4 + 4
+        r = ctx.traverse(g, src)
+        lv, pr, _, _ = O.msbfs(ro, ci, src)
+        np.testing.assert_array_equal(r.level, lv)
+        np.testing.assert_array_equal(r.parent, pr)
+    autotune.save(best, str(tmp_path / "t.json"))
+    assert autotune.load(str(tmp_path / "t.json")) == best
     g.close()

@@ -1031,3 +1031,24 @@ extern "C" xb_status xb_slots_release(xb_ctx* c) {
   for (auto& sl : c->batch->slots) xbe::slot_free(sl);
   return XB_OK;
 }
+
+extern "C" xb_status xb_host_alloc(int64_t bytes, void** out) {
+  xbi::clear_error();
+  if (!out || bytes < 0) return fail(XB_ERR_ARG, "bad argument");
+  *out = nullptr;
+  if (cudaMallocHost(out, (size_t)std::max<int64_t>(bytes, 1)) != cudaSuccess) {
+    cudaGetLastError();
+    *out = nullptr;
+    return fail(XB_ERR_OOM, "page-locked allocation of " + std::to_string(bytes) + " bytes failed");
+  }
+  return XB_OK;
+}
+
+extern "C" xb_status xb_host_free(void* p) {
+  xbi::clear_error();
+  if (p && cudaFreeHost(p) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(XB_ERR_ARG, "not a page-locked allocation of this library");
+  }
+  return XB_OK;
+}

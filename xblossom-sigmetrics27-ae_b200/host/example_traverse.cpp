@@ -1,16 +1,19 @@
 // example_traverse.cpp -- reference-style C++ caller of libxbtrav.so.
 //
-//   example_traverse <row_offsets.txt> <col_indices.txt> <k> <seed>
-//   example_traverse --rmat <scale> <edge_factor> <k> <seed>
+//   example_traverse <row_offsets.txt> <col_indices.txt> <k> <seed> [--batched]
+//   example_traverse --rmat <scale> <edge_factor> <k> <seed> [--batched]
 //
 // Loads (or generates) a CSR the way the reference runners do (HGraph from
 // two text files, apps/xb/runner/xblsm_gpu/run_xb_pp_by_dataset.cu:7-40),
 // uploads it, traverses k seeded sources and prints one summary line plus a
-// checksum of both tables.  Exit status 0 on success.
+// checksum of both tables.  --batched splits the sources into three queries
+// run in one launch (BatchedEngine); the tables, and so the checksum, are the
+// same.  Exit status 0 on success.
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <vector>
 
 #include "xbtrav.hpp"
 
@@ -29,7 +32,24 @@ int main(int argc, char** argv) {
     xbtrav::DGraph dg(ctx, g);
     xbtrav::TraversalEngine eng(dg);
     const auto sources = g.SelectSources(seed, k);
-    const xbtrav::Tables t = eng.Traverse(sources);
+    const bool batched = std::strcmp(argv[argc - 1], "--batched") == 0;
+    xbtrav::Tables t;
+    if (!batched) {
+      t = eng.Traverse(sources);
+    } else {
+      // three queries of the same graph: k/3, k/3 and the rest of the sources
+      std::vector<xbtrav::BatchedEngine::Query> qs;
+      const int cut[4] = {0, k / 3, 2 * k / 3, k};
+      for (int q = 0; q < 3; q++)
+        qs.push_back({&dg, std::vector<int32_t>(sources.begin() + cut[q], sources.begin() + cut[q + 1])});
+      const auto parts = xbtrav::BatchedEngine(ctx).Traverse(qs, &t.stats);
+      t.n = (int64_t)g.nnodes;
+      t.k = k;
+      for (const auto& p : parts) {
+        t.level.insert(t.level.end(), p.level.begin(), p.level.end());
+        t.parent.insert(t.parent.end(), p.parent.begin(), p.parent.end());
+      }
+    }
     uint64_t h = 1469598103934665603ull;  // FNV-1a over both tables
     for (int32_t x : t.level) h = (h ^ (uint32_t)x) * 1099511628211ull;
     for (int32_t x : t.parent) h = (h ^ (uint32_t)x) * 1099511628211ull;

@@ -157,4 +157,52 @@ class TraversalEngine {
   int64_t n_ = 0;
 };
 
+// Many source sets -- on one graph or several -- traversed in ONE launch
+// (xb_traverse_batched; no counterpart in the reference, whose engine runs
+// one source set per host-driven loop).  Tables come back on the host.
+class BatchedEngine {
+ public:
+  explicit BatchedEngine(Context& ctx) : ctx_(&ctx) {}
+  struct Query {
+    const DGraph* graph;
+    std::vector<int32_t> sources;
+  };
+  std::vector<Tables> Traverse(const std::vector<Query>& queries, xb_stats* stats = nullptr) const {
+    std::vector<xb_batch_item> items(queries.size());
+    std::vector<Tables> out(queries.size());
+    std::vector<int32_t*> bufs;  // page-locked: the copies run inside the launch
+    struct Free {
+      std::vector<int32_t*>& b;
+      ~Free() {
+        for (int32_t* p : b) xb_host_free(p);
+      }
+    } guard{bufs};
+    for (size_t i = 0; i < queries.size(); i++) {
+      int64_t n = 0;
+      check(xb_graph_info(queries[i].graph->get(), &n, nullptr, nullptr));
+      const int64_t k = (int64_t)queries[i].sources.size();
+      out[i].n = n;
+      out[i].k = (int32_t)k;
+      void* p = nullptr;
+      check(xb_host_alloc(sizeof(int32_t) * 2 * k * n, &p));
+      bufs.push_back((int32_t*)p);
+      items[i] = xb_batch_item{queries[i].graph->get(), queries[i].sources.data(), (int32_t)k, 0u, (int32_t*)p,
+                               (int32_t*)p + k * n};
+    }
+    xb_stats st{};
+    check(xb_traverse_batched(ctx_->get(), items.data(), (int32_t)items.size(), &st));
+    for (size_t i = 0; i < queries.size(); i++) {
+      const size_t kn = (size_t)out[i].k * (size_t)out[i].n;
+      out[i].level.assign(items[i].level, items[i].level + kn);
+      out[i].parent.assign(items[i].parent, items[i].parent + kn);
+      out[i].stats = st;
+    }
+    if (stats) *stats = st;
+    return out;
+  }
+
+ private:
+  Context* ctx_;
+};
+
 }  // namespace xbtrav

@@ -1,13 +1,14 @@
 """Autotuner for the traversal engine's tunables.
 
 Searches sources-per-word (32/64), words traversed together (1/2/4), the
-degree cutoff between the tile path and the per-vertex (heavy) path, and the
-push/pull switch factor alpha, by timing the engine's own calls (device-side
-CUDA events of xb_traverse) on a sample of the workload's sources.  The
+degree cutoff between the per-lane light pull and the per-warp heavy pull,
+the push/pull switch factor alpha and, for the batched path, the number of
+concurrent chains, by timing the engine's own calls (device-side CUDA events
+of xb_traverse or xb_traverse_batched) on the workload's sources.  The
 reference has no tuner; its only knobs are compile-time buffer ratios and a
 hybrid per-node/per-edge threshold (apps/xb/src/include/xbsm_gpu/xblossom_gpu_engine_hybrid.h:119).
 
-    best, table = autotune(ctx, graph, sources)
+    best, table = autotune(ctx, graph, sources, path="batched")
     save(best, "tuning.json"); ctx.set_tuning(**load("tuning.json"))
 """
 from __future__ import annotations
@@ -18,12 +19,14 @@ import json
 DEFAULT_SPACE = {
     "word_bits": [64, 32],
     "words": [1, 2, 4],
-    "heavy_degree": [128, 256, 512, 1024],
-    "pull_alpha": [4.0, 32.0, 128.0],
+    "heavy_degree": [128, 256, 512],
+    "pull_alpha": [16.0, 64.0, 256.0, 1024.0],
+    "chains": [1, 2, 4, 8],
 }
+KEYS = ("word_bits", "words", "heavy_degree", "pull_alpha", "chains")
 
 
-def _time_config(ctx, graph, sources, cfg: dict, reps: int) -> float:
+def _time_config(ctx, graph, sources, cfg: dict, reps: int, path: str) -> float:
     import torch
 
     ctx.set_tuning(timing=0, **cfg)
@@ -32,37 +35,47 @@ def _time_config(ctx, graph, sources, cfg: dict, reps: int) -> float:
     k, n = int(src.numel()), graph.n
     lv = torch.empty((k, n), dtype=torch.int32, device=dev)
     pr = torch.empty((k, n), dtype=torch.int32, device=dev)
-    ctx.traverse(graph, src, out="device", level=lv, parent=pr)  # warm-up (workspace, heavy lists)
-    best = float("inf")
-    for _ in range(reps):
-        r = ctx.traverse(graph, src, out="device", level=lv, parent=pr)
-        best = min(best, r.stats["device_ms"])
-    return best
+
+    def once():
+        if path == "batched":
+            return ctx.traverse_batched([(graph, src)], outputs=[(lv, pr)])[1]["device_ms"]
+        return ctx.traverse(graph, src, out="device", level=lv, parent=pr).stats["device_ms"]
+
+    once()  # warm-up (workspaces, heavy lists, the captured launch)
+    return min(once() for _ in range(reps))
 
 
-def autotune(ctx, graph, sources, space: dict | None = None, reps: int = 2, staged: bool = True):
-    """Returns (best tuning dict, list of (cfg, ms)).
+def autotune(ctx, graph, sources, space: dict | None = None, reps: int = 2, staged: bool = True,
+             path: str = "plain"):
+    """Returns (best tuning dict, list of (cfg, ms)); path "plain" times
+    xb_traverse, "batched" xb_traverse_batched (which also uses chains).
 
-    staged=True searches coordinate-wise (word layout first with the default
-    cutoffs, then the cutoffs for the winning layout) instead of the full grid.
+    staged=True searches coordinate-wise (word layout first with the current
+    cutoffs, then cutoffs and alpha for the winning layout, then chains)
+    instead of the full grid.
     """
     space = dict(DEFAULT_SPACE if space is None else space)
-    base = ctx.tuning()
+    if path != "batched":
+        space["chains"] = [ctx.tuning()["chains"]]
+    base = {k: v for k, v in ctx.tuning().items() if k in KEYS}
     table = []
+
+    def run(cfg):
+        table.append((dict(cfg), _time_config(ctx, graph, sources, cfg, reps, path)))
+
     if not staged:
-        keys = list(space)
+        keys = [k for k in KEYS if k in space]
         for vals in itertools.product(*(space[k] for k in keys)):
-            cfg = dict(zip(keys, vals))
-            table.append((cfg, _time_config(ctx, graph, sources, cfg, reps)))
+            run(dict(base, **dict(zip(keys, vals))))
     else:
-        fixed = {"heavy_degree": base["heavy_degree"], "pull_alpha": base["pull_alpha"]}
         for wb, nw in itertools.product(space["word_bits"], space["words"]):
-            cfg = dict(fixed, word_bits=wb, words=nw)
-            table.append((cfg, _time_config(ctx, graph, sources, cfg, reps)))
-        layout = min(table, key=lambda x: x[1])[0]
+            run(dict(base, word_bits=wb, words=nw))
+        best = min(table, key=lambda x: x[1])[0]
         for h, a in itertools.product(space["heavy_degree"], space["pull_alpha"]):
-            cfg = dict(word_bits=layout["word_bits"], words=layout["words"], heavy_degree=h, pull_alpha=a)
-            table.append((cfg, _time_config(ctx, graph, sources, cfg, reps)))
+            run(dict(best, heavy_degree=h, pull_alpha=a))
+        best = min(table, key=lambda x: x[1])[0]
+        for ch in space["chains"]:
+            run(dict(best, chains=ch))
     best = dict(min(table, key=lambda x: x[1])[0])
     ctx.set_tuning(**best)
     return best, table
@@ -76,4 +89,4 @@ def save(cfg: dict, path: str) -> None:
 def load(path: str) -> dict:
     with open(path) as f:
         d = json.load(f)
-    return {k: d[k] for k in ("word_bits", "words", "heavy_degree", "pull_alpha") if k in d}
+    return {k: d[k] for k in KEYS if k in d}
