@@ -55,6 +55,8 @@ WORKLOADS = {
     "serve_rmat22": dict(kind="serve", scale=22, ef=16, queries=96, rate=12.0, kmax=4096, slots=4),
     # the default graph with one word of sources: ncu DRAM-traffic captures (about 4 GB on the device)
     "rmat22_k64": dict(kind="rmat", scale=22, ef=16, k=64),
+    # one pass of the default layout (2 words x 64 sources): DRAM-traffic captures
+    "rmat22_k128": dict(kind="rmat", scale=22, ef=16, k=128),
     # smaller case for kernel profiles (graph > L2, a few hundred MB on the device)
     "rmat20_k64": dict(kind="rmat", scale=20, ef=16, k=64),
 }
@@ -318,6 +320,9 @@ def run_serve(args, w, name) -> None:
     csr = xbtrav.HostCSR.rmat(w["scale"], w["ef"], 0.57, 0.19, 0.19, seed=SEED)
     info = csr.info()
     ctx = xbtrav.Context(0)
+    # one word per pass: 64-source passes keep latency low, and per-slot memory
+    # (workspace + scratch rows, 28 GB per slot at scale 25) within the device
+    ctx.set_tuning(words=1)
     g = ctx.upload(csr)
     del csr
     slots = args.chains or w["slots"]
@@ -480,6 +485,14 @@ def main() -> None:
     plain_ms, plain_agg, _ = timed(plain_step, args.steps)
     plain_gteps = sum_over_ranks(plain_agg["edges_traversed"]) / (plain_ms / 1e3) / 1e9
 
+    # the plain path with one word (64 sources) per launch sequence
+    tun0 = ctx.tuning()
+    ctx.set_tuning(words=1)
+    plain_step()
+    pw_ms, pw_agg, _ = timed(plain_step, max(1, min(args.steps, 3)))
+    plain_word_gteps = sum_over_ranks(pw_agg["edges_traversed"]) / (pw_ms / 1e3) / 1e9
+    ctx.set_tuning(words=tun0["words"])
+
     # per-kernel-class device times of the same kernels (one step, event-timed per class)
     ctx.set_tuning(timing=1)
     _, cls_agg, _ = timed(plain_step, 1)
@@ -567,6 +580,7 @@ def main() -> None:
             "data": "synthetic (seeded R-MAT / uniform generator)",
             "config": dict(workload_config(args.workload, w, info), parallelism=f"replicas{world}", path=path_desc),
             "batched_gteps": value, "plain_gteps": plain_gteps, "batched_over_plain": value / plain_gteps,
+            "plain_one_word_gteps": plain_word_gteps, "batched_over_plain_one_word": value / plain_word_gteps,
             "plain_ms_per_step": plain_ms / args.steps,
             "undirected_gteps": headline / 2,
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,

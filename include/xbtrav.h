@@ -90,7 +90,7 @@ typedef struct xb_tuning {
   int32_t heavy_degree;    /* vertices above this degree get block-wide passes */
   int32_t timing;          /* 1 = record per-class CUDA events into xb_stats */
   int32_t chains;          /* xb_traverse_batched: passes in flight at once, each with its
-                              own workspace (1..16; 0 = default 2) */
+                              own workspace (1..16; 0 = default 4) */
 } xb_tuning;
 
 /* ---- status ------------------------------------------------------------ */

@@ -360,13 +360,13 @@ xb_status xb_ctx_create(int32_t device, xb_ctx** out) {
   XB_CUDA(cudaEventCreate(&c->evc0));
   XB_CUDA(cudaEventCreate(&c->evc1));
   c->tuning.word_bits = 64;
-  c->tuning.words = 1;
+  c->tuning.words = 2;  // 128 sources per pass: one gather of 16 bytes serves them all
   // pull unless the frontier's edges are under 1/256 of the unfinished edges:
   // pull steps record parents as they go, push steps leave them to a search
   c->tuning.pull_alpha = 256.0f;
   c->tuning.heavy_degree = 256;
   c->tuning.timing = 0;
-  c->tuning.chains = 2;
+  c->tuning.chains = 4;
   *out = c.release();
   return XB_OK;
 }
@@ -400,7 +400,7 @@ xb_status xb_ctx_set_tuning(xb_ctx* c, const xb_tuning* t) {
     return fail(XB_ERR_ARG, "heavy_degree must be in [32, 2^20]");
   if (t->chains < 0 || t->chains > 16) return fail(XB_ERR_ARG, "chains must be in [0, 16]");
   c->tuning = *t;
-  if (c->tuning.chains == 0) c->tuning.chains = 2;
+  if (c->tuning.chains == 0) c->tuning.chains = 4;
   return XB_OK;
 }
 
