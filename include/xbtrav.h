@@ -115,6 +115,27 @@ xb_status xb_csr_from_arrays(int64_t n, const int64_t* row_offsets, const int32_
  * indices file (HGraph(row_path, col_path), hgraph.h:37-48). */
 xb_status xb_csr_load_text(const char* row_path, const char* col_path, xb_host_csr** out);
 xb_status xb_csr_save_text(const xb_host_csr* g, const char* row_path, const char* col_path);
+/* Native binary CSR: 8-byte magic "XBCSR\0\1\0", int64 n, int64 m, int64
+ * row offsets (n+1), int32 column indices (m), little-endian. */
+xb_status xb_csr_save_binary(const xb_host_csr* g, const char* path);
+xb_status xb_csr_load_binary(const char* path, xb_host_csr** out);
+/* Source-list files of the reference's experiment scripts
+ * (scripts/2-datasets/src_nodes/generate_src_lists.py writes them,
+ * source_nodes_from_file in scripts/4-expr/common.sh reads them): "#" starts
+ * a comment (whole line or trailing), ids are separated by white space.
+ * Load writes up to capacity ids and sets *count to the number in the file
+ * (XB_ERR_CAPACITY if that is more). */
+xb_status xb_sources_load(const char* path, int32_t* out, int32_t capacity, int32_t* count);
+xb_status xb_sources_save(const char* path, const int32_t* sources, int32_t k, const char* comment);
+/* Exports for cross-checks with other engines: Ligra "AdjacencyGraph" text
+ * (n, m, n offsets, m targets) and Matrix Market coordinate pattern
+ * symmetric, one 1-based (i < j) entry per undirected edge in ascending
+ * order -- the entry lines of scripts/2-datasets/gunrock/csr_to_gunrock_mm.py.
+ * A Matrix Market coordinate file (any field; values ignored) loads as the
+ * symmetric, loop-free, duplicate-free pattern graph. */
+xb_status xb_csr_save_ligra(const xb_host_csr* g, const char* path);
+xb_status xb_csr_save_mtx(const xb_host_csr* g, const char* path);
+xb_status xb_csr_load_mtx(const char* path, xb_host_csr** out);
 xb_status xb_csr_info(const xb_host_csr* g, int64_t* n, int64_t* m, int64_t* max_degree,
                       int64_t* isolated);
 /* Borrowed pointers, valid until xb_csr_free. */

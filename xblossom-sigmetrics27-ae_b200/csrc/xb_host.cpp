@@ -56,8 +56,7 @@ xb_status validate_csr(int64_t n, const int64_t* ro, const int32_t* ci) {
 
 // Builds a symmetric, self-loop-free, duplicate-free CSR with ascending
 // adjacency from a list of sampled pairs (u, v) packed as (u << 32) | v.
-static void csr_from_pairs(int64_t n, const std::vector<uint64_t>& pairs, int threads,
-                           xb_host_csr* out) {
+void csr_from_pairs(int64_t n, const std::vector<uint64_t>& pairs, int threads, xb_host_csr* out) {
   const int64_t np = (int64_t)pairs.size();
   std::vector<int64_t> deg(n + 1, 0);
   {

@@ -48,6 +48,10 @@ inline uint64_t splitmix64_next(uint64_t& s) {
 // Validates a CSR: offsets start at 0, non-decreasing, ids in [0, n).
 xb_status validate_csr(int64_t n, const int64_t* ro, const int32_t* ci);
 
+// Builds a symmetric, self-loop-free, duplicate-free CSR with ascending
+// adjacency from pairs (u, v) packed as (u << 32) | v.
+void csr_from_pairs(int64_t n, const std::vector<uint64_t>& pairs, int threads, xb_host_csr* out);
+
 // Source selection over vertices of non-zero degree (host).
 xb_status select_sources(int64_t n, const int64_t* ro, uint64_t seed, int32_t k, int32_t* out);
 

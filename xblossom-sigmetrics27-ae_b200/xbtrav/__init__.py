@@ -132,6 +132,13 @@ def lib() -> C.CDLL:
         "xb_csr_from_arrays": (i32, [i64, vp, vp, P(vp)]),
         "xb_csr_load_text": (i32, [C.c_char_p, C.c_char_p, P(vp)]),
         "xb_csr_save_text": (i32, [vp, C.c_char_p, C.c_char_p]),
+        "xb_csr_save_binary": (i32, [vp, C.c_char_p]),
+        "xb_csr_load_binary": (i32, [C.c_char_p, P(vp)]),
+        "xb_csr_save_ligra": (i32, [vp, C.c_char_p]),
+        "xb_csr_save_mtx": (i32, [vp, C.c_char_p]),
+        "xb_csr_load_mtx": (i32, [C.c_char_p, P(vp)]),
+        "xb_sources_load": (i32, [C.c_char_p, vp, i32, P(i32)]),
+        "xb_sources_save": (i32, [C.c_char_p, vp, i32, C.c_char_p]),
         "xb_csr_info": (i32, [vp, P(i64), P(i64), P(i64), P(i64)]),
         "xb_csr_arrays": (i32, [vp, P(vp), P(vp)]),
         "xb_csr_free": (None, [vp]),
@@ -223,6 +230,27 @@ class HostCSR:
     def save_text(self, row_path: str, col_path: str) -> None:
         _check(lib().xb_csr_save_text(self._h, row_path.encode(), col_path.encode()))
 
+    @classmethod
+    def load_binary(cls, path: str) -> "HostCSR":
+        h = C.c_void_p()
+        _check(lib().xb_csr_load_binary(path.encode(), C.byref(h)))
+        return cls(h.value)
+
+    def save_binary(self, path: str) -> None:
+        _check(lib().xb_csr_save_binary(self._h, path.encode()))
+
+    @classmethod
+    def load_mtx(cls, path: str) -> "HostCSR":
+        h = C.c_void_p()
+        _check(lib().xb_csr_load_mtx(path.encode(), C.byref(h)))
+        return cls(h.value)
+
+    def save_mtx(self, path: str) -> None:
+        _check(lib().xb_csr_save_mtx(self._h, path.encode()))
+
+    def save_ligra(self, path: str) -> None:
+        _check(lib().xb_csr_save_ligra(self._h, path.encode()))
+
     def info(self) -> dict:
         n, m, md, iso = C.c_int64(), C.c_int64(), C.c_int64(), C.c_int64()
         _check(lib().xb_csr_info(self._h, C.byref(n), C.byref(m), C.byref(md), C.byref(iso)))
@@ -250,6 +278,24 @@ class HostCSR:
             self.close()
         except Exception:
             pass
+
+
+def load_sources(path: str) -> np.ndarray:
+    """Source-list file ("#" comments, ids separated by white space)."""
+    cnt = C.c_int32(0)
+    st = lib().xb_sources_load(path.encode(), None, 0, C.byref(cnt))
+    if st not in (XB_OK, XB_ERR_CAPACITY):
+        _check(st)
+    out = np.zeros(cnt.value, np.int32)
+    if cnt.value:
+        _check(lib().xb_sources_load(path.encode(), out.ctypes.data, cnt.value, C.byref(cnt)))
+    return out
+
+
+def save_sources(path: str, sources, comment: str = "") -> None:
+    src = np.ascontiguousarray(sources, dtype=np.int32)
+    _check(lib().xb_sources_save(path.encode(), src.ctypes.data if len(src) else None, len(src),
+                                 comment.encode() if comment else None))
 
 
 def select_sources_csr(row_offsets: np.ndarray, seed: int, k: int) -> np.ndarray:
