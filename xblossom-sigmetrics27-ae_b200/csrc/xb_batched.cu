@@ -278,7 +278,7 @@ xb_status capture_pass_tables(xb_ctx* c, const PassRes<W, NW, OffT>& p, const xb
   if (st != XB_OK) return st;
   const int hv = g->n_heavy > 0 ? 1 : 0;
   const int words = (kb + B - 1) / B;
-  const int fixed_k = hv + 2 + words * (1 + hv) + 1;
+  const int fixed_k = hv + 2 + words * hv + 1 + 1;  // fill, init x2, heavy scans, tables, accumulate
   const int push_k = 2 + 2 * hv;
   const int pull_k = 2 + hv + (g->n_hub_items > 0 ? 2 : 0);
   xbk::k_pass_accum<<<1, 1, 0, s>>>(p.ctr, sum, (long long)g->n, kb, (int)sizeof(OffT) * 2, (int)sizeof(W), NW,

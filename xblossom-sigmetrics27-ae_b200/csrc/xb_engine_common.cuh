@@ -388,9 +388,7 @@ xb_status emit_tables(const PassRes<W, NW, OffT>& p, const xb_graph* g, const in
   const int64_t ntiles = (p.n + 31) / 32;
   const int tab_grid = (int)std::max<int64_t>(1, std::min<int64_t>((ntiles + TAB_WARPS - 1) / TAB_WARPS, (int64_t)sms * 16));
   for (int wi = 0; wi < NW; wi++) {
-    const int kbw = std::min(B, kb - wi * B);
-    if (kbw <= 0) break;
-    const int32_t* wsrc = src + wi * B;
+    if (kb - wi * B <= 0) break;
     if (g->n_heavy > 0 && search_heavy) {
       // heavy vertices reached by a push step at level >= 2: search their parents
       const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(g->n_hitems, (int64_t)sms * 8));
@@ -399,11 +397,11 @@ xb_status emit_tables(const PassRes<W, NW, OffT>& p, const xb_graph* g, const in
                                                                  p.pushed);
       (*launches)++;
     }
-    xbk::k_tables<W, NW, OffT, TAB_WARPS, 4><<<tab_grid, TAB_WARPS * 32, 0, s>>>(
-        p.n, p.ro, p.ci, p.seen, p.pl, wi, kbw, p.heavy, rows + (int64_t)wi * 2 * B, p.ctr, p.ppos, p.pushed, wsrc,
-        g->d_hidx_of, p.hpar);
-    (*launches)++;
   }
+  // all words of the pass in one launch (a tile's words share sectors)
+  xbk::k_tables<W, NW, OffT, TAB_WARPS, 4><<<tab_grid, TAB_WARPS * 32, 0, s>>>(
+      p.n, p.ro, p.ci, p.seen, p.pl, kb, p.heavy, rows, p.ctr, p.ppos, p.pushed, src, g->d_hidx_of, p.hpar);
+  (*launches)++;
   XB_LAUNCH_CHECK("tables");
   return XB_OK;
 }

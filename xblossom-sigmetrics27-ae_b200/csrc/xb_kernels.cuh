@@ -1189,9 +1189,10 @@ __global__ void k_fill(T* p, int64_t count, T value) {
 }
 
 // ---------------------------------------------------------------------------
-// Table pass, word wi of the pass (its sources wsrc[0..kbw)).  rows[s] and
-// rows[B + s] are the level and parent rows (n int32 each) of source s, so the
-// sources of one word may belong to different queries and output buffers.
+// Table pass of a pass of kb sources (wsrc[0..kb)), all its words.  For word
+// wi, rows[wi*2B + s] and rows[wi*2B + B + s] are the level and parent rows (n
+// int32 each) of its source s, so the sources of one word may belong to
+// different queries and output buffers.
 //
 // The vertex's own level classes: root = the vertex is the source (level 0 is
 // the only level with every plane bit clear); lvl1 = level exactly 1, whose
@@ -1277,7 +1278,7 @@ __device__ __forceinline__ void vertex_levels(const W* __restrict__ seen, const 
 template <typename W, int NW, typename OffT, int WARPS, int U>
 __global__ void __launch_bounds__(WARPS * 32, 32 / WARPS) k_tables(int64_t n, const OffT* __restrict__ ro,
                                                        const int32_t* __restrict__ ci, const W* __restrict__ seen,
-                                                       Planes<W, NW> pl, int wi, int kbw, int heavy,
+                                                       Planes<W, NW> pl, int kb, int heavy,
                                                        int32_t* const* __restrict__ rows, Ctrs* ctr,
                                                        const W* __restrict__ ppos, const W* __restrict__ pushed,
                                                        const int32_t* __restrict__ wsrc,
@@ -1286,14 +1287,16 @@ __global__ void __launch_bounds__(WARPS * 32, 32 / WARPS) k_tables(int64_t n, co
   constexpr int B = WB<W>::bits;
   constexpr int ROW = B * NW;
   const int nplanes = ctr->b.nplanes;
-  __shared__ int32_t s_src[B];
-  __shared__ int32_t* s_row[2][B];
-  for (int s = threadIdx.x; s < B; s += blockDim.x) {
-    s_src[s] = s < kbw ? wsrc[s] : -1;
-    s_row[0][s] = s < kbw ? rows[s] : nullptr;
-    s_row[1][s] = s < kbw ? rows[B + s] : nullptr;
+  __shared__ int32_t s_src[NW][B];
+  __shared__ int32_t* s_row[NW][2][B];
+  for (int j = threadIdx.x; j < NW * B; j += blockDim.x) {
+    const int w = j / B, s = j % B;
+    s_src[w][s] = j < kb ? wsrc[j] : -1;
+    s_row[w][0][s] = j < kb ? rows[w * 2 * B + s] : nullptr;
+    s_row[w][1][s] = j < kb ? rows[w * 2 * B + B + s] : nullptr;
   }
   __syncthreads();
+  const int nwords = (kb + B - 1) / B;
   __shared__ int32_t s_off[WARPS][33];
   __shared__ int64_t s_pos[WARPS][32];
   __shared__ W s_need[WARPS][32];
@@ -1308,6 +1311,9 @@ __global__ void __launch_bounds__(WARPS * 32, 32 / WARPS) k_tables(int64_t n, co
   const int64_t nwarps = (int64_t)gridDim.x * WARPS;
   unsigned long long pe = 0;
   for (int64_t tile = warp; tile < ntiles; tile += nwarps) {
+   // the words of a tile back to back: their vertex words share sectors
+   for (int wi = 0; wi < nwords; wi++) {
+    const int kbw = min(B, kb - wi * B);
     const int64_t v = tile * 32 + lane;
     const bool valid = v < n;
     W sv = 0, p0 = 0, p1 = 0, root = 0, lvl1 = 0;
@@ -1395,7 +1401,7 @@ __global__ void __launch_bounds__(WARPS * 32, 32 / WARPS) k_tables(int64_t n, co
           W mine = eq & ~excl & ~s_found[wib][k];
           while (mine) {
             const int b = ffs0(mine);
-            __stcs(&s_row[1][b][tile * 32 + k], col[u]);
+            __stcs(&s_row[wi][1][b][tile * 32 + k], col[u]);
             mine &= mine - 1;
           }
         }
@@ -1485,7 +1491,7 @@ __global__ void __launch_bounds__(WARPS * 32, 32 / WARPS) k_tables(int64_t n, co
               const uint32_t pw = i < 4 ? plo : phi;
               if (((farb >> i) & 1) && !hrow) pr[i] = __ldg(&ci[beg + ((pw >> (8 * (i & 3))) & 0xFFu)]);
               if (hrow && sb + i < kbw) pr[i] = hrow[sb + i];
-              if ((l1b >> i) & 1) pr[i] = s_src[sb + i];
+              if ((l1b >> i) & 1) pr[i] = s_src[wi][sb + i];
               if ((rtb >> i) & 1) pr[i] = (int32_t)v;
             }
           }
@@ -1500,14 +1506,15 @@ __global__ void __launch_bounds__(WARPS * 32, 32 / WARPS) k_tables(int64_t n, co
             const int s = sb + i;
             if (s < kbw && valid) {
               const bool hit = (svb >> i) & 1;
-              __stcs(&s_row[0][s][v], hit ? lv[i] : -1);
-              if (!((ndb >> i) & 1)) __stcs(&s_row[1][s][v], hit ? pr[i] : -1);
+              __stcs(&s_row[wi][0][s][v], hit ? lv[i] : -1);
+              if (!((ndb >> i) & 1)) __stcs(&s_row[wi][1][s][v], hit ? pr[i] : -1);
             }
           }
         }
       }
     }
     __syncwarp();
+   }
   }
   pe = warp_sum_u64(pe);
   if (lane == 0 && pe) atomicAdd(&ctr->b.parent_edges, pe);

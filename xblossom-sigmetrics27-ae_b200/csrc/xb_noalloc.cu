@@ -264,7 +264,7 @@ extern "C" xb_status xb_traverse_noalloc(int64_t n, const int32_t* row_offsets, 
     // pageable source: the copy has taken hrows by the time the call returns
     NA_CUDA(cudaMemcpyAsync(rows, hrows, sizeof(hrows), cudaMemcpyHostToDevice, sm));
     xbk::k_tables<W, 1, int32_t, TAB_WARPS, U><<<tab_grid, TAB_WARPS * 32, 0, sm>>>(
-        n, row_offsets, col_indices, seen, pl, 0, kb, INT32_MAX, rows, ctr, ppos, pushed, sources + k0, nullptr,
+        n, row_offsets, col_indices, seen, pl, kb, INT32_MAX, rows, ctr, ppos, pushed, sources + k0, nullptr,
         nullptr);
     NA_CUDA(cudaGetLastError());
     NA_CUDA(cudaMemcpyAsync(&h, ctr, sizeof(h), cudaMemcpyDeviceToHost, sm));
