@@ -53,6 +53,7 @@ typedef int32_t xb_status;
 /* xb_traverse flags */
 #define XB_OUT_DEVICE 1u     /* level/parent are device pointers (else host) */
 #define XB_SOURCES_DEVICE 2u /* sources is a device pointer (else host) */
+#define XB_PARENT_FIFO 4u    /* xb_traverse only: parents by the FIFO rule (see xb_traverse) */
 
 typedef struct xb_host_csr xb_host_csr; /* host-resident CSR (int64 offsets) */
 typedef struct xb_ctx xb_ctx;           /* device, stream, workspace */
@@ -187,7 +188,13 @@ xb_status xb_select_sources(const xb_graph* g, uint64_t seed, int32_t k, int32_t
  * the smallest-id neighbour one level closer to the source (the source's own
  * parent is itself; -1 unreached).  Sources are processed 64 (or 32) per
  * word, one word per launch sequence, with a host-side level loop.
- * mode must be XB_MODE_PLAIN; matching and owner must be NULL. */
+ * mode must be XB_MODE_PLAIN; matching and owner must be NULL.
+ * With XB_PARENT_FIFO the parents follow the reference's sequential FIFO
+ * search instead (xblossom::Graph::findShortestPath, xgraph.h:155-191): a
+ * vertex's parent is the first vertex of the BFS queue adjacent to it, the
+ * queue of a level ordered by (parent's place, place in the parent's
+ * adjacency); levels are the same.  The graph must hold no duplicate
+ * adjacency entries for this rule. */
 xb_status xb_traverse(xb_ctx* ctx, const xb_graph* g, const int32_t* sources, int32_t k,
                       int32_t mode, const int32_t* matching, int32_t* level, int32_t* parent,
                       int32_t* owner, uint32_t flags, xb_stats* stats);

@@ -216,3 +216,38 @@ def test_autotuner_picks_a_config_that_keeps_parity(ctx, tmp_path):
     autotune.save(best, str(tmp_path / "t.json"))
     assert autotune.load(str(tmp_path / "t.json")) == best
     g.close()
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p)[:-4] for p in GOLDEN])
+def test_fifo_parents_match_the_reference_search(ctx, path):
+    """XB_PARENT_FIFO: parents equal those of the reference's own
+    findShortestPath (golden pairs) and the oracle's FIFO rule; levels are
+    the min-id run's."""
+    z = np.load(path)
+    ro, ci, src = z["ro"], z["ci"], z["sources"]
+    _tune(ctx)
+    g = ctx.upload_arrays(ro, ci)
+    r = ctx.traverse(g, src, parent_rule="fifo")
+    S, D = z["pair_src_idx"], z["pair_dst"]
+    np.testing.assert_array_equal(r.parent[S, D], z["pair_parent"])
+    lv, pr, _, _ = O.msbfs(ro, ci, src, rule=O.RULE_FIFO)
+    np.testing.assert_array_equal(r.level, lv)
+    np.testing.assert_array_equal(r.parent, pr)
+    g.close()
+
+
+@pytest.mark.parametrize("variant", [0, 1, 2, 4])
+@pytest.mark.parametrize("out", ["host", "device"])
+def test_fifo_parents_rmat_and_er(ctx, variant, out):
+    _tune(ctx, **VARIANTS[variant])
+    for csr, k in ((xbtrav.HostCSR.rmat(12, 16, seed=41), 150), (xbtrav.HostCSR.er(4000, 12000, seed=42), 70)):
+        ro, ci = csr.arrays()
+        src = xbtrav.select_sources_csr(ro, 43, k)
+        g = ctx.upload(csr)
+        r = ctx.traverse(g, src, out=out, parent_rule="fifo")
+        lv, pr, _, _ = O.msbfs(ro, ci, src, rule=O.RULE_FIFO)
+        level = r.level.cpu().numpy() if out == "device" else r.level
+        parent = r.parent.cpu().numpy() if out == "device" else r.parent
+        np.testing.assert_array_equal(level, lv)
+        np.testing.assert_array_equal(parent, pr)
+        g.close()

@@ -924,6 +924,7 @@ extern "C" xb_status xb_traverse_batched(xb_ctx* c, const xb_batch_item* items, 
     if (!it.graph) return fail(XB_ERR_ARG, at + "null graph");
     if (it.graph->ctx->device != c->device) return fail(XB_ERR_ARG, at + "graph lives on another device");
     if (it.k < 0) return fail(XB_ERR_ARG, at + "negative source count");
+    if (it.flags & XB_PARENT_FIFO) return fail(XB_ERR_ARG, at + "FIFO parents are computed by xb_traverse only");
     if (it.k == 0) continue;
     if (!it.sources || !it.level || !it.parent) return fail(XB_ERR_ARG, at + "null sources or output tables");
     if (!(it.flags & XB_OUT_DEVICE)) {

@@ -85,6 +85,20 @@ xb_status ensure_rows(xb_ctx* c, int64_t count) {
   return XB_OK;
 }
 
+// Work areas of the FIFO-parent pass (two queues and counts per source row).
+xb_status ensure_fifo(xb_ctx* c, size_t ints) {
+  if (c->fifo_cap >= ints) return XB_OK;
+  if (c->d_fifo) cudaFree(c->d_fifo);
+  c->d_fifo = nullptr;
+  c->fifo_cap = 0;
+  if (cudaMalloc(&c->d_fifo, sizeof(int32_t) * std::max<size_t>(ints, 1)) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(XB_ERR_OOM, "FIFO-parent work allocation failed");
+  }
+  c->fifo_cap = ints;
+  return XB_OK;
+}
+
 xb_status ensure_heavy(xb_graph* g, int thr) {
   if (g->heavy_thr == thr) return XB_OK;
   // heavy vertices by falling degree (ties by ascending id): every heavy
@@ -208,7 +222,7 @@ xb_status ensure_heavy(xb_graph* g, int thr) {
 
 template <typename W, int NW, typename OffT>
 xb_status run_plain(xb_ctx* c, xb_graph* g, const int32_t* d_sources, int32_t k, int32_t* level_out,
-                    int32_t* parent_out, bool out_dev, xb_stats* st) {
+                    int32_t* parent_out, bool out_dev, bool fifo, xb_stats* st) {
   constexpr int B = xbk::WB<W>::bits;
   constexpr int SPP = B * NW;  // sources per pass
   const int64_t n = g->n;
@@ -293,6 +307,17 @@ xb_status run_plain(xb_ctx* c, xb_graph* g, const int32_t* d_sources, int32_t k,
     s = emit_tables<W, NW, OffT>(p, g, d_sources + k0, kb, c->d_rows + (k0 / SPP) * 2 * SPP,
                                  c->h_ctr->b.pushed_deep != 0, c->stream, sms, &launches);
     if (s != XB_OK) return s;
+    if (fifo) {  // parents by the FIFO rule, rewritten from the finished level rows
+      const int group = std::min(kb, kFifoGroup);
+      s = ensure_fifo(c, (size_t)group * 3 * (size_t)n);
+      if (s != XB_OK) return s;
+      for (int j0 = 0; j0 < kb; j0 += group) {
+        xbk::k_fifo_parents<OffT><<<std::min(group, kb - j0), 1024, 0, c->stream>>>(
+            n, p.ro, p.ci, c->d_rows + (k0 / SPP) * 2 * SPP, B, j0, kb, d_sources + k0, c->d_fifo, 3 * n);
+        launches++;
+      }
+      XB_LAUNCH_CHECK("fifo parents");
+    }
     timer.end(1, launches);
     if (!out_dev) {
       XB_CUDA(cudaMemcpyAsync(level_out + k0 * n, lv_base, sizeof(int32_t) * (size_t)kb * n, cudaMemcpyDeviceToHost,
@@ -324,11 +349,12 @@ xb_status run_plain(xb_ctx* c, xb_graph* g, const int32_t* d_sources, int32_t k,
 
 template <typename W, typename OffT>
 xb_status dispatch_nw(xb_ctx* c, xb_graph* g, const int32_t* d_src, int32_t k, int32_t* lv, int32_t* pr, bool od,
+                      bool fifo,
                       xb_stats* st) {
   switch (c->tuning.words) {
-    case 1: return run_plain<W, 1, OffT>(c, g, d_src, k, lv, pr, od, st);
-    case 2: return run_plain<W, 2, OffT>(c, g, d_src, k, lv, pr, od, st);
-    case 4: return run_plain<W, 4, OffT>(c, g, d_src, k, lv, pr, od, st);
+    case 1: return run_plain<W, 1, OffT>(c, g, d_src, k, lv, pr, od, fifo, st);
+    case 2: return run_plain<W, 2, OffT>(c, g, d_src, k, lv, pr, od, fifo, st);
+    case 4: return run_plain<W, 4, OffT>(c, g, d_src, k, lv, pr, od, fifo, st);
     default: return fail(XB_ERR_ARG, "tuning.words must be 1, 2 or 4");
   }
 }
@@ -381,6 +407,7 @@ xb_status xb_ctx_destroy(xb_ctx* c) {
   if (c->d_src) cudaFree(c->d_src);
   if (c->d_stage) cudaFree(c->d_stage);
   if (c->d_rows) cudaFree(c->d_rows);
+  if (c->d_fifo) cudaFree(c->d_fifo);
   if (c->d_ctr) cudaFree(c->d_ctr);
   if (c->h_ctr) cudaFreeHost(c->h_ctr);
   for (cudaEvent_t ev : {c->ev0, c->ev1, c->evc0, c->evc1})
@@ -599,6 +626,7 @@ xb_status xb_traverse(xb_ctx* c, const xb_graph* gc, const int32_t* sources, int
   XB_CUDA(cudaSetDevice(c->device));
   const bool src_dev = (flags & XB_SOURCES_DEVICE) != 0;
   const bool out_dev = (flags & XB_OUT_DEVICE) != 0;
+  const bool fifo = (flags & XB_PARENT_FIFO) != 0;
   // validate sources (host copy)
   std::vector<int32_t> hs((size_t)k);
   if (src_dev) {
@@ -613,11 +641,11 @@ xb_status xb_traverse(xb_ctx* c, const xb_graph* gc, const int32_t* sources, int
   XB_CUDA(cudaMemcpyAsync(c->d_src, hs.data(), sizeof(int32_t) * k, cudaMemcpyHostToDevice, c->stream));
   XB_CUDA(cudaEventRecord(c->ev0, c->stream));
   if (c->tuning.word_bits == 64) {
-    s = g->off64 ? xbe::dispatch_nw<unsigned long long, int64_t>(c, g, c->d_src, k, level, parent, out_dev, st)
-                 : xbe::dispatch_nw<unsigned long long, int32_t>(c, g, c->d_src, k, level, parent, out_dev, st);
+    s = g->off64 ? xbe::dispatch_nw<unsigned long long, int64_t>(c, g, c->d_src, k, level, parent, out_dev, fifo, st)
+                 : xbe::dispatch_nw<unsigned long long, int32_t>(c, g, c->d_src, k, level, parent, out_dev, fifo, st);
   } else {
-    s = g->off64 ? xbe::dispatch_nw<unsigned int, int64_t>(c, g, c->d_src, k, level, parent, out_dev, st)
-                 : xbe::dispatch_nw<unsigned int, int32_t>(c, g, c->d_src, k, level, parent, out_dev, st);
+    s = g->off64 ? xbe::dispatch_nw<unsigned int, int64_t>(c, g, c->d_src, k, level, parent, out_dev, fifo, st)
+                 : xbe::dispatch_nw<unsigned int, int32_t>(c, g, c->d_src, k, level, parent, out_dev, fifo, st);
   }
   if (s != XB_OK) {
     cudaStreamSynchronize(c->stream);

@@ -48,6 +48,8 @@ struct xb_ctx {
   size_t stage_bytes = 0;
   int32_t** d_rows = nullptr;  // row-pointer tables of the table pass (2*B per word)
   int64_t rows_cap = 0;
+  int32_t* d_fifo = nullptr;  // work areas of the FIFO-parent pass
+  size_t fifo_cap = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, evc0 = nullptr, evc1 = nullptr;
   xbe::BatchState* batch = nullptr;  // resources of xb_traverse_batched (created on first use)
 };
@@ -103,6 +105,8 @@ constexpr int kHubDegree = 4096;
 constexpr int kHubChunk = 2048;
 // Parent slots per heavy vertex: up to 64 sources x 4 words.
 constexpr int kHparRow = 256;
+// Source rows whose FIFO parents are computed at once (one block each).
+constexpr int kFifoGroup = 64;
 // Zero entries allocated past the end of a resident colIndices array.
 constexpr int64_t kCiPad = 16;
 

@@ -1764,6 +1764,143 @@ static __global__ void k_pass_accum(const Ctrs* ctr, PassSum* sum, long long n, 
   if (b.err) sum->errors += 1;
 }
 
+// ---------------------------------------------------------------------------
+// FIFO parents: the parent rule of a sequential FIFO breadth-first search
+// (xblossom::Graph::findShortestPath, apps/xb/src/include/graph/xgraph.h:155-191):
+// a vertex's parent is the first dequeued vertex adjacent to it, and a
+// level's queue is ordered by (place of the parent in its own level's queue,
+// place in the parent's adjacency).  Computed after the traversal from the
+// finished level row, one block per source, level by level:
+//   keys    every frontier vertex (queue rank r; one warp per vertex) offers r
+//           to its next-level neighbours with atomicMin, in the parent row
+//   counts  children of rank r = next-level neighbours whose key is r
+//   scan    block-wide exclusive scan of the counts: first child's rank
+//   queue   each frontier vertex writes its children in adjacency order
+//           (warp ballots); then the keys become parent ids
+// The adjacency must hold no duplicate entries.  work: 3*n int32 per block
+// (two queues and the counts).
+
+// Exclusive prefix sum of a[0..len) in place over the whole block; returns
+// the total to every thread.
+__device__ __forceinline__ int64_t block_exclusive_scan(int32_t* a, int64_t len) {
+  __shared__ int32_t s_w[32];
+  __shared__ int64_t s_carry;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  if (threadIdx.x == 0) s_carry = 0;
+  __syncthreads();
+  for (int64_t base = 0; base < len; base += blockDim.x) {
+    const int64_t i = base + threadIdx.x;
+    const int32_t x = i < len ? a[i] : 0;
+    int32_t incl = x;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    if (lane == 31) s_w[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+      int32_t t = lane < nwarps ? s_w[lane] : 0;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int32_t y = __shfl_up_sync(0xffffffffu, t, o);
+        if (lane >= o) t += y;
+      }
+      if (lane < nwarps) s_w[lane] = t;
+    }
+    __syncthreads();
+    const int64_t carry = s_carry;
+    if (i < len) a[i] = (int32_t)(carry + (warp > 0 ? s_w[warp - 1] : 0) + incl - x);
+    __syncthreads();
+    if (threadIdx.x == 0) s_carry = carry + s_w[nwarps - 1];
+    __syncthreads();
+  }
+  return s_carry;
+}
+
+// Block b handles source j = j0 + b of the pass (rows in the table pass
+// layout: word j/B, level row rows[wi*2B + j%B], parent row rows[wi*2B + B +
+// j%B]).  The parent row holds the traversal's parents on entry (the source
+// its own parent, -1 unreached); levels >= 1 are rewritten.
+template <typename OffT>
+__global__ void __launch_bounds__(1024) k_fifo_parents(int64_t n, const OffT* __restrict__ ro,
+                                                       const int32_t* __restrict__ ci, int32_t* const* __restrict__ rows,
+                                                       int B, int j0, int kb, const int32_t* __restrict__ src,
+                                                       int32_t* work, int64_t wstride) {
+  const int j = j0 + (int)blockIdx.x;
+  if (j >= kb) return;  // block-uniform
+  const int wi = j / B, b = j % B;
+  const int32_t* lv = rows[wi * 2 * B + b];
+  int32_t* pr = rows[wi * 2 * B + B + b];
+  int32_t* q0 = work + (int64_t)blockIdx.x * wstride;
+  int32_t* q1 = q0 + n;
+  int32_t* cnt = q1 + n;
+  __shared__ int64_t s_qn;
+  for (int64_t v = threadIdx.x; v < n; v += blockDim.x)
+    if (lv[v] >= 1) pr[v] = INT32_MAX;
+  if (threadIdx.x == 0) {
+    q0[0] = src[j];
+    s_qn = 1;
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  for (int32_t d = 0;; d++) {
+    const int64_t qn = s_qn;
+    if (qn == 0) break;  // block-uniform
+    for (int64_t r = warp; r < qn; r += nwarps) {  // keys
+      const int32_t u = q0[r];
+      const int64_t end = ro[u + 1];
+      for (int64_t e = (int64_t)ro[u] + lane; e < end; e += 32) {
+        const int32_t w = ci[e];
+        if (lv[w] == d + 1) atomicMin(&pr[w], (int32_t)r);
+      }
+    }
+    __syncthreads();
+    for (int64_t r = warp; r < qn; r += nwarps) {  // counts
+      const int32_t u = q0[r];
+      const int64_t end = ro[u + 1];
+      int32_t c = 0;
+      for (int64_t e = (int64_t)ro[u] + lane; e < end; e += 32) {
+        const int32_t w = ci[e];
+        c += (lv[w] == d + 1 && pr[w] == (int32_t)r) ? 1 : 0;
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+      if (lane == 0) cnt[r] = c;
+    }
+    __syncthreads();
+    const int64_t total = block_exclusive_scan(cnt, qn);
+    for (int64_t r = warp; r < qn; r += nwarps) {  // next queue, children in adjacency order
+      const int32_t u = q0[r];
+      const int64_t beg = ro[u], end = ro[u + 1];
+      int64_t pos = cnt[r];
+      for (int64_t e0 = beg; e0 < end; e0 += 32) {
+        const int64_t e = e0 + lane;
+        int32_t w = 0;
+        bool hit = false;
+        if (e < end) {
+          w = ci[e];
+          hit = lv[w] == d + 1 && pr[w] == (int32_t)r;
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, hit);
+        if (hit) q1[pos + __popc(m & ((1u << lane) - 1u))] = w;
+        pos += __popc(m);
+      }
+    }
+    __syncthreads();
+    for (int64_t i = threadIdx.x; i < total; i += blockDim.x) {  // keys -> parent ids
+      const int32_t w = q1[i];
+      pr[w] = q0[pr[w]];
+    }
+    __syncthreads();
+    int32_t* t = q0;
+    q0 = q1;
+    q1 = t;
+    if (threadIdx.x == 0) s_qn = total;
+    __syncthreads();
+  }
+}
+
 // Digest of one table row pair (level row, parent row of a source): the
 // summary a serving client gets instead of the full tables.
 struct RowDigest {

@@ -41,6 +41,7 @@ XB_MODE_PLAIN = 0
 XB_MODE_ALTERNATING = 1
 XB_OUT_DEVICE = 1
 XB_SOURCES_DEVICE = 2
+XB_PARENT_FIFO = 4
 XB_MAX_SLOTS = 16
 SLOT_MAX_ROWS = 256  # sources per slot pass at most (64 per word x 4 words)
 
@@ -409,15 +410,20 @@ class Context:
         return Graph(self, h.value)
 
     # traversal --------------------------------------------------------------
-    def traverse(self, graph: Graph, sources, out: str = "host", level=None, parent=None) -> TraversalResult:
+    def traverse(self, graph: Graph, sources, out: str = "host", level=None, parent=None,
+                 parent_rule: str = "minid") -> TraversalResult:
         """Plain multi-source traversal through xb_traverse.
 
         out="host": numpy (k, n) int32 tables (host buffers, the drop-in path);
         out="device": torch int32 CUDA tensors (k, n) (allocated here unless
         given).  sources: numpy int32 (host) or a torch int32 CUDA tensor.
+        parent_rule: "minid" (smallest-id neighbour one level up) or "fifo"
+        (the reference's sequential FIFO search, XB_PARENT_FIFO).
         """
         st = XbStats()
-        flags = 0
+        if parent_rule not in ("minid", "fifo"):
+            raise ValueError("parent_rule must be 'minid' or 'fifo'")
+        flags = XB_PARENT_FIFO if parent_rule == "fifo" else 0
         src_keep = sources
         if hasattr(sources, "data_ptr"):
             flags |= XB_SOURCES_DEVICE
