@@ -729,8 +729,13 @@ __device__ __forceinline__ void pull_lane_vertex(bool act, int32_t v, const W (&
                                                  const W* __restrict__ F, W* seen, W* N, const Planes<W, NW>& pl,
                                                  const Masks<W, NW>& active, int heavy, int level, Lists nl,
                                                  LevelCtr* nctr, W* __restrict__ ppos, StatAcc<W, NW>& sacc,
-                                                 unsigned long long& e_scan) {
-  W want[NW], acc[NW], pp[NW][8];
+                                                 unsigned long long& e_scan, W* spp) {
+  // position planes of this lane's claims: registers for one word, the
+  // lane's shared-memory column for more (plane-major, 32 lanes apart, so a
+  // warp's accesses hit distinct banks; they change only on a claim)
+  constexpr bool kRegPP = NW == 1;
+  W want[NW], acc[NW], rpp[kRegPP ? 8 : 1];
+  auto pp = [&](int i, int k) -> W& { return kRegPP ? rpp[k] : spp[(i * 8 + k) * 32]; };
   int64_t beg = 0, end = 0;
   if (act) {
     beg = ro[v];
@@ -741,27 +746,40 @@ __device__ __forceinline__ void pull_lane_vertex(bool act, int32_t v, const W (&
     want[i] = act ? (live[i] & ~sw[i]) : (W)0;
     acc[i] = 0;
 #pragma unroll
-    for (int k = 0; k < 8; k++) pp[i][k] = 0;
+    for (int k = 0; k < 8; k++) pp(i, k) = 0;
   }
   const bool rec = end - beg <= kP8MaxDegree;
-  // aligned groups of 8 entries (two 16-byte loads); entries outside
-  // [beg, end) are masked off.  The next group's colIndices are loaded before
-  // this group's frontier words are gathered, so the two latencies overlap.
+  // aligned groups of G entries (G/4 16-byte loads; G = 8 for one word per
+  // vertex, 4 for more, so the gathered words fit in registers); entries
+  // outside [beg, end) are masked off.  The next group's colIndices are
+  // loaded before this group's frontier words are gathered, so the two
+  // latencies overlap.
+  constexpr int G = NW == 1 ? 8 : 4;
+  constexpr int Q = G / 4;
   int64_t j0 = beg & ~(int64_t)3;
-  int4 qa = make_int4(0, 0, 0, 0), qb = make_int4(0, 0, 0, 0);
-  if (j0 < end) {
-    qa = __ldcs(reinterpret_cast<const int4*>(ci + j0));
-    qb = __ldcs(reinterpret_cast<const int4*>(ci + j0 + 4));
-  }
-  for (; j0 < end; j0 += 8) {
-    const int32_t cols[8] = {qa.x, qa.y, qa.z, qa.w, qb.x, qb.y, qb.z, qb.w};
-    if (j0 + 8 < end) {
-      qa = __ldcs(reinterpret_cast<const int4*>(ci + j0 + 8));
-      qb = __ldcs(reinterpret_cast<const int4*>(ci + j0 + 12));
-    }
-    W f[8][NW];
+  int4 q[Q];
 #pragma unroll
-    for (int t = 0; t < 8; t++) {
+  for (int h = 0; h < Q; h++) q[h] = make_int4(0, 0, 0, 0);
+  if (j0 < end) {
+#pragma unroll
+    for (int h = 0; h < Q; h++) q[h] = __ldcs(reinterpret_cast<const int4*>(ci + j0 + 4 * h));
+  }
+  for (; j0 < end; j0 += G) {
+    int32_t cols[G];
+#pragma unroll
+    for (int h = 0; h < Q; h++) {
+      cols[4 * h] = q[h].x;
+      cols[4 * h + 1] = q[h].y;
+      cols[4 * h + 2] = q[h].z;
+      cols[4 * h + 3] = q[h].w;
+    }
+    if (j0 + G < end) {
+#pragma unroll
+      for (int h = 0; h < Q; h++) q[h] = __ldcs(reinterpret_cast<const int4*>(ci + j0 + G + 4 * h));
+    }
+    W f[G][NW];
+#pragma unroll
+    for (int t = 0; t < G; t++) {
       const int64_t j = j0 + t;
       if (j >= beg && j < end) {
         load_words<W, NW>(F + (int64_t)cols[t] * NW, f[t]);
@@ -772,7 +790,7 @@ __device__ __forceinline__ void pull_lane_vertex(bool act, int32_t v, const W (&
     }
     bool done = true;
 #pragma unroll
-    for (int t = 0; t < 8; t++) {
+    for (int t = 0; t < G; t++) {
       const int pos = (int)(j0 + t - beg);
 #pragma unroll
       for (int i = 0; i < NW; i++) {
@@ -782,7 +800,7 @@ __device__ __forceinline__ void pull_lane_vertex(bool act, int32_t v, const W (&
           if (rec) {
 #pragma unroll
             for (int k = 0; k < 8; k++)
-              if ((pos >> k) & 1) pp[i][k] |= c;
+              if ((pos >> k) & 1) pp(i, k) |= c;
           }
         }
       }
@@ -790,7 +808,7 @@ __device__ __forceinline__ void pull_lane_vertex(bool act, int32_t v, const W (&
 #pragma unroll
     for (int i = 0; i < NW; i++) done = done && acc[i] == want[i];
     if (done) {
-      j0 += 8;
+      j0 += G;
       break;
     }
   }
@@ -806,7 +824,7 @@ __device__ __forceinline__ void pull_lane_vertex(bool act, int32_t v, const W (&
         W* prow = ppos + ((int64_t)v * NW + i) * 8;
 #pragma unroll
         for (int k = 0; k < 8; k++)
-          if (pp[i][k]) prow[k] |= pp[i][k];
+          if (pp(i, k)) prow[k] |= pp(i, k);
       }
     }
   }
@@ -824,6 +842,7 @@ __global__ void __launch_bounds__(WARPS * 32, 3) k_pull_lanes(int32_t nchunks, c
   const int level = ctr->b.level;
   __shared__ int32_t s_qv[WARPS][64];
   __shared__ W s_qs[WARPS][64][NW];
+  __shared__ W s_pp[NW > 1 ? WARPS : 1][NW > 1 ? NW * 8 : 1][32];
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
   LevelCtr* cctr = &ctr->lv[cur];
@@ -834,6 +853,7 @@ __global__ void __launch_bounds__(WARPS * 32, 3) k_pull_lanes(int32_t nchunks, c
   unsigned long long e_scan = 0, v_scan = 0, v_sweep = 0;
   StatAcc<W, NW> sacc;
   int qn = 0;  // queued vertices (warp-uniform)
+  W* spp = NW > 1 ? &s_pp[NW > 1 ? wib : 0][0][lane] : nullptr;
   for (;;) {
     int chunk = 0;
     if (lane == 0) chunk = atomicAdd(&nctr->work, 1);
@@ -888,7 +908,7 @@ __global__ void __launch_bounds__(WARPS * 32, 3) k_pull_lanes(int32_t nchunks, c
           __syncwarp();
           v_scan++;
           pull_lane_vertex<W, NW, OffT>(true, qv, qs, live, ro, ci, F, seen, N, pl, active, heavy, level, nl, nctr,
-                                        ppos, sacc, e_scan);
+                                        ppos, sacc, e_scan, spp);
         }
       }
     }
@@ -903,7 +923,7 @@ __global__ void __launch_bounds__(WARPS * 32, 3) k_pull_lanes(int32_t nchunks, c
         if (act) qv = s_qv[wib][lane];
         v_scan += act ? 1 : 0;
         pull_lane_vertex<W, NW, OffT>(act, qv, qs, live, ro, ci, F, seen, N, pl, active, heavy, level, nl, nctr,
-                                      ppos, sacc, e_scan);
+                                      ppos, sacc, e_scan, spp);
       }
       break;
     }
