@@ -205,6 +205,8 @@ def test_autotuner_picks_a_config_that_keeps_parity(ctx, tmp_path):
     space = {"word_bits": [64, 32], "words": [1, 2], "heavy_degree": [128, 256], "pull_alpha": [64.0, 256.0],
              "chains": [1, 2]}
     for path in ("plain", "batched"):
+        # the first stage keeps the current cutoffs: start inside the space
+        _tune(ctx, heavy_degree=256, pull_alpha=256.0, chains=2)
         best, table = autotune.autotune(ctx, g, src, space=space, reps=1, path=path)
         assert all(best[k] in space[k] for k in space if path == "batched" or k != "chains")
         assert best == {k: ctx.tuning()[k] for k in best}
@@ -251,3 +253,22 @@ def test_fifo_parents_rmat_and_er(ctx, variant, out):
         np.testing.assert_array_equal(level, lv)
         np.testing.assert_array_equal(parent, pr)
         g.close()
+
+
+def test_graph_outliving_its_context():
+    """A graph freed after its context was destroyed (e.g. by a garbage
+    collector at exit) is released without touching the context; using it
+    fails cleanly."""
+    c2 = xbtrav.Context(0)
+    csr = xbtrav.HostCSR.rmat(8, 4, seed=5)
+    g = c2.upload(csr)
+    views = c2.upload_batch([csr, csr])
+    c2.close()
+    c3 = xbtrav.Context(0)
+    with pytest.raises(xbtrav.XbError) as e:
+        c3.traverse(g, np.array([0], np.int32))
+    assert e.value.status == xbtrav.XB_ERR_STATE
+    g.close()
+    for v in views:
+        v.close()
+    c3.close()

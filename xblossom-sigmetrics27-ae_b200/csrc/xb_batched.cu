@@ -922,6 +922,7 @@ extern "C" xb_status xb_traverse_batched(xb_ctx* c, const xb_batch_item* items, 
     const xb_batch_item& it = its[(size_t)i];
     const std::string at = "item " + std::to_string(i) + ": ";
     if (!it.graph) return fail(XB_ERR_ARG, at + "null graph");
+    if (!it.graph->ctx) return fail(XB_ERR_STATE, at + "the graph's context was destroyed");
     if (it.graph->ctx->device != c->device) return fail(XB_ERR_ARG, at + "graph lives on another device");
     if (it.k < 0) return fail(XB_ERR_ARG, at + "negative source count");
     if (it.flags & XB_PARENT_FIFO) return fail(XB_ERR_ARG, at + "FIFO parents are computed by xb_traverse only");
@@ -971,6 +972,7 @@ extern "C" xb_status xb_slot_launch(xb_ctx* c, int32_t slot, const xb_graph* gc,
   xb_graph* g = const_cast<xb_graph*>(gc);
   if (!c || !g || !sources || !level_rows || !parent_rows) return fail(XB_ERR_ARG, "null argument");
   if (slot < 0 || slot >= xbe::kMaxSlots) return fail(XB_ERR_ARG, "slot out of range");
+  if (!g->ctx) return fail(XB_ERR_STATE, "the graph's context was destroyed");
   if (g->ctx->device != c->device) return fail(XB_ERR_ARG, "graph lives on another device");
   for (int32_t j = 0; j < kb; j++)
     if (sources[j] < 0 || sources[j] >= g->n) return fail(XB_ERR_ARG, "source " + std::to_string(j) + " out of range");

@@ -402,6 +402,7 @@ xb_status xb_ctx_destroy(xb_ctx* c) {
   if (!c) return XB_OK;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  for (xb_graph* g : c->graphs) g->ctx = nullptr;  // graphs outliving the context can still be freed
   xbe::batch_state_free(c->batch);
   if (c->ws) cudaFree(c->ws);
   if (c->d_src) cudaFree(c->d_src);
@@ -496,6 +497,7 @@ xb_status xb_graph_upload(xb_ctx* c, int64_t n, const void* row_offsets, int32_t
   XB_CUDA(cudaMemset(g->d_ci + m, 0, sizeof(int32_t) * xbe::kCiPad));
   if (m > 0) XB_CUDA(cudaMemcpy(g->d_ci, col_indices, sizeof(int32_t) * (size_t)m, cudaMemcpyHostToDevice));
   g->h_ro = std::move(ro);
+  c->graphs.push_back(g.get());
   *out = g.release();
   return XB_OK;
 }
@@ -559,7 +561,10 @@ xb_status xb_graph_upload_batch(xb_ctx* c, int32_t ninst, const int64_t* inst_n,
     for (int64_t v = 0; v < n; v++) g->max_deg = std::max(g->max_deg, ro[v + 1] - ro[v]);
     gs.push_back(std::move(g));
   }
-  for (int32_t i = 0; i < ninst; i++) out[i] = gs[(size_t)i].release();
+  for (int32_t i = 0; i < ninst; i++) {
+    c->graphs.push_back(gs[(size_t)i].get());
+    out[i] = gs[(size_t)i].release();
+  }
   return XB_OK;
 }
 
@@ -581,8 +586,14 @@ xb_status xb_graph_load_csr_text(xb_ctx* c, const char* row_path, const char* co
 xb_status xb_graph_free(xb_graph* g) {
   xbi::clear_error();
   if (!g) return XB_OK;
-  cudaSetDevice(g->ctx->device);
-  xbe::batch_forget_graph(g->ctx, g);
+  if (g->ctx) {
+    xb_ctx* c = g->ctx;
+    cudaSetDevice(c->device);
+    xbe::batch_forget_graph(c, g);
+    c->graphs.erase(std::remove(c->graphs.begin(), c->graphs.end(), g), c->graphs.end());
+  } else if (g->store) {
+    cudaSetDevice(g->store->device);
+  }
   g->store.reset();  // frees the CSR arrays with the last graph viewing them
   if (g->d_heavy) cudaFree(g->d_heavy);
   if (g->d_hpar) cudaFree(g->d_hpar);
@@ -616,6 +627,7 @@ xb_status xb_traverse(xb_ctx* c, const xb_graph* gc, const int32_t* sources, int
   xbi::clear_error();
   xb_graph* g = const_cast<xb_graph*>(gc);
   if (!c || !g) return fail(XB_ERR_ARG, "null context or graph");
+  if (!g->ctx) return fail(XB_ERR_STATE, "the graph's context was destroyed");
   if (g->ctx->device != c->device) return fail(XB_ERR_ARG, "graph lives on another device");
   if (mode != XB_MODE_PLAIN) return fail(XB_ERR_ARG, "only XB_MODE_PLAIN is supported by xb_traverse");
   if (matching || owner) return fail(XB_ERR_ARG, "matching/owner must be NULL in plain mode");

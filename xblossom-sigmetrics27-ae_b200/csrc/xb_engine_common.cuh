@@ -52,6 +52,7 @@ struct xb_ctx {
   size_t fifo_cap = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, evc0 = nullptr, evc1 = nullptr;
   xbe::BatchState* batch = nullptr;  // resources of xb_traverse_batched (created on first use)
+  std::vector<xb_graph*> graphs;     // live graphs uploaded through this context
 };
 
 // Device CSR arrays, shared by the graphs that view them (one upload, or all
@@ -70,7 +71,7 @@ struct xb_csr_store {
 };
 
 struct xb_graph {
-  xb_ctx* ctx = nullptr;
+  xb_ctx* ctx = nullptr;  // null once the context is destroyed (the graph can only be freed then)
   int64_t n = 0, m = 0, max_deg = 0;
   bool off64 = false;
   std::shared_ptr<xb_csr_store> store;

@@ -1296,7 +1296,7 @@ __device__ __forceinline__ void vertex_levels(const W* __restrict__ seen, const 
 // exclusive prefix OR in edge order hands each needed bit to its first
 // (= smallest-id) matching neighbour.
 template <typename W, int NW, typename OffT, int WARPS, int U>
-__global__ void __launch_bounds__(WARPS * 32, 32 / WARPS) k_tables(int64_t n, const OffT* __restrict__ ro,
+__global__ void __launch_bounds__(WARPS * 32, 24 / WARPS) k_tables(int64_t n, const OffT* __restrict__ ro,
                                                        const int32_t* __restrict__ ci, const W* __restrict__ seen,
                                                        Planes<W, NW> pl, int kb, int heavy,
                                                        int32_t* const* __restrict__ rows, Ctrs* ctr,
