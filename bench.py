@@ -249,8 +249,10 @@ def run_multi(args, w, name) -> None:
     specs = multi_instances(w["instances"], SEED)
     hosts = [xbtrav.HostCSR.rmat(sc, ef, 0.57, 0.19, 0.19, seed=gs) for sc, ef, _, gs in specs]
     ctx = xbtrav.Context(0)
-    if args.chains:
-        ctx.set_tuning(chains=args.chains)
+    # this workload's tuning (autotuner, batched path): many small queries fill
+    # 64-source passes better than 128-source ones, and more chains overlap
+    # the many short passes
+    ctx.set_tuning(words=1, chains=args.chains or 8)
     graphs = ctx.upload_batch(hosts)
     queries = []
     for (sc, ef, k, gs), g in zip(specs, graphs):
