@@ -59,6 +59,8 @@ WORKLOADS = {
     "rmat22_k128": dict(kind="rmat", scale=22, ef=16, k=128),
     # smaller case for kernel profiles (graph > L2, a few hundred MB on the device)
     "rmat20_k64": dict(kind="rmat", scale=20, ef=16, k=64),
+    # one pass of the default layout (2 words x 64 sources) for kernel profiles
+    "rmat20_k128": dict(kind="rmat", scale=20, ef=16, k=128),
 }
 SEED = 0x5EED
 METRIC = "multi-source GTEPS at 1 B200, batched vs plain; p50/p99 query latency"
