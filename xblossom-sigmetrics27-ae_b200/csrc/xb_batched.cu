@@ -261,7 +261,7 @@ template <typename W, int NW, typename OffT>
 xb_status capture_pass_levels(xb_ctx* c, BatchState* bs, const PassRes<W, NW, OffT>& p, const xb_graph* g,
                               const int32_t* src, int kb, cudaStream_t s) {
   const int sms = c->num_sms;
-  const float alpha = c->tuning.pull_alpha > 0 ? c->tuning.pull_alpha : 256.0f;
+  const float alpha = c->tuning.pull_alpha > 0 ? c->tuning.pull_alpha : 1024.0f;
   const StepShape sh = graph_shape<W, NW, OffT>(g, sms);
   xb_status st = emit_pass_init<W, NW, OffT>(p, g, src, kb, s, sms, true);
   if (st != XB_OK) return st;
