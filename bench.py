@@ -397,6 +397,7 @@ def main() -> None:
     import torch
 
     import xbtrav
+    from xbtrav import replicas
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -421,7 +422,7 @@ def main() -> None:
         ctx.set_tuning(chains=args.chains)
     g = ctx.upload(csr)
     k = w["k"]
-    sources = g.select_sources(SEED + 1 + 7919 * rank, k)
+    sources = g.select_sources(replicas.rank_seed(SEED + 1, rank), k)
     src_dev = torch.from_numpy(sources).to(dev)
     level = torch.empty((k, g.n), dtype=torch.int32, device=dev)
     parent = torch.empty((k, g.n), dtype=torch.int32, device=dev)
@@ -435,18 +436,10 @@ def main() -> None:
         torch.cuda.synchronize(dev)
 
     def max_over_ranks(x: float) -> float:
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return replicas.max_over_ranks(dist, x, dev)
 
     def sum_over_ranks(x: float) -> float:
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        return float(t.item())
+        return replicas.sum_over_ranks(dist, x, dev)
 
     def plain_step():
         return ctx.traverse(g, src_dev, out="device", level=level, parent=parent).stats
