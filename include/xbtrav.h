@@ -269,6 +269,22 @@ xb_status xb_slot_wait(xb_ctx* ctx, int32_t slot, xb_stats* stats, xb_row_digest
 /* Frees every slot's device memory (all slots must be idle). */
 xb_status xb_slots_release(xb_ctx* ctx);
 
+/* ---- weighted: multi-source shortest paths ------------------------------ */
+/* Attaches int32 edge weights to a resident graph, one per column index
+ * (weights[e] belongs to col_indices[e]; an undirected edge carries its
+ * weight in both directions).  Host pointer. */
+xb_status xb_graph_set_weights(xb_graph* g, const int32_t* weights, int64_t m);
+/* Multi-source shortest-path distances: dist[v] (n floats) = the smallest
+ * float sum of weights over paths from any of the k sources to v, the
+ * semantics of Ligra's MultiSSSP in the reference's baselines
+ * (apps/ligra/apps/MultiSSSP.C): unreached vertices get FLT_MAX / 4, and every
+ * vertex -FLT_MAX / 4 when the distances still change after n rounds (a
+ * negative cycle -- in an undirected graph, any reachable negative weight).
+ * flags: XB_OUT_DEVICE (dist is a device pointer), XB_SOURCES_DEVICE.  Uses
+ * the context's workspace (a later xb_traverse rebuilds its state). */
+xb_status xb_multi_sssp(xb_ctx* ctx, const xb_graph* g, const int32_t* sources, int32_t k, float* dist,
+                        uint32_t flags, xb_stats* stats);
+
 /* ---- traversal without device allocation -------------------------------- */
 /* No counterpart in the reference (whose engine allocates all its device
  * buffers itself): an entry point for callers that may not allocate device

@@ -39,6 +39,7 @@
  * compiled from the reference sources by oracle/Makefile into oracle/_ref/)
  * through the fixtures in tests/golden/.
  */
+#include <float.h>
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
@@ -185,4 +186,71 @@ long long oracle_check_parents(int64_t n, const int64_t *ro, const int32_t *ci,
         if (!found) bad++;
     }
     return bad;
+}
+
+/* Multi-source single-shortest-path distances (one shared distance array,
+ * every source at distance 0), restating Ligra's MultiSSSP
+ * (apps/ligra/apps/MultiSSSP.C: SSSP_F, Reset_F and the round loop of
+ * Compute): rounds of relaxation of the frontier's edges with float
+ * distances dist[v] = min(dist[v], dist[u] + (float)w); a vertex whose
+ * distance dropped joins the next frontier; unreached vertices keep
+ * FLT_MAX / 4; if the frontier is still non-empty after n rounds (a negative
+ * cycle; in an undirected graph any negative edge) every distance becomes
+ * -FLT_MAX / 4.  Sequential; the fixed point -- the minimum over paths of the
+ * path's float sum taken from the source -- does not depend on the order.
+ * Returns 0, or -1 on a bad argument. */
+int oracle_msssp(int64_t n, const int64_t *row_offsets, const int32_t *col_indices, const int32_t *weights,
+                 const int32_t *sources, int32_t k, float *dist) {
+  if (n <= 0 || k <= 0 || !dist || !row_offsets) return -1;
+  for (int32_t q = 0; q < k; q++)
+    if (sources[q] < 0 || sources[q] >= n) return -1;
+  const float inf = FLT_MAX / 4;
+  int32_t *cur = (int32_t *)malloc(sizeof(int32_t) * (size_t)n);
+  int32_t *nxt = (int32_t *)malloc(sizeof(int32_t) * (size_t)n);
+  char *in_next = (char *)calloc((size_t)n, 1);
+  if (!cur || !nxt || !in_next) {
+    free(cur);
+    free(nxt);
+    free(in_next);
+    return -1;
+  }
+  for (int64_t v = 0; v < n; v++) dist[v] = inf;
+  int64_t nc = 0;
+  for (int32_t q = 0; q < k; q++)
+    if (dist[sources[q]] != 0.0f) {
+      dist[sources[q]] = 0.0f;
+      cur[nc++] = sources[q];
+    }
+  int64_t round = 0;
+  while (nc > 0) {
+    if (round == n) {
+      for (int64_t v = 0; v < n; v++) dist[v] = -inf;
+      break;
+    }
+    int64_t nn = 0;
+    for (int64_t i = 0; i < nc; i++) {
+      const int32_t u = cur[i];
+      for (int64_t e = row_offsets[u]; e < row_offsets[u + 1]; e++) {
+        const int32_t v = col_indices[e];
+        const float nd = dist[u] + (float)weights[e];
+        if (nd < dist[v]) {
+          dist[v] = nd;
+          if (!in_next[v]) {
+            in_next[v] = 1;
+            nxt[nn++] = v;
+          }
+        }
+      }
+    }
+    for (int64_t i = 0; i < nn; i++) in_next[nxt[i]] = 0;
+    int32_t *t = cur;
+    cur = nxt;
+    nxt = t;
+    nc = nn;
+    round++;
+  }
+  free(cur);
+  free(nxt);
+  free(in_next);
+  return 0;
 }

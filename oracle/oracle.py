@@ -19,6 +19,7 @@ ORACLE_SO = os.path.join(HERE, "liboracle_msbfs.so")
 REF_DIR = os.path.join(HERE, "_ref")
 LIGRA_SO = os.path.join(REF_DIR, "libligra_bfs_ref.so")
 XGRAPH_SO = os.path.join(REF_DIR, "libxgraph_fifo_ref.so")
+MSSSP_SO = os.path.join(REF_DIR, "libligra_msssp_ref.so")
 
 RULE_MINID = 0
 RULE_FIFO = 1
@@ -72,6 +73,24 @@ def msbfs(ro: np.ndarray, ci: np.ndarray, sources: np.ndarray, rule: int = RULE_
     return lvl, par, e.value, r.value
 
 
+def msssp(ro, ci, weights, sources) -> np.ndarray:
+    """Multi-source SSSP distances (float32, n) on the CPU: the restatement of
+    Ligra's MultiSSSP (one shared distance array, every source at 0)."""
+    ro = np.ascontiguousarray(ro, dtype=np.int64)
+    ci = np.ascontiguousarray(ci, dtype=np.int32)
+    w = np.ascontiguousarray(weights, dtype=np.int32)
+    src = np.ascontiguousarray(sources, dtype=np.int32)
+    dist = np.empty(len(ro) - 1, np.float32)
+    L = _load()
+    L.oracle_msssp.restype = C.c_int
+    L.oracle_msssp.argtypes = [C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]
+    rc = L.oracle_msssp(len(ro) - 1, ro.ctypes.data, ci.ctypes.data if len(ci) else None,
+                        w.ctypes.data if len(w) else None, src.ctypes.data, len(src), dist.ctypes.data)
+    if rc != 0:
+        raise ValueError("oracle_msssp rejected its arguments")
+    return dist
+
+
 def check_parents(ro, ci, s: int, level_row: np.ndarray, parent_row: np.ndarray) -> int:
     """Number of entries of parent_row that are not a valid BFS predecessor under level_row."""
     ro = np.ascontiguousarray(ro, dtype=np.int64)
@@ -90,6 +109,28 @@ def ligra_available() -> bool:
 
 def xgraph_available() -> bool:
     return os.path.exists(XGRAPH_SO)
+
+
+def ligra_msssp_available() -> bool:
+    return os.path.exists(MSSSP_SO)
+
+
+def ligra_msssp(ro, ci, weights, sources, threads: int = 1) -> np.ndarray:
+    """Reference Ligra MultiSSSP (apps/ligra/apps/MultiSSSP.C) distances."""
+    ro = np.ascontiguousarray(ro, dtype=np.int64)
+    ci = np.ascontiguousarray(ci, dtype=np.int32)
+    w = np.ascontiguousarray(weights, dtype=np.int32)
+    src = np.ascontiguousarray(sources, dtype=np.int32)
+    L = C.CDLL(MSSSP_SO)
+    L.ligra_ref_msssp.restype = C.c_int
+    L.ligra_ref_msssp.argtypes = [C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p,
+                                  C.c_int32]
+    dist = np.empty(len(ro) - 1, np.float32)
+    rc = L.ligra_ref_msssp(len(ro) - 1, ro.ctypes.data, ci.ctypes.data if len(ci) else None,
+                           w.ctypes.data if len(w) else None, src.ctypes.data, len(src), dist.ctypes.data, threads)
+    if rc != 0:
+        raise ValueError("ligra_ref_msssp rejected its arguments")
+    return dist
 
 
 def _ligra() -> C.CDLL:

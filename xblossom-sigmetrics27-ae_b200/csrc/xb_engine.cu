@@ -602,6 +602,7 @@ xb_status xb_graph_free(xb_graph* g) {
   if (g->d_hidx_of) cudaFree(g->d_hidx_of);
   if (g->d_lorder) cudaFree(g->d_lorder);
   if (g->d_lchunk) cudaFree(g->d_lchunk);
+  if (g->d_w) cudaFree(g->d_w);
   delete g;
   return XB_OK;
 }

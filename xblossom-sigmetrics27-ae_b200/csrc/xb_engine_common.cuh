@@ -92,6 +92,7 @@ struct xb_graph {
   int32_t n_heavy = 0;
   int32_t heavy_thr = -1;
   uint64_t version = 0;  // bumped whenever the heavy-vertex arrays are rebuilt
+  int32_t* d_w = nullptr;  // edge weights (xb_graph_set_weights), one per colIndices entry
 };
 
 namespace xbe {

@@ -163,6 +163,8 @@ def lib() -> C.CDLL:
         "xb_slot_poll": (i32, [vp, i32, P(i32), P(XbStats), vp]),
         "xb_slot_wait": (i32, [vp, i32, P(XbStats), vp]),
         "xb_slots_release": (i32, [vp]),
+        "xb_graph_set_weights": (i32, [vp, vp, i64]),
+        "xb_multi_sssp": (i32, [vp, vp, vp, i32, vp, u32, P(XbStats)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -306,6 +308,20 @@ def select_sources_csr(row_offsets: np.ndarray, seed: int, k: int) -> np.ndarray
     return out
 
 
+def symmetric_weights(row_offsets, col_indices, seed: int, wmin: int = 1, wmax: int = 100) -> np.ndarray:
+    """Seeded int32 edge weights in [wmin, wmax], one per column index, equal
+    for the two directions of an undirected edge (a hash of the unordered
+    pair), so a symmetric CSR stays a symmetric weighted graph."""
+    ro = np.ascontiguousarray(row_offsets, dtype=np.int64)
+    ci = np.ascontiguousarray(col_indices, dtype=np.int64)
+    if wmax < wmin:
+        raise ValueError("wmax < wmin")
+    u = np.repeat(np.arange(len(ro) - 1, dtype=np.int64), np.diff(ro))
+    a, b = np.minimum(u, ci), np.maximum(u, ci)
+    h = (a * 1000003 + b * 7919 + int(seed) % (1 << 31)) % (wmax - wmin + 1)
+    return (h + wmin).astype(np.int32)
+
+
 class Graph:
     """Device-resident CSR owned by a Context."""
 
@@ -320,6 +336,13 @@ class Graph:
         out = np.zeros(k, np.int32)
         _check(lib().xb_select_sources(self._h, seed, k, out.ctypes.data))
         return out
+
+    def set_weights(self, weights) -> None:
+        """Attaches int32 edge weights, one per column index (xb_graph_set_weights)."""
+        w = np.ascontiguousarray(weights, dtype=np.int32)
+        if w.shape != (self.m,):
+            raise ValueError(f"weights must have shape ({self.m},)")
+        _check(lib().xb_graph_set_weights(self._h, w.ctypes.data if len(w) else None, self.m))
 
     def close(self) -> None:
         if self._h and self._h.value:
@@ -454,6 +477,37 @@ class Context:
         _check(lib().xb_traverse(self._h, graph._h, sptr, k, XB_MODE_PLAIN, None, lp, pp, None, flags,
                                  C.byref(st)))
         return TraversalResult(level, parent, st.as_dict())
+
+    def multi_sssp(self, graph: Graph, sources, out: str = "host", dist=None) -> tuple[object, dict]:
+        """Multi-source shortest-path distances through xb_multi_sssp on a
+        graph with weights (Graph.set_weights): float32 (n,), FLT_MAX / 4 for
+        unreached vertices, all -FLT_MAX / 4 after a negative cycle.
+        out="host" gives numpy, out="device" a torch CUDA tensor."""
+        st = XbStats()
+        flags = 0
+        src_keep = sources
+        if hasattr(sources, "data_ptr"):
+            flags |= XB_SOURCES_DEVICE
+            k = int(sources.numel())
+            sptr = sources.data_ptr()
+        else:
+            src_keep = np.ascontiguousarray(sources, dtype=np.int32)
+            k = len(src_keep)
+            sptr = src_keep.ctypes.data
+        if out == "device":
+            import torch
+
+            flags |= XB_OUT_DEVICE
+            if dist is None:
+                dist = torch.empty(graph.n, dtype=torch.float32, device=torch.device("cuda", self.device))
+            torch.cuda.synchronize(dist.device)
+            dp = dist.data_ptr()
+        else:
+            if dist is None:
+                dist = np.empty(graph.n, np.float32)
+            dp = dist.ctypes.data
+        _check(lib().xb_multi_sssp(self._h, graph._h, sptr, k, dp, flags, C.byref(st)))
+        return dist, st.as_dict()
 
     def traverse_batched(self, queries, out: str = "device", outputs=None) -> tuple[list, dict]:
         """All queries in one launch through xb_traverse_batched.
