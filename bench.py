@@ -61,15 +61,19 @@ WORKLOADS = {
     "rmat20_k64": dict(kind="rmat", scale=20, ef=16, k=64),
     # one pass of the default layout (2 words x 64 sources) for kernel profiles
     "rmat20_k128": dict(kind="rmat", scale=20, ef=16, k=128),
+    # weighted: multi-source SSSP distances (xb_multi_sssp), seeded symmetric int32 weights in [1, 100]
+    "msssp_rmat22_k64": dict(kind="sssp", graph="rmat", scale=22, ef=16, k=64, wmin=1, wmax=100),
+    "msssp_rmat20_k64": dict(kind="sssp", graph="rmat", scale=20, ef=16, k=64, wmin=1, wmax=100),
 }
 SEED = 0x5EED
 METRIC = "multi-source GTEPS at 1 B200, batched vs plain; p50/p99 query latency"
+SSSP_METRIC = "multi-source SSSP GTEPS (directed edges of the graph / time of one call)"
 
 
 def make_graph(w: dict):
     import xbtrav
 
-    if w["kind"] == "rmat":
+    if w["kind"] == "rmat" or w.get("graph") == "rmat":
         return xbtrav.HostCSR.rmat(w["scale"], w["ef"], 0.57, 0.19, 0.19, seed=SEED)
     return xbtrav.HostCSR.er(w["n"], w["pairs"], seed=SEED)
 
@@ -77,7 +81,7 @@ def make_graph(w: dict):
 def workload_config(name: str, w: dict, info: dict) -> dict:
     cfg = {"workload": name, "n": info["n"], "m_directed": info["m"], "sources": w["k"], "seed": SEED,
            "l2": "inputs larger than L2 (colIndices > 126 MB); no flush"}
-    if w["kind"] == "rmat":
+    if w["kind"] == "rmat" or w.get("graph") == "rmat":
         cfg.update(graph=f"rmat scale {w['scale']} ef {w['ef']} a/b/c/d .57/.19/.19/.05")
     else:
         cfg.update(graph=f"uniform n {w['n']} pairs {w['pairs']}")
@@ -182,9 +186,144 @@ def cpu_baseline_port(ro, ci, sources, budget_s: float = 15.0) -> dict:
             "sample": f"{len(sample)} of the workload's sources, levels + min-id parents, {dt:.1f} s"}
 
 
+def sssp_weights(ro, ci, w):
+    import xbtrav
+
+    return xbtrav.symmetric_weights(ro, ci, SEED, w["wmin"], w["wmax"])
+
+
+def sssp_cpu(ro, ci, wts, sources, cores):
+    """One multi-source SSSP call on the host: the reference's Ligra MultiSSSP
+    (oracle/_ref) on all cores, else the C restatement (one core)."""
+    from oracle import oracle
+
+    t0 = time.perf_counter()
+    if oracle.ligra_msssp_available():
+        oracle.ligra_msssp(ro, ci, wts, sources, threads=cores)
+        kind, used, what = "reference", cores, "Ligra MultiSSSP from the reference sources (oracle/_ref)"
+    else:
+        oracle.msssp(ro, ci, wts, sources)
+        kind, used, what = "port", 1, "C restatement (oracle/)"
+    return time.perf_counter() - t0, kind, used, what
+
+
+def run_reference_sssp(args, w, name) -> None:
+    csr = make_graph(w)
+    ro, ci = csr.arrays()
+    info = csr.info()
+    import xbtrav
+
+    wts = sssp_weights(ro, ci, w)
+    sources = xbtrav.select_sources_csr(ro, SEED + 1, w["k"])
+    cores = os.cpu_count() or 1
+    times = []
+    for step in range(args.warmup + args.steps):
+        secs, kind, used, what = sssp_cpu(ro, ci, wts, sources, cores)
+        if step >= args.warmup:
+            times.append(secs)
+    value = info["m"] / (sum(times) / len(times)) / 1e9
+    cfg = workload_config(name, w, info)
+    cfg.update(weights=f"symmetric int32 in [{w['wmin']}, {w['wmax']}]")
+    print(json.dumps({
+        "impl": "reference", "metric": SSSP_METRIC, "value": value, "unit": "GTEPS", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * sum(times) / len(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded generator)", "config": cfg,
+        "cpu_baseline": {"value": value, "unit": "GTEPS", "cores": used, "kind": kind,
+                         "sample": f"the whole workload ({w['k']} sources) per step, {what}"},
+        "e2e": {"value": value, "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def run_sssp(args, w, name) -> None:
+    """Multi-source SSSP (xb_multi_sssp) on one weighted resident graph: one
+    step = one call over the workload's sources producing the float distance
+    array in HBM."""
+    import torch
+
+    import xbtrav
+
+    dev = torch.device("cuda", 0)
+    t0 = time.perf_counter()
+    csr = make_graph(w)
+    ro, ci = csr.arrays()
+    info = csr.info()
+    wts = sssp_weights(ro, ci, w)
+    ctx = xbtrav.Context(0)
+    g = ctx.upload(csr)
+    g.set_weights(wts)
+    sources = g.select_sources(SEED + 1, w["k"])
+    src_dev = torch.from_numpy(sources).to(dev)
+    dist_dev = torch.empty(g.n, dtype=torch.float32, device=dev)
+    stream = torch.cuda.ExternalStream(ctx.stream_handle(), device=dev)
+    setup_s = time.perf_counter() - t0
+
+    def timed(fn, steps):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize(dev)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        stats = [fn() for _ in range(steps)]
+        ev1.record(stream)
+        torch.cuda.synchronize(dev)
+        return ev0.elapsed_time(ev1), stats
+
+    clocks = ClockSampler(0)
+    clocks.start()
+    ms, stats = timed(lambda: ctx.multi_sssp(g, src_dev, out="device", dist=dist_dev)[1], args.steps)
+    clk = clocks.stop()
+    value = g.m * args.steps / (ms / 1e3) / 1e9
+    relaxed = sum(st["edges_scanned"] for st in stats) / args.steps
+    # the relax kernel alone (per-launch CUDA events on the engine's stream)
+    ctx.set_tuning(timing=1)
+    _, tstats = timed(lambda: ctx.multi_sssp(g, src_dev, out="device", dist=dist_dev)[1], args.steps)
+    ctx.set_tuning(timing=0)
+    relax_ms = sum(st["class_ms"][0] for st in tstats)
+    relax_bytes = sum(st["class_bytes"][0] for st in tstats)
+    relax_launches = sum(st["class_launches"][0] for st in tstats)
+    peak, peak_src = measured_peaks()
+    achieved = relax_bytes / (relax_ms / 1e3) / 1e9 if relax_ms > 0 else None
+    launches = sum(sum(st["class_launches"]) for st in stats)
+    # end to end through the host-buffer call: sources in, distances out
+    host_dist = np.empty(g.n, np.float32)
+    e2e_ms, _ = timed(lambda: ctx.multi_sssp(g, sources, out="host", dist=host_dist)[1], args.steps)
+    cpu = None
+    if not args.no_cpu_baseline:
+        cores = os.cpu_count() or 1
+        secs, kind, used, what = sssp_cpu(ro, ci, wts, sources, cores)
+        cpu = {"value": g.m / secs / 1e9, "unit": "GTEPS", "cores": used, "kind": kind,
+               "sample": f"one call over all {w['k']} sources ({secs:.2f} s), {what}"}
+    cfg = workload_config(name, w, info)
+    cfg.update(weights=f"symmetric int32 in [{w['wmin']}, {w['wmax']}]", parallelism="replicas1",
+               path="xb_multi_sssp (edge-balanced rounds, host loop over rounds)")
+    line = {
+        "metric": SSSP_METRIC, "value": value, "unit": "GTEPS", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded R-MAT generator, seeded weights)",
+        "config": cfg,
+        "relaxations_per_step": relaxed, "grelax_per_s": relaxed * args.steps / (ms / 1e3) / 1e9,
+        "rounds": stats[-1]["levels"],
+        "roofline": {"bound": "hbm", "kernel": "k_sssp_relax", "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak if achieved else None, "peak_source": peak_src,
+                     "traffic": None, "bytes_model": "8 B per relaxation (column index + weight)",
+                     "relax_ms_per_step": relax_ms / args.steps, "relax_launches_per_step": relax_launches / args.steps},
+        "cpu_baseline": cpu,
+        "e2e": {"value": g.m * args.steps / (e2e_ms / 1e3) / 1e9, "unit": "GTEPS",
+                "h2d_bytes_per_step": 4 * len(sources), "d2h_bytes_per_step": 4 * g.n},
+        "clocks": clk, "gpu_launches": launches, "setup_s": setup_s,
+    }
+    print(json.dumps(line), flush=True)
+    g.close()
+    ctx.close()
+
+
 def run_reference(args, w, name) -> None:
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
+        return
+    if w["kind"] == "sssp":
+        run_reference_sssp(args, w, name)
         return
     from oracle import oracle
 
@@ -392,6 +531,9 @@ def main() -> None:
         return
     if w["kind"] == "serve":
         run_serve(args, w, args.workload)
+        return
+    if w["kind"] == "sssp":
+        run_sssp(args, w, args.workload)
         return
 
     import torch

@@ -181,17 +181,18 @@ __global__ void __launch_bounds__(kThreads) k_lb_offsets(const int32_t* __restri
 // frontier vertices gather in the warp's buffer and go out with one atomic
 // per flush.
 template <typename OffT>
-__global__ void __launch_bounds__(32 * kRelaxWarps) k_sssp_relax(
+__global__ void __launch_bounds__(32 * kRelaxWarps, 10) k_sssp_relax(
     const int32_t* __restrict__ list, const int32_t* __restrict__ count, const int64_t* __restrict__ eoff,
     const int64_t* __restrict__ ebase, const int32_t* __restrict__ chunk_first, const int64_t* __restrict__ edges_p,
     const int64_t* __restrict__ nchunks_p, const int32_t* __restrict__ ci, const int32_t* __restrict__ w,
     int32_t* dkey, int32_t* claim, int32_t* next, int32_t* next_count, int32_t* next_zero) {
-  __shared__ int64_t s_base_all[kRelaxWarps][kChunk + 1];  // spanned vertex: column-index position minus eoff
+  // spanned vertex: column-index position minus eoff (fits OffT: both lie in [0, m])
+  __shared__ OffT s_base_all[kRelaxWarps][kChunk + 1];
   __shared__ float s_du_all[kRelaxWarps][kChunk + 1];      // spanned vertex: its distance
   __shared__ uint32_t s_mask_all[kRelaxWarps][kItems];     // bit e: a spanned vertex starts at chunk edge e
   __shared__ int32_t s_app_all[kRelaxWarps][kAppCap];      // vertices for the next frontier
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  int64_t* s_base = s_base_all[wib];
+  OffT* s_base = s_base_all[wib];
   float* s_du = s_du_all[wib];
   uint32_t* s_mask = s_mask_all[wib];
   int32_t* s_app = s_app_all[wib];
@@ -213,7 +214,7 @@ __global__ void __launch_bounds__(32 * kRelaxWarps) k_sssp_relax(
     for (int32_t j = lane; j < nv; j += 32) {
       const int32_t u = list[vlo + j];
       const int64_t rel = __ldcs(&eoff[vlo + j]) - E0;
-      s_base[j] = __ldcs(&ebase[vlo + j]);
+      s_base[j] = (OffT)__ldcs(&ebase[vlo + j]);
       s_du[j] = key_float(__ldcg(&dkey[u]));
       if (j == 0) rel0 = (int32_t)max(rel, (int64_t)-1);
       if (rel >= 0 && rel < kChunk) atomicOr(&s_mask[rel >> 5], 1u << (rel & 31));
@@ -232,7 +233,7 @@ __global__ void __launch_bounds__(32 * kRelaxWarps) k_sssp_relax(
       idx[it] = -1;
       du[it] = 0.f;
       if (e < len) {
-        idx[it] = s_base[j] + E0 + e;
+        idx[it] = (int64_t)s_base[j] + E0 + e;
         du[it] = s_du[j];
       }
     }
@@ -334,9 +335,14 @@ xb_status run_sssp(xb_ctx* c, xb_graph* g, const int32_t* d_src, int32_t k, floa
   XB_CUDA(cudaMemcpyAsync(h_cnt, wk.cnt, 4 * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
   XB_CUDA(cudaStreamSynchronize(s));
   int32_t fcount = h_cnt[0], zero = h_cnt[2];
-  int64_t launches = 2, rounds = 0;
+  int64_t rounds = 0;
   int cur = 0, negative = 0;
-  const int relax_grid = sms * 8;  // resident blocks (4 warps, 21 KB of tables each)
+  // classes: 0 = relax rounds, 1 = frontier partition (scan, offsets, unclaim), 2 = init and output
+  xbe::ClassTimer timer{c, st, c->tuning.timing != 0};
+  if (st) st->class_launches[2] += 2;
+  int relax_per_sm = 0;  // resident blocks of 4 warps (about 20 KB of tables each)
+  XB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&relax_per_sm, k_sssp_relax<OffT>, 32 * kRelaxWarps, 0));
+  const int relax_grid = sms * std::max(relax_per_sm, 1);
   while (fcount > 0 || zero > 0) {
     if (rounds == n) {  // still changing after n rounds: a negative cycle
       negative = 1;
@@ -347,17 +353,21 @@ xb_status run_sssp(xb_ctx* c, xb_graph* g, const int32_t* d_src, int32_t k, floa
     const int32_t ntiles = (fcount + kTile - 1) / kTile;
     XB_CUDA(cudaMemsetAsync(wk.cnt + (cur ^ 1), 0, sizeof(int32_t), s));
     XB_CUDA(cudaMemsetAsync(wk.cnt + 2, 0, sizeof(int32_t), s));
+    timer.begin();
     k_lb_tile_sums<OffT><<<ntiles, kThreads, 0, s>>>(wk.list[cur], fcount, ro, wk.tsum);
     k_lb_tile_scan<<<1, 1024, 0, s>>>(wk.tsum, ntiles, wk.scal, wk.scal + 1, wk.relaxed);
     k_lb_offsets<OffT><<<ntiles, kThreads, 0, s>>>(wk.list[cur], fcount, ro, wk.tsum, wk.eoff, wk.ebase,
                                                    wk.chunk_first);
+    timer.end(1, 3);
+    timer.begin();
     k_sssp_relax<OffT><<<relax_grid, 32 * kRelaxWarps, 0, s>>>(wk.list[cur], wk.cnt + cur, wk.eoff, wk.ebase,
                                                                wk.chunk_first, wk.scal, wk.scal + 1, g->d_ci,
                                                                g->d_w, wk.dkey, wk.claim, wk.list[cur ^ 1],
                                                                wk.cnt + (cur ^ 1), wk.cnt + 2);
+    timer.end(0, 1);
     k_sssp_unclaim<<<vgrid, 256, 0, s>>>(wk.list[cur ^ 1], wk.cnt + (cur ^ 1), wk.claim);
     XB_LAUNCH_CHECK("sssp round");
-    launches += 5;
+    if (st) st->class_launches[1] += 1;
     XB_CUDA(cudaMemcpyAsync(h_cnt, wk.cnt, 4 * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
     XB_CUDA(cudaStreamSynchronize(s));
     cur ^= 1;
@@ -368,7 +378,7 @@ xb_status run_sssp(xb_ctx* c, xb_graph* g, const int32_t* d_src, int32_t k, floa
   if (!out_dev) out = (float*)c->d_stage;  // sized by the caller
   k_sssp_out<<<vgrid, 256, 0, s>>>(wk.dkey, n, out, negative);
   XB_LAUNCH_CHECK("sssp out");
-  launches++;
+  if (st) st->class_launches[2] += 1;
   if (!out_dev) XB_CUDA(cudaMemcpyAsync(dist, out, sizeof(float) * (size_t)n, cudaMemcpyDeviceToHost, s));
   unsigned long long relaxed = 0;
   XB_CUDA(cudaMemcpyAsync(&relaxed, wk.relaxed, sizeof(relaxed), cudaMemcpyDeviceToHost, s));
@@ -376,7 +386,10 @@ xb_status run_sssp(xb_ctx* c, xb_graph* g, const int32_t* d_src, int32_t k, floa
   if (st) {
     st->edges_scanned = (int64_t)relaxed;
     st->levels = (int32_t)rounds;
-    st->class_launches[0] = launches;
+    // algorithmic bytes of the relax rounds: a column index and a weight per relaxation
+    // (the distance array is read at random but stays in L2 up to about 2^24 vertices)
+    st->class_bytes[0] = (int64_t)relaxed * 8;
+    st->algo_bytes = st->class_bytes[0];
   }
   return XB_OK;
 }
