@@ -254,3 +254,132 @@ int oracle_msssp(int64_t n, const int64_t *row_offsets, const int32_t *col_indic
   free(in_next);
   return 0;
 }
+
+/* Maximum-cardinality matching in a general graph: Edmonds' blossom
+ * algorithm (J. Edmonds, "Paths, trees, and flowers", Canad. J. Math. 17,
+ * 1965), restated as the checker of the matching path.  The reference's
+ * engines (apps/xb/src/xblsm_cpu/par_pro_pernode.cu:42-90, the GPU engine
+ * apps/xb/src/xblsm_gpu/xblossom_gpu_engine_10.cu:72-80) compute a maximum
+ * matching of the same graph; matchings are not unique, so the checks are
+ * validity and size.
+ *
+ * One alternating tree per exposed root, grown breadth first; a blossom is
+ * an edge between two outer vertices of the tree, contracted by pointing the
+ * base of every vertex on its cycle to the cycle's top and making its inner
+ * vertices outer; `pred` is rerouted along the cycle so an augmenting path
+ * can be read back through blossoms.  Exposed roots are tried once each: an
+ * exposed vertex without an augmenting path keeps none after augmentations
+ * elsewhere.  mate: n ints in/out (-1 exposed).  Returns the matching size
+ * or -1 on a bad argument. */
+struct mm_state {
+  int64_t n;
+  const int64_t *ro;
+  const int32_t *ci;
+  int32_t *mate, *base, *pred, *queue, *stamp;
+  char *outer, *cyc;
+  int32_t tick;
+};
+
+static int32_t mm_top(struct mm_state *S, int32_t a, int32_t b) {
+  S->tick++;
+  for (;;) { /* up from a to the root, stamping the bases */
+    a = S->base[a];
+    S->stamp[a] = S->tick;
+    if (S->mate[a] < 0) break;
+    a = S->pred[S->mate[a]];
+  }
+  for (;;) { /* up from b to the first stamped base */
+    b = S->base[b];
+    if (S->stamp[b] == S->tick) return b;
+    b = S->pred[S->mate[b]];
+  }
+}
+
+static void mm_cycle_side(struct mm_state *S, int32_t v, int32_t top, int32_t across) {
+  while (S->base[v] != top) {
+    const int32_t m = S->mate[v];
+    S->cyc[S->base[v]] = 1;
+    S->cyc[S->base[m]] = 1;
+    S->pred[v] = across;  /* leave v through the cycle edge instead */
+    across = m;
+    v = S->pred[m];
+  }
+}
+
+static int32_t mm_search(struct mm_state *S, int32_t root) {
+  const int64_t n = S->n;
+  for (int64_t v = 0; v < n; v++) {
+    S->base[v] = (int32_t)v;
+    S->pred[v] = -1;
+    S->outer[v] = 0;
+  }
+  int64_t qh = 0, qt = 0;
+  S->outer[root] = 1;
+  S->queue[qt++] = root;
+  while (qh < qt) {
+    const int32_t v = S->queue[qh++];
+    for (int64_t e = S->ro[v]; e < S->ro[v + 1]; e++) {
+      const int32_t w = S->ci[e];
+      if (S->base[v] == S->base[w] || S->mate[v] == w) continue;
+      const int w_outer = w == root || (S->mate[w] >= 0 && S->pred[S->mate[w]] >= 0);
+      if (w_outer) {
+        const int32_t top = mm_top(S, v, w);
+        memset(S->cyc, 0, (size_t)n);
+        mm_cycle_side(S, v, top, w);
+        mm_cycle_side(S, w, top, v);
+        for (int64_t x = 0; x < n; x++) {
+          if (!S->cyc[S->base[x]]) continue;
+          S->base[x] = top;
+          if (!S->outer[x]) {
+            S->outer[x] = 1;
+            S->queue[qt++] = (int32_t)x;
+          }
+        }
+      } else if (S->pred[w] < 0) {
+        S->pred[w] = v;
+        if (S->mate[w] < 0) return w;
+        S->outer[S->mate[w]] = 1;
+        S->queue[qt++] = S->mate[w];
+      }
+    }
+  }
+  return -1;
+}
+
+int64_t oracle_max_match(int64_t n, const int64_t *row_offsets, const int32_t *col_indices, int32_t *mate) {
+  if (n <= 0 || n > INT32_MAX || !row_offsets || !mate) return -1;
+  for (int64_t v = 0; v < n; v++) {
+    const int32_t m = mate[v];
+    if (m < -1 || m >= n || (m >= 0 && mate[m] != v)) return -1;
+  }
+  struct mm_state S;
+  S.n = n;
+  S.ro = row_offsets;
+  S.ci = col_indices;
+  S.mate = mate;
+  S.base = (int32_t *)malloc(sizeof(int32_t) * (size_t)n);
+  S.pred = (int32_t *)malloc(sizeof(int32_t) * (size_t)n);
+  S.queue = (int32_t *)malloc(sizeof(int32_t) * (size_t)n);
+  S.stamp = (int32_t *)calloc((size_t)n, sizeof(int32_t));
+  S.outer = (char *)malloc((size_t)n);
+  S.cyc = (char *)malloc((size_t)n);
+  S.tick = 0;
+  if (!S.base || !S.pred || !S.queue || !S.stamp || !S.outer || !S.cyc) {
+    free(S.base); free(S.pred); free(S.queue); free(S.stamp); free(S.outer); free(S.cyc);
+    return -1;
+  }
+  for (int64_t r = 0; r < n; r++) {
+    if (mate[r] >= 0) continue;
+    int32_t u = mm_search(&S, (int32_t)r);
+    while (u >= 0) { /* flip the path from u back to r */
+      const int32_t p = S.pred[u], next = mate[p];
+      mate[u] = p;
+      mate[p] = u;
+      u = next;
+    }
+  }
+  int64_t size = 0;
+  for (int64_t v = 0; v < n; v++) size += mate[v] >= 0;
+  free(S.base); free(S.pred); free(S.queue); free(S.stamp); free(S.outer); free(S.cyc);
+  return size / 2;
+}

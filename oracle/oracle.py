@@ -20,6 +20,7 @@ REF_DIR = os.path.join(HERE, "_ref")
 LIGRA_SO = os.path.join(REF_DIR, "libligra_bfs_ref.so")
 XGRAPH_SO = os.path.join(REF_DIR, "libxgraph_fifo_ref.so")
 MSSSP_SO = os.path.join(REF_DIR, "libligra_msssp_ref.so")
+MATCH_SO = os.path.join(REF_DIR, "libxb_match_ref.so")
 
 RULE_MINID = 0
 RULE_FIFO = 1
@@ -109,6 +110,62 @@ def ligra_available() -> bool:
 
 def xgraph_available() -> bool:
     return os.path.exists(XGRAPH_SO)
+
+
+def max_match(ro, ci, init=None) -> tuple[int, np.ndarray]:
+    """Maximum-cardinality matching (Edmonds' blossom algorithm restated in
+    C): (size, mate) with mate[v] = -1 for exposed vertices.  init: an
+    optional starting matching (mate array)."""
+    ro = np.ascontiguousarray(ro, dtype=np.int64)
+    ci = np.ascontiguousarray(ci, dtype=np.int32)
+    n = len(ro) - 1
+    mate = np.full(n, -1, np.int32) if init is None else np.array(init, dtype=np.int32, copy=True)
+    L = _load()
+    L.oracle_max_match.restype = C.c_int64
+    L.oracle_max_match.argtypes = [C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p]
+    size = L.oracle_max_match(n, ro.ctypes.data, ci.ctypes.data if len(ci) else None, mate.ctypes.data)
+    if size < 0:
+        raise ValueError("oracle_max_match rejected its arguments")
+    return int(size), mate
+
+
+def ref_match_available() -> bool:
+    return os.path.exists(MATCH_SO)
+
+
+def ref_max_match(ro, ci, threads: int = 1, init=None) -> tuple[int, np.ndarray]:
+    """The reference's own CPU maximum-matching engine
+    (apps/xb/src/xblsm_cpu/par_pro_pernode.cu) built into oracle/_ref."""
+    ro = np.ascontiguousarray(ro, dtype=np.int64)
+    ci = np.ascontiguousarray(ci, dtype=np.int32)
+    n = len(ro) - 1
+    mate = np.full(n, -1, np.int32) if init is None else np.array(init, dtype=np.int32, copy=True)
+    L = C.CDLL(MATCH_SO)
+    L.xb_ref_max_match.restype = C.c_int64
+    L.xb_ref_max_match.argtypes = [C.c_int64, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]
+    size = L.xb_ref_max_match(n, ro.ctypes.data, ci.ctypes.data if len(ci) else None, threads, mate.ctypes.data)
+    if size < 0:
+        raise ValueError("xb_ref_max_match failed")
+    return int(size), mate
+
+
+def check_matching(ro, ci, mate) -> int:
+    """Number of violations: mate not symmetric, or a matched pair that is not an edge."""
+    ro = np.asarray(ro, dtype=np.int64)
+    ci = np.asarray(ci, dtype=np.int32)
+    mate = np.asarray(mate)
+    n = len(ro) - 1
+    bad = 0
+    for v in np.nonzero(mate >= 0)[0]:
+        m = int(mate[v])
+        if m >= n or mate[m] != v or m == v:
+            bad += 1
+            continue
+        adj = ci[ro[v]:ro[v + 1]]
+        i = np.searchsorted(adj, m)
+        if i >= len(adj) or adj[i] != m:
+            bad += 1
+    return bad
 
 
 def ligra_msssp_available() -> bool:
