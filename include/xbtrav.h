@@ -285,6 +285,24 @@ xb_status xb_graph_set_weights(xb_graph* g, const int32_t* weights, int64_t m);
 xb_status xb_multi_sssp(xb_ctx* ctx, const xb_graph* g, const int32_t* sources, int32_t k, float* dist,
                         uint32_t flags, xb_stats* stats);
 
+/* ---- alternating mode: maximum matching --------------------------------- */
+/* Maximum-cardinality matching of a resident graph (undirected: symmetric
+ * CSR), replacing the reference's FindMaximumMatch(const Matching&)
+ * (apps/xb/src/include/xbsm_gpu/max_match_engine.h:93-113, engine
+ * apps/xb/src/xblsm_gpu/xblossom_gpu_engine_10.cu:72-80): repeated forest
+ * searches from all exposed vertices, augmenting along vertex-disjoint
+ * paths, blossoms contracted, until a search finds no augmenting path.
+ * mate: n ints, in = the initial matching (-1 = exposed; the reference's
+ * engines use nnodes as that value), out = a maximum matching.  Host
+ * pointer, or device pointer with XB_OUT_DEVICE.  An initial mate array
+ * that is not a matching of the graph gives XB_ERR_ARG.  stats: batches =
+ * search phases, levels = forest levels, pull_levels = levels that
+ * contracted blossoms, vertices_scanned = augmenting paths flipped,
+ * edges_scanned = adjacency entries expanded, reached = matching size (host
+ * mate only).  Graphs of up to 2^29 - 1 vertices; uses the context's
+ * workspace (a later xb_traverse rebuilds its state). */
+xb_status xb_max_match(xb_ctx* ctx, const xb_graph* g, int32_t* mate, uint32_t flags, xb_stats* stats);
+
 /* ---- traversal without device allocation -------------------------------- */
 /* No counterpart in the reference (whose engine allocates all its device
  * buffers itself): an entry point for callers that may not allocate device

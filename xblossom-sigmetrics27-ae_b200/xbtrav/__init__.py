@@ -165,6 +165,7 @@ def lib() -> C.CDLL:
         "xb_slots_release": (i32, [vp]),
         "xb_graph_set_weights": (i32, [vp, vp, i64]),
         "xb_multi_sssp": (i32, [vp, vp, vp, i32, vp, u32, P(XbStats)]),
+        "xb_max_match": (i32, [vp, vp, vp, u32, P(XbStats)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -508,6 +509,32 @@ class Context:
             dp = dist.ctypes.data
         _check(lib().xb_multi_sssp(self._h, graph._h, sptr, k, dp, flags, C.byref(st)))
         return dist, st.as_dict()
+
+    def max_match(self, graph: Graph, init=None, out: str = "host") -> tuple[object, dict]:
+        """Maximum-cardinality matching through xb_max_match: (mate, stats),
+        mate[v] = -1 for exposed vertices.  init: starting matching (numpy
+        or a torch int32 CUDA tensor, -1 exposed), empty when None.  A torch
+        tensor is updated in place; out="device" returns a torch tensor."""
+        st = XbStats()
+        if hasattr(init, "data_ptr"):
+            import torch
+
+            torch.cuda.synchronize(init.device)
+            _check(lib().xb_max_match(self._h, graph._h, init.data_ptr(), XB_OUT_DEVICE, C.byref(st)))
+            return init, st.as_dict()
+        mate = (np.full(graph.n, -1, np.int32) if init is None
+                else np.array(init, dtype=np.int32, copy=True))
+        if mate.shape != (graph.n,):
+            raise ValueError(f"init must have shape ({graph.n},)")
+        if out == "device":
+            import torch
+
+            t = torch.from_numpy(mate).to(torch.device("cuda", self.device))
+            torch.cuda.synchronize(t.device)
+            _check(lib().xb_max_match(self._h, graph._h, t.data_ptr(), XB_OUT_DEVICE, C.byref(st)))
+            return t, st.as_dict()
+        _check(lib().xb_max_match(self._h, graph._h, mate.ctypes.data, 0, C.byref(st)))
+        return mate, st.as_dict()
 
     def traverse_batched(self, queries, out: str = "device", outputs=None) -> tuple[list, dict]:
         """All queries in one launch through xb_traverse_batched.
