@@ -64,10 +64,14 @@ WORKLOADS = {
     # weighted: multi-source SSSP distances (xb_multi_sssp), seeded symmetric int32 weights in [1, 100]
     "msssp_rmat22_k64": dict(kind="sssp", graph="rmat", scale=22, ef=16, k=64, wmin=1, wmax=100),
     "msssp_rmat20_k64": dict(kind="sssp", graph="rmat", scale=20, ef=16, k=64, wmin=1, wmax=100),
+    # alternating mode: maximum matching from the empty matching (xb_max_match)
+    "match_rmat22": dict(kind="match", graph="rmat", scale=22, ef=16, k=0),
+    "match_rmat20": dict(kind="match", graph="rmat", scale=20, ef=16, k=0),
 }
 SEED = 0x5EED
 METRIC = "multi-source GTEPS at 1 B200, batched vs plain; p50/p99 query latency"
 SSSP_METRIC = "multi-source SSSP GTEPS (directed edges of the graph / time of one call)"
+MATCH_METRIC = "maximum matching GTEPS (directed edges of the graph / time of one FindMaximumMatch)"
 
 
 def make_graph(w: dict):
@@ -318,12 +322,131 @@ def run_sssp(args, w, name) -> None:
     ctx.close()
 
 
+def match_cpu(ro, ci, cores):
+    """One maximum matching on the host: the reference's own CPU engine
+    (oracle/_ref) on all cores, else the Edmonds restatement (one core)."""
+    from oracle import oracle
+
+    t0 = time.perf_counter()
+    if oracle.ref_match_available():
+        size, _ = oracle.ref_max_match(ro, ci, threads=cores)
+        kind, used, what = "reference", cores, "X-Blossom CPU engine par_pro_pernode from the reference sources (oracle/_ref)"
+    else:
+        size, _ = oracle.max_match(ro, ci)
+        kind, used, what = "port", 1, "Edmonds restatement (oracle/)"
+    return time.perf_counter() - t0, size, kind, used, what
+
+
+def run_reference_match(args, w, name) -> None:
+    csr = make_graph(w)
+    ro, ci = csr.arrays()
+    info = csr.info()
+    cores = os.cpu_count() or 1
+    times = []
+    for step in range(args.warmup + args.steps):
+        secs, size, kind, used, what = match_cpu(ro, ci, cores)
+        if step >= args.warmup:
+            times.append(secs)
+    value = info["m"] / (sum(times) / len(times)) / 1e9
+    print(json.dumps({
+        "impl": "reference", "metric": MATCH_METRIC, "value": value, "unit": "GTEPS", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * sum(times) / len(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+        "data": "synthetic (seeded generator)", "config": workload_config(name, w, info), "matching_size": size,
+        "cpu_baseline": {"value": value, "unit": "GTEPS", "cores": used, "kind": kind,
+                         "sample": f"the whole workload (one maximum matching from the empty one) per step, {what}"},
+        "e2e": {"value": value, "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def run_match(args, w, name) -> None:
+    """Alternating mode: one step = a maximum matching of the resident graph
+    from the empty matching (xb_max_match), mate array in HBM."""
+    import torch
+
+    import xbtrav
+
+    dev = torch.device("cuda", 0)
+    t0 = time.perf_counter()
+    csr = make_graph(w)
+    ro, ci = csr.arrays()
+    info = csr.info()
+    ctx = xbtrav.Context(0)
+    g = ctx.upload(csr)
+    empty = torch.full((g.n,), -1, dtype=torch.int32, device=dev)
+    mate = torch.empty_like(empty)
+    stream = torch.cuda.ExternalStream(ctx.stream_handle(), device=dev)
+    setup_s = time.perf_counter() - t0
+
+    def step():
+        mate.copy_(empty)
+        return ctx.max_match(g, init=mate)[1]
+
+    def timed(fn, steps):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize(dev)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        stats = [fn() for _ in range(steps)]
+        ev1.record(stream)
+        torch.cuda.synchronize(dev)
+        return ev0.elapsed_time(ev1), stats
+
+    clocks = ClockSampler(0)
+    clocks.start()
+    ms, stats = timed(step, args.steps)
+    clk = clocks.stop()
+    size = int((mate >= 0).sum().item()) // 2
+    value = g.m * args.steps / (ms / 1e3) / 1e9
+    ctx.set_tuning(timing=1)
+    _, tstats = timed(step, args.steps)
+    ctx.set_tuning(timing=0)
+    exp_ms = sum(st["class_ms"][0] for st in tstats)
+    exp_bytes = sum(st["class_bytes"][0] for st in tstats)
+    peak, peak_src = measured_peaks()
+    achieved = exp_bytes / (exp_ms / 1e3) / 1e9 if exp_ms > 0 else None
+    launches = sum(sum(st["class_launches"]) for st in stats)
+    host_mate = np.full(g.n, -1, np.int32)
+    e2e_ms, _ = timed(lambda: ctx.max_match(g, init=host_mate)[1], args.steps)
+    cpu = None
+    if not args.no_cpu_baseline:
+        secs, rsize, kind, used, what = match_cpu(ro, ci, os.cpu_count() or 1)
+        cpu = {"value": g.m / secs / 1e9, "unit": "GTEPS", "cores": used, "kind": kind,
+               "sample": f"one maximum matching ({secs:.2f} s, size {rsize}), {what}"}
+    cfg = workload_config(name, w, info)
+    cfg.update(parallelism="replicas1", path="xb_max_match from the empty matching (host loop over phases and levels)")
+    cfg.pop("sources", None)
+    last = stats[-1]
+    print(json.dumps({
+        "metric": MATCH_METRIC, "value": value, "unit": "GTEPS", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded R-MAT generator)", "config": cfg,
+        "matching_size": size, "phases": last["batches"], "levels": last["levels"],
+        "blossom_levels": last["pull_levels"], "augmentations": last["vertices_scanned"],
+        "entries_scanned": last["edges_scanned"],
+        "roofline": {"bound": "hbm", "kernel": "k_mm_expand", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak if achieved else None, "peak_source": peak_src, "traffic": None,
+                     "bytes_model": "8 B per scanned adjacency entry (column index + neighbour state)",
+                     "expand_ms_per_step": exp_ms / args.steps},
+        "cpu_baseline": cpu,
+        "e2e": {"value": g.m * args.steps / (e2e_ms / 1e3) / 1e9, "unit": "GTEPS",
+                "h2d_bytes_per_step": 4 * g.n, "d2h_bytes_per_step": 4 * g.n},
+        "clocks": clk, "gpu_launches": launches, "setup_s": setup_s,
+    }), flush=True)
+    g.close()
+    ctx.close()
+
+
 def run_reference(args, w, name) -> None:
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     if w["kind"] == "sssp":
         run_reference_sssp(args, w, name)
+        return
+    if w["kind"] == "match":
+        run_reference_match(args, w, name)
         return
     from oracle import oracle
 
@@ -534,6 +657,9 @@ def main() -> None:
         return
     if w["kind"] == "sssp":
         run_sssp(args, w, args.workload)
+        return
+    if w["kind"] == "match":
+        run_match(args, w, args.workload)
         return
 
     import torch

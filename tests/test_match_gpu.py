@@ -119,3 +119,20 @@ def test_invalid_initial_matching(ctx):
     mate, _ = ctx.max_match(g, init=np.array([-1, 2, 1, -1], np.int32))  # augments through 1-2
     assert int((mate >= 0).sum()) == 4
     g.close()
+
+
+def test_cpp_engine_matches_oracle(tmp_path):
+    """The reference-shaped C++ class (MaximumMatchingEngine::FindMaximumMatch,
+    nnodes = exposed) through the example program."""
+    import subprocess
+
+    from test_host_abi import _build_example
+
+    exe = _build_example(tmp_path)
+    out = subprocess.run([exe, "--rmat", "12", "16", "1", "1", "--match"], capture_output=True, text=True,
+                         check=True).stdout
+    kv = dict(x.split("=") for x in out.split())
+    h = xbtrav.HostCSR.rmat(12, 16, seed=0x5EED)
+    ro, ci = h.arrays()
+    h.close()
+    assert int(kv["matching_size"]) == O.max_match(ro, ci)[0]

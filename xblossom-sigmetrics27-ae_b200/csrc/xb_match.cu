@@ -305,15 +305,18 @@ xb_status run_match(xb_ctx* c, xb_graph* g, int32_t* d_mate, const MmWork& wk, i
   const int vgrid = (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)sms * 8));
   MmLevel* h = (MmLevel*)c->h_ctr;  // pinned host scratch
   static_assert(sizeof(MmLevel) <= sizeof(xbk::Ctrs), "pinned scratch too small");
-  int64_t phases = 0, levels = 0, blossom_levels = 0, flips = 0, launches = 0;
+  int64_t phases = 0, levels = 0, blossom_levels = 0, flips = 0;
   unsigned long long scanned = 0;
+  // classes: 0 = forest expansion, 1 = flips and blossom contraction, 2 = phase init
+  xbe::ClassTimer timer{c, st, c->tuning.timing != 0};
   for (;;) {
     if (phases > n / 2 + 1) return fail(XB_ERR_STATE, "matching: phase bound exceeded");
     phases++;
     XB_CUDA(cudaMemsetAsync(wk.fcount, 0, sizeof(int32_t), s));
+    timer.begin();
     k_mm_init<<<vgrid, 256, 0, s>>>(n, d_mate, wk.st, wk.pred, wk.base, wk.lock, wk.head, wk.front[0], wk.fcount);
     XB_LAUNCH_CHECK("matching init");
-    launches++;
+    timer.end(2, 1);
     int32_t fcount = 0;
     XB_CUDA(cudaMemcpyAsync(&h->next_count, wk.fcount, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
     XB_CUDA(cudaStreamSynchronize(s));
@@ -326,20 +329,22 @@ xb_status run_match(xb_ctx* c, xb_graph* g, int32_t* d_mate, const MmWork& wk, i
       levels++;
       XB_CUDA(cudaMemsetAsync(wk.lv, 0, sizeof(MmLevel), s));
       const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(((int64_t)fcount + 7) / 8, (int64_t)sms * 16));
+      timer.begin();
       k_mm_expand<OffT><<<grid, 256, 0, s>>>(wk.front[cur], fcount, ro, g->d_ci, d_mate, wk.st, wk.pred, wk.base,
                                              wk.lock, wk.front[cur ^ 1], wk.found, wk.cand, wk.cand_next, wk.head,
                                              cand_cap, n, wk.lv);
       XB_LAUNCH_CHECK("matching expand");
-      launches++;
+      timer.end(0, 1);
       XB_CUDA(cudaMemcpyAsync(h, wk.lv, sizeof(MmLevel), cudaMemcpyDeviceToHost, s));
       XB_CUDA(cudaStreamSynchronize(s));
       if (h->err) return fail(XB_ERR_STATE, "matching: expand found an inconsistent forest (" + std::to_string(h->err) + ")");
       scanned += h->scanned;
       if (h->found > 0) {
         const int32_t nf = h->found;
+        timer.begin();
         k_mm_flip<<<(nf + 127) / 128, 128, 0, s>>>(wk.found, nf, d_mate, wk.pred, n, wk.lv);
         XB_LAUNCH_CHECK("matching flip");
-        launches++;
+        timer.end(1, 1);
         XB_CUDA(cudaMemcpyAsync(&h->err, &wk.lv->err, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
         XB_CUDA(cudaStreamSynchronize(s));
         if (h->err) return fail(XB_ERR_STATE, "matching: flip walk failed");
@@ -350,10 +355,11 @@ xb_status run_match(xb_ctx* c, xb_graph* g, int32_t* d_mate, const MmWork& wk, i
       if (h->cand > 0) {
         const int32_t nc = h->cand;
         blossom_levels++;
+        timer.begin();
         k_mm_blossom<<<(nc + 127) / 128, 128, 0, s>>>(wk.cand, nc, wk.cand_next, wk.head, wk.st, d_mate, wk.pred,
                                                       wk.base, wk.stamp, wk.tick, wk.front[cur ^ 1], n, wk.lv);
         XB_LAUNCH_CHECK("matching blossoms");
-        launches++;
+        timer.end(1, 1);
         XB_CUDA(cudaMemcpyAsync(h, wk.lv, sizeof(MmLevel), cudaMemcpyDeviceToHost, s));
         XB_CUDA(cudaStreamSynchronize(s));
         if (h->err) return fail(XB_ERR_STATE, "matching: blossom walk failed (" + std::to_string(h->err) + ")");
@@ -370,7 +376,9 @@ xb_status run_match(xb_ctx* c, xb_graph* g, int32_t* d_mate, const MmWork& wk, i
     st->edges_scanned = (int64_t)scanned;
     st->edges_traversed = (int64_t)scanned;
     st->vertices_scanned = flips;
-    st->class_launches[0] = launches;
+    // algorithmic bytes of the expansion: a column index and the neighbour's state word per scanned entry
+    st->class_bytes[0] = (int64_t)scanned * 8;
+    st->algo_bytes = st->class_bytes[0];
   }
   return XB_OK;
 }

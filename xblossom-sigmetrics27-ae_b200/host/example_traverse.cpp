@@ -1,14 +1,15 @@
 // example_traverse.cpp -- reference-style C++ caller of libxbtrav.so.
 //
-//   example_traverse <row_offsets.txt> <col_indices.txt> <k> <seed> [--batched]
-//   example_traverse --rmat <scale> <edge_factor> <k> <seed> [--batched]
+//   example_traverse <row_offsets.txt> <col_indices.txt> <k> <seed> [--batched | --match]
+//   example_traverse --rmat <scale> <edge_factor> <k> <seed> [--batched | --match]
 //
 // Loads (or generates) a CSR the way the reference runners do (HGraph from
 // two text files, apps/xb/runner/xblsm_gpu/run_xb_pp_by_dataset.cu:7-40),
 // uploads it, traverses k seeded sources and prints one summary line plus a
 // checksum of both tables.  --batched splits the sources into three queries
 // run in one launch (BatchedEngine); the tables, and so the checksum, are the
-// same.  Exit status 0 on success.
+// same.  --match runs FindMaximumMatch (MaximumMatchingEngine) from the empty
+// matching instead and prints its size.  Exit status 0 on success.
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -31,6 +32,18 @@ int main(int argc, char** argv) {
     xbtrav::Context ctx(0);
     xbtrav::DGraph dg(ctx, g);
     xbtrav::TraversalEngine eng(dg);
+    if (std::strcmp(argv[argc - 1], "--match") == 0) {
+      xb_stats st{};
+      const xbtrav::Matching mt = xbtrav::MaximumMatchingEngine(dg).FindMaximumMatch(&st);
+      size_t matched = 0;
+      for (size_t v = 0; v < mt.size(); v++) {
+        if (mt[v] == (int32_t)g.nnodes) continue;
+        if (mt[(size_t)mt[v]] != (int32_t)v) throw xbtrav::Error(XB_ERR_STATE, "matching not symmetric");
+        matched++;
+      }
+      std::printf("nnodes=%zu nedges=%zu matching_size=%zu phases=%d\n", g.nnodes, g.nedges, matched / 2, st.batches);
+      return 0;
+    }
     const auto sources = g.SelectSources(seed, k);
     const bool batched = std::strcmp(argv[argc - 1], "--batched") == 0;
     xbtrav::Tables t;

@@ -205,4 +205,34 @@ class BatchedEngine {
   Context* ctx_;
 };
 
+// Maximum matching with the reference engine's interface
+// (AbstractMaximumMatchingEngine, apps/xb/src/include/xbsm_gpu/max_match_engine.h:8-15):
+// Matching[v] = the mate of v, nnodes for an exposed vertex.
+using Matching = std::vector<int32_t>;
+
+class MaximumMatchingEngine {
+ public:
+  explicit MaximumMatchingEngine(const DGraph& g) : g_(&g) { check(xb_graph_info(g.get(), &n_, nullptr, nullptr)); }
+  // From the empty matching.
+  Matching FindMaximumMatch(xb_stats* stats = nullptr) const {
+    return FindMaximumMatch(Matching((size_t)n_, (int32_t)n_), stats);
+  }
+  // From an initial matching (xb_max_match; XB_ERR_ARG if it is not one).
+  Matching FindMaximumMatch(const Matching& initial, xb_stats* stats = nullptr) const {
+    if ((int64_t)initial.size() != n_) check(XB_ERR_ARG);
+    std::vector<int32_t> mate(initial.size());
+    for (size_t v = 0; v < initial.size(); v++) mate[v] = initial[v] == (int32_t)n_ ? -1 : initial[v];
+    xb_stats st{};
+    check(xb_max_match(g_->ctx().get(), g_->get(), mate.data(), 0u, &st));
+    if (stats) *stats = st;
+    Matching out(mate.size());
+    for (size_t v = 0; v < mate.size(); v++) out[v] = mate[v] < 0 ? (int32_t)n_ : mate[v];
+    return out;
+  }
+
+ private:
+  const DGraph* g_;
+  int64_t n_ = 0;
+};
+
 }  // namespace xbtrav
