@@ -10,7 +10,8 @@
 // and flowers", 1965) in a forest:
 //
 //  - a phase starts a fresh forest: every exposed vertex is an outer root;
-//  - a level expands all outer frontier vertices (warp per vertex):
+//  - a level expands all outer frontier vertices (edge-balanced chunks of
+//    the frontier's adjacency, xb_partition.cuh):
 //      * a matched pair (w, mate w) not in any tree is claimed by one CAS on
 //        the state word of min(w, mate w): w becomes inner (pred = v), its
 //        mate outer and part of the next frontier;
@@ -21,15 +22,17 @@
 //      * an outer neighbour of the same tree in another blossom is a
 //        blossom candidate, linked into a per-tree list;
 //  - after a level with augmenting paths, every recorded path is flipped
-//    (thread per path) and the phase ends;
-//  - otherwise the candidates are contracted, one thread per tree walking
-//    its list: the cycle's top is the first common blossom base on the two
+//    (thread per path); the flipped trees keep their locks and drop out, the
+//    other trees keep growing in the same phase (so a phase gathers a large
+//    set of disjoint paths, as a Hopcroft-Karp phase does);
+//  - the candidates of the live trees are contracted, one thread per tree
+//    walking its list: the cycle's top is the first common blossom base on the two
 //    paths to the root, `pred` of the outer vertices on the cycle is
 //    rerouted across it (so a later augmenting path can be read back
 //    through the blossom), the bases are merged into the top (union-find),
 //    and the inner vertices on the cycle become outer frontier vertices;
-//  - a search whose frontier runs empty without augmenting paths proves the
-//    matching maximum.
+//  - a phase whose frontier runs empty without any two trees meeting proves
+//    the matching maximum (no lock was tried, so no edge was skipped).
 //
 // State word per vertex: -1 outside the forest, else root * 4 + label
 // (1 outer, 2 inner), written in one store so a reader sees a whole state.
@@ -38,6 +41,7 @@
 // blossom pointers is bounded by n steps and reports XB_ERR_STATE on
 // overrun instead of looping.
 #include "xb_engine_common.cuh"
+#include "xb_partition.cuh"
 
 using xbi::fail;
 
@@ -90,96 +94,161 @@ __global__ void k_mm_check(int64_t n, const OffT* __restrict__ ro, const int32_t
   }
 }
 
-__global__ void k_mm_init(int64_t n, const int32_t* __restrict__ mate, int32_t* st, int32_t* pred, int32_t* base,
-                          int32_t* lock, int32_t* head, int32_t* front, int32_t* fcount) {
+template <typename OffT>
+__global__ void k_mm_init(int64_t n, const OffT* __restrict__ ro, const int32_t* __restrict__ mate, int32_t* st,
+                          int32_t* pred, int32_t* base, int32_t* lock, int32_t* head, int32_t* front,
+                          int32_t* fcount) {
   for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+    const bool has_edge = ro[v + 1] > ro[v];
     const bool exposed = mate[v] < 0;
     st[v] = exposed ? mm_state((int32_t)v, kOuter) : -1;
     pred[v] = -1;
     base[v] = (int32_t)v;
     lock[v] = 0;
     head[v] = -1;
-    if (exposed) front[atomicAdd(fcount, 1)] = (int32_t)v;
+    if (exposed && has_edge) front[atomicAdd(fcount, 1)] = (int32_t)v;  // isolated roots grow nothing
   }
 }
 
 struct MmLevel {
   int32_t next_count, found, cand, err;
   unsigned long long scanned;
+  int32_t attempts;  // set when an edge between two trees tried the locks
+  int32_t pad;
 };
 
+constexpr int kExpandWarps = 4;                  // warps per expand block
+constexpr int kAppCap = 2 * xbp::kChunk;         // per-warp buffer of grown outer vertices
+
+// One level: the frontier's adjacency entries in chunks of xbp::kChunk, one
+// chunk per warp iteration (lane l of step it takes chunk entry 32 * it + l;
+// the owner of an entry comes from the chunk's mask of entry starts).  Outer
+// vertices grown by pair claims gather in the warp's buffer and go out with
+// one atomic per flush.
 template <typename OffT>
-__global__ void k_mm_expand(const int32_t* __restrict__ front, int32_t fcount, const OffT* __restrict__ ro,
-                            const int32_t* __restrict__ ci, const int32_t* __restrict__ mate, int32_t* st,
-                            int32_t* pred, const int32_t* __restrict__ base, int32_t* lock, int32_t* next,
-                            int2* found, int2* cand, int32_t* cand_next, int32_t* head, int64_t cand_cap,
-                            int64_t n, MmLevel* lv) {
-  const int lane = threadIdx.x & 31;
-  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  unsigned long long scanned = 0;
-  for (int64_t i = warp; i < fcount; i += nwarps) {
-    const int32_t v = front[i];
-    const int32_t mv = mate[v];
-    const int32_t rv = st[v] >> 2;  // outer, stable during the level
-    const int64_t beg = ro[v], end = ro[v + 1];
-    scanned += (unsigned long long)(end - beg);
-    int32_t bv = -2;  // base of v, looked up on first need
-    for (int64_t e0 = beg; e0 < end; e0 += 32) {  // warp-uniform windows
-      const int64_t e = e0 + lane;
+__global__ void __launch_bounds__(32 * kExpandWarps) k_mm_expand(
+    const int32_t* __restrict__ front, const int64_t* __restrict__ eoff, const int64_t* __restrict__ ebase,
+    const int32_t* __restrict__ chunk_first, const int64_t* __restrict__ edges_p,
+    const int64_t* __restrict__ nchunks_p, int32_t fcount, const int32_t* __restrict__ ci,
+    const int32_t* __restrict__ mate, int32_t* st, int32_t* pred, const int32_t* __restrict__ base, int32_t* lock,
+    int32_t* next, int2* found, int2* cand, int32_t* cand_next, int32_t* head, int64_t cand_cap, int64_t n,
+    MmLevel* lv) {
+  constexpr int kItems = xbp::kItems, kChunk = xbp::kChunk;
+  __shared__ OffT s_base_all[kExpandWarps][kChunk + 1];   // spanned entry: column-index position minus eoff
+  __shared__ int32_t s_v_all[kExpandWarps][kChunk + 1];   // spanned entry: its vertex
+  __shared__ uint32_t s_mask_all[kExpandWarps][kItems];   // bit e: a spanned entry starts at chunk edge e
+  __shared__ int32_t s_app_all[kExpandWarps][kAppCap];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  OffT* s_base = s_base_all[wib];
+  int32_t* s_v = s_v_all[wib];
+  uint32_t* s_mask = s_mask_all[wib];
+  int32_t* s_app = s_app_all[wib];
+  const uint32_t le_mask = (2u << lane) - 1u;
+  const int64_t E = *edges_p, nchunks = *nchunks_p;
+  const int64_t gw = (int64_t)blockIdx.x * kExpandWarps + wib, nw = (int64_t)gridDim.x * kExpandWarps;
+  int32_t napp = 0;  // warp-uniform
+  for (int64_t c = gw; c < nchunks; c += nw) {
+    const int64_t E0 = c * kChunk;
+    const int32_t len = (int32_t)min((int64_t)kChunk, E - E0);
+    const int32_t vlo = chunk_first[c];
+    const int32_t vhi = c + 1 < nchunks ? chunk_first[c + 1] : fcount - 1;
+    const int32_t nv = vhi - vlo + 1;
+    __syncwarp();
+    if (lane < kItems) s_mask[lane] = 0u;
+    __syncwarp();
+    int32_t rel0 = 0;
+    for (int32_t j = lane; j < nv; j += 32) {
+      const int64_t rel = eoff[vlo + j] - E0;
+      s_base[j] = (OffT)ebase[vlo + j];
+      s_v[j] = front[vlo + j];
+      if (j == 0) rel0 = (int32_t)max(rel, (int64_t)-1);
+      if (rel >= 0 && rel < kChunk) atomicOr(&s_mask[rel >> 5], 1u << (rel & 31));
+    }
+    __syncwarp();
+    int32_t run = (__shfl_sync(0xffffffffu, rel0, 0) < 0 ? 1 : 0) - 1;
+    int32_t vv[kItems], w[kItems];
+#pragma unroll
+    for (int it = 0; it < kItems; it++) {
+      const uint32_t m = s_mask[it];
+      const int32_t e = 32 * it + lane;
+      const int32_t j = run + __popc(m & le_mask);
+      run += __popc(m);
+      vv[it] = -1;
+      w[it] = 0;
+      if (e < len) {
+        vv[it] = s_v[j];
+        w[it] = ci[(int64_t)s_base[j] + E0 + e];
+      }
+    }
+    int32_t sw[kItems], mv[kItems];
+#pragma unroll
+    for (int it = 0; it < kItems; it++) {
+      sw[it] = vv[it] >= 0 ? *(volatile int32_t*)&st[w[it]] : -2;
+      mv[it] = vv[it] >= 0 ? mate[vv[it]] : -1;
+    }
+#pragma unroll
+    for (int it = 0; it < kItems; it++) {
       bool grow = false;
       int32_t grown = 0;
-      if (e < end) {
-        const int32_t w = ci[e];
-        if (w != mv) {
-          const int32_t sw = *(volatile int32_t*)&st[w];
-          if (sw == -1) {
-            const int32_t mw = mate[w];
-            if (mw >= 0) {
-              const int32_t lk = min(w, mw), other = max(w, mw);
-              const int32_t lab_lk = lk == w ? kInner : kOuter;
-              if (atomicCAS(&st[lk], -1, mm_state(rv, lab_lk)) == -1) {
-                pred[w] = v;
-                st[other] = mm_state(rv, lab_lk == kInner ? kOuter : kInner);
-                grow = true;
-                grown = mw;
+      const int32_t v = vv[it];
+      // a locked tree holds an augmenting path of this phase (or is being
+      // tried for one right now): its vertices take no further part
+      const int32_t rv = v >= 0 ? st[v] >> 2 : 0;  // outer, stable during the level
+      if (v >= 0 && w[it] != mv[it] && sw[it] != -2 && *(volatile int32_t*)&lock[rv] == 0) {
+        if (sw[it] == -1) {
+          const int32_t mw = mate[w[it]];
+          if (mw >= 0) {
+            const int32_t lk = min(w[it], mw), other = max(w[it], mw);
+            const int32_t lab_lk = lk == w[it] ? kInner : kOuter;
+            if (atomicCAS(&st[lk], -1, mm_state(rv, lab_lk)) == -1) {
+              pred[w[it]] = v;
+              st[other] = mm_state(rv, lab_lk == kInner ? kOuter : kInner);
+              grow = true;
+              grown = mw;
+            }
+          }
+        } else if ((sw[it] & 3) == kOuter && *(volatile int32_t*)&lock[sw[it] >> 2] == 0) {
+          const int32_t rw = sw[it] >> 2;
+          if (rw != rv) {
+            lv->attempts = 1;
+            const int32_t a = min(rv, rw), b = max(rv, rw);
+            if (atomicExch(&lock[a], 1) == 0) {
+              if (atomicExch(&lock[b], 1) == 0) {
+                const int32_t k = atomicAdd(&lv->found, 1);
+                found[k] = make_int2(v, w[it]);
+              } else {
+                atomicExch(&lock[a], 0);
               }
             }
-          } else if ((sw & 3) == kOuter) {
-            const int32_t rw = sw >> 2;
-            if (rw != rv) {
-              const int32_t a = min(rv, rw), b = max(rv, rw);
-              if (atomicExch(&lock[a], 1) == 0) {
-                if (atomicExch(&lock[b], 1) == 0) {
-                  const int32_t k = atomicAdd(&lv->found, 1);
-                  found[k] = make_int2(v, w);
-                } else {
-                  atomicExch(&lock[a], 0);
-                }
-              }
-            } else {
-              if (bv == -2) bv = mm_find_ro(base, v, n);
-              const int32_t bw = mm_find_ro(base, w, n);
-              if (bv < 0 || bw < 0) {
-                atomicExch(&lv->err, 1);
-              } else if (bv != bw) {
-                const int32_t k = atomicAdd(&lv->cand, 1);
-                if (k < cand_cap) {
-                  cand[k] = make_int2(v, w);
-                  cand_next[k] = atomicExch(&head[rv], k);
-                } else {
-                  atomicExch(&lv->err, 2);
-                }
+          } else {
+            const int32_t bv = mm_find_ro(base, v, n), bw = mm_find_ro(base, w[it], n);
+            if (bv < 0 || bw < 0) {
+              atomicExch(&lv->err, 1);
+            } else if (bv != bw) {
+              const int32_t k = atomicAdd(&lv->cand, 1);
+              if (k < cand_cap) {
+                cand[k] = make_int2(v, w[it]);
+                cand_next[k] = atomicExch(&head[rv], k);
+              } else {
+                atomicExch(&lv->err, 2);
               }
             }
           }
         }
       }
-      xbk::warp_append(grow, grown, next, &lv->next_count);
+      const unsigned bal = __ballot_sync(0xffffffffu, grow);
+      if (grow) s_app[napp + __popc(bal & (le_mask >> 1))] = grown;
+      napp += __popc(bal);
+    }
+    if (napp > kAppCap - kChunk || c + nw >= nchunks) {  // room for one more chunk, or the warp's last chunk
+      __syncwarp();
+      int32_t basei = 0;
+      if (lane == 0 && napp) basei = atomicAdd(&lv->next_count, napp);
+      basei = __shfl_sync(0xffffffffu, basei, 0);
+      for (int32_t i = lane; i < napp; i += 32) next[basei + i] = s_app[i];
+      napp = 0;
     }
   }
-  scanned = xbk::warp_sum_u64(scanned);
-  if (lane == 0 && scanned) atomicAdd(&lv->scanned, scanned);
 }
 
 // Flips the recorded augmenting paths (their trees are disjoint).
@@ -214,11 +283,15 @@ __global__ void k_mm_flip(const int2* __restrict__ found, int32_t nfound, int32_
 // processes that tree's whole list.
 __global__ void k_mm_blossom(const int2* __restrict__ cand, int32_t ncand, const int32_t* __restrict__ cand_next,
                              int32_t* head, int32_t* st, const int32_t* __restrict__ mate, int32_t* pred,
-                             int32_t* base, int32_t* stamp, int32_t* tick, int32_t* next, int64_t n,
-                             MmLevel* lv) {
+                             int32_t* base, int32_t* stamp, int32_t* tick, const int32_t* __restrict__ lock,
+                             int32_t* next, int64_t n, MmLevel* lv) {
   for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < ncand; i += gridDim.x * blockDim.x) {
     const int32_t r = st[cand[i].x] >> 2;
     if (head[r] != i) continue;
+    if (lock[r]) {  // the tree's augmenting path was flipped this level: it is out of the phase
+      head[r] = -1;
+      continue;
+    }
     int32_t* err = &lv->err;
     int64_t guard = 0;
     for (int32_t c = i; c >= 0; c = cand_next[c]) {
@@ -291,8 +364,9 @@ __global__ void k_mm_blossom(const int2* __restrict__ cand, int32_t ncand, const
 }
 
 struct MmWork {
-  int32_t *st, *pred, *base, *lock, *head, *stamp, *front[2], *cand_next, *tick, *fcount;
+  int32_t *st, *pred, *base, *lock, *head, *stamp, *front[2], *cand_next, *tick, *fcount, *chunk_first;
   int2 *found, *cand;
+  int64_t *eoff, *ebase, *tsum, *scal;
   MmLevel* lv;
 };
 
@@ -305,16 +379,20 @@ xb_status run_match(xb_ctx* c, xb_graph* g, int32_t* d_mate, const MmWork& wk, i
   const int vgrid = (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)sms * 8));
   MmLevel* h = (MmLevel*)c->h_ctr;  // pinned host scratch
   static_assert(sizeof(MmLevel) <= sizeof(xbk::Ctrs), "pinned scratch too small");
-  int64_t phases = 0, levels = 0, blossom_levels = 0, flips = 0;
+  int64_t phases = 0, levels = 0, blossom_levels = 0, flips = 0, idle_phases = 0;
   unsigned long long scanned = 0;
-  // classes: 0 = forest expansion, 1 = flips and blossom contraction, 2 = phase init
+  // classes: 0 = forest expansion, 1 = flips and blossom contraction, 2 = phase init and frontier partition
   xbe::ClassTimer timer{c, st, c->tuning.timing != 0};
+  int expand_per_sm = 0;
+  XB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&expand_per_sm, k_mm_expand<OffT>, 32 * kExpandWarps, 0));
+  const int expand_grid = sms * std::max(expand_per_sm, 1);
   for (;;) {
     if (phases > n / 2 + 1) return fail(XB_ERR_STATE, "matching: phase bound exceeded");
     phases++;
     XB_CUDA(cudaMemsetAsync(wk.fcount, 0, sizeof(int32_t), s));
     timer.begin();
-    k_mm_init<<<vgrid, 256, 0, s>>>(n, d_mate, wk.st, wk.pred, wk.base, wk.lock, wk.head, wk.front[0], wk.fcount);
+    k_mm_init<OffT><<<vgrid, 256, 0, s>>>(n, ro, d_mate, wk.st, wk.pred, wk.base, wk.lock, wk.head, wk.front[0],
+                                          wk.fcount);
     XB_LAUNCH_CHECK("matching init");
     timer.end(2, 1);
     int32_t fcount = 0;
@@ -323,22 +401,31 @@ xb_status run_match(xb_ctx* c, xb_graph* g, int32_t* d_mate, const MmWork& wk, i
     fcount = h->next_count;
     if (fcount == 0) break;  // perfect matching
     int cur = 0;
-    bool flipped = false;
+    int64_t phase_found = 0;
+    bool attempted = false;
     for (int64_t lvl = 0; fcount > 0; lvl++) {
       if (lvl > n) return fail(XB_ERR_STATE, "matching: level bound exceeded");
       levels++;
       XB_CUDA(cudaMemsetAsync(wk.lv, 0, sizeof(MmLevel), s));
-      const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(((int64_t)fcount + 7) / 8, (int64_t)sms * 16));
+      const int32_t ntiles = (fcount + xbp::kTile - 1) / xbp::kTile;
       timer.begin();
-      k_mm_expand<OffT><<<grid, 256, 0, s>>>(wk.front[cur], fcount, ro, g->d_ci, d_mate, wk.st, wk.pred, wk.base,
-                                             wk.lock, wk.front[cur ^ 1], wk.found, wk.cand, wk.cand_next, wk.head,
-                                             cand_cap, n, wk.lv);
+      xbp::k_lb_tile_sums<OffT><<<ntiles, xbp::kThreads, 0, s>>>(wk.front[cur], fcount, ro, wk.tsum);
+      xbp::k_lb_tile_scan<<<1, 1024, 0, s>>>(wk.tsum, ntiles, wk.scal, wk.scal + 1, &wk.lv->scanned);
+      xbp::k_lb_offsets<OffT><<<ntiles, xbp::kThreads, 0, s>>>(wk.front[cur], fcount, ro, wk.tsum, wk.eoff,
+                                                                wk.ebase, wk.chunk_first);
+      XB_LAUNCH_CHECK("matching partition");
+      timer.end(2, 3);
+      timer.begin();
+      k_mm_expand<OffT><<<expand_grid, 32 * kExpandWarps, 0, s>>>(
+          wk.front[cur], wk.eoff, wk.ebase, wk.chunk_first, wk.scal, wk.scal + 1, fcount, g->d_ci, d_mate, wk.st,
+          wk.pred, wk.base, wk.lock, wk.front[cur ^ 1], wk.found, wk.cand, wk.cand_next, wk.head, cand_cap, n, wk.lv);
       XB_LAUNCH_CHECK("matching expand");
       timer.end(0, 1);
       XB_CUDA(cudaMemcpyAsync(h, wk.lv, sizeof(MmLevel), cudaMemcpyDeviceToHost, s));
       XB_CUDA(cudaStreamSynchronize(s));
       if (h->err) return fail(XB_ERR_STATE, "matching: expand found an inconsistent forest (" + std::to_string(h->err) + ")");
       scanned += h->scanned;
+      attempted = attempted || h->attempts != 0;
       if (h->found > 0) {
         const int32_t nf = h->found;
         timer.begin();
@@ -349,15 +436,18 @@ xb_status run_match(xb_ctx* c, xb_graph* g, int32_t* d_mate, const MmWork& wk, i
         XB_CUDA(cudaStreamSynchronize(s));
         if (h->err) return fail(XB_ERR_STATE, "matching: flip walk failed");
         flips += nf;
-        flipped = true;
-        break;
+        phase_found += nf;
+        // the flipped trees stay locked; the other trees keep growing in this phase
+        XB_CUDA(cudaMemcpyAsync(h, wk.lv, sizeof(MmLevel), cudaMemcpyDeviceToHost, s));
+        XB_CUDA(cudaStreamSynchronize(s));
       }
       if (h->cand > 0) {
         const int32_t nc = h->cand;
         blossom_levels++;
         timer.begin();
         k_mm_blossom<<<(nc + 127) / 128, 128, 0, s>>>(wk.cand, nc, wk.cand_next, wk.head, wk.st, d_mate, wk.pred,
-                                                      wk.base, wk.stamp, wk.tick, wk.front[cur ^ 1], n, wk.lv);
+                                                      wk.base, wk.stamp, wk.tick, wk.lock, wk.front[cur ^ 1], n,
+                                                      wk.lv);
         XB_LAUNCH_CHECK("matching blossoms");
         timer.end(1, 1);
         XB_CUDA(cudaMemcpyAsync(h, wk.lv, sizeof(MmLevel), cudaMemcpyDeviceToHost, s));
@@ -367,7 +457,14 @@ xb_status run_match(xb_ctx* c, xb_graph* g, int32_t* d_mate, const MmWork& wk, i
       fcount = h->next_count;
       cur ^= 1;
     }
-    if (!flipped) break;  // the search ran out without an augmenting path: maximum
+    if (phase_found > 0) {
+      idle_phases = 0;
+      continue;
+    }
+    // No path flipped.  A search in which no two trees ever met proves the
+    // matching maximum; one whose lock attempts all gave way is repeated.
+    if (!attempted) break;
+    if (++idle_phases > 64) return fail(XB_ERR_STATE, "matching: searches keep failing to lock their paths");
   }
   if (st) {
     st->batches = (int32_t)std::min<int64_t>(phases, INT32_MAX);
@@ -405,9 +502,11 @@ xb_status xb_max_match(xb_ctx* c, const xb_graph* gc, int32_t* mate, uint32_t fl
   XB_CUDA(cudaSetDevice(c->device));
   const int64_t n = g->n, m = g->m;
   const int64_t cand_cap = std::max<int64_t>(m, 1);
-  // state, pred, base, lock, head, stamp, two frontiers, tick, count: int32 x n;
-  // found: n int2; candidates: m int2 + m links; mate: n; the level counters
-  const size_t bytes = 256 * 16 + 4 * (size_t)n * 9 + 8 * (size_t)n + 12 * (size_t)cand_cap + 4 * (size_t)n + 256;
+  // state, pred, base, lock, head, stamp, two frontiers, mate: int32 x n; found: n int2;
+  // candidates: m int2 + m links; partition: eoff and ebase (n int64), tile sums, chunk owners;
+  // counters.  Each region is rounded up to 256 bytes.
+  const size_t bytes = 256 * 24 + 4 * (size_t)n * 9 + 8 * (size_t)n + 12 * (size_t)cand_cap + 16 * (size_t)n +
+                       8 * (size_t)(n / xbp::kTile + 2) + 4 * (size_t)(m / xbp::kChunk + 2) + 256;
   if (c->ws_bytes < bytes || !c->ws) {
     if (c->ws) cudaFree(c->ws);
     c->ws = nullptr;
@@ -436,6 +535,11 @@ xb_status xb_max_match(xb_ctx* c, const xb_graph* gc, int32_t* mate, uint32_t fl
   wk.tick = carve_ints<int32_t>(p, 1);
   wk.fcount = carve_ints<int32_t>(p, 1);
   wk.lv = carve_ints<MmLevel>(p, 1);
+  wk.eoff = carve_ints<int64_t>(p, n);
+  wk.ebase = carve_ints<int64_t>(p, n);
+  wk.tsum = carve_ints<int64_t>(p, n / xbp::kTile + 2);
+  wk.scal = carve_ints<int64_t>(p, 4);
+  wk.chunk_first = carve_ints<int32_t>(p, m / xbp::kChunk + 2);
   if ((size_t)(p - (char*)c->ws) > bytes) return fail(XB_ERR_STATE, "matching workspace layout");
   cudaStream_t s = c->stream;
   const bool dev = (flags & XB_OUT_DEVICE) != 0;
