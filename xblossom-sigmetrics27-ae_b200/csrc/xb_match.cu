@@ -367,7 +367,7 @@ struct MmWork {
   int32_t *st, *pred, *base, *lock, *head, *stamp, *front[2], *cand_next, *tick, *fcount, *chunk_first;
   int2 *found, *cand;
   int64_t *eoff, *ebase, *tsum, *scal;
-  MmLevel* lv;
+  MmLevel *lv, *sticky;  // per-level counters; errors of the flips (cleared per call)
 };
 
 template <typename OffT>
@@ -409,12 +409,17 @@ xb_status run_match(xb_ctx* c, xb_graph* g, int32_t* d_mate, const MmWork& wk, i
       XB_CUDA(cudaMemsetAsync(wk.lv, 0, sizeof(MmLevel), s));
       const int32_t ntiles = (fcount + xbp::kTile - 1) / xbp::kTile;
       timer.begin();
-      xbp::k_lb_tile_sums<OffT><<<ntiles, xbp::kThreads, 0, s>>>(wk.front[cur], fcount, ro, wk.tsum);
-      xbp::k_lb_tile_scan<<<1, 1024, 0, s>>>(wk.tsum, ntiles, wk.scal, wk.scal + 1, &wk.lv->scanned);
-      xbp::k_lb_offsets<OffT><<<ntiles, xbp::kThreads, 0, s>>>(wk.front[cur], fcount, ro, wk.tsum, wk.eoff,
-                                                                wk.ebase, wk.chunk_first);
+      if (ntiles == 1) {
+        xbp::k_lb_single<OffT><<<1, xbp::kThreads, 0, s>>>(wk.front[cur], fcount, ro, wk.eoff, wk.ebase,
+                                                           wk.chunk_first, wk.scal, wk.scal + 1, &wk.lv->scanned);
+      } else {
+        xbp::k_lb_tile_sums<OffT><<<ntiles, xbp::kThreads, 0, s>>>(wk.front[cur], fcount, ro, wk.tsum);
+        xbp::k_lb_tile_scan<<<1, 1024, 0, s>>>(wk.tsum, ntiles, wk.scal, wk.scal + 1, &wk.lv->scanned);
+        xbp::k_lb_offsets<OffT><<<ntiles, xbp::kThreads, 0, s>>>(wk.front[cur], fcount, ro, wk.tsum, wk.eoff,
+                                                                  wk.ebase, wk.chunk_first);
+      }
       XB_LAUNCH_CHECK("matching partition");
-      timer.end(2, 3);
+      timer.end(2, ntiles == 1 ? 1 : 3);
       timer.begin();
       k_mm_expand<OffT><<<expand_grid, 32 * kExpandWarps, 0, s>>>(
           wk.front[cur], wk.eoff, wk.ebase, wk.chunk_first, wk.scal, wk.scal + 1, fcount, g->d_ci, d_mate, wk.st,
@@ -429,17 +434,13 @@ xb_status run_match(xb_ctx* c, xb_graph* g, int32_t* d_mate, const MmWork& wk, i
       if (h->found > 0) {
         const int32_t nf = h->found;
         timer.begin();
-        k_mm_flip<<<(nf + 127) / 128, 128, 0, s>>>(wk.found, nf, d_mate, wk.pred, n, wk.lv);
+        // errors of the flips go to the phase's sticky record, read at the phase end
+        k_mm_flip<<<(nf + 127) / 128, 128, 0, s>>>(wk.found, nf, d_mate, wk.pred, n, wk.sticky);
         XB_LAUNCH_CHECK("matching flip");
         timer.end(1, 1);
-        XB_CUDA(cudaMemcpyAsync(&h->err, &wk.lv->err, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
-        XB_CUDA(cudaStreamSynchronize(s));
-        if (h->err) return fail(XB_ERR_STATE, "matching: flip walk failed");
         flips += nf;
         phase_found += nf;
         // the flipped trees stay locked; the other trees keep growing in this phase
-        XB_CUDA(cudaMemcpyAsync(h, wk.lv, sizeof(MmLevel), cudaMemcpyDeviceToHost, s));
-        XB_CUDA(cudaStreamSynchronize(s));
       }
       if (h->cand > 0) {
         const int32_t nc = h->cand;
@@ -457,6 +458,9 @@ xb_status run_match(xb_ctx* c, xb_graph* g, int32_t* d_mate, const MmWork& wk, i
       fcount = h->next_count;
       cur ^= 1;
     }
+    XB_CUDA(cudaMemcpyAsync(&h->err, &wk.sticky->err, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    XB_CUDA(cudaStreamSynchronize(s));
+    if (h->err) return fail(XB_ERR_STATE, "matching: flip walk failed");
     if (phase_found > 0) {
       idle_phases = 0;
       continue;
@@ -505,7 +509,7 @@ xb_status xb_max_match(xb_ctx* c, const xb_graph* gc, int32_t* mate, uint32_t fl
   // state, pred, base, lock, head, stamp, two frontiers, mate: int32 x n; found: n int2;
   // candidates: m int2 + m links; partition: eoff and ebase (n int64), tile sums, chunk owners;
   // counters.  Each region is rounded up to 256 bytes.
-  const size_t bytes = 256 * 24 + 4 * (size_t)n * 9 + 8 * (size_t)n + 12 * (size_t)cand_cap + 16 * (size_t)n +
+  const size_t bytes = 256 * 26 + 4 * (size_t)n * 9 + 8 * (size_t)n + 12 * (size_t)cand_cap + 16 * (size_t)n +
                        8 * (size_t)(n / xbp::kTile + 2) + 4 * (size_t)(m / xbp::kChunk + 2) + 256;
   if (c->ws_bytes < bytes || !c->ws) {
     if (c->ws) cudaFree(c->ws);
@@ -535,6 +539,7 @@ xb_status xb_max_match(xb_ctx* c, const xb_graph* gc, int32_t* mate, uint32_t fl
   wk.tick = carve_ints<int32_t>(p, 1);
   wk.fcount = carve_ints<int32_t>(p, 1);
   wk.lv = carve_ints<MmLevel>(p, 1);
+  wk.sticky = carve_ints<MmLevel>(p, 1);
   wk.eoff = carve_ints<int64_t>(p, n);
   wk.ebase = carve_ints<int64_t>(p, n);
   wk.tsum = carve_ints<int64_t>(p, n / xbp::kTile + 2);
@@ -548,6 +553,7 @@ xb_status xb_max_match(xb_ctx* c, const xb_graph* gc, int32_t* mate, uint32_t fl
   XB_CUDA(cudaMemsetAsync(wk.tick, 0, sizeof(int32_t), s));
   XB_CUDA(cudaMemsetAsync(wk.stamp, 0, sizeof(int32_t) * (size_t)n, s));
   XB_CUDA(cudaMemsetAsync(wk.lv, 0, sizeof(MmLevel), s));
+  XB_CUDA(cudaMemsetAsync(wk.sticky, 0, sizeof(MmLevel), s));
   const int vgrid = (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)c->num_sms * 8));
   if (g->off64)
     k_mm_check<int64_t><<<vgrid, 256, 0, s>>>(n, (const int64_t*)g->d_ro, g->d_ci, d_mate, &wk.lv->err);

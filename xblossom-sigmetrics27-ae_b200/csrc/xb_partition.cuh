@@ -128,5 +128,46 @@ __global__ void __launch_bounds__(kThreads) k_lb_offsets(const int32_t* __restri
   }
 }
 
+// All three phases in one block (kThreads threads) for a frontier of at
+// most kTile entries: the common case of a round's first and last levels,
+// where launches, not bytes, are the cost.
+template <typename OffT>
+__global__ void __launch_bounds__(kThreads) k_lb_single(const int32_t* __restrict__ list, int32_t cnt,
+                                                        const OffT* __restrict__ ro, int64_t* eoff, int64_t* ebase,
+                                                        int32_t* chunk_first, int64_t* edges, int64_t* nchunks,
+                                                        unsigned long long* relaxed) {
+  const int64_t i0 = (int64_t)threadIdx.x * kItems;
+  int64_t deg[kItems], beg[kItems];
+  int64_t sum = 0;
+#pragma unroll
+  for (int j = 0; j < kItems; j++) {
+    const int64_t i = i0 + j;
+    deg[j] = beg[j] = 0;
+    if (i < cnt) {
+      const int32_t u = list[i];
+      beg[j] = (int64_t)ro[u];
+      deg[j] = (int64_t)ro[u + 1] - beg[j];
+    }
+    sum += deg[j];
+  }
+  int64_t total;
+  int64_t off = block_scan_i64(sum, &total);
+#pragma unroll
+  for (int j = 0; j < kItems; j++) {
+    const int64_t i = i0 + j;
+    if (i < cnt) {
+      eoff[i] = off;
+      ebase[i] = beg[j] - off;
+      for (int64_t c = (off + kChunk - 1) / kChunk; c * kChunk < off + deg[j]; c++) chunk_first[c] = (int32_t)i;
+    }
+    off += deg[j];
+  }
+  if (threadIdx.x == 0) {
+    *edges = total;
+    *nchunks = (total + kChunk - 1) / kChunk;
+    *relaxed += (unsigned long long)total;
+  }
+}
+
 }  // namespace
 }  // namespace xbp

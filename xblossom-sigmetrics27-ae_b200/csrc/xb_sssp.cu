@@ -250,11 +250,17 @@ xb_status run_sssp(xb_ctx* c, xb_graph* g, const int32_t* d_src, int32_t k, floa
     XB_CUDA(cudaMemsetAsync(wk.cnt + (cur ^ 1), 0, sizeof(int32_t), s));
     XB_CUDA(cudaMemsetAsync(wk.cnt + 2, 0, sizeof(int32_t), s));
     timer.begin();
-    xbp::k_lb_tile_sums<OffT><<<ntiles, kThreads, 0, s>>>(wk.list[cur], fcount, ro, wk.tsum);
-    xbp::k_lb_tile_scan<<<1, 1024, 0, s>>>(wk.tsum, ntiles, wk.scal, wk.scal + 1, wk.relaxed);
-    xbp::k_lb_offsets<OffT><<<ntiles, kThreads, 0, s>>>(wk.list[cur], fcount, ro, wk.tsum, wk.eoff, wk.ebase,
-                                                   wk.chunk_first);
-    timer.end(1, 3);
+    if (ntiles == 1) {
+      xbp::k_lb_single<OffT><<<1, kThreads, 0, s>>>(wk.list[cur], fcount, ro, wk.eoff, wk.ebase, wk.chunk_first,
+                                                    wk.scal, wk.scal + 1, wk.relaxed);
+      timer.end(1, 1);
+    } else {
+      xbp::k_lb_tile_sums<OffT><<<ntiles, kThreads, 0, s>>>(wk.list[cur], fcount, ro, wk.tsum);
+      xbp::k_lb_tile_scan<<<1, 1024, 0, s>>>(wk.tsum, ntiles, wk.scal, wk.scal + 1, wk.relaxed);
+      xbp::k_lb_offsets<OffT><<<ntiles, kThreads, 0, s>>>(wk.list[cur], fcount, ro, wk.tsum, wk.eoff, wk.ebase,
+                                                          wk.chunk_first);
+      timer.end(1, 3);
+    }
     timer.begin();
     k_sssp_relax<OffT><<<relax_grid, 32 * kRelaxWarps, 0, s>>>(wk.list[cur], wk.cnt + cur, wk.eoff, wk.ebase,
                                                                wk.chunk_first, wk.scal, wk.scal + 1, g->d_ci,
@@ -362,8 +368,11 @@ xb_status xb_multi_sssp(xb_ctx* c, const xb_graph* gc, const int32_t* sources, i
   const SsspWork wk = carve(c->ws, n, g->m, kd, &d_src);
   XB_CUDA(cudaMemcpyAsync(d_src, hs.data(), sizeof(int32_t) * kd, cudaMemcpyHostToDevice, c->stream));
   XB_CUDA(cudaEventRecord(c->ev0, c->stream));
-  xb_status s = g->off64 ? run_sssp<int64_t>(c, g, d_src, kd, dist, out_dev, wk, &c->h_ctr->lv[0].n_light, st)
-                         : run_sssp<int32_t>(c, g, d_src, kd, dist, out_dev, wk, &c->h_ctr->lv[0].n_light, st);
+  // four pinned ints of host scratch: the counters of the first level record
+  static_assert(sizeof(xbk::LevelCtr) >= 4 * sizeof(int32_t), "pinned scratch too small");
+  int32_t* h4 = reinterpret_cast<int32_t*>(&c->h_ctr->lv[0]);
+  xb_status s = g->off64 ? run_sssp<int64_t>(c, g, d_src, kd, dist, out_dev, wk, h4, st)
+                         : run_sssp<int32_t>(c, g, d_src, kd, dist, out_dev, wk, h4, st);
   if (s != XB_OK) {
     cudaStreamSynchronize(c->stream);
     return s;
