@@ -179,7 +179,13 @@ xb_status xb_graph_upload_batch(xb_ctx* ctx, int32_t ninst, const int64_t* inst_
 xb_status xb_graph_load_csr_text(xb_ctx* ctx, const char* row_path, const char* col_path,
                                  xb_graph** out);
 xb_status xb_graph_free(xb_graph* g);
+/* Row offsets live on the device as int32 when the graph has fewer than
+ * 2^31 - 1 entries, else as int64.  Setting XB_OFFSETS64=1 in the
+ * environment keeps int64 offsets for every graph uploaded meanwhile (tests
+ * of the int64 kernels on small graphs). */
 xb_status xb_graph_info(const xb_graph* g, int64_t* n, int64_t* m, int64_t* max_degree);
+/* Width of the graph's device row offsets: 4 or 8 bytes. */
+xb_status xb_graph_offset_bytes(const xb_graph* g, int32_t* bytes);
 xb_status xb_select_sources(const xb_graph* g, uint64_t seed, int32_t k, int32_t* out);
 
 /* ---- traversal ---------------------------------------------------------- */

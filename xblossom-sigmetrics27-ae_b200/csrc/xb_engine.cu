@@ -8,6 +8,7 @@
 // decides the next step.  Unlike the reference it reads one 200-byte counter
 // block per level (instead of four D2H scalars plus a device sync per queue
 // swap) and traverses B (32 or 64) sources per launch sequence.
+#include <cstdlib>
 #include <memory>
 #include <new>
 
@@ -16,6 +17,15 @@
 using xbi::fail;
 
 namespace xbe {
+
+// Row offsets are stored as int32 unless the graph has 2^31 - 1 or more
+// entries; XB_OFFSETS64=1 in the environment keeps int64 offsets for every
+// graph uploaded while it is set (the int64 kernels' parity tests).
+bool wide_offsets(int64_t m) {
+  if (m >= (int64_t)INT32_MAX) return true;
+  const char* e = std::getenv("XB_OFFSETS64");
+  return e && e[0] == '1';
+}
 
 // The F/N "all zero between calls" invariant and the epoch stamps hold per
 // layout; a call with another (n, word size, words) places the regions at
@@ -473,7 +483,7 @@ xb_status xb_graph_upload(xb_ctx* c, int64_t n, const void* row_offsets, int32_t
   g->ctx = c;
   g->n = n;
   g->m = m;
-  g->off64 = m >= (int64_t)INT32_MAX;
+  g->off64 = xbe::wide_offsets(m);
   for (int64_t v = 0; v < n; v++) g->max_deg = std::max(g->max_deg, ro[v + 1] - ro[v]);
   const size_t ro_bytes = (g->off64 ? 8 : 4) * (size_t)(n + 1);
   // colIndices carries kCiPad zero entries past the end: the 16-byte loads of
@@ -518,7 +528,7 @@ xb_status xb_graph_upload_batch(xb_ctx* c, int32_t ninst, const int64_t* inst_n,
     const int64_t m = ro[n];
     xb_status s = xbi::validate_csr(n, ro, col_indices ? col_indices + edge_src[(size_t)i] : nullptr);
     if (s != XB_OK) return fail(s, "instance " + std::to_string(i) + ": " + xb_last_error());
-    off64 = off64 || m >= (int64_t)INT32_MAX;
+    off64 = off64 || xbe::wide_offsets(m);
     vtx_off[(size_t)i + 1] = vtx_off[(size_t)i] + n + 1;
     edge_src[(size_t)i + 1] = edge_src[(size_t)i] + m;
     edge_dev[(size_t)i + 1] = edge_dev[(size_t)i] + ((m + 3) & ~(int64_t)3);  // instances start 16-byte aligned
@@ -613,6 +623,13 @@ xb_status xb_graph_info(const xb_graph* g, int64_t* n, int64_t* m, int64_t* max_
   if (n) *n = g->n;
   if (m) *m = g->m;
   if (max_degree) *max_degree = g->max_deg;
+  return XB_OK;
+}
+
+xb_status xb_graph_offset_bytes(const xb_graph* g, int32_t* bytes) {
+  xbi::clear_error();
+  if (!g || !bytes) return fail(XB_ERR_ARG, "null argument");
+  *bytes = g->off64 ? 8 : 4;
   return XB_OK;
 }
 

@@ -166,6 +166,7 @@ def lib() -> C.CDLL:
         "xb_graph_set_weights": (i32, [vp, vp, i64]),
         "xb_multi_sssp": (i32, [vp, vp, vp, i32, vp, u32, P(XbStats)]),
         "xb_max_match": (i32, [vp, vp, vp, u32, P(XbStats)]),
+        "xb_graph_offset_bytes": (i32, [vp, P(i32)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -337,6 +338,13 @@ class Graph:
         out = np.zeros(k, np.int32)
         _check(lib().xb_select_sources(self._h, seed, k, out.ctypes.data))
         return out
+
+    @property
+    def offset_bytes(self) -> int:
+        """Width of the device row offsets (4, or 8 for huge graphs and under XB_OFFSETS64=1)."""
+        b = C.c_int32()
+        _check(lib().xb_graph_offset_bytes(self._h, C.byref(b)))
+        return b.value
 
     def set_weights(self, weights) -> None:
         """Attaches int32 edge weights, one per column index (xb_graph_set_weights)."""
