@@ -780,7 +780,8 @@ def main() -> None:
     # roofline of the dominant kernel class (its kernels event-timed per class)
     peak, peak_kind = measured_peaks()
     dom = 0 if cls_agg["class_ms"][0] >= cls_agg["class_ms"][1] else 1
-    dom_name = ["level steps (k_pull_tiles/k_push_*)", "table pass (k_tables)"][dom]
+    dom_name = ["level steps (k_pull_lanes / k_pull_heavy / k_pull_hubs; k_pull_tiles for four words; k_push_*)",
+                "table pass (k_tables)"][dom]
     achieved = (cls_agg["class_bytes"][dom] / (cls_agg["class_ms"][dom] / 1e3) / 1e9
                 if cls_agg["class_ms"][dom] > 0 else None)
     tr = traffic_from_profile(args.workload)
