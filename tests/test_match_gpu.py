@@ -136,3 +136,17 @@ def test_cpp_engine_matches_oracle(tmp_path):
     ro, ci = h.arrays()
     h.close()
     assert int(kv["matching_size"]) == O.max_match(ro, ci)[0]
+
+
+def test_degenerate_graphs(ctx):
+    # one vertex; isolated vertices only; a single edge; a perfect matching given as the start
+    cases = [(np.array([0, 0], np.int64), np.zeros(0, np.int32), None, 0),
+             (np.zeros(6, np.int64), np.zeros(0, np.int32), None, 0),
+             (np.array([0, 1, 2], np.int64), np.array([1, 0], np.int32), None, 1),
+             (np.array([0, 1, 2], np.int64), np.array([1, 0], np.int32), np.array([1, 0], np.int32), 1)]
+    for ro, ci, init, want in cases:
+        g = ctx.upload_arrays(ro, ci)
+        mate, st = ctx.max_match(g, init=init)
+        g.close()
+        assert O.check_matching(ro, ci, mate) == 0
+        assert int((mate >= 0).sum()) // 2 == want == st["reached"]
