@@ -162,48 +162,6 @@ struct PassPlan {
   double cost = 0;
 };
 
-// Creates a conditional handle in the graph stream s is capturing into.
-xb_status make_handle(cudaStream_t s, unsigned dflt, unsigned flags, cudaGraphConditionalHandle* h) {
-  cudaStreamCaptureStatus cst = cudaStreamCaptureStatusNone;
-  cudaGraph_t g = nullptr;
-  XB_CUDA(cudaStreamGetCaptureInfo(s, &cst, nullptr, &g, nullptr, nullptr));
-  if (cst != cudaStreamCaptureStatusActive) return fail(XB_ERR_STATE, "stream is not capturing");
-  XB_CUDA(cudaGraphConditionalHandleCreate(h, g, dflt, flags));
-  return XB_OK;
-}
-
-// Adds a conditional node on handle h after the work captured so far on s and
-// makes it the stream's only dependency; returns its body graphs.
-xb_status add_conditional(cudaStream_t s, cudaGraphConditionalHandle h, cudaGraphConditionalNodeType type,
-                          unsigned size, cudaGraph_t* bodies) {
-  cudaStreamCaptureStatus cst = cudaStreamCaptureStatusNone;
-  cudaGraph_t g = nullptr;
-  const cudaGraphNode_t* deps = nullptr;
-  size_t nd = 0;
-  XB_CUDA(cudaStreamGetCaptureInfo(s, &cst, nullptr, &g, &deps, &nd));
-  if (cst != cudaStreamCaptureStatusActive) return fail(XB_ERR_STATE, "stream is not capturing");
-  cudaGraphNodeParams np = {};
-  np.type = cudaGraphNodeTypeConditional;
-  np.conditional.handle = h;
-  np.conditional.type = type;
-  np.conditional.size = size;
-  cudaGraphNode_t node = nullptr;
-  XB_CUDA(cudaGraphAddNode(&node, g, deps, nd, &np));
-  for (unsigned i = 0; i < size; i++) bodies[i] = np.conditional.phGraph_out[i];
-  XB_CUDA(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
-  return XB_OK;
-}
-
-// Ends a capture into a body graph whatever happened inside it; keeps the
-// first error.
-xb_status end_body(cudaStream_t s, xb_status st) {
-  cudaGraph_t out = nullptr;
-  const cudaError_t e = cudaStreamEndCapture(s, &out);
-  if (st != XB_OK) return st;
-  if (e != cudaSuccess) return fail(XB_ERR_CUDA, std::string("body capture: ") + cudaGetErrorString(e));
-  return XB_OK;
-}
-
 // One level step inside the WHILE body (captured on b0): decide, clear the
 // new level plane, then SWITCH into the push or the pull body (captured on b1).
 template <typename W, int NW, typename OffT>

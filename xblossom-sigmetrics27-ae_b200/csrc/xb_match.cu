@@ -9,7 +9,10 @@
 // file does the same with Edmonds' blossom rule (J. Edmonds, "Paths, trees,
 // and flowers", 1965) in a forest:
 //
-//  - a phase starts a fresh forest: every exposed vertex is an outer root;
+//  - the first phase starts a fresh forest (every exposed vertex an outer
+//    root); a later phase keeps the trees that flipped nothing and restarts
+//    from all their outer vertices (the reference engines reuse trees the
+//    same way, xblossom_gpu_engine_10.cu:83-166);
 //  - a level expands all outer frontier vertices (edge-balanced chunks of
 //    the frontier's adjacency, xb_partition.cuh):
 //      * a matched pair (w, mate w) not in any tree is claimed by one CAS on
@@ -110,11 +113,41 @@ __global__ void k_mm_init(int64_t n, const OffT* __restrict__ ro, const int32_t*
   }
 }
 
+// Next phase from the current forest: the trees whose augmenting paths were
+// flipped (locked roots) dissolve -- their vertices, all matched now, leave
+// the forest -- and every other tree stays as it is (labels, pred, blossom
+// bases); all outer vertices of the kept trees form the first frontier, so
+// the search re-examines every edge of the forest against the vertices that
+// just became free.  The locks are cleared afterwards (separate memset).
+template <typename OffT>
+__global__ void k_mm_reinit(int64_t n, const OffT* __restrict__ ro, int32_t* st, int32_t* pred, int32_t* base,
+                            const int32_t* __restrict__ lock, int32_t* head, int32_t* front, int32_t* fcount) {
+  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+    head[v] = -1;
+    const int32_t sv = st[v];
+    if (sv == -1) continue;
+    if (lock[sv >> 2]) {
+      st[v] = -1;
+      pred[v] = -1;
+      base[v] = (int32_t)v;
+    } else if ((sv & 3) == kOuter && ro[v + 1] > ro[v]) {
+      front[atomicAdd(fcount, 1)] = (int32_t)v;
+    }
+  }
+}
+
+// Counters of one forest level (cleared at its start).
 struct MmLevel {
-  int32_t next_count, found, cand, err;
-  unsigned long long scanned;
+  int32_t found, cand, err;
   int32_t attempts;  // set when an edge between two trees tried the locks
-  int32_t pad;
+  unsigned long long scanned;
+};
+
+// Totals of one phase, accumulated by k_mm_level_end (cleared per phase).
+struct MmPhase {
+  unsigned long long scanned;
+  int64_t found, levels, blossom_levels;
+  int32_t attempted, err;
 };
 
 constexpr int kExpandWarps = 4;                  // warps per expand block
@@ -129,10 +162,10 @@ template <typename OffT>
 __global__ void __launch_bounds__(32 * kExpandWarps) k_mm_expand(
     const int32_t* __restrict__ front, const int64_t* __restrict__ eoff, const int64_t* __restrict__ ebase,
     const int32_t* __restrict__ chunk_first, const int64_t* __restrict__ edges_p,
-    const int64_t* __restrict__ nchunks_p, int32_t fcount, const int32_t* __restrict__ ci,
+    const int64_t* __restrict__ nchunks_p, const int32_t* __restrict__ fcount_p, const int32_t* __restrict__ ci,
     const int32_t* __restrict__ mate, int32_t* st, int32_t* pred, const int32_t* __restrict__ base, int32_t* lock,
-    int32_t* next, int2* found, int2* cand, int32_t* cand_next, int32_t* head, int64_t cand_cap, int64_t n,
-    MmLevel* lv) {
+    int32_t* next, int32_t* next_count, int2* found, int2* cand, int32_t* cand_next, int32_t* head,
+    int64_t cand_cap, int64_t n, MmLevel* lv) {
   constexpr int kItems = xbp::kItems, kChunk = xbp::kChunk;
   __shared__ OffT s_base_all[kExpandWarps][kChunk + 1];   // spanned entry: column-index position minus eoff
   __shared__ int32_t s_v_all[kExpandWarps][kChunk + 1];   // spanned entry: its vertex
@@ -145,6 +178,7 @@ __global__ void __launch_bounds__(32 * kExpandWarps) k_mm_expand(
   int32_t* s_app = s_app_all[wib];
   const uint32_t le_mask = (2u << lane) - 1u;
   const int64_t E = *edges_p, nchunks = *nchunks_p;
+  const int32_t fcount = *fcount_p;
   const int64_t gw = (int64_t)blockIdx.x * kExpandWarps + wib, nw = (int64_t)gridDim.x * kExpandWarps;
   int32_t napp = 0;  // warp-uniform
   for (int64_t c = gw; c < nchunks; c += nw) {
@@ -243,7 +277,7 @@ __global__ void __launch_bounds__(32 * kExpandWarps) k_mm_expand(
     if (napp > kAppCap - kChunk || c + nw >= nchunks) {  // room for one more chunk, or the warp's last chunk
       __syncwarp();
       int32_t basei = 0;
-      if (lane == 0 && napp) basei = atomicAdd(&lv->next_count, napp);
+      if (lane == 0 && napp) basei = atomicAdd(next_count, napp);
       basei = __shfl_sync(0xffffffffu, basei, 0);
       for (int32_t i = lane; i < napp; i += 32) next[basei + i] = s_app[i];
       napp = 0;
@@ -265,8 +299,9 @@ __device__ __forceinline__ bool mm_flip_walk(int32_t u, int32_t pu, int32_t* mat
   return false;
 }
 
-__global__ void k_mm_flip(const int2* __restrict__ found, int32_t nfound, int32_t* mate,
+__global__ void k_mm_flip(const int2* __restrict__ found, const int32_t* __restrict__ nfound_p, int32_t* mate,
                           const int32_t* __restrict__ pred, int64_t n, MmLevel* lv) {
+  const int32_t nfound = *nfound_p;
   for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nfound; i += gridDim.x * blockDim.x) {
     const int32_t v = found[i].x, w = found[i].y;
     const int32_t ow = mate[w];
@@ -281,10 +316,12 @@ __global__ void k_mm_flip(const int2* __restrict__ found, int32_t nfound, int32_
 
 // Contracts the blossom candidates; the thread holding a tree's list head
 // processes that tree's whole list.
-__global__ void k_mm_blossom(const int2* __restrict__ cand, int32_t ncand, const int32_t* __restrict__ cand_next,
-                             int32_t* head, int32_t* st, const int32_t* __restrict__ mate, int32_t* pred,
-                             int32_t* base, int32_t* stamp, int32_t* tick, const int32_t* __restrict__ lock,
-                             int32_t* next, int64_t n, MmLevel* lv) {
+__global__ void k_mm_blossom(const int2* __restrict__ cand, const int32_t* __restrict__ ncand_p,
+                             const int32_t* __restrict__ cand_next, int32_t* head, int32_t* st,
+                             const int32_t* __restrict__ mate, int32_t* pred, int32_t* base, int32_t* stamp,
+                             int32_t* tick, const int32_t* __restrict__ lock, int32_t* next, int32_t* next_count,
+                             int64_t n, MmLevel* lv) {
+  const int32_t ncand = *ncand_p;
   for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < ncand; i += gridDim.x * blockDim.x) {
     const int32_t r = st[cand[i].x] >> 2;
     if (head[r] != i) continue;
@@ -353,7 +390,7 @@ __global__ void k_mm_blossom(const int2* __restrict__ cand, int32_t ncand, const
           base[top] = top;
           if ((st[m] & 3) == kInner) {
             st[m] = mm_state(r, kOuter);
-            next[atomicAdd(&lv->next_count, 1)] = m;
+            next[atomicAdd(next_count, 1)] = m;
           }
           x = pred[m];
         }
@@ -363,12 +400,105 @@ __global__ void k_mm_blossom(const int2* __restrict__ cand, int32_t ncand, const
   }
 }
 
+// Level control for the device-side loop: clear the level's counters and
+// the output frontier's count; afterwards fold them into the phase totals
+// and decide whether the WHILE loop takes another level.
+__global__ void k_mm_level_begin(int32_t* next_count, MmLevel* lv) {
+  *next_count = 0;
+  lv->found = lv->cand = lv->err = lv->attempts = 0;
+  lv->scanned = 0;
+}
+
+__global__ void k_mm_level_end(const int32_t* __restrict__ in_count, const int32_t* __restrict__ next_count,
+                               const MmLevel* __restrict__ lv, MmPhase* ph, int64_t level_cap, int in_graph,
+                               cudaGraphConditionalHandle loop) {
+  if (*in_count > 0) {
+    ph->levels++;
+    ph->scanned += lv->scanned;
+    ph->found += lv->found;
+    ph->blossom_levels += lv->cand > 0;
+    ph->attempted |= lv->attempts;
+    ph->err |= lv->err;
+  }
+  if (ph->levels > level_cap) ph->err |= 8;
+  if (in_graph) cudaGraphSetConditional(loop, (*next_count > 0 && ph->err == 0) ? 1u : 0u);
+}
+
 struct MmWork {
-  int32_t *st, *pred, *base, *lock, *head, *stamp, *front[2], *cand_next, *tick, *fcount, *chunk_first;
+  int32_t *st, *pred, *base, *lock, *head, *stamp, *front[2], *cand_next, *tick, *fcnt, *chunk_first;
   int2 *found, *cand;
   int64_t *eoff, *ebase, *tsum, *scal;
   MmLevel *lv, *sticky;  // per-level counters; errors of the flips (cleared per call)
+  MmPhase* ph;
 };
+
+// One forest level on stream s from front[cur] into front[cur ^ 1], every
+// count read on the device (so the same launches serve the captured loop).
+template <typename OffT>
+void emit_level(const MmWork& wk, const xb_graph* g, int32_t* d_mate, int64_t cand_cap, int cur, int max_tiles,
+                int expand_grid, int sms, cudaStream_t s, xbe::ClassTimer* timer = nullptr) {
+  const OffT* ro = (const OffT*)g->d_ro;
+  const int64_t n = g->n;
+  int32_t* in_cnt = wk.fcnt + cur;
+  int32_t* out_cnt = wk.fcnt + (cur ^ 1);
+  // classes when timed: 2 = control and partition, 0 = expansion, 1 = flips and blossoms
+  if (timer) timer->begin();
+  k_mm_level_begin<<<1, 1, 0, s>>>(out_cnt, wk.lv);
+  xbp::k_lb_tile_sums<OffT><<<max_tiles, xbp::kThreads, 0, s>>>(wk.front[cur], in_cnt, ro, wk.tsum);
+  xbp::k_lb_tile_scan<<<1, 1024, 0, s>>>(wk.tsum, in_cnt, wk.scal, wk.scal + 1, &wk.lv->scanned);
+  xbp::k_lb_offsets<OffT><<<max_tiles, xbp::kThreads, 0, s>>>(wk.front[cur], in_cnt, ro, wk.tsum, wk.eoff, wk.ebase,
+                                                               wk.chunk_first);
+  if (timer) {
+    timer->end(2, 4);
+    timer->begin();
+  }
+  k_mm_expand<OffT><<<expand_grid, 32 * kExpandWarps, 0, s>>>(
+      wk.front[cur], wk.eoff, wk.ebase, wk.chunk_first, wk.scal, wk.scal + 1, in_cnt, g->d_ci, d_mate, wk.st, wk.pred,
+      wk.base, wk.lock, wk.front[cur ^ 1], out_cnt, wk.found, wk.cand, wk.cand_next, wk.head, cand_cap, n, wk.lv);
+  if (timer) {
+    timer->end(0, 1);
+    timer->begin();
+  }
+  // flips first: their trees stay locked, so the blossom pass skips them
+  k_mm_flip<<<sms * 4, 128, 0, s>>>(wk.found, &wk.lv->found, d_mate, wk.pred, n, wk.sticky);
+  k_mm_blossom<<<sms * 8, 128, 0, s>>>(wk.cand, &wk.lv->cand, wk.cand_next, wk.head, wk.st, d_mate, wk.pred, wk.base,
+                                       wk.stamp, wk.tick, wk.lock, wk.front[cur ^ 1], out_cnt, n, wk.lv);
+  if (timer) timer->end(1, 2);
+}
+
+// The level loop of one phase as a graph: a WHILE node whose body takes a
+// level from front[0] into front[1] and one back; k_mm_level_end keeps the
+// loop going while the next frontier is not empty.
+template <typename OffT>
+xb_status capture_phase_loop(const MmWork& wk, const xb_graph* g, int32_t* d_mate, int64_t cand_cap, int max_tiles,
+                             int expand_grid, int sms, cudaStream_t s, cudaStream_t body, cudaGraphExec_t* exec) {
+  XB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
+  cudaGraphConditionalHandle h;
+  xb_status st = xbe::make_handle(s, 1, cudaGraphCondAssignDefault, &h);
+  cudaGraph_t wbody = nullptr;
+  if (st == XB_OK) st = xbe::add_conditional(s, h, cudaGraphCondTypeWhile, 1, &wbody);
+  if (st == XB_OK) {
+    if (cudaStreamBeginCaptureToGraph(body, wbody, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) != cudaSuccess) {
+      st = fail(XB_ERR_CUDA, "matching: body capture failed to start");
+    } else {
+      for (int cur = 0; cur < 2; cur++) {
+        emit_level<OffT>(wk, g, d_mate, cand_cap, cur, max_tiles, expand_grid, sms, body);
+        k_mm_level_end<<<1, 1, 0, body>>>(wk.fcnt + cur, wk.fcnt + (cur ^ 1), wk.lv, wk.ph, g->n + 1, 1, h);
+      }
+      if (cudaGetLastError() != cudaSuccess) st = fail(XB_ERR_CUDA, "matching: a captured launch failed");
+      st = xbe::end_body(body, st);
+    }
+  }
+  cudaGraph_t graph = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(s, &graph);
+  if (st == XB_OK && e != cudaSuccess) st = fail(XB_ERR_CUDA, std::string("matching capture: ") + cudaGetErrorString(e));
+  if (st == XB_OK && cudaGraphInstantiate(exec, graph, 0) != cudaSuccess) {
+    cudaGetLastError();
+    st = fail(XB_ERR_CUDA, "matching: graph instantiation failed");
+  }
+  if (graph) cudaGraphDestroy(graph);
+  return st;
+}
 
 template <typename OffT>
 xb_status run_match(xb_ctx* c, xb_graph* g, int32_t* d_mate, const MmWork& wk, int64_t cand_cap, xb_stats* st) {
@@ -377,97 +507,91 @@ xb_status run_match(xb_ctx* c, xb_graph* g, int32_t* d_mate, const MmWork& wk, i
   const OffT* ro = (const OffT*)g->d_ro;
   const int sms = c->num_sms;
   const int vgrid = (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)sms * 8));
-  MmLevel* h = (MmLevel*)c->h_ctr;  // pinned host scratch
-  static_assert(sizeof(MmLevel) <= sizeof(xbk::Ctrs), "pinned scratch too small");
-  int64_t phases = 0, levels = 0, blossom_levels = 0, flips = 0, idle_phases = 0;
-  unsigned long long scanned = 0;
-  // classes: 0 = forest expansion, 1 = flips and blossom contraction, 2 = phase init and frontier partition
-  xbe::ClassTimer timer{c, st, c->tuning.timing != 0};
+  const int max_tiles = (int)((n + xbp::kTile - 1) / xbp::kTile);
+  MmPhase* h = (MmPhase*)c->h_ctr;  // pinned host scratch
+  static_assert(sizeof(MmPhase) + 2 * sizeof(int32_t) <= sizeof(xbk::Ctrs), "pinned scratch too small");
+  int32_t* h_cnt = (int32_t*)(h + 1);
   int expand_per_sm = 0;
   XB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&expand_per_sm, k_mm_expand<OffT>, 32 * kExpandWarps, 0));
   const int expand_grid = sms * std::max(expand_per_sm, 1);
+  // per-class timing needs a host-driven loop (events around each launch);
+  // otherwise each phase's levels run as one captured WHILE loop
+  const bool timed = c->tuning.timing != 0;
+  xbe::ClassTimer timer{c, st, timed};
+  cudaStream_t body = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  struct Cleanup {
+    cudaStream_t& b;
+    cudaGraphExec_t& e;
+    ~Cleanup() {
+      if (e) cudaGraphExecDestroy(e);
+      if (b) cudaStreamDestroy(b);
+    }
+  } cleanup{body, exec};
+  if (!timed) {
+    XB_CUDA(cudaStreamCreateWithFlags(&body, cudaStreamNonBlocking));
+    xb_status cs = capture_phase_loop<OffT>(wk, g, d_mate, cand_cap, max_tiles, expand_grid, sms, s, body, &exec);
+    if (cs != XB_OK) return cs;
+  }
+  int64_t phases = 0, levels = 0, blossom_levels = 0, flips = 0, idle_phases = 0, launches = 0;
+  unsigned long long scanned = 0;
+  bool reuse = false;  // next phase keeps the trees that flipped nothing
   for (;;) {
     if (phases > n / 2 + 1) return fail(XB_ERR_STATE, "matching: phase bound exceeded");
     phases++;
-    XB_CUDA(cudaMemsetAsync(wk.fcount, 0, sizeof(int32_t), s));
+    XB_CUDA(cudaMemsetAsync(wk.fcnt, 0, 2 * sizeof(int32_t), s));
+    XB_CUDA(cudaMemsetAsync(wk.ph, 0, sizeof(MmPhase), s));
     timer.begin();
-    k_mm_init<OffT><<<vgrid, 256, 0, s>>>(n, ro, d_mate, wk.st, wk.pred, wk.base, wk.lock, wk.head, wk.front[0],
-                                          wk.fcount);
+    if (!reuse) {
+      k_mm_init<OffT><<<vgrid, 256, 0, s>>>(n, ro, d_mate, wk.st, wk.pred, wk.base, wk.lock, wk.head, wk.front[0],
+                                            wk.fcnt);
+    } else {
+      k_mm_reinit<OffT><<<vgrid, 256, 0, s>>>(n, ro, wk.st, wk.pred, wk.base, wk.lock, wk.head, wk.front[0], wk.fcnt);
+      XB_CUDA(cudaMemsetAsync(wk.lock, 0, sizeof(int32_t) * (size_t)n, s));
+    }
     XB_LAUNCH_CHECK("matching init");
     timer.end(2, 1);
-    int32_t fcount = 0;
-    XB_CUDA(cudaMemcpyAsync(&h->next_count, wk.fcount, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
-    XB_CUDA(cudaStreamSynchronize(s));
-    fcount = h->next_count;
-    if (fcount == 0) break;  // perfect matching
-    int cur = 0;
-    int64_t phase_found = 0;
-    bool attempted = false;
-    for (int64_t lvl = 0; fcount > 0; lvl++) {
-      if (lvl > n) return fail(XB_ERR_STATE, "matching: level bound exceeded");
-      levels++;
-      XB_CUDA(cudaMemsetAsync(wk.lv, 0, sizeof(MmLevel), s));
-      const int32_t ntiles = (fcount + xbp::kTile - 1) / xbp::kTile;
-      timer.begin();
-      if (ntiles == 1) {
-        xbp::k_lb_single<OffT><<<1, xbp::kThreads, 0, s>>>(wk.front[cur], fcount, ro, wk.eoff, wk.ebase,
-                                                           wk.chunk_first, wk.scal, wk.scal + 1, &wk.lv->scanned);
-      } else {
-        xbp::k_lb_tile_sums<OffT><<<ntiles, xbp::kThreads, 0, s>>>(wk.front[cur], fcount, ro, wk.tsum);
-        xbp::k_lb_tile_scan<<<1, 1024, 0, s>>>(wk.tsum, ntiles, wk.scal, wk.scal + 1, &wk.lv->scanned);
-        xbp::k_lb_offsets<OffT><<<ntiles, xbp::kThreads, 0, s>>>(wk.front[cur], fcount, ro, wk.tsum, wk.eoff,
-                                                                  wk.ebase, wk.chunk_first);
-      }
-      XB_LAUNCH_CHECK("matching partition");
-      timer.end(2, ntiles == 1 ? 1 : 3);
-      timer.begin();
-      k_mm_expand<OffT><<<expand_grid, 32 * kExpandWarps, 0, s>>>(
-          wk.front[cur], wk.eoff, wk.ebase, wk.chunk_first, wk.scal, wk.scal + 1, fcount, g->d_ci, d_mate, wk.st,
-          wk.pred, wk.base, wk.lock, wk.front[cur ^ 1], wk.found, wk.cand, wk.cand_next, wk.head, cand_cap, n, wk.lv);
-      XB_LAUNCH_CHECK("matching expand");
-      timer.end(0, 1);
-      XB_CUDA(cudaMemcpyAsync(h, wk.lv, sizeof(MmLevel), cudaMemcpyDeviceToHost, s));
+    if (!timed) {
+      XB_CUDA(cudaGraphLaunch(exec, s));
+    } else {
+      // the same levels, one by one from the host
+      XB_CUDA(cudaMemcpyAsync(h_cnt, wk.fcnt, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
       XB_CUDA(cudaStreamSynchronize(s));
-      if (h->err) return fail(XB_ERR_STATE, "matching: expand found an inconsistent forest (" + std::to_string(h->err) + ")");
-      scanned += h->scanned;
-      attempted = attempted || h->attempts != 0;
-      if (h->found > 0) {
-        const int32_t nf = h->found;
-        timer.begin();
-        // errors of the flips go to the phase's sticky record, read at the phase end
-        k_mm_flip<<<(nf + 127) / 128, 128, 0, s>>>(wk.found, nf, d_mate, wk.pred, n, wk.sticky);
-        XB_LAUNCH_CHECK("matching flip");
-        timer.end(1, 1);
-        flips += nf;
-        phase_found += nf;
-        // the flipped trees stay locked; the other trees keep growing in this phase
-      }
-      if (h->cand > 0) {
-        const int32_t nc = h->cand;
-        blossom_levels++;
-        timer.begin();
-        k_mm_blossom<<<(nc + 127) / 128, 128, 0, s>>>(wk.cand, nc, wk.cand_next, wk.head, wk.st, d_mate, wk.pred,
-                                                      wk.base, wk.stamp, wk.tick, wk.lock, wk.front[cur ^ 1], n,
-                                                      wk.lv);
-        XB_LAUNCH_CHECK("matching blossoms");
-        timer.end(1, 1);
-        XB_CUDA(cudaMemcpyAsync(h, wk.lv, sizeof(MmLevel), cudaMemcpyDeviceToHost, s));
+      int cur = 0;
+      for (int64_t lvl = 0; h_cnt[0] > 0; lvl++) {
+        if (lvl > n) return fail(XB_ERR_STATE, "matching: level bound exceeded");
+        emit_level<OffT>(wk, g, d_mate, cand_cap, cur, max_tiles, expand_grid, sms, s, &timer);
+        k_mm_level_end<<<1, 1, 0, s>>>(wk.fcnt + cur, wk.fcnt + (cur ^ 1), wk.lv, wk.ph, n + 1, 0, 0);
+        XB_LAUNCH_CHECK("matching level");
+        launches++;
+        XB_CUDA(cudaMemcpyAsync(h_cnt, wk.fcnt + (cur ^ 1), sizeof(int32_t), cudaMemcpyDeviceToHost, s));
         XB_CUDA(cudaStreamSynchronize(s));
-        if (h->err) return fail(XB_ERR_STATE, "matching: blossom walk failed (" + std::to_string(h->err) + ")");
+        cur ^= 1;
       }
-      fcount = h->next_count;
-      cur ^= 1;
     }
-    XB_CUDA(cudaMemcpyAsync(&h->err, &wk.sticky->err, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    XB_CUDA(cudaMemcpyAsync(h, wk.ph, sizeof(MmPhase), cudaMemcpyDeviceToHost, s));
+    XB_CUDA(cudaMemcpyAsync(h_cnt, &wk.sticky->err, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
     XB_CUDA(cudaStreamSynchronize(s));
-    if (h->err) return fail(XB_ERR_STATE, "matching: flip walk failed");
-    if (phase_found > 0) {
+    if (h->err) return fail(XB_ERR_STATE, "matching: inconsistent forest (" + std::to_string(h->err) + ")");
+    if (h_cnt[0]) return fail(XB_ERR_STATE, "matching: flip walk failed");
+    levels += h->levels;
+    if (!timed) {  // kernels the graph ran: 8 per level, levels in pairs (an odd count runs one empty level)
+      const int64_t L = h->levels;
+      launches += 8 * (L == 0 ? 2 : L + (L & 1));
+    }
+    blossom_levels += h->blossom_levels;
+    scanned += h->scanned;
+    flips += h->found;
+    if (h->found > 0) {
       idle_phases = 0;
+      reuse = true;
       continue;
     }
     // No path flipped.  A search in which no two trees ever met proves the
-    // matching maximum; one whose lock attempts all gave way is repeated.
-    if (!attempted) break;
+    // matching maximum; one whose lock attempts all gave way is repeated
+    // from a fresh forest.
+    if (!h->attempted) break;
+    reuse = false;
     if (++idle_phases > 64) return fail(XB_ERR_STATE, "matching: searches keep failing to lock their paths");
   }
   if (st) {
@@ -477,6 +601,7 @@ xb_status run_match(xb_ctx* c, xb_graph* g, int32_t* d_mate, const MmWork& wk, i
     st->edges_scanned = (int64_t)scanned;
     st->edges_traversed = (int64_t)scanned;
     st->vertices_scanned = flips;
+    st->class_launches[0] += launches;  // the level kernels (timed runs count them per class instead)
     // algorithmic bytes of the expansion: a column index and the neighbour's state word per scanned entry
     st->class_bytes[0] = (int64_t)scanned * 8;
     st->algo_bytes = st->class_bytes[0];
@@ -509,7 +634,7 @@ xb_status xb_max_match(xb_ctx* c, const xb_graph* gc, int32_t* mate, uint32_t fl
   // state, pred, base, lock, head, stamp, two frontiers, mate: int32 x n; found: n int2;
   // candidates: m int2 + m links; partition: eoff and ebase (n int64), tile sums, chunk owners;
   // counters.  Each region is rounded up to 256 bytes.
-  const size_t bytes = 256 * 26 + 4 * (size_t)n * 9 + 8 * (size_t)n + 12 * (size_t)cand_cap + 16 * (size_t)n +
+  const size_t bytes = 256 * 28 + 4 * (size_t)n * 9 + 8 * (size_t)n + 12 * (size_t)cand_cap + 16 * (size_t)n +
                        8 * (size_t)(n / xbp::kTile + 2) + 4 * (size_t)(m / xbp::kChunk + 2) + 256;
   if (c->ws_bytes < bytes || !c->ws) {
     if (c->ws) cudaFree(c->ws);
@@ -537,9 +662,10 @@ xb_status xb_max_match(xb_ctx* c, const xb_graph* gc, int32_t* mate, uint32_t fl
   wk.cand_next = carve_ints<int32_t>(p, cand_cap);
   int32_t* d_mate = carve_ints<int32_t>(p, n);
   wk.tick = carve_ints<int32_t>(p, 1);
-  wk.fcount = carve_ints<int32_t>(p, 1);
+  wk.fcnt = carve_ints<int32_t>(p, 2);
   wk.lv = carve_ints<MmLevel>(p, 1);
   wk.sticky = carve_ints<MmLevel>(p, 1);
+  wk.ph = carve_ints<MmPhase>(p, 1);
   wk.eoff = carve_ints<int64_t>(p, n);
   wk.ebase = carve_ints<int64_t>(p, n);
   wk.tsum = carve_ints<int64_t>(p, n / xbp::kTile + 2);

@@ -55,8 +55,11 @@ __device__ __forceinline__ int64_t block_scan_i64(int64_t x, int64_t* total) {
 
 // Scan phase 1: the degree sum of each tile of kTile frontier entries.
 template <typename OffT>
-__global__ void __launch_bounds__(kThreads) k_lb_tile_sums(const int32_t* __restrict__ list, int32_t cnt,
+__global__ void __launch_bounds__(kThreads) k_lb_tile_sums(const int32_t* __restrict__ list,
+                                                           const int32_t* __restrict__ cnt_p,
                                                            const OffT* __restrict__ ro, int64_t* tsum) {
+  const int32_t cnt = *cnt_p;
+  if ((int64_t)blockIdx.x * kTile >= cnt) return;  // grids may be sized for the largest frontier
   const int64_t i0 = (int64_t)blockIdx.x * kTile + (int64_t)threadIdx.x * kItems;
   int64_t sum = 0;
 #pragma unroll
@@ -74,8 +77,10 @@ __global__ void __launch_bounds__(kThreads) k_lb_tile_sums(const int32_t* __rest
 
 // Scan phase 2 (one block of 1024): tile offsets in place, the round's edge
 // total and chunk count.
-__global__ void __launch_bounds__(1024) k_lb_tile_scan(int64_t* tsum, int32_t ntiles, int64_t* edges,
-                                                       int64_t* nchunks, unsigned long long* relaxed) {
+__global__ void __launch_bounds__(1024) k_lb_tile_scan(int64_t* tsum, const int32_t* __restrict__ cnt_p,
+                                                       int64_t* edges, int64_t* nchunks,
+                                                       unsigned long long* relaxed) {
+  const int32_t ntiles = (*cnt_p + kTile - 1) / kTile;
   int64_t carry = 0;
   for (int32_t b0 = 0; b0 < ntiles; b0 += blockDim.x) {
     const int32_t b = b0 + threadIdx.x;
@@ -96,10 +101,13 @@ __global__ void __launch_bounds__(1024) k_lb_tile_scan(int64_t* tsum, int32_t nt
 // (eoff) and its column-index position minus that (ebase); for every chunk
 // boundary inside its edges, the owner's index (chunk_first).
 template <typename OffT>
-__global__ void __launch_bounds__(kThreads) k_lb_offsets(const int32_t* __restrict__ list, int32_t cnt,
+__global__ void __launch_bounds__(kThreads) k_lb_offsets(const int32_t* __restrict__ list,
+                                                         const int32_t* __restrict__ cnt_p,
                                                          const OffT* __restrict__ ro,
                                                          const int64_t* __restrict__ tsum, int64_t* eoff,
                                                          int64_t* ebase, int32_t* chunk_first) {
+  const int32_t cnt = *cnt_p;
+  if ((int64_t)blockIdx.x * kTile >= cnt) return;
   const int64_t i0 = (int64_t)blockIdx.x * kTile + (int64_t)threadIdx.x * kItems;
   int64_t deg[kItems], beg[kItems];
   int64_t sum = 0;
@@ -132,10 +140,12 @@ __global__ void __launch_bounds__(kThreads) k_lb_offsets(const int32_t* __restri
 // most kTile entries: the common case of a round's first and last levels,
 // where launches, not bytes, are the cost.
 template <typename OffT>
-__global__ void __launch_bounds__(kThreads) k_lb_single(const int32_t* __restrict__ list, int32_t cnt,
+__global__ void __launch_bounds__(kThreads) k_lb_single(const int32_t* __restrict__ list,
+                                                        const int32_t* __restrict__ cnt_p,
                                                         const OffT* __restrict__ ro, int64_t* eoff, int64_t* ebase,
                                                         int32_t* chunk_first, int64_t* edges, int64_t* nchunks,
                                                         unsigned long long* relaxed) {
+  const int32_t cnt = *cnt_p;
   const int64_t i0 = (int64_t)threadIdx.x * kItems;
   int64_t deg[kItems], beg[kItems];
   int64_t sum = 0;

@@ -251,13 +251,13 @@ xb_status run_sssp(xb_ctx* c, xb_graph* g, const int32_t* d_src, int32_t k, floa
     XB_CUDA(cudaMemsetAsync(wk.cnt + 2, 0, sizeof(int32_t), s));
     timer.begin();
     if (ntiles == 1) {
-      xbp::k_lb_single<OffT><<<1, kThreads, 0, s>>>(wk.list[cur], fcount, ro, wk.eoff, wk.ebase, wk.chunk_first,
+      xbp::k_lb_single<OffT><<<1, kThreads, 0, s>>>(wk.list[cur], wk.cnt + cur, ro, wk.eoff, wk.ebase, wk.chunk_first,
                                                     wk.scal, wk.scal + 1, wk.relaxed);
       timer.end(1, 1);
     } else {
-      xbp::k_lb_tile_sums<OffT><<<ntiles, kThreads, 0, s>>>(wk.list[cur], fcount, ro, wk.tsum);
-      xbp::k_lb_tile_scan<<<1, 1024, 0, s>>>(wk.tsum, ntiles, wk.scal, wk.scal + 1, wk.relaxed);
-      xbp::k_lb_offsets<OffT><<<ntiles, kThreads, 0, s>>>(wk.list[cur], fcount, ro, wk.tsum, wk.eoff, wk.ebase,
+      xbp::k_lb_tile_sums<OffT><<<ntiles, kThreads, 0, s>>>(wk.list[cur], wk.cnt + cur, ro, wk.tsum);
+      xbp::k_lb_tile_scan<<<1, 1024, 0, s>>>(wk.tsum, wk.cnt + cur, wk.scal, wk.scal + 1, wk.relaxed);
+      xbp::k_lb_offsets<OffT><<<ntiles, kThreads, 0, s>>>(wk.list[cur], wk.cnt + cur, ro, wk.tsum, wk.eoff, wk.ebase,
                                                           wk.chunk_first);
       timer.end(1, 3);
     }
