@@ -136,7 +136,7 @@ def test_context_without_device_reports_nodev():
     assert e.value.status == xbtrav.XB_ERR_NODEV
 
 
-def _build_example(tmp_path):
+def _build_example(tmp_path, name="example_traverse"):
     import os
     import subprocess
 
@@ -144,11 +144,27 @@ def _build_example(tmp_path):
 
     pkg = os.path.dirname(X.LIB_PATH)
     root = os.path.dirname(pkg)
-    exe = str(tmp_path / "example_traverse")
+    exe = str(tmp_path / name)
     subprocess.run(["g++", "-std=c++17", "-O2", "-I", os.path.join(root, "include"), "-I", os.path.join(pkg, "host"),
-                    os.path.join(pkg, "host", "example_traverse.cpp"), "-L", pkg, "-lxbtrav",
+                    os.path.join(pkg, "host", name + ".cpp"), "-L", pkg, "-lxbtrav",
                     f"-Wl,-rpath,{pkg}", "-o", exe], check=True)
     return exe
+
+
+def test_runner_cli_compiles_and_parses_flags(tmp_path):
+    """xbtrav_run takes the reference runners' gflags-style flags; usage and
+    flag errors need no GPU."""
+    import subprocess
+
+    exe = _build_example(tmp_path, "xbtrav_run")
+    r = subprocess.run([exe, "--help"], capture_output=True, text=True)
+    assert r.returncode == 0 and "--row_offsets" in r.stderr and "--path_buffer_ratio" in r.stderr
+    assert subprocess.run([exe], capture_output=True, text=True).returncode == 2
+    assert subprocess.run([exe, "--rmat=8:4", "--mode=bogus"], capture_output=True, text=True).returncode == 2
+    # a full command line of the reference runner reaches the device step (no GPU here: a clean error)
+    r = subprocess.run([exe, "--dataset=Tiny", "--rmat", "8:4", "--rounds=3", "--num_threads=4",
+                        "--path_buffer_ratio=2", "--max_cuda_sms=0"], capture_output=True, text=True)
+    assert "Run xbtrav (match) on Dataset Tiny" in r.stdout and r.returncode == 1 and "xbtrav error" in r.stderr
 
 
 def test_cpp_host_api_compiles_and_links(tmp_path):

@@ -150,3 +150,35 @@ def test_degenerate_graphs(ctx):
         g.close()
         assert O.check_matching(ro, ci, mate) == 0
         assert int((mate >= 0).sum()) // 2 == want == st["reached"]
+
+
+def test_runner_cli_modes(tmp_path):
+    """xbtrav_run (the reference runners' flags) on a text CSR: match, traverse
+    and sssp summaries agree with the oracle."""
+    import subprocess
+
+    from test_host_abi import _build_example
+
+    exe = _build_example(tmp_path, "xbtrav_run")
+    h = xbtrav.HostCSR.rmat(11, 8, seed=0x5EED)
+    ro, ci = h.arrays()
+    rp, cp = str(tmp_path / "row.txt"), str(tmp_path / "col.txt")
+    h.save_text(rp, cp)
+    h.close()
+
+    def run(*extra):
+        out = subprocess.run([exe, f"--row_offsets={rp}", f"--col_indices={cp}", "--rounds=3", *extra],
+                             capture_output=True, text=True, check=True).stdout
+        return dict(line.split(": ", 1) for line in out.splitlines() if ": " in line)
+
+    kv = run("--mode=match")
+    assert int(kv["Matching Size"]) == O.max_match(ro, ci)[0]
+    assert int(kv["Num of Nodes"]) == len(ro) - 1 and len([k for k in kv if k == "Average runtime"]) == 1
+    src = xbtrav.select_sources_csr(ro, 99, 50)
+    kv = run("--mode=traverse", "--src_count=50", "--seed=99")
+    _, _, edges, reached = O.msbfs(ro, ci, src)
+    assert int(kv["Number of Processed Edges"]) == edges
+    assert int(kv["Reached (source, vertex) pairs"]) == reached
+    kv = run("--mode=sssp", "--src_count=50", "--seed=99", "--weight_max=20")
+    d = O.msssp(ro, ci, xbtrav.symmetric_weights(ro, ci, 99, 1, 20), src)
+    assert int(kv["Reached Vertices"]) == int((d < 3.0e37).sum())
