@@ -48,7 +48,7 @@ typedef int32_t xb_status;
 #define XB_ERR_STATE (-8)    /* object used in the wrong state */
 
 #define XB_MODE_PLAIN 0       /* independent BFS per source */
-#define XB_MODE_ALTERNATING 1 /* reserved: alternating forest over a matching */
+#define XB_MODE_ALTERNATING 1 /* alternating forest of a matching from its exposed vertices */
 
 /* xb_traverse flags */
 #define XB_OUT_DEVICE 1u     /* level/parent are device pointers (else host) */
@@ -194,7 +194,21 @@ xb_status xb_select_sources(const xb_graph* g, uint64_t seed, int32_t k, int32_t
  * the smallest-id neighbour one level closer to the source (the source's own
  * parent is itself; -1 unreached).  Sources are processed 64 (or 32) per
  * word, one word per launch sequence, with a host-side level loop.
- * mode must be XB_MODE_PLAIN; matching and owner must be NULL.
+ * In plain mode matching and owner must be NULL.
+ * XB_MODE_ALTERNATING: the alternating forest of `matching` (n ints, -1 =
+ * exposed) grown from every exposed vertex, the expansion of the reference's
+ * alternating mode (ExpandAlternatingForest, xblossom_gpu_engine_10.cu:270-359;
+ * ExpandTwoNodes records, path_table.h:256-271); sources and k are ignored.
+ * level, parent, owner: n ints each -- exposed vertices level 0 and their own
+ * parent and owner; an inner vertex w at level 2d+1 has parent = its
+ * smallest outer neighbour of level 2d; its mate is outer at level 2d+2 with
+ * parent w; owner = the tree's root; -1 unreached.  When both ends of a
+ * matched pair qualify at one level, the end with the smaller such
+ * neighbour (then the smaller id) is the inner one.  Edges between outer
+ * vertices label nothing.  XB_OUT_DEVICE: matching and the three outputs
+ * are device pointers.  stats.levels = expansion rounds, stats.reached =
+ * labeled vertices (host outputs).  XB_ERR_ARG if matching is not a
+ * matching of the graph.
  * With XB_PARENT_FIFO the parents follow the reference's sequential FIFO
  * search instead (xblossom::Graph::findShortestPath, xgraph.h:155-191): a
  * vertex's parent is the first vertex of the BFS queue adjacent to it, the

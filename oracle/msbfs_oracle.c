@@ -383,3 +383,76 @@ int64_t oracle_max_match(int64_t n, const int64_t *row_offsets, const int32_t *c
   free(S.base); free(S.pred); free(S.queue); free(S.stamp); free(S.outer); free(S.cyc);
   return size / 2;
 }
+
+/* Alternating forest of a matching (the expansion of the reference's
+ * alternating mode, ExpandAlternatingForest in
+ * apps/xb/src/xblsm_gpu/xblossom_gpu_engine_10.cu:270-359 and
+ * ExpandTwoNodes in apps/xb/src/include/path_table/path_table.h:256-271),
+ * grown level by level from every exposed vertex (mate -1), with a
+ * deterministic rule where the reference's claims race:
+ *   level 0: exposed vertices, parent = owner = itself;
+ *   level 2d+1 (inner): an unlabeled matched vertex w next to an outer vertex
+ *     of level 2d; parent = the smallest such neighbour, owner = its owner;
+ *   level 2d+2 (outer): the mate of that inner vertex; parent = the inner.
+ * When both ends of a matched pair qualify at the same level, the end whose
+ * smallest outer neighbour is smaller (then the smaller id) is the inner
+ * one.  Edges between outer vertices (augmenting paths, blossoms) do not
+ * label anything.  Unreached vertices: -1 in all three arrays.  Returns the
+ * number of expansion rounds, or -1 on a bad argument. */
+int64_t oracle_alt_forest(int64_t n, const int64_t *row_offsets, const int32_t *col_indices, const int32_t *mate,
+                          int32_t *level, int32_t *parent, int32_t *owner) {
+  if (n <= 0 || n > INT32_MAX || !row_offsets || !mate || !level || !parent || !owner) return -1;
+  int32_t *front = (int32_t *)malloc(sizeof(int32_t) * (size_t)n);
+  int32_t *next = (int32_t *)malloc(sizeof(int32_t) * (size_t)n);
+  int32_t *cand = (int32_t *)malloc(sizeof(int32_t) * (size_t)n);
+  int32_t *touched = (int32_t *)malloc(sizeof(int32_t) * (size_t)n);
+  if (!front || !next || !cand || !touched) {
+    free(front); free(next); free(cand); free(touched);
+    return -1;
+  }
+  int64_t nf = 0;
+  for (int64_t v = 0; v < n; v++) {
+    cand[v] = INT32_MAX;
+    if (mate[v] < 0) {
+      level[v] = 0;
+      parent[v] = owner[v] = (int32_t)v;
+      front[nf++] = (int32_t)v;
+    } else {
+      level[v] = parent[v] = owner[v] = -1;
+    }
+  }
+  int64_t rounds = 0;
+  for (int32_t d = 0; nf > 0; d++) {
+    rounds++;
+    int64_t nt = 0, nn = 0;
+    for (int64_t i = 0; i < nf; i++) {
+      const int32_t v = front[i];
+      for (int64_t e = row_offsets[v]; e < row_offsets[v + 1]; e++) {
+        const int32_t w = col_indices[e];
+        if (level[w] != -1 || mate[w] < 0) continue;
+        if (cand[w] == INT32_MAX) touched[nt++] = w;
+        if (v < cand[w]) cand[w] = v;
+      }
+    }
+    for (int64_t i = 0; i < nt; i++) {
+      const int32_t w = touched[i], x = mate[w];
+      const int32_t cw = cand[w], cx = cand[x];
+      const int inner = cx == INT32_MAX || cw < cx || (cw == cx && w < x);
+      if (!inner) continue;
+      level[w] = 2 * d + 1;
+      parent[w] = cw;
+      owner[w] = owner[cw];
+      level[x] = 2 * d + 2;
+      parent[x] = w;
+      owner[x] = owner[w];
+      next[nn++] = x;
+    }
+    for (int64_t i = 0; i < nt; i++) cand[touched[i]] = INT32_MAX;
+    int32_t *t = front;
+    front = next;
+    next = t;
+    nf = nn;
+  }
+  free(front); free(next); free(cand); free(touched);
+  return rounds;
+}

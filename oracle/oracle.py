@@ -129,6 +129,25 @@ def max_match(ro, ci, init=None) -> tuple[int, np.ndarray]:
     return int(size), mate
 
 
+def alt_forest(ro, ci, mate) -> tuple[np.ndarray, np.ndarray, np.ndarray, int]:
+    """Alternating forest of a matching from every exposed vertex (level,
+    parent, owner per vertex; -1 unreached) and the number of rounds."""
+    ro = np.ascontiguousarray(ro, dtype=np.int64)
+    ci = np.ascontiguousarray(ci, dtype=np.int32)
+    mate = np.ascontiguousarray(mate, dtype=np.int32)
+    n = len(ro) - 1
+    lv, pr, ow = (np.empty(n, np.int32) for _ in range(3))
+    L = _load()
+    L.oracle_alt_forest.restype = C.c_int64
+    L.oracle_alt_forest.argtypes = [C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                    C.c_void_p]
+    r = L.oracle_alt_forest(n, ro.ctypes.data, ci.ctypes.data if len(ci) else None, mate.ctypes.data,
+                            lv.ctypes.data, pr.ctypes.data, ow.ctypes.data)
+    if r < 0:
+        raise ValueError("oracle_alt_forest rejected its arguments")
+    return lv, pr, ow, int(r)
+
+
 def ref_match_available() -> bool:
     return os.path.exists(MATCH_SO)
 

@@ -647,7 +647,12 @@ xb_status xb_traverse(xb_ctx* c, const xb_graph* gc, const int32_t* sources, int
   if (!c || !g) return fail(XB_ERR_ARG, "null context or graph");
   if (!g->ctx) return fail(XB_ERR_STATE, "the graph's context was destroyed");
   if (g->ctx->device != c->device) return fail(XB_ERR_ARG, "graph lives on another device");
-  if (mode != XB_MODE_PLAIN) return fail(XB_ERR_ARG, "only XB_MODE_PLAIN is supported by xb_traverse");
+  if (mode == XB_MODE_ALTERNATING) {
+    if (st) std::memset(st, 0, sizeof(*st));
+    XB_CUDA(cudaSetDevice(c->device));
+    return xbe::traverse_alternating(c, g, matching, level, parent, owner, flags, st);
+  }
+  if (mode != XB_MODE_PLAIN) return fail(XB_ERR_ARG, "unknown traversal mode");
   if (matching || owner) return fail(XB_ERR_ARG, "matching/owner must be NULL in plain mode");
   if (k < 0) return fail(XB_ERR_ARG, "negative source count");
   if (k > 0 && (!sources || !level || !parent)) return fail(XB_ERR_ARG, "null sources or output tables");

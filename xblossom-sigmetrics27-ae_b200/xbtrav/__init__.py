@@ -518,6 +518,27 @@ class Context:
         _check(lib().xb_multi_sssp(self._h, graph._h, sptr, k, dp, flags, C.byref(st)))
         return dist, st.as_dict()
 
+    def alternating_forest(self, graph: Graph, mate) -> tuple[np.ndarray, np.ndarray, np.ndarray, dict]:
+        """xb_traverse in XB_MODE_ALTERNATING: the alternating forest of the
+        matching `mate` (-1 exposed) from all exposed vertices; numpy (level,
+        parent, owner, stats), or torch CUDA tensors when mate is one."""
+        st = XbStats()
+        if hasattr(mate, "data_ptr"):
+            import torch
+
+            lv, pr, ow = (torch.empty_like(mate) for _ in range(3))
+            torch.cuda.synchronize(mate.device)
+            _check(lib().xb_traverse(self._h, graph._h, None, 0, XB_MODE_ALTERNATING, mate.data_ptr(), lv.data_ptr(),
+                                     pr.data_ptr(), ow.data_ptr(), XB_OUT_DEVICE, C.byref(st)))
+            return lv, pr, ow, st.as_dict()
+        m = np.ascontiguousarray(mate, dtype=np.int32)
+        if m.shape != (graph.n,):
+            raise ValueError(f"mate must have shape ({graph.n},)")
+        lv, pr, ow = (np.empty(graph.n, np.int32) for _ in range(3))
+        _check(lib().xb_traverse(self._h, graph._h, None, 0, XB_MODE_ALTERNATING, m.ctypes.data, lv.ctypes.data,
+                                 pr.ctypes.data, ow.ctypes.data, 0, C.byref(st)))
+        return lv, pr, ow, st.as_dict()
+
     def max_match(self, graph: Graph, init=None, out: str = "host") -> tuple[object, dict]:
         """Maximum-cardinality matching through xb_max_match: (mate, stats),
         mate[v] = -1 for exposed vertices.  init: starting matching (numpy
