@@ -795,8 +795,20 @@ def main() -> None:
 
     # end to end through the C ABI with host buffers (pinned), copies in the timed region
     def e2e_run(batched: bool, steps: int):
-        hl = torch.empty((k, g.n), dtype=torch.int32, pin_memory=True)
-        hp = torch.empty((k, g.n), dtype=torch.int32, pin_memory=True)
+        # every rank takes the same branch: a rank whose page-locked tables
+        # cannot be allocated makes all ranks skip the measurement together
+        # (no rank waits in a collective the others never reach)
+        try:
+            hl = torch.empty((k, g.n), dtype=torch.int32, pin_memory=True)
+            hp = torch.empty((k, g.n), dtype=torch.int32, pin_memory=True)
+            ok = 1.0
+        except Exception:  # noqa: BLE001
+            hl = hp = None
+            ok = 0.0
+        if dist is not None:
+            ok = -max_over_ranks(-ok)  # the minimum over ranks
+        if ok < 1.0:
+            raise RuntimeError("page-locked host tables could not be allocated on every rank")
         hs = torch.from_numpy(sources).pin_memory().numpy()
         ln, pn = hl.numpy(), hp.numpy()
 
