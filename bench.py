@@ -415,7 +415,9 @@ def run_match(args, w, name) -> None:
         cpu = {"value": g.m / secs / 1e9, "unit": "GTEPS", "cores": used, "kind": kind,
                "sample": f"one maximum matching ({secs:.2f} s, size {rsize}), {what}"}
     cfg = workload_config(name, w, info)
-    cfg.update(parallelism="replicas1", path="xb_max_match from the empty matching (host loop over phases and levels)")
+    cfg.update(parallelism="replicas1",
+               path="xb_max_match from the empty matching (host loop over phases, each phase's levels in a "
+                    "captured CUDA-graph WHILE loop)")
     cfg.pop("sources", None)
     last = stats[-1]
     print(json.dumps({
