@@ -75,3 +75,27 @@ def test_int32_by_default(ctx):
     h.close()
     assert g.offset_bytes == 4
     g.close()
+
+
+def test_serving_slots(ctx, wide):
+    """Serving slots (xb_slot_launch / poll) on an int64-offset graph: tables
+    and digests equal the oracle's."""
+    from xbtrav import serve
+
+    g, ro, ci = wide
+    ctx.set_tuning(words=2)
+    srv = serve.Server(ctx, slots=2, reserve_bytes=1 << 30)
+    qs = []
+    for i, k in enumerate([3, 64, 130]):
+        src = g.select_sources(700 + i, k)
+        qs.append((src, srv.submit(g, src, want="tables" if i != 1 else "digest")))
+    srv.drain()
+    for src, q in qs:
+        lv, pr, _, _ = O.msbfs(ro, ci, src, rule=O.RULE_MINID)
+        if q.want == "tables":
+            np.testing.assert_array_equal(q.level.cpu().numpy(), lv)
+            np.testing.assert_array_equal(q.parent.cpu().numpy(), pr)
+        else:
+            from test_serve_gpu import _oracle_digest
+
+            np.testing.assert_array_equal(q.digest, _oracle_digest(lv, pr))
