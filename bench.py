@@ -55,12 +55,16 @@ WORKLOADS = {
     "serve_rmat22": dict(kind="serve", scale=22, ef=16, queries=96, rate=12.0, kmax=4096, slots=4),
     # the default graph with one word of sources: ncu DRAM-traffic captures (about 4 GB on the device)
     "rmat22_k64": dict(kind="rmat", scale=22, ef=16, k=64),
-    # one pass of the default layout (2 words x 64 sources): DRAM-traffic captures
+    # one pass of the two-word layout (2 words x 64 sources): DRAM-traffic captures
     "rmat22_k128": dict(kind="rmat", scale=22, ef=16, k=128),
     # smaller case for kernel profiles (graph > L2, a few hundred MB on the device)
     "rmat20_k64": dict(kind="rmat", scale=20, ef=16, k=64),
-    # one pass of the default layout (2 words x 64 sources) for kernel profiles
+    # one pass of the default layout (4 words x 64 sources) on the default graph: DRAM-traffic captures
+    "rmat22_k256": dict(kind="rmat", scale=22, ef=16, k=256),
+    # one pass of the two-word layout (2 words x 64 sources) for kernel profiles
     "rmat20_k128": dict(kind="rmat", scale=20, ef=16, k=128),
+    # one pass of the default layout (4 words x 64 sources): kernel profiles and DRAM-traffic captures
+    "rmat20_k256": dict(kind="rmat", scale=20, ef=16, k=256),
     # weighted: multi-source SSSP distances (xb_multi_sssp), seeded symmetric int32 weights in [1, 100]
     "msssp_rmat22_k64": dict(kind="sssp", graph="rmat", scale=22, ef=16, k=64, wmin=1, wmax=100),
     "msssp_rmat20_k64": dict(kind="sssp", graph="rmat", scale=20, ef=16, k=64, wmin=1, wmax=100),
@@ -782,7 +786,7 @@ def main() -> None:
     # roofline of the dominant kernel class (its kernels event-timed per class)
     peak, peak_kind = measured_peaks()
     dom = 0 if cls_agg["class_ms"][0] >= cls_agg["class_ms"][1] else 1
-    dom_name = ["level steps (k_pull_lanes / k_pull_heavy / k_pull_hubs; k_pull_tiles for four words; k_push_*)",
+    dom_name = ["level steps (k_pull_lanes / k_pull_heavy / k_pull_hubs; k_push_*)",
                 "table pass (k_tables)"][dom]
     achieved = (cls_agg["class_bytes"][dom] / (cls_agg["class_ms"][dom] / 1e3) / 1e9
                 if cls_agg["class_ms"][dom] > 0 else None)

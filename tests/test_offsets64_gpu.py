@@ -50,7 +50,7 @@ def test_traversal(ctx, wide, words):
         _, prf, _, _ = O.msbfs(ro, ci, src, rule=O.RULE_FIFO)
         np.testing.assert_array_equal(rf.parent, prf)
     finally:
-        ctx.set_tuning(words=2)
+        ctx.set_tuning(words=4)
 
 
 def test_sssp(ctx, wide):
@@ -83,7 +83,7 @@ def test_serving_slots(ctx, wide):
     from xbtrav import serve
 
     g, ro, ci = wide
-    ctx.set_tuning(words=2)
+    ctx.set_tuning(words=4)
     srv = serve.Server(ctx, slots=2, reserve_bytes=1 << 30)
     qs = []
     for i, k in enumerate([3, 64, 130]):

@@ -396,7 +396,7 @@ xb_status xb_ctx_create(int32_t device, xb_ctx** out) {
   XB_CUDA(cudaEventCreate(&c->evc0));
   XB_CUDA(cudaEventCreate(&c->evc1));
   c->tuning.word_bits = 64;
-  c->tuning.words = 2;  // 128 sources per pass: one gather of 16 bytes serves them all
+  c->tuning.words = 4;  // 256 sources per pass: one gather of a whole 32-byte sector serves them all
   // pull unless the frontier's edges are under 1/1024 of the unfinished edges:
   // pull steps record parents as they go, push steps leave them to a search
   c->tuning.pull_alpha = 1024.0f;

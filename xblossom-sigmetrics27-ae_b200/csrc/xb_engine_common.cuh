@@ -380,13 +380,18 @@ int resident_blocks(K kernel, int threads) {
   return std::max(1, b);
 }
 
-// Light vertices pulled one per lane (k_pull_lanes) for up to two words per
-// vertex; wider layouts keep the edge-flat tiles (k_pull_tiles).
+// Light vertices pulled one per lane (k_pull_lanes) for every layout up to
+// four words per vertex; warps per block shrink with the words so the
+// per-warp queues and position-plane columns stay within static shared
+// memory (8 warps up to two words, 4 for four).
 template <int NW>
 constexpr bool pull_by_lanes() {
-  return NW <= 2;
+  return NW <= 4;
 }
-constexpr int kLaneWarps = 8;
+template <int NW>
+constexpr int lane_warps() {
+  return NW <= 2 ? 8 : 4;
+}
 
 template <typename W, int NW, typename OffT>
 xb_status emit_pull(const PassRes<W, NW, OffT>& p, const xb_graph* g, int cur, const StepShape& sh, int kb,
@@ -398,7 +403,7 @@ xb_status emit_pull(const PassRes<W, NW, OffT>& p, const xb_graph* g, int cur, c
   const xbk::Masks<W, NW> active = active_mask<W, NW>(kb);
   if constexpr (pull_by_lanes<NW>()) {
     if (g->n_lorder > 0) {
-      xbk::k_pull_lanes<W, NW, OffT, kLaneWarps><<<sh.pull_grid, kLaneWarps * 32, 0, s>>>(
+      xbk::k_pull_lanes<W, NW, OffT, lane_warps<NW>()><<<sh.pull_grid, lane_warps<NW>() * 32, 0, s>>>(
           g->n_lchunks, g->d_lchunk, g->d_lorder, p.ro, p.ci, F, p.seen, N, p.pl, active, p.heavy, nl, p.ctr, cur,
           p.ppos);
       (*launches)++;
@@ -484,9 +489,10 @@ StepShape max_shape(const xb_graph* g, int sms) {
   sh.finalize_grid = (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)sms * 8));
   if constexpr (pull_by_lanes<NW>()) {
     // persistent: warps take chunks of the light list from a counter
-    static const int lane_res = resident_blocks(xbk::k_pull_lanes<W, NW, OffT, kLaneWarps>, kLaneWarps * 32);
+    constexpr int LW = lane_warps<NW>();
+    static const int lane_res = resident_blocks(xbk::k_pull_lanes<W, NW, OffT, LW>, LW * 32);
     sh.pull_grid = (int)std::max<int64_t>(
-        1, std::min<int64_t>(((int64_t)g->n_lchunks + kLaneWarps - 1) / kLaneWarps, (int64_t)sms * lane_res));
+        1, std::min<int64_t>(((int64_t)g->n_lchunks + LW - 1) / LW, (int64_t)sms * lane_res));
   } else {
     sh.pull_grid = (int)std::max<int64_t>(1, std::min<int64_t>((ntiles + PW - 1) / PW, (int64_t)sms * 8));
   }

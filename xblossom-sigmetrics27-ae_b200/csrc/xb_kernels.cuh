@@ -832,7 +832,7 @@ __device__ __forceinline__ void pull_lane_vertex(bool act, int32_t v, const W (&
 }
 
 template <typename W, int NW, typename OffT, int WARPS>
-__global__ void __launch_bounds__(WARPS * 32, 3) k_pull_lanes(int32_t nchunks, const int32_t* __restrict__ lchunk,
+__global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 3) k_pull_lanes(int32_t nchunks, const int32_t* __restrict__ lchunk,
                                                            const int32_t* __restrict__ lorder,
                                                            const OffT* __restrict__ ro,
                                                            const int32_t* __restrict__ ci, const W* __restrict__ F,
