@@ -393,6 +393,14 @@ constexpr int lane_warps() {
   return NW <= 2 ? 8 : 4;
 }
 
+// Rounds of 32 edges a heavy-pull warp keeps in flight: one at four words
+// per vertex, where the gathered words of a round fill the registers and
+// three blocks per SM (80 registers) beat more rounds at two blocks.
+template <int NW>
+constexpr int heavy_rounds() {
+  return NW == 4 ? 1 : 4;
+}
+
 template <typename W, int NW, typename OffT>
 xb_status emit_pull(const PassRes<W, NW, OffT>& p, const xb_graph* g, int cur, const StepShape& sh, int kb,
                     cudaStream_t s, int64_t* launches) {
@@ -414,7 +422,7 @@ xb_status emit_pull(const PassRes<W, NW, OffT>& p, const xb_graph* g, int cur, c
     (*launches)++;
   }
   if (g->n_heavy > 0) {
-    xbk::k_pull_heavy<W, NW, OffT, 4><<<sh.heavy_grid, 256, 0, s>>>(g->d_heavy, g->n_heavy, p.ro, p.ci, F, p.seen, N,
+    xbk::k_pull_heavy<W, NW, OffT, heavy_rounds<NW>()><<<sh.heavy_grid, 256, 0, s>>>(g->d_heavy, g->n_heavy, p.ro, p.ci, F, p.seen, N,
                                                                     p.pl, active, p.heavy, kHubDegree, nl, p.ctr, cur,
                                                                     p.hpar);
     (*launches)++;
@@ -496,7 +504,7 @@ StepShape max_shape(const xb_graph* g, int sms) {
   } else {
     sh.pull_grid = (int)std::max<int64_t>(1, std::min<int64_t>((ntiles + PW - 1) / PW, (int64_t)sms * 8));
   }
-  static const int heavy_res = resident_blocks(xbk::k_pull_heavy<W, NW, OffT, 4>, 256);
+  static const int heavy_res = resident_blocks(xbk::k_pull_heavy<W, NW, OffT, heavy_rounds<NW>()>, 256);
   sh.heavy_grid = (int)std::max<int64_t>(1, std::min<int64_t>((g->n_heavy + 7) / 8, (int64_t)sms * heavy_res));
   sh.hub_grid = (int)std::max<int64_t>(1, std::min<int64_t>((g->n_hub_items + 7) / 8, (int64_t)sms * 16));
   sh.commit_grid = (int)std::max<int64_t>(1, std::min<int64_t>((g->n_heavy + 255) / 256, (int64_t)sms * 4));

@@ -963,7 +963,7 @@ __device__ __forceinline__ W first_bits(W f, W before, W* grp) {
 // reached bit is its min-id parent; it is stored in hpar[idx*ROW + bit] (ROW =
 // B*NW) for the table pass.  Hubs (degree > hub) are left to k_pull_hubs.
 template <typename W, int NW, typename OffT, int U>
-__global__ void k_pull_heavy(const int32_t* __restrict__ hlist, int32_t nh, const OffT* __restrict__ ro,
+__global__ void __launch_bounds__(256, (NW == 4 ? 3 : 1)) k_pull_heavy(const int32_t* __restrict__ hlist, int32_t nh, const OffT* __restrict__ ro,
                              const int32_t* __restrict__ ci, const W* __restrict__ F, W* seen, W* N,
                              Planes<W, NW> pl, Masks<W, NW> active, int heavy, int hub, Lists nl, Ctrs* ctr,
                              int cur, int32_t* __restrict__ hpar) {
