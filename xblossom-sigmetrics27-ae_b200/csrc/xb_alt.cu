@@ -176,17 +176,10 @@ xb_status traverse_alternating(xb_ctx* c, xb_graph* g, const int32_t* matching, 
   // work: mate copy, 3 output arrays (host output), proposals, two frontiers, touched list, counters
   const size_t ints = (size_t)n * (dev ? 5 : 8);
   const size_t bytes = sizeof(int32_t) * ints + 16 * 256 + sizeof(AltCounters);
-  if (c->ws_bytes < bytes || !c->ws) {
-    if (c->ws) cudaFree(c->ws);
-    c->ws = nullptr;
-    c->ws_bytes = 0;
-    if (cudaMalloc(&c->ws, bytes) != cudaSuccess) {
-      cudaGetLastError();
-      return fail(XB_ERR_OOM, "alternating-mode work allocation failed");
-    }
-    c->ws_bytes = bytes;
+  {
+    const xb_status ws = ensure_scratch(c, bytes, "alternating-mode");
+    if (ws != XB_OK) return ws;
   }
-  c->ws_key[0] = -1;  // the plain path's zero invariants no longer hold in the workspace
   char* p = (char*)c->ws;
   auto take = [&](size_t count) {
     int32_t* r = (int32_t*)p;

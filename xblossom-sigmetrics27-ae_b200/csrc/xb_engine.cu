@@ -69,6 +69,25 @@ xb_status ensure_sources(xb_ctx* c, int64_t k) {
   return XB_OK;
 }
 
+// The context workspace as plain scratch of at least `bytes` for the paths
+// other than the plain traversal (SSSP, matching, alternating mode); they
+// leave the traversal's zero invariants broken, so its next call clears the
+// workspace again.
+xb_status ensure_scratch(xb_ctx* c, size_t bytes, const char* what) {
+  if (c->ws_bytes < bytes || !c->ws) {
+    if (c->ws) cudaFree(c->ws);
+    c->ws = nullptr;
+    c->ws_bytes = 0;
+    if (cudaMalloc(&c->ws, bytes) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(XB_ERR_OOM, std::string(what) + " work allocation of " + std::to_string(bytes) + " bytes failed");
+    }
+    c->ws_bytes = bytes;
+  }
+  c->ws_key[0] = -1;
+  return XB_OK;
+}
+
 xb_status ensure_stage(xb_ctx* c, size_t bytes) {
   if (c->stage_bytes >= bytes) return XB_OK;
   if (c->d_stage) cudaFree(c->d_stage);

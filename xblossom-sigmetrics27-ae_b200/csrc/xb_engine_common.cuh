@@ -205,6 +205,7 @@ inline xb_status end_body(cudaStream_t s, xb_status st) {
   return XB_OK;
 }
 
+xb_status ensure_scratch(xb_ctx* c, size_t bytes, const char* what);
 xb_status traverse_alternating(xb_ctx* c, xb_graph* g, const int32_t* matching, int32_t* level, int32_t* parent,
                                int32_t* owner, uint32_t flags, xb_stats* st);
 

@@ -636,17 +636,10 @@ xb_status xb_max_match(xb_ctx* c, const xb_graph* gc, int32_t* mate, uint32_t fl
   // counters.  Each region is rounded up to 256 bytes.
   const size_t bytes = 256 * 28 + 4 * (size_t)n * 9 + 8 * (size_t)n + 12 * (size_t)cand_cap + 16 * (size_t)n +
                        8 * (size_t)(n / xbp::kTile + 2) + 4 * (size_t)(m / xbp::kChunk + 2) + 256;
-  if (c->ws_bytes < bytes || !c->ws) {
-    if (c->ws) cudaFree(c->ws);
-    c->ws = nullptr;
-    c->ws_bytes = 0;
-    if (cudaMalloc(&c->ws, bytes) != cudaSuccess) {
-      cudaGetLastError();
-      return fail(XB_ERR_OOM, "matching work allocation failed");
-    }
-    c->ws_bytes = bytes;
+  {
+    const xb_status ws = xbe::ensure_scratch(c, bytes, "matching");
+    if (ws != XB_OK) return ws;
   }
-  c->ws_key[0] = -1;  // the traversal's zero invariants no longer hold in the workspace
   char* p = (char*)c->ws;
   MmWork wk;
   wk.st = carve_ints<int32_t>(p, n);

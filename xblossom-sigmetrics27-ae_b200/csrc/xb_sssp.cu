@@ -340,17 +340,10 @@ xb_status xb_multi_sssp(xb_ctx* c, const xb_graph* gc, const int32_t* sources, i
   const int32_t kd = (int32_t)hs.size();
   const int64_t n = g->n;
   const size_t bytes = sizeof(int64_t) * (size_t)sssp_work_words(n, g->m, kd);
-  if (c->ws_bytes < bytes || !c->ws) {
-    if (c->ws) cudaFree(c->ws);
-    c->ws = nullptr;
-    c->ws_bytes = 0;
-    if (cudaMalloc(&c->ws, bytes) != cudaSuccess) {
-      cudaGetLastError();
-      return fail(XB_ERR_OOM, "SSSP work allocation failed");
-    }
-    c->ws_bytes = bytes;
+  {
+    const xb_status ws = xbe::ensure_scratch(c, bytes, "SSSP");
+    if (ws != XB_OK) return ws;
   }
-  c->ws_key[0] = -1;  // the traversal's zero invariants no longer hold in the workspace
   const bool out_dev = (flags & XB_OUT_DEVICE) != 0;
   if (!out_dev) {
     if (c->stage_bytes < sizeof(float) * (size_t)n) {
