@@ -86,7 +86,18 @@ def make_graph(w: dict):
     return xbtrav.HostCSR.er(w["n"], w["pairs"], seed=SEED)
 
 
+def make_graph_cpu(w: dict):
+    """The workload's graph for the CPU arms, rebuilt without the product
+    library (oracle/inputs.py gives the same CSR as make_graph)."""
+    from oracle import inputs
+
+    if w["kind"] == "rmat" or w.get("graph") == "rmat":
+        return inputs.rmat_csr(w["scale"], w["ef"], 0.57, 0.19, 0.19, seed=SEED)
+    return inputs.er_csr(w["n"], w["pairs"], seed=SEED)
+
+
 def workload_config(name: str, w: dict, info: dict) -> dict:
+    """The workload's identity (same keys and values on every arm)."""
     cfg = {"workload": name, "n": info["n"], "m_directed": info["m"], "sources": w["k"], "seed": SEED,
            "l2": "inputs larger than L2 (colIndices > 126 MB); no flush"}
     if w["kind"] == "rmat" or w.get("graph") == "rmat":
@@ -121,7 +132,7 @@ class ClockSampler:
         try:
             self.f = tempfile.TemporaryFile(mode="w+")
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                          "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.f,
                                          stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
@@ -216,13 +227,12 @@ def sssp_cpu(ro, ci, wts, sources, cores):
 
 
 def run_reference_sssp(args, w, name) -> None:
-    csr = make_graph(w)
-    ro, ci = csr.arrays()
-    info = csr.info()
-    import xbtrav
+    from oracle import inputs
 
-    wts = sssp_weights(ro, ci, w)
-    sources = xbtrav.select_sources_csr(ro, SEED + 1, w["k"])
+    ro, ci = make_graph_cpu(w)
+    info = {"n": len(ro) - 1, "m": len(ci)}
+    wts = inputs.symmetric_weights(ro, ci, SEED, w["wmin"], w["wmax"])
+    sources = inputs.select_sources(ro, SEED + 1, w["k"])
     cores = os.cpu_count() or 1
     times = []
     for step in range(args.warmup + args.steps):
@@ -233,7 +243,7 @@ def run_reference_sssp(args, w, name) -> None:
     cfg = workload_config(name, w, info)
     cfg.update(weights=f"symmetric int32 in [{w['wmin']}, {w['wmax']}]")
     print(json.dumps({
-        "impl": "reference", "metric": SSSP_METRIC, "value": value, "unit": "GTEPS", "n_gpus": args.gpus,
+        "impl": "reference", "metric": SSSP_METRIC, "path": "Ligra MultiSSSP (reference CPU code)", "value": value, "unit": "GTEPS", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * sum(times) / len(times),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded generator)", "config": cfg,
@@ -303,10 +313,10 @@ def run_sssp(args, w, name) -> None:
         cpu = {"value": g.m / secs / 1e9, "unit": "GTEPS", "cores": used, "kind": kind,
                "sample": f"one call over all {w['k']} sources ({secs:.2f} s), {what}"}
     cfg = workload_config(name, w, info)
-    cfg.update(weights=f"symmetric int32 in [{w['wmin']}, {w['wmax']}]", parallelism="replicas1",
-               path="xb_multi_sssp (edge-balanced rounds, host loop over rounds)")
+    cfg.update(weights=f"symmetric int32 in [{w['wmin']}, {w['wmax']}]")
     line = {
-        "metric": SSSP_METRIC, "value": value, "unit": "GTEPS", "n_gpus": 1, "steps": args.steps,
+        "metric": SSSP_METRIC, "parallelism": "replicas1",
+        "path": "xb_multi_sssp (edge-balanced rounds, host loop over rounds)", "value": value, "unit": "GTEPS", "n_gpus": 1, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded R-MAT generator, seeded weights)",
         "config": cfg,
@@ -342,9 +352,8 @@ def match_cpu(ro, ci, cores):
 
 
 def run_reference_match(args, w, name) -> None:
-    csr = make_graph(w)
-    ro, ci = csr.arrays()
-    info = csr.info()
+    ro, ci = make_graph_cpu(w)
+    info = {"n": len(ro) - 1, "m": len(ci)}
     cores = os.cpu_count() or 1
     times = []
     for step in range(args.warmup + args.steps):
@@ -419,13 +428,11 @@ def run_match(args, w, name) -> None:
         cpu = {"value": g.m / secs / 1e9, "unit": "GTEPS", "cores": used, "kind": kind,
                "sample": f"one maximum matching ({secs:.2f} s, size {rsize}), {what}"}
     cfg = workload_config(name, w, info)
-    cfg.update(parallelism="replicas1",
-               path="xb_max_match from the empty matching (host loop over phases, each phase's levels in a "
-                    "captured CUDA-graph WHILE loop)")
-    cfg.pop("sources", None)
     last = stats[-1]
     print(json.dumps({
-        "metric": MATCH_METRIC, "value": value, "unit": "GTEPS", "n_gpus": 1, "steps": args.steps,
+        "metric": MATCH_METRIC, "parallelism": "replicas1",
+        "path": "xb_max_match from the empty matching (host loop over phases, each phase's levels in a "
+                "captured CUDA-graph WHILE loop)", "value": value, "unit": "GTEPS", "n_gpus": 1, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded R-MAT generator)", "config": cfg,
         "matching_size": size, "phases": last["batches"], "levels": last["levels"],
@@ -454,21 +461,20 @@ def run_reference(args, w, name) -> None:
     if w["kind"] == "match":
         run_reference_match(args, w, name)
         return
-    from oracle import oracle
+    from oracle import inputs, oracle
 
     t_gen = time.perf_counter()
-    csr = make_graph(w)
-    ro, ci = csr.arrays()
-    info = csr.info()
-    import xbtrav
-
-    sources = xbtrav.select_sources_csr(ro, SEED + 1, w["k"])
+    ro, ci = make_graph_cpu(w)
+    info = {"n": len(ro) - 1, "m": len(ci)}
+    sources = inputs.select_sources(ro, SEED + 1, w["k"])
     cores = os.cpu_count() or 1
     use_ligra = oracle.ligra_available()
-    per_step = 8 if w["kind"] == "rmat" and w.get("scale", 0) >= 20 else min(w["k"], 64)
+    # a bounded sample of the workload's sources per step (the whole run stays
+    # within a few minutes); consecutive steps take consecutive slices
+    per_step = min(w["k"], 64)
     times, edges = [], []
     for step in range(args.warmup + args.steps):
-        sel = sources[(step * per_step) % len(sources):][:per_step]
+        sel = np.roll(sources, -step * per_step)[:per_step]
         if use_ligra:
             _, secs, e = oracle.ligra_bfs(ro, ci, sel, threads=cores, want_parents=False)
         else:
@@ -488,8 +494,10 @@ def run_reference(args, w, name) -> None:
         "ms_per_step": 1000.0 * sum(times) / len(times), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded generator)",
         "config": workload_config(name, w, info),
+        "path": what,
         "cpu_baseline": {"value": value, "unit": "GTEPS", "cores": cores, "kind": kind,
-                         "sample": f"{per_step} sources per step, {what}"},
+                         "sample": f"{per_step} of the workload's {w['k']} sources per step (consecutive slices), "
+                                   f"{what}; inputs rebuilt in numpy (oracle/inputs.py)"},
         "e2e": {"value": value, "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "setup_s": time.perf_counter() - t_gen,
     }
@@ -568,8 +576,8 @@ def run_multi(args, w, name) -> None:
         "dtype": "u64", "data": "synthetic (seeded R-MAT generator)",
         "config": {"workload": name, "instances": len(specs), "sources": int(sum(s[2] for s in specs)),
                    "vertices": int(sum(g.n for g in graphs)), "m_directed": int(sum(g.m for g in graphs)),
-                   "seed": SEED, "layout": "one concatenated CSR, per-instance offsets (xb_graph_upload_batch)",
-                   "path": f"xb_traverse_batched, {tun['chains']} chains"},
+                   "seed": SEED, "layout": "one concatenated CSR, per-instance offsets (xb_graph_upload_batch)"},
+        "path": f"xb_traverse_batched, {tun['chains']} chains",
         "batched_gteps": value, "plain_gteps": plain_v, "batched_over_plain": value / plain_v,
         "plain_ms_per_step": p_ms / args.steps, "clocks": clk, "setup_s": setup_s,
     }
@@ -620,8 +628,8 @@ def run_serve(args, w, name) -> None:
         "config": {"workload": name, "n": info["n"], "m_directed": info["m"], "seed": SEED,
                    "graph": f"rmat scale {w['scale']} ef {w['ef']} a/b/c/d .57/.19/.19/.05",
                    "queries": len(trace), "sources_total": int(sum(ks)), "k_range": [1, w["kmax"]],
-                   "arrival_rate_per_s": w["rate"], "slots": slots, "result": "per-source digests",
-                   "path": "xbtrav.serve.Server over xb_slot_launch (continuous batching)"},
+                   "arrival_rate_per_s": w["rate"], "slots": slots, "result": "per-source digests"},
+        "path": "xbtrav.serve.Server over xb_slot_launch (continuous batching)",
         "latency_ms": {"p50": out["p50_ms"], "p99": out["p99_ms"], "mean": out["mean_ms"], "max": out["max_ms"]},
         "passes": out["passes"], "trace_seconds": out["seconds"], "clocks": clk, "setup_s": setup_s,
     }
@@ -629,6 +637,47 @@ def run_serve(args, w, name) -> None:
     ctx.slots_release()
     g.close()
     ctx.close()
+
+
+SERVE_LEG = dict(queries=48, rate=12.0, kmax=4096, slots=4)
+
+
+def serve_leg(ctx, g, dev, rank, dist, max_over_ranks, sum_over_ranks, barrier) -> dict:
+    """Serving on the headline's resident graph: seeded Poisson arrivals (rate
+    12/s), 1..4096 sources per query (log-uniform), digests, continuous
+    batching over 4 slots of one 64-source word each (xbtrav.serve).  Latency
+    = arrival to the query's last digest; p50/p99 are the largest over ranks,
+    throughput the sum of the ranks' processed edges over the longest trace."""
+    from xbtrav import replicas, serve
+
+    ctx.set_tuning(words=1)
+    srv = serve.Server(ctx, slots=SERVE_LEG["slots"])
+    for s in range(SERVE_LEG["slots"]):  # warm-up: capture each slot's one-pass graph
+        srv.submit(g, g.select_sources(SEED + 99 + s, srv.rows_per_pass), want="digest")
+    srv.drain()
+    srv.completed.clear()
+    srv.edges = 0
+    srv.passes = 0
+    trace = serve.poisson_trace([g], SERVE_LEG["rate"], SERVE_LEG["queries"],
+                                replicas.rank_seed(SEED + 3, rank), kmax=SERVE_LEG["kmax"])
+    barrier()
+    clocks = ClockSampler(dev.index)
+    clocks.start()
+    out = srv.run_trace(trace)
+    clk = clocks.stop()
+    barrier()
+    ctx.slots_release()
+    secs = max_over_ranks(out["seconds"])
+    edges = sum_over_ranks(srv.edges)
+    return {
+        "latency_ms": {"p50": max_over_ranks(out["p50_ms"]), "p99": max_over_ranks(out["p99_ms"]),
+                       "mean": max_over_ranks(out["mean_ms"]), "max": max_over_ranks(out["max_ms"])},
+        "gteps": edges / secs / 1e9, "trace_seconds": secs, "queries": len(trace),
+        "sources_total": int(sum(len(t[2]) for t in trace)), "arrival_rate_per_s": SERVE_LEG["rate"],
+        "k_range": [1, SERVE_LEG["kmax"]], "slots": SERVE_LEG["slots"], "sources_per_pass": srv.rows_per_pass,
+        "passes": out["passes"], "result": "per-source digests", "clocks": clk,
+        "path": "xbtrav.serve.Server over xb_slot_launch (continuous batching, admission by free HBM)",
+    }
 
 
 def main() -> None:
@@ -645,6 +694,7 @@ def main() -> None:
                     help="time the plain path only (short runs for kernel profiles)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving (latency) leg")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     w = WORKLOADS[args.workload]
@@ -775,9 +825,13 @@ def main() -> None:
         args.path = "plain"
         b_ms, b_agg, clk = plain_ms, plain_agg, {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["not sampled"]}
     else:
+        # clocks sampled from the warm-up on: the timed region alone is shorter
+        # than a few sampling periods
+        clocks.start()
         for _ in range(args.warmup):
             batched_step()
-        b_ms, b_agg, clk = timed(batched_step, args.steps, clocks)
+        b_ms, b_agg, _ = timed(batched_step, args.steps)
+        clk = clocks.stop()
     edges_total = sum_over_ranks(b_agg["edges_traversed"])
     value = edges_total / (b_ms / 1e3) / 1e9
     headline = value if args.path == "batched" else plain_gteps
@@ -838,21 +892,29 @@ def main() -> None:
     e2e = None
     if not args.no_e2e:
         try:
-            e2e_steps = max(1, min(args.steps, 3))
+            e2e_steps = args.steps
             e2e = {"value": e2e_run(args.path == "batched", e2e_steps), "unit": "GTEPS",
                    "h2d_bytes_per_step": 4 * k, "d2h_bytes_per_step": 8 * k * g.n, "steps": e2e_steps,
                    "note": ("xb_traverse_batched" if args.path == "batched" else "xb_traverse") +
                            " with a host source list and page-locked host level/parent tables; graph resident"}
-            e2e["plain_value"] = e2e_run(False, 1) if args.path == "batched" else e2e["value"]
+            e2e["plain_value"] = e2e_run(False, e2e_steps) if args.path == "batched" else e2e["value"]
         except Exception as ex:  # noqa: BLE001
             e2e = {"value": None, "unit": "GTEPS", "error": str(ex)[:200]}
+
+    # the latency half of the metric: a seeded Poisson trace of queries served
+    # on the same resident graph with continuous batching over slots
+    tun = ctx.tuning()
+    serving = None
+    if not args.plain_only and not args.no_serve:
+        del level, parent
+        torch.cuda.empty_cache()
+        serving = serve_leg(ctx, g, dev, rank, dist, max_over_ranks, sum_over_ranks, barrier)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_port(ro, ci, sources)
 
     if rank == 0:
-        tun = ctx.tuning()
         path_desc = (f"xb_traverse_batched (one CUDA-graph launch per step, device level loop, "
                      f"{tun['chains']} chains, {tun['word_bits']} sources per word x {tun['words']})"
                      if args.path == "batched" else "xb_traverse (host level loop, one word per launch sequence)")
@@ -862,12 +924,14 @@ def main() -> None:
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
             "data": "synthetic (seeded R-MAT / uniform generator)",
-            "config": dict(workload_config(args.workload, w, info), parallelism=f"replicas{world}", path=path_desc),
+            "config": workload_config(args.workload, w, info),
+            "parallelism": f"replicas{world}", "path": path_desc,
             "batched_gteps": value, "plain_gteps": plain_gteps, "batched_over_plain": value / plain_gteps,
             "plain_one_word_gteps": plain_word_gteps, "batched_over_plain_one_word": value / plain_word_gteps,
             "plain_ms_per_step": plain_ms / args.steps,
             "undirected_gteps": headline / 2,
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
+            "latency_ms": serving["latency_ms"] if serving else None, "serving": serving,
             "gpu_launches": sum(agg["class_launches"]),
             "levels": agg["levels"], "push_levels_per_step": agg["push_levels"] / args.steps,
             "pull_levels_per_step": agg["pull_levels"] / args.steps, "setup_s": setup_s,

@@ -34,7 +34,7 @@
 extern "C" {
 #endif
 
-#define XB_ABI_VERSION 1
+#define XB_ABI_VERSION 2
 
 typedef int32_t xb_status;
 #define XB_OK 0
@@ -92,6 +92,17 @@ typedef struct xb_tuning {
   int32_t timing;          /* 1 = record per-class CUDA events into xb_stats */
   int32_t chains;          /* xb_traverse_batched: passes in flight at once, each with its
                               own workspace (1..16; 0 = default 4) */
+  /* Limits for exercising the error paths without faulting anything (0 =
+   * off, the default).  level_cap: a pass whose frontier is still alive at
+   * this level stops there, as a pass beyond the structural bound (levels <
+   * 2^planes, which a correct traversal never reaches) does, and the call
+   * returns XB_ERR_STATE.  workspace_cap: a working-memory allocation of the
+   * traversal paths (plain workspace and staging, batched chain workspaces,
+   * serving slot workspaces, SSSP / matching scratch) above this many bytes
+   * fails with XB_ERR_OOM before cudaMalloc is called. */
+  int32_t level_cap;
+  int32_t pad;
+  int64_t workspace_cap;
 } xb_tuning;
 
 /* ---- status ------------------------------------------------------------ */
@@ -192,8 +203,10 @@ xb_status xb_select_sources(const xb_graph* g, uint64_t seed, int32_t k, int32_t
 /* Plain per-call path (the drop-in).  k sources; level and parent receive
  * k*n int32 each, source-major.  level = hop distance (-1 unreached); parent =
  * the smallest-id neighbour one level closer to the source (the source's own
- * parent is itself; -1 unreached).  Sources are processed 64 (or 32) per
- * word, one word per launch sequence, with a host-side level loop.
+ * parent is itself; -1 unreached).  Sources are processed in passes of
+ * tuning.word_bits * tuning.words sources (64-bit words, four per vertex by
+ * default: 256 sources per pass), one pass per launch sequence, with a
+ * host-side level loop.
  * In plain mode matching and owner must be NULL.
  * XB_MODE_ALTERNATING: the alternating forest of `matching` (n ints, -1 =
  * exposed) grown from every exposed vertex, the expansion of the reference's
@@ -256,12 +269,17 @@ xb_status xb_traverse_batched(xb_ctx* ctx, const xb_batch_item* items, int32_t n
 
 /* ---- serving slots ------------------------------------------------------ */
 /* Summary of one source's tables, for serving clients that need no full
- * tables: reached = vertices with level >= 0, level_sum and parent_sum over
- * them, depth = the largest level. */
+ * tables: reached = vertices with level >= 0, level_sum over them, depth =
+ * the largest level, and row_hash = the wrapping 64-bit sum over reached
+ * vertices v of h(v, level[v], parent[v]), where h is the splitmix64
+ * finalizer of (v * 0x9E3779B97F4A7C15) XOR ((uint32 level << 32) | uint32
+ * parent) -- position-sensitive (a parent moved between vertices changes it)
+ * and independent of the order the entries are summed in.  Stored as the
+ * int64 with the same bits. */
 typedef struct xb_row_digest {
   int64_t reached;
   int64_t level_sum;
-  int64_t parent_sum;
+  int64_t row_hash;
   int32_t depth; /* -1 for a row written to a caller buffer (no digest taken) */
   int32_t pad;
 } xb_row_digest;
@@ -337,9 +355,13 @@ xb_status xb_max_match(xb_ctx* ctx, const xb_graph* g, int32_t* mate, uint32_t f
  * about 32 MiB compiled into the library, held by every GPU that loads the
  * library until exit; graphs above XB_NOALLOC_MAX_VERTICES vertices are
  * rejected with XB_ERR_CAPACITY.  The first call on a device looks up the
- * array's address (do it before any stream capture on that device).  Calls
- * share the array: calls that overlap on the GPU race and must be
- * serialised by the caller.  stats may be NULL. */
+ * array's address (do it before any stream capture on that device); the
+ * address is kept per device context, so after cudaDeviceReset the next call
+ * looks it up again.  Every call first checks the CSR and the sources on the
+ * device (one read of row_offsets, col_indices and sources, two short host
+ * waits) before it traverses.  Calls share the array: calls that overlap on
+ * the GPU race and must be serialised by the caller; a call that fails after
+ * queuing work waits for that work before it returns.  stats may be NULL. */
 #define XB_NOALLOC_MAX_VERTICES 131072
 xb_status xb_traverse_noalloc(int64_t n, const int32_t* row_offsets, const int32_t* col_indices,
                               const int32_t* sources, int32_t k, int32_t* level, int32_t* parent,

@@ -31,10 +31,11 @@ _xg = None
 
 
 def build(ref_root: str | None = None) -> None:
-    """Builds the C restatement, and the reference checkers when the reference tree exists."""
+    """Builds the C restatement, and the reference checkers when a reference
+    checkout is given (ref_root, else the XB_REF_ROOT environment variable)."""
     subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
-    root = ref_root or "/root/reference"
-    if os.path.isdir(os.path.join(root, "apps")):
+    root = ref_root or os.environ.get("XB_REF_ROOT", "")
+    if root and os.path.isdir(os.path.join(root, "apps")):
         subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF_ROOT={root}"], check=True)
 
 
@@ -266,3 +267,36 @@ def xgraph_paths(ro, ci, src: np.ndarray, dst: np.ndarray):
     if rc != 0:
         raise ValueError("xgraph_ref_paths rejected its arguments")
     return lv, pr
+
+
+def row_entry_hash(v: np.ndarray, level: np.ndarray, parent: np.ndarray) -> np.ndarray:
+    """Hash of (vertex, level, parent) entries as the serving digests define
+    it: the splitmix64 finalizer of (v * 0x9E3779B97F4A7C15) XOR ((uint32 level
+    << 32) | uint32 parent), as uint64."""
+    with np.errstate(over="ignore"):
+        z = v.astype(np.uint64) * np.uint64(0x9E3779B97F4A7C15)
+        z ^= (level.astype(np.int64).astype(np.uint64) & np.uint64(0xFFFFFFFF)) << np.uint64(32)
+        z ^= parent.astype(np.int64).astype(np.uint64) & np.uint64(0xFFFFFFFF)
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        return z ^ (z >> np.uint64(31))
+
+
+def row_digests(level: np.ndarray, parent: np.ndarray) -> np.ndarray:
+    """Serving digests of (k, n) level / parent tables: int64 (k, 4) rows of
+    reached, level sum, row hash (wrapping sum of row_entry_hash over reached
+    vertices, as the int64 with the same bits) and depth."""
+    level = np.atleast_2d(level)
+    parent = np.atleast_2d(parent)
+    k, n = level.shape
+    out = np.zeros((k, 4), np.int64)
+    v = np.arange(n, dtype=np.int64)
+    for r in range(k):
+        m = level[r] >= 0
+        h = row_entry_hash(v[m], level[r][m], parent[r][m])
+        with np.errstate(over="ignore"):
+            out[r, 2] = np.sum(h, dtype=np.uint64).astype(np.int64)
+        out[r, 0] = int(m.sum())
+        out[r, 1] = int(level[r][m].astype(np.int64).sum())
+        out[r, 3] = int(level[r][m].max()) if m.any() else -1
+    return out

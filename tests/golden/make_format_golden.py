@@ -1,7 +1,7 @@
 """Generates the format fixtures (tests/golden/formats_*) with the reference's
 own converters and readers.  Run where the reference tree is mounted:
 
-    python tests/golden/make_format_golden.py [reference root]
+    python tests/golden/make_format_golden.py <reference root>
 
 The fixture graph is R-MAT scale 7 / ef 4 from the product's generator,
 stored in the reference's text CSR format (formats_rmat7_rowOffsets.txt,
@@ -31,7 +31,9 @@ sys.path.insert(0, os.path.join(ROOT, "xblossom-sigmetrics27-ae_b200"))
 import xbtrav  # noqa: E402
 
 OUT = os.path.dirname(os.path.abspath(__file__))
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) < 2:
+    sys.exit("usage: make_format_golden.py <reference checkout>")
+REF = sys.argv[1]
 
 TRICKY = """# source list with the forms the experiment scripts accept
    # indented comment line

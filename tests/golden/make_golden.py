@@ -3,7 +3,7 @@
 Run where the reference tree is mounted (it builds oracle/_ref/ from the
 reference sources first):
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py <reference root>
 
 For every fixture graph it records
   ro, ci, sources                          the input (int64 / int32 CSR)
@@ -94,7 +94,9 @@ def fixtures():
 
 
 def main() -> None:
-    O.build()
+    if len(sys.argv) < 2:
+        sys.exit("usage: make_golden.py <reference root>")
+    O.build(sys.argv[1])
     assert O.ligra_available() and O.xgraph_available(), "reference checkers were not built"
     for name, (ro, ci, src) in fixtures().items():
         n, k = len(ro) - 1, len(src)

@@ -18,6 +18,7 @@ LAYOUTS = [
     dict(word_bits=32, words=1),
     dict(word_bits=64, words=2),
     dict(word_bits=32, words=4),
+    dict(word_bits=64, words=4),  # the default layout (256 sources per pass)
 ]
 
 

@@ -9,9 +9,14 @@ edge 6-7 its AddAugmentingPath(6, 7) flips.  Tree 1's flip result is pinned
 exactly (the reference test's EXPECT_EQs; that maximum matching is unique).
 Trees 2-5 have one exposed vertex, so their matching is already maximum;
 each is also run with a pendant exposed vertex on an inner vertex of a
-blossom, which forces an augmenting path around the blossom.  The
-reference's root distances belong to its path-table layout, which this
-engine does not keep (its forest stores pred / blossom base instead)."""
+blossom, which forces an augmenting path around the blossom.
+
+The same trees also pin the alternating mode (xb_traverse with
+XB_MODE_ALTERNATING): grown from the exposed vertex 0 over the tree edges
+alone, each outer vertex x of ExpandTwoNodes(v, w, x) is labeled at the level
+equal to the reference's root_distance[x] (the EXPECT_EQs at
+path_table_test.cu:93-96, 149-156, 192-194, 224-227, 257-260), w at that
+level minus one, with parent[w] = v, parent[x] = w and owner 0."""
 import numpy as np
 import pytest
 
@@ -31,6 +36,59 @@ TREES = {
 PENDANT_AT = {2: 9, 3: 3, 4: 5, 5: 3}
 # tree 1 after AddAugmentingPath(6, 7): the reference test's expectations
 GOLDEN_1 = {0: 3, 3: 0, 1: 2, 2: 1, 4: 5, 5: 4, 6: 7, 7: 6}
+
+
+# root_distance expectations of the reference test, per tree
+ROOT_DISTANCE = {
+    1: {0: 0, 2: 2, 4: 2, 6: 4},
+    2: {0: 0, 2: 2, 4: 4, 6: 4, 8: 6, 10: 8, 12: 8, 18: 8},
+    3: {0: 0, 2: 2, 4: 4},
+    4: {0: 0, 2: 2, 4: 4, 6: 4},
+    5: {0: 0, 2: 2, 4: 4, 6: 2},
+}
+
+
+def tree_only_case(t):
+    """The tree of ExpandTwoNodes calls alone: edges v-w and w-x, matching
+    w-x, vertex 0 the exposed root."""
+    n, expands, _ = TREES[t]
+    pairs = [(v, w) for v, w, _ in expands] + [(w, x) for _, w, x in expands]
+    mate = np.full(n, -1, np.int32)
+    for _, w, x in expands:
+        mate[w], mate[x] = x, w
+    ro, ci = _csr(n, pairs)
+    return n, ro, ci, mate
+
+
+def _check_root_distances(t, level, parent, owner):
+    for x, d in ROOT_DISTANCE[t].items():
+        assert level[x] == d, (t, x, level[x], d)
+    for v, w, x in TREES[t][1]:
+        assert level[w] == level[v] + 1 and level[x] == level[w] + 1, (t, v, w, x)
+        assert parent[w] == v and parent[x] == w, (t, v, w, x)
+        assert owner[w] == 0 and owner[x] == 0
+    assert level[0] == 0 and parent[0] == 0 and owner[0] == 0
+
+
+@pytest.mark.parametrize("t", [1, 2, 3, 4, 5])
+def test_oracle_alternating_forest_root_distances(t):
+    n, ro, ci, mate = tree_only_case(t)
+    level, parent, owner, _ = O.alt_forest(ro, ci, mate)
+    _check_root_distances(t, level, parent, owner)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("t", [1, 2, 3, 4, 5])
+def test_gpu_alternating_forest_root_distances(ctx, t):
+    n, ro, ci, mate = tree_only_case(t)
+    g = ctx.upload_arrays(ro, ci)
+    level, parent, owner, _ = ctx.alternating_forest(g, mate)
+    g.close()
+    _check_root_distances(t, level, parent, owner)
+    lv_o, pr_o, ow_o, _ = O.alt_forest(ro, ci, mate)
+    np.testing.assert_array_equal(level, lv_o)
+    np.testing.assert_array_equal(parent, pr_o)
+    np.testing.assert_array_equal(owner, ow_o)
 
 
 def tree_case(t, pendant=False):

@@ -22,9 +22,9 @@ def _tune(ctx, **kw):
 
 
 def _oracle_digest(lv, pr):
-    m = lv >= 0
-    return np.stack([m.sum(1), np.where(m, lv, 0).sum(1), np.where(m, pr.astype(np.int64), 0).sum(1),
-                     np.where(m, lv, -1).max(1)], axis=1).astype(np.int64)
+    """Digests of the oracle's tables: reached, level sum, position-sensitive
+    row hash, depth (xb_row_digest)."""
+    return O.row_digests(lv, pr)
 
 
 @pytest.fixture(scope="module")
@@ -126,3 +126,28 @@ def test_slot_api_errors(ctx, graphs):
     np.testing.assert_array_equal(dig, _oracle_digest(lv, pr))
     ctx.slots_release()
     g.close()
+
+
+def test_digests_on_a_larger_graph_match_the_oracle():
+    """R-MAT 20 (hubs above degree 4096) at the default four-word layout:
+    digest-only queries of ragged sizes, submitted while earlier ones run;
+    every row's digest (with its position-sensitive row hash) equals the
+    digest of the oracle's tables."""
+    csr = xbtrav.HostCSR.rmat(20, 16, seed=0x5EED + 20)
+    ro, ci = csr.arrays()
+    c = xbtrav.Context(0)
+    g = c.upload(csr)
+    srv = serve.Server(c, slots=3, reserve_bytes=1 << 30)
+    qs = []
+    for i, k in enumerate((1, 37, 130, 5, 64)):
+        src = g.select_sources(4000 + i, k)
+        qs.append((src, srv.submit(g, src, want="digest")))
+        srv.step()
+    srv.drain()
+    for src, q in qs:
+        assert q.done
+        lv, pr, _, _ = O.msbfs(ro, ci, src)
+        np.testing.assert_array_equal(q.digest, _oracle_digest(lv, pr))
+    c.slots_release()
+    g.close()
+    c.close()

@@ -101,6 +101,7 @@ struct BatchState {
   uint64_t gen = 1;  // bumped whenever a buffer a cached graph points at is reallocated
   uint64_t tick = 0;
   std::vector<CachedGraph> cache;
+  int level_bound = 0;  // of the pass being captured (xbe::level_bound)
 };
 
 namespace {
@@ -171,7 +172,7 @@ xb_status capture_step(BatchState* bs, const PassRes<W, NW, OffT>& p, const xb_g
   cudaGraphConditionalHandle hsw;
   xb_status st = make_handle(b0, 2, cudaGraphCondAssignDefault, &hsw);
   if (st != XB_OK) return st;
-  xbk::k_step_begin<<<1, 1, 0, b0>>>(p.ctr, cur, alpha, p.nplanes_alloc, 1, hsw);
+  xbk::k_step_begin<<<1, 1, 0, b0>>>(p.ctr, cur, alpha, p.nplanes_alloc, bs->level_bound, 1, hsw);
   xbk::k_zero_plane<W><<<(int)std::max<int64_t>(1, std::min<int64_t>((p.n * NW + 255) / 256, (int64_t)sms * 8)), 256,
                          0, b0>>>(p.pl.ph, p.pl.stride, p.n * NW, p.ctr);
   XB_LAUNCH_CHECK("step control");
@@ -221,6 +222,7 @@ xb_status capture_pass_levels(xb_ctx* c, BatchState* bs, const PassRes<W, NW, Of
   const int sms = c->num_sms;
   const float alpha = c->tuning.pull_alpha > 0 ? c->tuning.pull_alpha : 1024.0f;
   const StepShape sh = graph_shape<W, NW, OffT>(g, sms);
+  bs->level_bound = level_bound(c, p.nplanes_alloc);
   xb_status st = emit_pass_init<W, NW, OffT>(p, g, src, kb, s, sms, true);
   if (st != XB_OK) return st;
   return capture_level_loop<W, NW, OffT>(bs, p, g, kb, alpha, sh, s, sms);
@@ -238,7 +240,7 @@ xb_status capture_pass_tables(xb_ctx* c, const PassRes<W, NW, OffT>& p, const xb
   const int words = (kb + B - 1) / B;
   const int fixed_k = hv + 2 + words * hv + 1 + 1;  // fill, init x2, heavy scans, tables, accumulate
   const int push_k = 2 + 2 * hv;
-  const int pull_k = 2 + hv + (g->n_hub_items > 0 ? 2 : 0);
+  const int pull_k = 2 + 2 * hv + (g->n_hub_items > 0 ? 2 : 0);
   xbk::k_pass_accum<<<1, 1, 0, s>>>(p.ctr, sum, (long long)g->n, kb, (int)sizeof(OffT) * 2, (int)sizeof(W), NW,
                                     fixed_k, push_k, pull_k);
   XB_LAUNCH_CHECK("pass accumulate");
@@ -429,7 +431,8 @@ xb_status run_batched(xb_ctx* c, const std::vector<xb_batch_item>& items, const 
     }
     Chain& ch = bs->chains[ci];
     size_t cap = ch.ws_bytes;
-    st = grow(&ch.ws, &cap, ws, &bs->gen, "chain workspace");
+    st = (cap < ws || !ch.ws) ? check_workspace_cap(c, ws, "chain workspace") : XB_OK;
+    if (st == XB_OK) st = grow(&ch.ws, &cap, ws, &bs->gen, "chain workspace");
     ch.ws_bytes = cap;
     if (st != XB_OK) return st;
     if (!ch.ctr) {
@@ -516,7 +519,8 @@ xb_status run_batched(xb_ctx* c, const std::vector<xb_batch_item>& items, const 
                                (uint64_t)heavy,
                                0,
                                (uint64_t)nch,
-                               (uint64_t)items.size()};
+                               (uint64_t)items.size(),
+                               (uint64_t)c->tuning.level_cap};
   {
     uint32_t abits = 0;
     std::memcpy(&abits, &c->tuning.pull_alpha, sizeof(abits));
@@ -695,7 +699,9 @@ xb_status slot_launch(xb_ctx* c, int slot, xb_graph* g, const int32_t* sources, 
   if (st != XB_OK) return st;
   // resources for this graph
   size_t cap = sl.ws_bytes;
-  st = grow(&sl.ws, &cap, layout_for(g->n, (int)sizeof(W), NW).total, &sl.gen, "slot workspace");
+  const size_t slot_ws = layout_for(g->n, (int)sizeof(W), NW).total;
+  st = (cap < slot_ws || !sl.ws) ? check_workspace_cap(c, slot_ws, "slot workspace") : XB_OK;
+  if (st == XB_OK) st = grow(&sl.ws, &cap, layout_for(g->n, (int)sizeof(W), NW).total, &sl.gen, "slot workspace");
   sl.ws_bytes = cap;
   if (st != XB_OK) return st;
   cap = sl.hpar_bytes;
@@ -738,7 +744,7 @@ xb_status slot_launch(xb_ctx* c, int slot, xb_graph* g, const int32_t* sources, 
   uint32_t abits = 0;
   std::memcpy(&abits, &c->tuning.pull_alpha, sizeof(abits));
   const std::vector<uint64_t> key = {sl.gen, (uint64_t)(uintptr_t)g, g->version, (uint64_t)kb, sizeof(W), NW,
-                                     (uint64_t)heavy, abits};
+                                     (uint64_t)heavy, abits, (uint64_t)c->tuning.level_cap};
   CachedGraph* hit = nullptr;
   for (auto& e : sl.cache)
     if (e.key == key) hit = &e;
@@ -803,7 +809,7 @@ xb_status slot_collect(SlotState& sl, xb_stats* stats, xb_row_digest* digests) {
       const xbk::RowDigest& d = sl.h_dig[j];
       digests[j].reached = (int64_t)d.reached;
       digests[j].level_sum = (int64_t)d.level_sum;
-      digests[j].parent_sum = (int64_t)d.parent_sum;
+      digests[j].row_hash = (int64_t)d.row_hash;
       digests[j].depth = sl.h_flags[j] ? (int32_t)d.depth : -1;
       digests[j].pad = 0;
     }

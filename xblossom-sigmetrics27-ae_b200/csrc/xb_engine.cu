@@ -39,6 +39,8 @@ xb_status ensure_workspace(xb_ctx* c, const WsLayout& L, int64_t n, int wbytes, 
     }
     return XB_OK;
   }
+  xb_status cs = check_workspace_cap(c, L.total, "traversal workspace");
+  if (cs != XB_OK) return cs;
   std::memcpy(c->ws_key, key, sizeof(key));
   if (c->ws) {
     cudaFree(c->ws);
@@ -75,6 +77,8 @@ xb_status ensure_sources(xb_ctx* c, int64_t k) {
 // workspace again.
 xb_status ensure_scratch(xb_ctx* c, size_t bytes, const char* what) {
   if (c->ws_bytes < bytes || !c->ws) {
+    const xb_status cs = check_workspace_cap(c, bytes, what);
+    if (cs != XB_OK) return cs;
     if (c->ws) cudaFree(c->ws);
     c->ws = nullptr;
     c->ws_bytes = 0;
@@ -90,6 +94,8 @@ xb_status ensure_scratch(xb_ctx* c, size_t bytes, const char* what) {
 
 xb_status ensure_stage(xb_ctx* c, size_t bytes) {
   if (c->stage_bytes >= bytes) return XB_OK;
+  const xb_status cs = check_workspace_cap(c, bytes, "table staging");
+  if (cs != XB_OK) return cs;
   if (c->d_stage) cudaFree(c->d_stage);
   c->d_stage = nullptr;
   c->stage_bytes = 0;
@@ -287,6 +293,7 @@ xb_status run_plain(xb_ctx* c, xb_graph* g, const int32_t* d_sources, int32_t k,
   const float alpha = c->tuning.pull_alpha > 0 ? c->tuning.pull_alpha : 1024.0f;
   ClassTimer timer{c, st, c->tuning.timing != 0};
   const StepShape mx = max_shape<W, NW, OffT>(g, sms);
+  const int bound = level_bound(c, p.nplanes_alloc);
   int max_levels = 0;
 
   for (int64_t k0 = 0; k0 < k; k0 += SPP) {
@@ -298,7 +305,7 @@ xb_status run_plain(xb_ctx* c, xb_graph* g, const int32_t* d_sources, int32_t k,
     int cur = 0;
     for (;;) {
       // the device decides the step; the host reads the decision back
-      xbk::k_step_begin<<<1, 1, 0, c->stream>>>(p.ctr, cur, alpha, p.nplanes_alloc, 0, 0);
+      xbk::k_step_begin<<<1, 1, 0, c->stream>>>(p.ctr, cur, alpha, p.nplanes_alloc, bound, 0, 0);
       XB_LAUNCH_CHECK("step begin");
       XB_CUDA(cudaMemcpyAsync(c->h_ctr, p.ctr, sizeof(xbk::Ctrs), cudaMemcpyDeviceToHost, c->stream));
       XB_CUDA(cudaStreamSynchronize(c->stream));
@@ -326,8 +333,12 @@ xb_status run_plain(xb_ctx* c, xb_graph* g, const int32_t* d_sources, int32_t k,
       timer.end(0, launches);
       cur ^= 1;
     }
-    if (c->h_ctr->b.err)
+    if (c->h_ctr->b.err) {
+      // the pass stopped with a live frontier: F / N are not all zero, so the
+      // next call clears the workspace before it relies on that
+      c->ws_key[0] = -1;
       return fail(XB_ERR_STATE, "the level loop ran past the level bound (corrupted traversal state)");
+    }
     max_levels = std::max(max_levels, c->h_ctr->b.level);
     timer.begin();
     int64_t launches = 0;
@@ -456,6 +467,7 @@ xb_status xb_ctx_set_tuning(xb_ctx* c, const xb_tuning* t) {
   if (t->heavy_degree < 32 || t->heavy_degree > (1 << 20))
     return fail(XB_ERR_ARG, "heavy_degree must be in [32, 2^20]");
   if (t->chains < 0 || t->chains > 16) return fail(XB_ERR_ARG, "chains must be in [0, 16]");
+  if (t->level_cap < 0 || t->workspace_cap < 0) return fail(XB_ERR_ARG, "level_cap and workspace_cap must be >= 0");
   c->tuning = *t;
   if (c->tuning.chains == 0) c->tuning.chains = 4;
   return XB_OK;

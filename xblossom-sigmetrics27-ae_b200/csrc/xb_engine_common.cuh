@@ -113,7 +113,7 @@ constexpr int kFifoGroup = 64;
 constexpr int64_t kCiPad = 16;
 
 struct WsLayout {
-  size_t seen, F, N, p01, ph, pushed, p8, touched, fl_light, fl_heavy, nl_light, nl_heavy, stamp, total;
+  size_t seen, F, N, p01, ph, pushed, p8, touched, fl_light, fl_heavy, nl_light, nl_heavy, stamp, fbits, nbits, total;
   int64_t plane_stride;  // in words
   int nplanes_alloc;
 };
@@ -151,6 +151,9 @@ inline WsLayout layout_for(int64_t n, int word_bytes, int nw) {
   L.nl_light = o; o += li;
   L.nl_heavy = o; o += li;
   L.stamp = o; o += li;
+  const size_t bw = align_up((size_t)((std::max<int64_t>(n, 1) + 31) / 32) * 4);  // one bit per vertex
+  L.fbits = o; o += bw;
+  L.nbits = o; o += bw;
   L.total = o;
   return L;
 }
@@ -206,6 +209,23 @@ inline xb_status end_body(cudaStream_t s, xb_status st) {
 }
 
 xb_status ensure_scratch(xb_ctx* c, size_t bytes, const char* what);
+
+// Level at which a pass's loop stops with the error flag: the structural
+// bound 2^planes (levels of a correct traversal stay below it), or the
+// context's tuning.level_cap when that is lower.
+inline int level_bound(const xb_ctx* c, int nplanes_alloc) {
+  int64_t b = nplanes_alloc >= 31 ? (int64_t)INT32_MAX : ((int64_t)1 << nplanes_alloc);
+  if (c->tuning.level_cap > 0) b = std::min<int64_t>(b, c->tuning.level_cap);
+  return (int)b;
+}
+
+// Refuses a working-memory allocation above the context's tuning.workspace_cap.
+inline xb_status check_workspace_cap(const xb_ctx* c, size_t bytes, const char* what) {
+  if (c->tuning.workspace_cap > 0 && (int64_t)bytes > c->tuning.workspace_cap)
+    return fail(XB_ERR_OOM, std::string(what) + " of " + std::to_string(bytes) +
+                                " bytes exceeds the workspace cap of " + std::to_string(c->tuning.workspace_cap));
+  return XB_OK;
+}
 xb_status traverse_alternating(xb_ctx* c, xb_graph* g, const int32_t* matching, int32_t* level, int32_t* parent,
                                int32_t* owner, uint32_t flags, xb_stats* st);
 
@@ -255,6 +275,7 @@ struct PassRes {
   int32_t* hpar = nullptr;
   int heavy = 256;
   size_t state_bytes = 0, plane_bytes = 0, ppos_bytes = 0;
+  int64_t bit_words = 0;  // 32-bit words of a frontier bitmap
   int nplanes_alloc = 3;
 };
 
@@ -273,8 +294,9 @@ PassRes<W, NW, OffT> pass_res(const xb_graph* g, void* ws, const WsLayout& L, xb
   p.pushed = (W*)(base + L.pushed);
   p.ppos = (W*)(base + L.p8);
   p.touched = (int32_t*)(base + L.touched);
-  p.lists[0] = xbk::Lists{(int32_t*)(base + L.fl_light), (int32_t*)(base + L.fl_heavy)};
-  p.lists[1] = xbk::Lists{(int32_t*)(base + L.nl_light), (int32_t*)(base + L.nl_heavy)};
+  p.lists[0] = xbk::Lists{(int32_t*)(base + L.fl_light), (int32_t*)(base + L.fl_heavy), (uint32_t*)(base + L.fbits)};
+  p.lists[1] = xbk::Lists{(int32_t*)(base + L.nl_light), (int32_t*)(base + L.nl_heavy), (uint32_t*)(base + L.nbits)};
+  p.bit_words = (g->n + 31) / 32;
   p.stamp = (int32_t*)(base + L.stamp);
   p.ctr = ctr;
   p.hpar = hpar;
@@ -327,6 +349,8 @@ xb_status emit_pass_init(const PassRes<W, NW, OffT>& p, const xb_graph* g, const
     XB_CUDA(cudaMemsetAsync(p.stamp, 0, sizeof(int32_t) * (size_t)p.n, s));
   }
   XB_CUDA(cudaMemsetAsync(p.seen, 0, p.state_bytes, s));
+  XB_CUDA(cudaMemsetAsync(p.lists[0].bits, 0, sizeof(uint32_t) * (size_t)p.bit_words, s));
+  XB_CUDA(cudaMemsetAsync(p.lists[1].bits, 0, sizeof(uint32_t) * (size_t)p.bit_words, s));
   XB_CUDA(cudaMemsetAsync(p.pl.p01, 0, 2 * p.plane_bytes, s));
   XB_CUDA(cudaMemsetAsync(p.pl.ph, 0, p.plane_bytes, s));
   XB_CUDA(cudaMemsetAsync(p.pushed, 0, p.state_bytes, s));
@@ -364,7 +388,7 @@ xb_status emit_push(const PassRes<W, NW, OffT>& p, const xb_graph* g, int cur, c
   }
   xbk::k_push_finalize<W, NW, OffT><<<sh.finalize_grid, 256, 0, s>>>(p.touched, p.ro, N, p.seen, p.pl,
                                                                      active_mask<W, NW>(kb), p.heavy, nl, p.ctr, cur,
-                                                                     p.pushed);
+                                                                     p.pushed, fl.bits, p.bit_words);
   (*launches)++;
   XB_LAUNCH_CHECK("push step");
   return XB_OK;
@@ -414,7 +438,7 @@ xb_status emit_pull(const PassRes<W, NW, OffT>& p, const xb_graph* g, int cur, c
     if (g->n_lorder > 0) {
       xbk::k_pull_lanes<W, NW, OffT, lane_warps<NW>()><<<sh.pull_grid, lane_warps<NW>() * 32, 0, s>>>(
           g->n_lchunks, g->d_lchunk, g->d_lorder, p.ro, p.ci, F, p.seen, N, p.pl, active, p.heavy, nl, p.ctr, cur,
-          p.ppos);
+          p.ppos, p.n, fl.bits);
       (*launches)++;
     }
   } else {
@@ -423,14 +447,18 @@ xb_status emit_pull(const PassRes<W, NW, OffT>& p, const xb_graph* g, int cur, c
     (*launches)++;
   }
   if (g->n_heavy > 0) {
-    xbk::k_pull_heavy<W, NW, OffT, heavy_rounds<NW>()><<<sh.heavy_grid, 256, 0, s>>>(g->d_heavy, g->n_heavy, p.ro, p.ci, F, p.seen, N,
-                                                                    p.pl, active, p.heavy, kHubDegree, nl, p.ctr, cur,
-                                                                    p.hpar);
-    (*launches)++;
+    // heavy vertices with wanted bits first (into the push steps' touched list,
+    // unused by a pull step), then one warp per listed vertex
+    xbk::k_heavy_want<W, NW, OffT><<<sh.commit_grid, 256, 0, s>>>(g->d_heavy, g->n_heavy, p.ro, p.seen, active,
+                                                                  kHubDegree, p.ctr, cur, p.touched);
+    xbk::k_pull_heavy<W, NW, OffT, heavy_rounds<NW>()><<<sh.heavy_grid, 256, 0, s>>>(
+        g->d_heavy, p.touched, p.ro, p.ci, F, p.seen, N, p.pl, active, p.heavy, kHubDegree, nl, p.ctr, cur, p.hpar,
+        p.n, fl.bits);
+    *launches += 2;
     if (g->n_hub_items > 0) {
       xbk::k_pull_hubs<W, NW, OffT, 4><<<sh.hub_grid, 256, 0, s>>>(g->d_heavy, g->d_hub_items, g->n_hub_items, p.ro,
                                                                    p.ci, F, p.seen, N, active, p.ctr, cur, kHubChunk,
-                                                                   p.hpar);
+                                                                   p.hpar, p.n, fl.bits);
       xbk::k_pull_hub_commit<W, NW, OffT><<<sh.commit_grid, 256, 0, s>>>(g->d_heavy, g->n_heavy, p.ro, p.seen, N, p.pl,
                                                                         active, p.heavy, kHubDegree, nl, p.ctr, cur);
       *launches += 2;

@@ -84,7 +84,7 @@ struct LevelCtr {
   int32_t n_touched;
   int32_t work;   // chunks handed out by the step that builds this frontier (k_pull_lanes)
   int32_t work2;  // heavy vertices handed out by the same step (k_pull_heavy)
-  int32_t pad;
+  int32_t n_hwant;  // heavy vertices with wanted bits, listed by the same step (k_heavy_want)
   unsigned long long edges;  // sum of degrees of the frontier
   unsigned long long live[4];
 };
@@ -121,11 +121,32 @@ struct Masks {
   W w[NW];
 };
 
-// Lists of one frontier: light (deg <= heavy) and heavy vertices.
+// Lists of one frontier: light (deg <= heavy) and heavy vertices, and
+// (when bits is set) one bit per vertex marking the frontier's vertices, so
+// the pull steps of a sparse frontier skip the gathers of neighbours outside
+// it.  The bitmap must be all zero before the step that builds the frontier.
 struct Lists {
   int32_t* light;
   int32_t* heavy;
+  uint32_t* bits;
 };
+
+// A pull step reads the frontier bitmap before each frontier-word gather when
+// the frontier holds fewer than n / kSparseDiv vertices: then most gathers
+// would return zero words, and the bit (a 4-byte word of a bitmap 1/256 the
+// size of the frontier words, mostly cache-resident) saves their HBM sectors.
+constexpr int kSparseDiv = 8;
+
+// Bitmap of the current frontier for a pull step, or null when the frontier
+// is dense (the check would only add latency).
+__device__ __forceinline__ const uint32_t* sparse_bits(const uint32_t* bits, const LevelCtr* cctr, int64_t n) {
+  return (bits != nullptr && ((long long)cctr->n_light + cctr->n_heavy) * kSparseDiv < n) ? bits : nullptr;
+}
+
+// Whether vertex u is in the frontier (always, without a bitmap).
+__device__ __forceinline__ bool in_frontier(const uint32_t* __restrict__ bits, int32_t u) {
+  return bits == nullptr || ((__ldg(&bits[u >> 5]) >> (u & 31)) & 1u);
+}
 
 // Vector types for loading NW consecutive words / a plane pair at once.
 template <typename W, int K>
@@ -151,7 +172,8 @@ struct Vec<unsigned int, 4> {
   using T = uint4;
 };
 
-// Loads K consecutive words starting at p (p aligned to K words).
+// Loads K consecutive words starting at p (p aligned to K words, read-only
+// for the rest of the kernel or written only by the loading thread).
 template <typename W, int K>
 __device__ __forceinline__ void load_words(const W* __restrict__ p, W (&out)[K]) {
   if constexpr (K == 1) {
@@ -161,12 +183,14 @@ __device__ __forceinline__ void load_words(const W* __restrict__ p, W (&out)[K])
     out[0] = x.x;
     out[1] = x.y;
   } else if constexpr (sizeof(W) == 8 && K == 4) {
-    const ulonglong2 x = __ldg(reinterpret_cast<const ulonglong2*>(p));
-    const ulonglong2 y = __ldg(reinterpret_cast<const ulonglong2*>(p) + 1);
-    out[0] = x.x;
-    out[1] = x.y;
-    out[2] = y.x;
-    out[3] = y.y;
+    // one 32-byte load (sm_100): a whole sector per lane in one instruction,
+    // half the L1 wavefronts of two 16-byte loads
+    unsigned long long a, b, c, d;
+    asm("ld.global.nc.v4.u64 {%0, %1, %2, %3}, [%4];" : "=l"(a), "=l"(b), "=l"(c), "=l"(d) : "l"(p));
+    out[0] = a;
+    out[1] = b;
+    out[2] = c;
+    out[3] = d;
   } else if constexpr (sizeof(W) == 4 && K == 2) {
     const uint2 x = __ldg(reinterpret_cast<const uint2*>(p));
     out[0] = x.x;
@@ -271,6 +295,7 @@ __device__ __forceinline__ void commit_new(bool has, int32_t w, const W (&nw)[NW
     acc.fe += (unsigned long long)dg;
     if (full) acc.fin -= dg;
   }
+  if (has && nl.bits) atomicOr(&nl.bits[w >> 5], 1u << (w & 31));
   const bool light = has && dg <= heavy;
   const bool hv = has && dg > heavy;
   warp_append(light, w, nl.light, &nctr->n_light);
@@ -450,11 +475,13 @@ __global__ void k_push_heavy(const int32_t* __restrict__ list, const int32_t* __
 template <typename W, int NW, typename OffT>
 __global__ void k_push_finalize(const int32_t* __restrict__ touched, const OffT* __restrict__ ro, const W* N,
                                 W* seen, Planes<W, NW> pl, Masks<W, NW> active, int heavy, Lists nl, Ctrs* ctr,
-                                int cur, W* pushed) {
+                                int cur, W* pushed, uint32_t* consumed_bits, int64_t bit_words) {
   const int level = ctr->b.level;
   LevelCtr* nctr = &ctr->lv[cur ^ 1];
   const int32_t cnt = nctr->n_touched;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  if (consumed_bits)  // the pushed frontier's bitmap (nothing reads it any more)
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < bit_words; i += stride) consumed_bits[i] = 0;
   StatAcc<W, NW> acc;
   for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < cnt; base += stride) {
     const int64_t idx = base + threadIdx.x;
@@ -729,7 +756,8 @@ __device__ __forceinline__ void pull_lane_vertex(bool act, int32_t v, const W (&
                                                  const W* __restrict__ F, W* seen, W* N, const Planes<W, NW>& pl,
                                                  const Masks<W, NW>& active, int heavy, int level, Lists nl,
                                                  LevelCtr* nctr, W* __restrict__ ppos, StatAcc<W, NW>& sacc,
-                                                 unsigned long long& e_scan, W* spp) {
+                                                 unsigned long long& e_scan, W* spp,
+                                                 const uint32_t* __restrict__ fb) {
   // position planes of this lane's claims: registers for one word, the
   // lane's shared-memory column for more (plane-major, 32 lanes apart, so a
   // warp's accesses hit distinct banks; they change only on a claim)
@@ -781,7 +809,7 @@ __device__ __forceinline__ void pull_lane_vertex(bool act, int32_t v, const W (&
 #pragma unroll
     for (int t = 0; t < G; t++) {
       const int64_t j = j0 + t;
-      if (j >= beg && j < end) {
+      if (j >= beg && j < end && in_frontier(fb, cols[t])) {
         load_words<W, NW>(F + (int64_t)cols[t] * NW, f[t]);
       } else {
 #pragma unroll
@@ -838,7 +866,8 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 3) k_pull_lanes(i
                                                            const int32_t* __restrict__ ci, const W* __restrict__ F,
                                                            W* seen, W* N, Planes<W, NW> pl, Masks<W, NW> active,
                                                            int heavy, Lists nl, Ctrs* ctr, int cur,
-                                                           W* __restrict__ ppos) {
+                                                           W* __restrict__ ppos, int64_t n,
+                                                           const uint32_t* __restrict__ fbits) {
   const int level = ctr->b.level;
   __shared__ int32_t s_qv[WARPS][64];
   __shared__ W s_qs[WARPS][64][NW];
@@ -854,6 +883,7 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 3) k_pull_lanes(i
   StatAcc<W, NW> sacc;
   int qn = 0;  // queued vertices (warp-uniform)
   W* spp = NW > 1 ? &s_pp[NW > 1 ? wib : 0][0][lane] : nullptr;
+  const uint32_t* fb = sparse_bits(fbits, cctr, n);
   for (;;) {
     int chunk = 0;
     if (lane == 0) chunk = atomicAdd(&nctr->work, 1);
@@ -908,7 +938,7 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 3) k_pull_lanes(i
           __syncwarp();
           v_scan++;
           pull_lane_vertex<W, NW, OffT>(true, qv, qs, live, ro, ci, F, seen, N, pl, active, heavy, level, nl, nctr,
-                                        ppos, sacc, e_scan, spp);
+                                        ppos, sacc, e_scan, spp, fb);
         }
       }
     }
@@ -923,7 +953,7 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 3) k_pull_lanes(i
         if (act) qv = s_qv[wib][lane];
         v_scan += act ? 1 : 0;
         pull_lane_vertex<W, NW, OffT>(act, qv, qs, live, ro, ci, F, seen, N, pl, active, heavy, level, nl, nctr,
-                                      ppos, sacc, e_scan, spp);
+                                      ppos, sacc, e_scan, spp, fb);
       }
       break;
     }
@@ -962,11 +992,43 @@ __device__ __forceinline__ W first_bits(W f, W before, W* grp) {
 // every wanted bit is found.  The first frontier neighbour of each newly
 // reached bit is its min-id parent; it is stored in hpar[idx*ROW + bit] (ROW =
 // B*NW) for the table pass.  Hubs (degree > hub) are left to k_pull_hubs.
+//
+// The heavy vertices a step must scan are listed first (k_heavy_want: one
+// thread per heavy vertex, warp-ballot compaction of their heavy indices), so
+// the warps of k_pull_heavy take only vertices with work from the counter.
+template <typename W, int NW, typename OffT>
+__global__ void __launch_bounds__(256) k_heavy_want(const int32_t* __restrict__ hlist, int32_t nh,
+                                                    const OffT* __restrict__ ro, const W* __restrict__ seen,
+                                                    Masks<W, NW> active, int hub, Ctrs* ctr, int cur,
+                                                    int32_t* __restrict__ wlist) {
+  const LevelCtr* cctr = &ctr->lv[cur];
+  LevelCtr* nctr = &ctr->lv[cur ^ 1];
+  W live[NW];
+#pragma unroll
+  for (int i = 0; i < NW; i++) live[i] = (W)cctr->live[i] & active.w[i];
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < nh; base += stride) {
+    const int64_t idx = base + threadIdx.x;
+    bool want = false;
+    if (idx < nh) {
+      const int32_t v = hlist[idx];
+      if (deg_of(ro, v) <= hub) {
+        W sw[NW];
+        load_words<W, NW>(seen + (int64_t)v * NW, sw);
+#pragma unroll
+        for (int i = 0; i < NW; i++) want = want || (live[i] & ~sw[i]) != 0;
+      }
+    }
+    warp_append(want, (int32_t)idx, wlist, &nctr->n_hwant);
+  }
+}
+
 template <typename W, int NW, typename OffT, int U>
-__global__ void __launch_bounds__(256, (NW == 4 ? 3 : 1)) k_pull_heavy(const int32_t* __restrict__ hlist, int32_t nh, const OffT* __restrict__ ro,
+__global__ void __launch_bounds__(256, (NW == 4 ? 3 : 1)) k_pull_heavy(const int32_t* __restrict__ hlist,
+                             const int32_t* __restrict__ wlist, const OffT* __restrict__ ro,
                              const int32_t* __restrict__ ci, const W* __restrict__ F, W* seen, W* N,
                              Planes<W, NW> pl, Masks<W, NW> active, int heavy, int hub, Lists nl, Ctrs* ctr,
-                             int cur, int32_t* __restrict__ hpar) {
+                             int cur, int32_t* __restrict__ hpar, int64_t n, const uint32_t* __restrict__ fbits) {
   const int level = ctr->b.level;
   constexpr int B = WB<W>::bits;
   constexpr int ROW = B * NW;
@@ -982,16 +1044,19 @@ __global__ void __launch_bounds__(256, (NW == 4 ? 3 : 1)) k_pull_heavy(const int
   unsigned long long scanned = 0, vcount = 0;
   (void)warp;
   (void)nwarps;
+  (void)hub;
+  const int32_t nwant = nctr->n_hwant;  // listed by k_heavy_want before this kernel
+  const uint32_t* fb = sparse_bits(fbits, cctr, n);
   for (;;) {
-    // the heavy list runs by falling degree: warps take vertices from a
-    // counter, the longest adjacencies first
-    int32_t idx = 0;
-    if (lane == 0) idx = atomicAdd(&nctr->work2, 1);
-    idx = __shfl_sync(0xffffffffu, idx, 0);
-    if (idx >= nh) break;
+    // the list keeps the heavy list's falling-degree order: warps take
+    // vertices from a counter, the longest adjacencies first
+    int32_t t = 0;
+    if (lane == 0) t = atomicAdd(&nctr->work2, 1);
+    t = __shfl_sync(0xffffffffu, t, 0);
+    if (t >= nwant) break;
+    const int32_t idx = wlist[t];
     const int32_t v = hlist[idx];
     const int64_t beg = ro[v], end = ro[v + 1];
-    if (end - beg > hub) continue;  // warp-uniform
     W sw[NW], want[NW];
     load_words<W, NW>(seen + (int64_t)v * NW, sw);
     bool any = false;
@@ -1023,7 +1088,7 @@ __global__ void __launch_bounds__(256, (NW == 4 ? 3 : 1)) k_pull_heavy(const int
       W f[U][NW];
 #pragma unroll
       for (int u = 0; u < U; u++) {
-        if (col[u] >= 0) {
+        if (col[u] >= 0 && in_frontier(fb, col[u])) {
           load_words<W, NW>(F + (int64_t)col[u] * NW, f[u]);
         } else {
 #pragma unroll
@@ -1083,7 +1148,7 @@ template <typename W, int NW, typename OffT, int U>
 __global__ void k_pull_hubs(const int32_t* __restrict__ hlist, const int2* __restrict__ items, int64_t nitems,
                             const OffT* __restrict__ ro, const int32_t* __restrict__ ci, const W* __restrict__ F,
                             const W* __restrict__ seen, W* N, Masks<W, NW> active, Ctrs* ctr, int cur, int chunk,
-                            int32_t* __restrict__ hpar) {
+                            int32_t* __restrict__ hpar, int64_t n, const uint32_t* __restrict__ fbits) {
   constexpr int B = WB<W>::bits;
   constexpr int ROW = B * NW;
   const int lane = threadIdx.x & 31;
@@ -1094,6 +1159,7 @@ __global__ void k_pull_hubs(const int32_t* __restrict__ hlist, const int2* __res
 #pragma unroll
   for (int i = 0; i < NW; i++) live[i] = (W)cctr->live[i] & active.w[i];
   unsigned long long scanned = 0;
+  const uint32_t* fb = sparse_bits(fbits, cctr, n);
   for (int64_t it = warp; it < nitems; it += nwarps) {
     const int2 item = items[it];
     const int64_t idx = item.x;
@@ -1123,7 +1189,7 @@ __global__ void k_pull_hubs(const int32_t* __restrict__ hlist, const int2* __res
       W f[U][NW];
 #pragma unroll
       for (int u = 0; u < U; u++) {
-        if (col[u] >= 0) {
+        if (col[u] >= 0 && in_frontier(fb, col[u])) {
           load_words<W, NW>(F + (int64_t)col[u] * NW, f[u]);
         } else {
 #pragma unroll
@@ -1659,9 +1725,10 @@ static __global__ void k_pass_init(Ctrs* ctr, long long m) {
 // Decides the next step from the current frontier's counters lv[cur]:
 // dir = 0 push, 1 pull (frontier edges * alpha > unfinished edges), 2 done.
 // Advances the level, picks the level plane to clear, bumps the stamp epoch
-// and zeroes the next frontier's counters.
-static __global__ void k_step_begin(Ctrs* ctr, int cur, float alpha, int nplanes_alloc, int graph_mode,
-                                    cudaGraphConditionalHandle hswitch) {
+// and zeroes the next frontier's counters.  A frontier still alive at
+// level_bound stops the loop with the error flag set.
+static __global__ void k_step_begin(Ctrs* ctr, int cur, float alpha, int nplanes_alloc, int level_bound,
+                                    int graph_mode, cudaGraphConditionalHandle hswitch) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   BatchCtr& b = ctr->b;
   const LevelCtr& lc = ctr->lv[cur];
@@ -1669,9 +1736,11 @@ static __global__ void k_step_begin(Ctrs* ctr, int cur, float alpha, int nplanes
   b.step_calls += 1;
   b.zero_plane = -1;  // k_zero_plane runs after every decision in a graph, "done" included
   // a traversal has at most n <= 2^nplanes_alloc levels; a frontier still alive
-  // beyond that means corrupted state: stop the loop and flag it
-  if (b.dir != 2 && b.err == 0 && b.level >= (1 << nplanes_alloc)) b.err = 2;
-  if (b.dir != 2 && b.err == 0 && (long long)lc.n_light + lc.n_heavy > 0) {
+  // beyond that (or beyond a lower bound the caller set) means corrupted
+  // state: stop the loop and flag it
+  const bool alive = (long long)lc.n_light + lc.n_heavy > 0;
+  if (b.dir != 2 && b.err == 0 && alive && b.level >= level_bound) b.err = 2;
+  if (b.dir != 2 && b.err == 0 && alive) {
     dir = ((double)lc.edges * (double)alpha > (double)b.m_unfinished) ? 1 : 0;
     b.level += 1;
     if (b.nplanes < nplanes_alloc && (1 << b.nplanes) <= b.level) {
@@ -1709,6 +1778,8 @@ __global__ void k_clear_frontier(W* F, int64_t n, Lists fl, const Ctrs* ctr, int
   const int32_t nlight = ctr->lv[cur].n_light, nheavy = ctr->lv[cur].n_heavy;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (fl.bits)
+    for (int64_t i = tid; i < (n + 31) / 32; i += stride) fl.bits[i] = 0;
   if (((int64_t)nlight + nheavy) * 16 < n) {
     for (int64_t i = tid; i < ((int64_t)nlight + nheavy) * NW; i += stride) {
       const int64_t j = i / NW;
@@ -1922,14 +1993,29 @@ __global__ void __launch_bounds__(1024) k_fifo_parents(int64_t n, const OffT* __
 }
 
 // Digest of one table row pair (level row, parent row of a source): the
-// summary a serving client gets instead of the full tables.
+// summary a serving client gets instead of the full tables.  row_hash is
+// position-sensitive: the wrapping sum over reached vertices v of
+// row_entry_hash(v, level[v], parent[v]), so moving a parent or a level from
+// one vertex to another changes it, while the sum keeps it independent of the
+// order the GPU visits the vertices in.
 struct RowDigest {
-  unsigned long long reached;     // vertices with level >= 0
-  unsigned long long level_sum;   // sum of their levels
-  unsigned long long parent_sum;  // sum of their parent ids
-  unsigned int depth;             // largest level
+  unsigned long long reached;    // vertices with level >= 0
+  unsigned long long level_sum;  // sum of their levels
+  unsigned long long row_hash;   // sum of row_entry_hash over them (mod 2^64)
+  unsigned int depth;            // largest level
   unsigned int pad;
 };
+
+// Hash of one (vertex, level, parent) entry: the splitmix64 finalizer
+// (Steele, Lea, Flood 2014) of the vertex id times the golden-ratio constant
+// XOR the (level, parent) pair packed into 64 bits.
+__host__ __device__ __forceinline__ unsigned long long row_entry_hash(int64_t v, int32_t level, int32_t parent) {
+  unsigned long long z = (unsigned long long)v * 0x9E3779B97F4A7C15ull;
+  z ^= ((unsigned long long)(uint32_t)level << 32) | (unsigned long long)(uint32_t)parent;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
 
 // Digests of the pass rows the flags mark; rows are in the table pass layout
 // (word wi: level rows at rows[wi*2B + b], parent rows at rows[wi*2B + B + b]).
@@ -1942,25 +2028,25 @@ static __global__ void __launch_bounds__(256) k_row_digest(int32_t* const* __res
   const int wi = r / B, b = r % B;
   const int32_t* lv = rows[wi * 2 * B + b];
   const int32_t* pr = rows[wi * 2 * B + B + b];
-  unsigned long long cnt = 0, ls = 0, ps = 0;
+  unsigned long long cnt = 0, ls = 0, hs = 0;
   unsigned int dep = 0;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     const int32_t l = __ldcs(&lv[i]);
     if (l >= 0) {
       cnt++;
       ls += (unsigned long long)l;
-      ps += (unsigned long long)(uint32_t)__ldcs(&pr[i]);
+      hs += row_entry_hash(i, l, __ldcs(&pr[i]));
       dep = max(dep, (unsigned int)l);
     }
   }
   cnt = warp_sum_u64(cnt);
   ls = warp_sum_u64(ls);
-  ps = warp_sum_u64(ps);
+  hs = warp_sum_u64(hs);
   for (int o = 16; o > 0; o >>= 1) dep = max(dep, __shfl_xor_sync(0xffffffffu, dep, o));
   if ((threadIdx.x & 31) == 0 && cnt) {
     atomicAdd(&out[r].reached, cnt);
     atomicAdd(&out[r].level_sum, ls);
-    atomicAdd(&out[r].parent_sum, ps);
+    atomicAdd(&out[r].row_hash, hs);
     atomicMax(&out[r].depth, dep);
   }
 }

@@ -19,12 +19,16 @@
 // streams, at once on the same device) race on the array and give wrong
 // results: serialise them.
 //
-// The device address of the array is looked up once per device, on the first
-// call made with that device current (cudaGetSymbolAddress); make that first
-// call before any stream capture begins on the device.
+// The device address of the array is looked up once per device context, on
+// the first call made with that device current (cudaGetSymbolAddress); make
+// that first call before any stream capture begins on the device.  The
+// address is cached under the context's unique id, so a host that resets the
+// device (cudaDeviceReset) or otherwise replaces its context gets a fresh
+// lookup on its next call instead of a pointer into the old context.
 //
 // No cudaMalloc, cudaFree, cudaMallocHost or allocating library routine is
 // called here, on the host or the device.
+#include <cuda.h>  // CUcontext and the prototypes of the two driver calls fetched below
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -67,23 +71,65 @@ static __device__ __align__(256) unsigned long long g_noalloc_scratch[kTotalWord
 namespace {
 
 std::mutex g_setup_mu;
-unsigned long long* g_scratch_ptr[kMaxDevices] = {};
+struct ScratchSlot {
+  unsigned long long ctx_id = 0;  // unique id of the context the address belongs to (0: none yet)
+  unsigned long long* ptr = nullptr;
+};
+ScratchSlot g_scratch[kMaxDevices];
 
-// One-time, per-device lookup of the array's device address.
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
+
+// Unique id of the context current on the calling thread (0 when none is).
+// The two driver calls are fetched through the runtime, so the library needs
+// no link against libcuda.
+xb_status current_context_id(unsigned long long* id) {
+  static CtxGetCurrentFn get_current = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  if (!get_current || !get_id) {
+    void* f1 = nullptr;
+    void* f2 = nullptr;
+    cudaDriverEntryPointQueryResult q1 = cudaDriverEntryPointSymbolNotFound, q2 = cudaDriverEntryPointSymbolNotFound;
+    const cudaError_t e1 = cudaGetDriverEntryPoint("cuCtxGetCurrent", &f1, cudaEnableDefault, &q1);
+    const cudaError_t e2 = cudaGetDriverEntryPoint("cuCtxGetId", &f2, cudaEnableDefault, &q2);
+    if (e1 != cudaSuccess || e2 != cudaSuccess || q1 != cudaDriverEntryPointSuccess ||
+        q2 != cudaDriverEntryPointSuccess || !f1 || !f2)
+      return fail(XB_ERR_CUDA, "driver entry points cuCtxGetCurrent / cuCtxGetId are unavailable");
+    get_current = (CtxGetCurrentFn)f1;
+    get_id = (CtxGetIdFn)f2;
+  }
+  CUcontext ctx = nullptr;
+  if (get_current(&ctx) != CUDA_SUCCESS) return fail(XB_ERR_CUDA, "cuCtxGetCurrent failed");
+  *id = 0;
+  if (ctx && get_id(ctx, id) != CUDA_SUCCESS) return fail(XB_ERR_CUDA, "cuCtxGetId failed");
+  return XB_OK;
+}
+
+// Set-up: the array's device address in the current device's context, looked
+// up with cudaGetSymbolAddress once per context and cached under its id.
 xb_status scratch_for_current_device(unsigned long long** out) {
   int dev = -1;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return fail(XB_ERR_NODEV, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
   if (dev < 0 || dev >= kMaxDevices) return fail(XB_ERR_ARG, "device index beyond the supported range");
   std::lock_guard<std::mutex> lock(g_setup_mu);
-  if (!g_scratch_ptr[dev]) {
+  unsigned long long id = 0;
+  xb_status s = current_context_id(&id);
+  if (s != XB_OK) return s;
+  ScratchSlot& slot = g_scratch[dev];
+  if (id == 0 || slot.ctx_id != id || !slot.ptr) {
+    // cudaGetSymbolAddress makes the device's primary context current when
+    // none is, so the id is read again after it
     void* p = nullptr;
     e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess || !p)
       return fail(XB_ERR_CUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
-    g_scratch_ptr[dev] = (unsigned long long*)p;
+    s = current_context_id(&id);
+    if (s != XB_OK) return s;
+    slot.ctx_id = id;
+    slot.ptr = (unsigned long long*)p;
   }
-  *out = g_scratch_ptr[dev];
+  *out = slot.ptr;
   return XB_OK;
 }
 
@@ -115,10 +161,20 @@ __global__ void k_heavy_list(int64_t n, const int32_t* __restrict__ ro, int thr,
   }
 }
 
-#define NA_CUDA(call)                                                                                    \
-  do {                                                                                                   \
-    cudaError_t e_ = (call);                                                                             \
-    if (e_ != cudaSuccess) return fail(XB_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+// Error exits of the entry point once it may have queued work on the caller's
+// stream: the stream is drained first (its result ignored), so no kernel or
+// copy of this call is still using the shared array when the call returns.
+xb_status drained(cudaStream_t sm, xb_status s) {
+  cudaStreamSynchronize(sm);
+  cudaGetLastError();
+  return s;
+}
+
+#define NA_CUDA(call)                                                                                 \
+  do {                                                                                                \
+    cudaError_t e_ = (call);                                                                          \
+    if (e_ != cudaSuccess)                                                                            \
+      return drained(sm, fail(XB_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)));      \
   } while (0)
 
 }  // namespace
@@ -168,8 +224,8 @@ extern "C" xb_status xb_traverse_noalloc(int64_t n, const int32_t* row_offsets, 
   int32_t m32 = 0;
   NA_CUDA(cudaMemcpyAsync(&m32, row_offsets + n, sizeof(int32_t), cudaMemcpyDeviceToHost, sm));
   NA_CUDA(cudaStreamSynchronize(sm));
-  if (m32 < 0) return fail(XB_ERR_ARG, "row_offsets[n] is negative");
-  if (m32 > 0 && !col_indices) return fail(XB_ERR_ARG, "null column indices");
+  if (m32 < 0) return drained(sm, fail(XB_ERR_ARG, "row_offsets[n] is negative"));
+  if (m32 > 0 && !col_indices) return drained(sm, fail(XB_ERR_ARG, "null column indices"));
   NA_CUDA(cudaMemsetAsync(misc, 0, 4 * sizeof(int32_t), sm));
   const int vgrid = sms * 4;
   k_validate<<<vgrid, 256, 0, sm>>>(n, row_offsets, col_indices, sources, k, misc + 1);
@@ -177,9 +233,9 @@ extern "C" xb_status xb_traverse_noalloc(int64_t n, const int32_t* row_offsets, 
   int32_t hmisc[2] = {0, 0};
   NA_CUDA(cudaMemcpyAsync(hmisc, misc, sizeof(hmisc), cudaMemcpyDeviceToHost, sm));
   NA_CUDA(cudaStreamSynchronize(sm));
-  if (hmisc[1] == 1) return fail(XB_ERR_ARG, "row offsets must start at 0 and not decrease");
-  if (hmisc[1] == 2) return fail(XB_ERR_ARG, "a column index is out of range");
-  if (hmisc[1] == 3) return fail(XB_ERR_ARG, "a source id is out of range");
+  if (hmisc[1] == 1) return drained(sm, fail(XB_ERR_ARG, "row offsets must start at 0 and not decrease"));
+  if (hmisc[1] == 2) return drained(sm, fail(XB_ERR_ARG, "a column index is out of range"));
+  if (hmisc[1] == 3) return drained(sm, fail(XB_ERR_ARG, "a source id is out of range"));
   k_heavy_list<<<(int)std::min<int64_t>((n + 255) / 256, (int64_t)sms * 8), 256, 0, sm>>>(n, row_offsets, kHeavy,
                                                                                         heavy_list, misc);
   NA_CUDA(cudaGetLastError());
@@ -214,7 +270,7 @@ extern "C" xb_status xb_traverse_noalloc(int64_t n, const int32_t* row_offsets, 
     int cur = 0;
     for (;;) {
       // the device picks the step (push / pull / done); the host reads it back
-      xbk::k_step_begin<<<1, 1, 0, sm>>>(ctr, cur, kAlpha, kPlanes, 0, 0);
+      xbk::k_step_begin<<<1, 1, 0, sm>>>(ctr, cur, kAlpha, kPlanes, 1 << kPlanes, 0, 0);
       NA_CUDA(cudaMemcpyAsync(&h, ctr, sizeof(h), cudaMemcpyDeviceToHost, sm));
       NA_CUDA(cudaStreamSynchronize(sm));
       if (h.b.dir == 2) break;
@@ -237,23 +293,31 @@ extern "C" xb_status xb_traverse_noalloc(int64_t n, const int32_t* row_offsets, 
         }
         xbk::k_push_finalize<W, 1, int32_t><<<(int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)sms * 8)),
                                               256, 0, sm>>>(touched, row_offsets, N, seen, pl, active, kHeavy, nl, ctr,
-                                                            cur, pushed);
+                                                            cur, pushed, nullptr, 0);
       } else {
         xbk::k_pull_tiles<W, 1, int32_t, PULL_WARPS, U><<<pull_grid, PULL_WARPS * 32, 0, sm>>>(
             n, row_offsets, col_indices, F, seen, N, pl, active, kHeavy, nl, ctr, cur, ppos);
         // one warp per heavy vertex; their parents are searched by the table pass
-        if (n_heavy > 0)
+        if (n_heavy > 0) {
+          // heavy vertices with wanted bits (listed into the push steps' touched list), then a warp per vertex
+          xbk::k_heavy_want<W, 1, int32_t><<<(int)std::min<int64_t>((n_heavy + 255) / 256, (int64_t)sms * 4), 256, 0,
+                                             sm>>>(heavy_list, n_heavy, row_offsets, seen, active, INT32_MAX, ctr, cur,
+                                                   touched);
           xbk::k_pull_heavy<W, 1, int32_t, 4><<<(int)std::min<int64_t>((n_heavy + 7) / 8, (int64_t)sms * 16), 256, 0,
-                                                sm>>>(heavy_list, n_heavy, row_offsets, col_indices, F, seen, N, pl,
-                                                      active, kHeavy, INT32_MAX, nl, ctr, cur, nullptr);
-        NA_CUDA(cudaMemsetAsync(F, 0, state_bytes, sm));
+                                                sm>>>(heavy_list, touched, row_offsets, col_indices, F, seen, N, pl,
+                                                      active, kHeavy, INT32_MAX, nl, ctr, cur, nullptr, n, nullptr);
+        }
+        // zero the consumed frontier: its listed vertices, or all of F when it is large
+        xbk::k_clear_frontier<W, 1><<<(int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)sms * 8)),
+                                      256, 0, sm>>>(F, n, fl, ctr, cur);
       }
       NA_CUDA(cudaGetLastError());
       std::swap(F, N);
       std::swap(fl, nl);
       cur ^= 1;
     }
-    if (h.b.err) return fail(XB_ERR_STATE, "the level loop ran past the level bound (corrupted traversal state)");
+    if (h.b.err)
+      return drained(sm, fail(XB_ERR_STATE, "the level loop ran past the level bound (corrupted traversal state)"));
     max_levels = std::max(max_levels, h.b.level);
     // every vertex takes the edge-flat table path here (no heavy-vertex staging)
     int32_t* hrows[2 * B];

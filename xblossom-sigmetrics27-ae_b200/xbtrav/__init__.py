@@ -87,6 +87,9 @@ class XbTuning(C.Structure):
         ("heavy_degree", C.c_int32),
         ("timing", C.c_int32),
         ("chains", C.c_int32),
+        ("level_cap", C.c_int32),
+        ("pad", C.c_int32),
+        ("workspace_cap", C.c_int64),
     ]
 
 
@@ -94,7 +97,7 @@ class XbRowDigest(C.Structure):
     _fields_ = [
         ("reached", C.c_int64),
         ("level_sum", C.c_int64),
-        ("parent_sum", C.c_int64),
+        ("row_hash", C.c_int64),
         ("depth", C.c_int32),
         ("pad", C.c_int32),
     ]
@@ -640,7 +643,7 @@ class Context:
 
     def slot_poll(self, slot: int, wait: bool = False):
         """(done, stats, digests) of a slot's pass; digests: int64 (kb, 4)
-        array of reached, level_sum, parent_sum, depth (depth -1 for rows
+        array of reached, level_sum, row_hash, depth (depth -1 for rows
         written to caller buffers)."""
         keep = getattr(self, "_slot_keep", {}).get(slot)
         kb = len(keep[0]) if keep is not None else 0
@@ -655,7 +658,7 @@ class Context:
             done = d.value
         if not done:
             return False, None, None
-        arr = np.array([(x.reached, x.level_sum, x.parent_sum, x.depth) for x in dig[:kb]], dtype=np.int64)
+        arr = np.array([(x.reached, x.level_sum, x.row_hash, x.depth) for x in dig[:kb]], dtype=np.int64)
         return True, st.as_dict(), arr.reshape(kb, 4)
 
     def slots_release(self) -> None:

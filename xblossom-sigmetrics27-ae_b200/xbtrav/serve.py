@@ -14,8 +14,9 @@ Each query asks for one of two results:
       memory.  The tables are allocated when the query is admitted, which
       happens once they fit into free HBM above a reserve, in arrival order;
       digest queries may pass a tables query that waits for memory.
-  want="digest": per source the reached-vertex count, level sum, parent sum
-      and depth (xb_row_digest), computed on the device from the slot's
+  want="digest": per source the reached-vertex count, level sum, a
+      position-sensitive hash of its (vertex, level, parent) entries and the
+      depth (xb_row_digest), computed on the device from the slot's
       scratch rows; no admission memory.  This is the mode for graphs whose
       tables cannot be held (R-MAT scale 25: 268 MB per source).
 
@@ -45,7 +46,7 @@ class Query:
     arrival: float
     level: object = None   # torch (k, n) int32 on the device (want="tables")
     parent: object = None
-    digest: np.ndarray = None  # (k, 4) int64: reached, level_sum, parent_sum, depth (want="digest")
+    digest: np.ndarray = None  # (k, 4) int64: reached, level_sum, row_hash, depth (want="digest")
     admitted: float = None
     done_at: float = None
     rows_done: int = 0
