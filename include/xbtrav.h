@@ -34,7 +34,7 @@
 extern "C" {
 #endif
 
-#define XB_ABI_VERSION 2
+#define XB_ABI_VERSION 3
 
 typedef int32_t xb_status;
 #define XB_OK 0
@@ -101,7 +101,11 @@ typedef struct xb_tuning {
    * serving slot workspaces, SSSP / matching scratch) above this many bytes
    * fails with XB_ERR_OOM before cudaMalloc is called. */
   int32_t level_cap;
-  int32_t pad;
+  /* Launch tile of the pull and table kernels (the autotuner's tile axis):
+   * 0 (default) = heavy-vertex pull with one 32-edge round in flight per warp
+   * at four words per vertex (four rounds otherwise) and 4-warp table blocks;
+   * 1 = two rounds in flight at every layout and 8-warp table blocks. */
+  int32_t tile;
   int64_t workspace_cap;
 } xb_tuning;
 

@@ -23,7 +23,7 @@ LAYOUTS = [
 
 
 def _tune(ctx, **kw):
-    base = dict(word_bits=64, words=1, pull_alpha=64.0, heavy_degree=256, timing=0, chains=2)
+    base = dict(word_bits=64, words=1, pull_alpha=64.0, heavy_degree=256, timing=0, chains=2, tile=0)
     base.update(kw)
     ctx.set_tuning(**base)
 
@@ -57,6 +57,23 @@ def test_single_graph_device_outputs(ctx, rmat12, layout, chains):
     assert st["edges_traversed"] == edges
     assert st["reached"] == reached
     g.close()
+
+
+@pytest.mark.parametrize("layout", [0, 2, 3, 4])
+@pytest.mark.parametrize("heavy", [32, 256])
+def test_launch_tile_one(ctx, rmat12, layout, heavy):
+    """xb_tuning.tile = 1 (two rounds in flight per heavy-pull warp, 8-warp
+    table blocks): same tables as the oracle, with most vertices routed
+    through the heavy pull when the cutoff is 32."""
+    ro, ci = rmat12
+    _tune(ctx, chains=2, heavy_degree=heavy, tile=1, **LAYOUTS[layout])
+    g = ctx.upload_arrays(ro, ci)
+    src = xbtrav.select_sources_csr(ro, 77, 200)
+    res, _ = ctx.traverse_batched([(g, src)])
+    _check(ro, ci, src, res[0])
+    _check(ro, ci, src, ctx.traverse(g, src))
+    g.close()
+    _tune(ctx)
 
 
 @pytest.mark.parametrize("alpha", [1e-6, 1e6])

@@ -11,7 +11,7 @@ def test_library_exports_every_declared_symbol():
     assert "xb_traverse" in names and "xb_ctx_create" in names
     missing = [n for n in names if not hasattr(L, n)]
     assert not missing, missing
-    assert L.xb_abi_version() == 2
+    assert L.xb_abi_version() == 3
 
 
 def test_status_strings():

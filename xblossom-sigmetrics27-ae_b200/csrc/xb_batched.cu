@@ -212,7 +212,9 @@ xb_status capture_level_loop(BatchState* bs, const PassRes<W, NW, OffT>& p, cons
 template <typename W, int NW, typename OffT>
 PassRes<W, NW, OffT> capture_res(xb_ctx* c, const xb_graph* g, void* ws, xbk::Ctrs* ctr, int32_t* hpar) {
   const int heavy = std::max(32, c->tuning.heavy_degree);
-  return pass_res<W, NW, OffT>(g, ws, layout_for(g->n, (int)sizeof(W), NW), ctr, hpar, heavy);
+  PassRes<W, NW, OffT> p = pass_res<W, NW, OffT>(g, ws, layout_for(g->n, (int)sizeof(W), NW), ctr, hpar, heavy);
+  p.tile = c->tuning.tile;
+  return p;
 }
 
 // First half of a captured pass on stream s: init and the device level loop.
@@ -221,7 +223,7 @@ xb_status capture_pass_levels(xb_ctx* c, BatchState* bs, const PassRes<W, NW, Of
                               const int32_t* src, int kb, cudaStream_t s) {
   const int sms = c->num_sms;
   const float alpha = c->tuning.pull_alpha > 0 ? c->tuning.pull_alpha : 1024.0f;
-  const StepShape sh = graph_shape<W, NW, OffT>(g, sms);
+  const StepShape sh = graph_shape<W, NW, OffT>(g, sms, p.tile);
   bs->level_bound = level_bound(c, p.nplanes_alloc);
   xb_status st = emit_pass_init<W, NW, OffT>(p, g, src, kb, s, sms, true);
   if (st != XB_OK) return st;
@@ -520,7 +522,8 @@ xb_status run_batched(xb_ctx* c, const std::vector<xb_batch_item>& items, const 
                                0,
                                (uint64_t)nch,
                                (uint64_t)items.size(),
-                               (uint64_t)c->tuning.level_cap};
+                               (uint64_t)c->tuning.level_cap,
+                               (uint64_t)c->tuning.tile};
   {
     uint32_t abits = 0;
     std::memcpy(&abits, &c->tuning.pull_alpha, sizeof(abits));
@@ -744,7 +747,8 @@ xb_status slot_launch(xb_ctx* c, int slot, xb_graph* g, const int32_t* sources, 
   uint32_t abits = 0;
   std::memcpy(&abits, &c->tuning.pull_alpha, sizeof(abits));
   const std::vector<uint64_t> key = {sl.gen, (uint64_t)(uintptr_t)g, g->version, (uint64_t)kb, sizeof(W), NW,
-                                     (uint64_t)heavy, abits, (uint64_t)c->tuning.level_cap};
+                                     (uint64_t)heavy, abits, (uint64_t)c->tuning.level_cap,
+                                     (uint64_t)c->tuning.tile};
   CachedGraph* hit = nullptr;
   for (auto& e : sl.cache)
     if (e.key == key) hit = &e;

@@ -289,10 +289,11 @@ xb_status run_plain(xb_ctx* c, xb_graph* g, const int32_t* d_sources, int32_t k,
     XB_CUDA(cudaStreamSynchronize(c->stream));
   }
   PassRes<W, NW, OffT> p = pass_res<W, NW, OffT>(g, c->ws, L, c->d_ctr, g->d_hpar, heavy);
+  p.tile = c->tuning.tile;
   const int sms = c->num_sms;
   const float alpha = c->tuning.pull_alpha > 0 ? c->tuning.pull_alpha : 1024.0f;
   ClassTimer timer{c, st, c->tuning.timing != 0};
-  const StepShape mx = max_shape<W, NW, OffT>(g, sms);
+  const StepShape mx = max_shape<W, NW, OffT>(g, sms, p.tile);
   const int bound = level_bound(c, p.nplanes_alloc);
   int max_levels = 0;
 
@@ -468,6 +469,7 @@ xb_status xb_ctx_set_tuning(xb_ctx* c, const xb_tuning* t) {
     return fail(XB_ERR_ARG, "heavy_degree must be in [32, 2^20]");
   if (t->chains < 0 || t->chains > 16) return fail(XB_ERR_ARG, "chains must be in [0, 16]");
   if (t->level_cap < 0 || t->workspace_cap < 0) return fail(XB_ERR_ARG, "level_cap and workspace_cap must be >= 0");
+  if (t->tile != 0 && t->tile != 1) return fail(XB_ERR_ARG, "tile must be 0 or 1");
   c->tuning = *t;
   if (c->tuning.chains == 0) c->tuning.chains = 4;
   return XB_OK;

@@ -274,6 +274,7 @@ struct PassRes {
   xbk::Ctrs* ctr = nullptr;
   int32_t* hpar = nullptr;
   int heavy = 256;
+  int tile = 0;  // xb_tuning.tile: launch tile of the pull and table kernels
   size_t state_bytes = 0, plane_bytes = 0, ppos_bytes = 0;
   int64_t bit_words = 0;  // 32-bit words of a frontier bitmap
   int nplanes_alloc = 3;
@@ -420,11 +421,15 @@ constexpr int lane_warps() {
 
 // Rounds of 32 edges a heavy-pull warp keeps in flight: one at four words
 // per vertex, where the gathered words of a round fill the registers and
-// three blocks per SM (80 registers) beat more rounds at two blocks.
+// three blocks per SM (80 registers) beat more rounds at two blocks.  Tile 1
+// (xb_tuning.tile) keeps two rounds in flight at every layout.
 template <int NW>
 constexpr int heavy_rounds() {
   return NW == 4 ? 1 : 4;
 }
+constexpr int kHeavyRoundsTile1 = 2;
+// Warps per block of the table pass: 4 at tile 0, 8 at tile 1.
+constexpr int kTabWarps0 = 4, kTabWarps1 = 8;
 
 template <typename W, int NW, typename OffT>
 xb_status emit_pull(const PassRes<W, NW, OffT>& p, const xb_graph* g, int cur, const StepShape& sh, int kb,
@@ -451,9 +456,14 @@ xb_status emit_pull(const PassRes<W, NW, OffT>& p, const xb_graph* g, int cur, c
     // unused by a pull step), then one warp per listed vertex
     xbk::k_heavy_want<W, NW, OffT><<<sh.commit_grid, 256, 0, s>>>(g->d_heavy, g->n_heavy, p.ro, p.seen, active,
                                                                   kHubDegree, p.ctr, cur, p.touched);
-    xbk::k_pull_heavy<W, NW, OffT, heavy_rounds<NW>()><<<sh.heavy_grid, 256, 0, s>>>(
-        g->d_heavy, p.touched, p.ro, p.ci, F, p.seen, N, p.pl, active, p.heavy, kHubDegree, nl, p.ctr, cur, p.hpar,
-        p.n, fl.bits);
+    if (p.tile == 1)
+      xbk::k_pull_heavy<W, NW, OffT, kHeavyRoundsTile1><<<sh.heavy_grid, 256, 0, s>>>(
+          g->d_heavy, p.touched, p.ro, p.ci, F, p.seen, N, p.pl, active, p.heavy, kHubDegree, nl, p.ctr, cur, p.hpar,
+          p.n, fl.bits);
+    else
+      xbk::k_pull_heavy<W, NW, OffT, heavy_rounds<NW>()><<<sh.heavy_grid, 256, 0, s>>>(
+          g->d_heavy, p.touched, p.ro, p.ci, F, p.seen, N, p.pl, active, p.heavy, kHubDegree, nl, p.ctr, cur, p.hpar,
+          p.n, fl.bits);
     *launches += 2;
     if (g->n_hub_items > 0) {
       xbk::k_pull_hubs<W, NW, OffT, 4><<<sh.hub_grid, 256, 0, s>>>(g->d_heavy, g->d_hub_items, g->n_hub_items, p.ro,
@@ -477,9 +487,10 @@ template <typename W, int NW, typename OffT>
 xb_status emit_tables(const PassRes<W, NW, OffT>& p, const xb_graph* g, const int32_t* src, int kb,
                       int32_t* const* rows, bool search_heavy, cudaStream_t s, int sms, int64_t* launches) {
   constexpr int B = xbk::WB<W>::bits;
-  constexpr int TAB_WARPS = 4;
+  const int TAB_WARPS = p.tile == 1 ? kTabWarps1 : kTabWarps0;
   const int64_t ntiles = (p.n + 31) / 32;
-  const int tab_grid = (int)std::max<int64_t>(1, std::min<int64_t>((ntiles + TAB_WARPS - 1) / TAB_WARPS, (int64_t)sms * 16));
+  const int tab_grid = (int)std::max<int64_t>(
+      1, std::min<int64_t>((ntiles + TAB_WARPS - 1) / TAB_WARPS, (int64_t)sms * 16 * kTabWarps0 / TAB_WARPS));
   for (int wi = 0; wi < NW; wi++) {
     if (kb - wi * B <= 0) break;
     if (g->n_heavy > 0 && search_heavy) {
@@ -492,8 +503,12 @@ xb_status emit_tables(const PassRes<W, NW, OffT>& p, const xb_graph* g, const in
     }
   }
   // all words of the pass in one launch (a tile's words share sectors)
-  xbk::k_tables<W, NW, OffT, TAB_WARPS, 4><<<tab_grid, TAB_WARPS * 32, 0, s>>>(
-      p.n, p.ro, p.ci, p.seen, p.pl, kb, p.heavy, rows, p.ctr, p.ppos, p.pushed, src, g->d_hidx_of, p.hpar);
+  if (p.tile == 1)
+    xbk::k_tables<W, NW, OffT, kTabWarps1, 2><<<tab_grid, kTabWarps1 * 32, 0, s>>>(
+        p.n, p.ro, p.ci, p.seen, p.pl, kb, p.heavy, rows, p.ctr, p.ppos, p.pushed, src, g->d_hidx_of, p.hpar);
+  else
+    xbk::k_tables<W, NW, OffT, kTabWarps0, 4><<<tab_grid, kTabWarps0 * 32, 0, s>>>(
+        p.n, p.ro, p.ci, p.seen, p.pl, kb, p.heavy, rows, p.ctr, p.ppos, p.pushed, src, g->d_hidx_of, p.hpar);
   (*launches)++;
   XB_LAUNCH_CHECK("tables");
   return XB_OK;
@@ -514,7 +529,7 @@ void fill_rows(int32_t** rows, int kb, int32_t* lv0, int32_t* pr0, int64_t n) {
 }
 
 template <typename W, int NW, typename OffT>
-StepShape max_shape(const xb_graph* g, int sms) {
+StepShape max_shape(const xb_graph* g, int sms, int tile) {
   constexpr int PW = pull_warps<W, NW>();
   StepShape sh{};
   const int64_t n = g->n;
@@ -533,7 +548,9 @@ StepShape max_shape(const xb_graph* g, int sms) {
   } else {
     sh.pull_grid = (int)std::max<int64_t>(1, std::min<int64_t>((ntiles + PW - 1) / PW, (int64_t)sms * 8));
   }
-  static const int heavy_res = resident_blocks(xbk::k_pull_heavy<W, NW, OffT, heavy_rounds<NW>()>, 256);
+  static const int heavy_res0 = resident_blocks(xbk::k_pull_heavy<W, NW, OffT, heavy_rounds<NW>()>, 256);
+  static const int heavy_res1 = resident_blocks(xbk::k_pull_heavy<W, NW, OffT, kHeavyRoundsTile1>, 256);
+  const int heavy_res = tile == 1 ? heavy_res1 : heavy_res0;
   sh.heavy_grid = (int)std::max<int64_t>(1, std::min<int64_t>((g->n_heavy + 7) / 8, (int64_t)sms * heavy_res));
   sh.hub_grid = (int)std::max<int64_t>(1, std::min<int64_t>((g->n_hub_items + 7) / 8, (int64_t)sms * 16));
   sh.commit_grid = (int)std::max<int64_t>(1, std::min<int64_t>((g->n_heavy + 255) / 256, (int64_t)sms * 4));
@@ -545,8 +562,8 @@ StepShape max_shape(const xb_graph* g, int sms) {
 // driven kernels stride over whatever the frontier holds, so their grids are
 // fixed, bounded by the graph's size and by a few waves of the GPU.
 template <typename W, int NW, typename OffT>
-StepShape graph_shape(const xb_graph* g, int sms) {
-  StepShape sh = max_shape<W, NW, OffT>(g, sms);
+StepShape graph_shape(const xb_graph* g, int sms, int tile) {
+  StepShape sh = max_shape<W, NW, OffT>(g, sms, tile);
   const int64_t n = g->n;
   sh.push_light_grid = (int)std::max<int64_t>(1, std::min<int64_t>((n + 7) / 8, (int64_t)sms * 16));
   if (g->n_heavy > 0)

@@ -1024,7 +1024,7 @@ __global__ void __launch_bounds__(256) k_heavy_want(const int32_t* __restrict__ 
 }
 
 template <typename W, int NW, typename OffT, int U>
-__global__ void __launch_bounds__(256, (NW == 4 ? 3 : 1)) k_pull_heavy(const int32_t* __restrict__ hlist,
+__global__ void __launch_bounds__(256, (NW == 4 && U == 1) ? 3 : (NW == 4 ? 2 : 1)) k_pull_heavy(const int32_t* __restrict__ hlist,
                              const int32_t* __restrict__ wlist, const OffT* __restrict__ ro,
                              const int32_t* __restrict__ ci, const W* __restrict__ F, W* seen, W* N,
                              Planes<W, NW> pl, Masks<W, NW> active, int heavy, int hub, Lists nl, Ctrs* ctr,

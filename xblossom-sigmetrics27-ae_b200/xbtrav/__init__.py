@@ -88,7 +88,7 @@ class XbTuning(C.Structure):
         ("timing", C.c_int32),
         ("chains", C.c_int32),
         ("level_cap", C.c_int32),
-        ("pad", C.c_int32),
+        ("tile", C.c_int32),
         ("workspace_cap", C.c_int64),
     ]
 

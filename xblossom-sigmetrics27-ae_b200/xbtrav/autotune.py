@@ -2,9 +2,11 @@
 
 Searches sources-per-word (32/64), words traversed together (1/2/4), the
 degree cutoff between the per-lane light pull and the per-warp heavy pull,
-the push/pull switch factor alpha and, for the batched path, the number of
-concurrent chains, by timing the engine's own calls (device-side CUDA events
-of xb_traverse or xb_traverse_batched) on the workload's sources.  The
+the push/pull switch factor alpha, the launch tile of the pull and table
+kernels (xb_tuning.tile: rounds in flight per heavy-pull warp, warps per
+table block) and, for the batched path, the number of concurrent chains, by
+timing the engine's own calls (device-side CUDA events of xb_traverse or
+xb_traverse_batched, median of `reps` runs) on the workload's sources.  The
 reference has no tuner; its only knobs are compile-time buffer ratios and a
 hybrid per-node/per-edge threshold (apps/xb/src/include/xbsm_gpu/xblossom_gpu_engine_hybrid.h:119).
 
@@ -21,9 +23,10 @@ DEFAULT_SPACE = {
     "words": [1, 2, 4],
     "heavy_degree": [128, 256, 512],
     "pull_alpha": [16.0, 64.0, 256.0, 1024.0],
+    "tile": [0, 1],
     "chains": [1, 2, 4, 8],
 }
-KEYS = ("word_bits", "words", "heavy_degree", "pull_alpha", "chains")
+KEYS = ("word_bits", "words", "heavy_degree", "pull_alpha", "tile", "chains")
 
 
 def _time_config(ctx, graph, sources, cfg: dict, reps: int, path: str) -> float:
@@ -42,17 +45,18 @@ def _time_config(ctx, graph, sources, cfg: dict, reps: int, path: str) -> float:
         return ctx.traverse(graph, src, out="device", level=lv, parent=pr).stats["device_ms"]
 
     once()  # warm-up (workspaces, heavy lists, the captured launch)
-    return min(once() for _ in range(reps))
+    times = sorted(once() for _ in range(max(1, reps)))
+    return times[len(times) // 2]  # median: one slow or fast outlier does not pick the winner
 
 
-def autotune(ctx, graph, sources, space: dict | None = None, reps: int = 2, staged: bool = True,
+def autotune(ctx, graph, sources, space: dict | None = None, reps: int = 5, staged: bool = True,
              path: str = "plain"):
     """Returns (best tuning dict, list of (cfg, ms)); path "plain" times
     xb_traverse, "batched" xb_traverse_batched (which also uses chains).
 
     staged=True searches coordinate-wise (word layout first with the current
-    cutoffs, then cutoffs and alpha for the winning layout, then chains)
-    instead of the full grid.
+    cutoffs, then cutoffs and alpha for the winning layout, then the launch
+    tile, then chains) instead of the full grid.
     """
     space = dict(DEFAULT_SPACE if space is None else space)
     if path != "batched":
@@ -73,6 +77,9 @@ def autotune(ctx, graph, sources, space: dict | None = None, reps: int = 2, stag
         best = min(table, key=lambda x: x[1])[0]
         for h, a in itertools.product(space["heavy_degree"], space["pull_alpha"]):
             run(dict(best, heavy_degree=h, pull_alpha=a))
+        best = min(table, key=lambda x: x[1])[0]
+        for tl in space.get("tile", [best.get("tile", 0)]):
+            run(dict(best, tile=tl))
         best = min(table, key=lambda x: x[1])[0]
         for ch in space["chains"]:
             run(dict(best, chains=ch))
