@@ -52,7 +52,7 @@ WORKLOADS = {
     # serving: resident graph, Poisson arrivals (seeded rate), 1..4096 sources per query (log-uniform),
     # digests per source, continuous batching over slots; reports GTEPS and p50/p99 latency
     "serve_rmat25": dict(kind="serve", scale=25, ef=32, queries=48, rate=2.0, kmax=4096, slots=4),
-    "serve_rmat22": dict(kind="serve", scale=22, ef=16, queries=96, rate=12.0, kmax=4096, slots=4),
+    "serve_rmat22": dict(kind="serve", scale=22, ef=16, queries=96, rate=12.0, kmax=4096, slots=2, max_words=4),
     # the default graph with one word of sources: ncu DRAM-traffic captures (about 4 GB on the device)
     "rmat22_k64": dict(kind="rmat", scale=22, ef=16, k=64),
     # one pass of the two-word layout (2 words x 64 sources): DRAM-traffic captures
@@ -600,17 +600,17 @@ def run_serve(args, w, name) -> None:
     csr = xbtrav.HostCSR.rmat(w["scale"], w["ef"], 0.57, 0.19, 0.19, seed=SEED)
     info = csr.info()
     ctx = xbtrav.Context(0)
-    # one word per pass: 64-source passes keep latency low, and per-slot memory
-    # (workspace + scratch rows, 28 GB per slot at scale 25) within the device
+    # passes start at one word (64 sources: low latency); max_words lets large
+    # queries open wider passes where per-slot memory allows (workspace +
+    # scratch rows: 28 GB per slot at scale 25 with one word, so that graph
+    # stays at one word)
     ctx.set_tuning(words=1)
     g = ctx.upload(csr)
     del csr
     slots = args.chains or w["slots"]
-    srv = serve.Server(ctx, slots=slots)
-    # warm-up: one full pass per slot (captures each slot's one-pass graph)
-    for s in range(slots):
-        srv.submit(g, g.select_sources(SEED + 99 + s, srv.rows_per_pass), want="digest")
-    srv.drain()
+    srv = serve.Server(ctx, slots=slots, max_words=w.get("max_words", 1))
+    # warm-up: one full pass per slot and width (workspaces, scratch, captured pass graphs)
+    srv.warmup(g, SEED + 99)
     srv.completed.clear()
     srv.edges = 0
     srv.passes = 0
@@ -628,7 +628,8 @@ def run_serve(args, w, name) -> None:
         "config": {"workload": name, "n": info["n"], "m_directed": info["m"], "seed": SEED,
                    "graph": f"rmat scale {w['scale']} ef {w['ef']} a/b/c/d .57/.19/.19/.05",
                    "queries": len(trace), "sources_total": int(sum(ks)), "k_range": [1, w["kmax"]],
-                   "arrival_rate_per_s": w["rate"], "slots": slots, "result": "per-source digests"},
+                   "arrival_rate_per_s": w["rate"], "slots": slots, "max_words": srv.max_words,
+                   "result": "per-source digests"},
         "path": "xbtrav.serve.Server over xb_slot_launch (continuous batching)",
         "latency_ms": {"p50": out["p50_ms"], "p99": out["p99_ms"], "mean": out["mean_ms"], "max": out["max_ms"]},
         "passes": out["passes"], "trace_seconds": out["seconds"], "clocks": clk, "setup_s": setup_s,
@@ -639,22 +640,21 @@ def run_serve(args, w, name) -> None:
     ctx.close()
 
 
-SERVE_LEG = dict(queries=48, rate=12.0, kmax=4096, slots=4)
+SERVE_LEG = dict(queries=48, rate=12.0, kmax=4096, slots=2, max_words=4)
 
 
 def serve_leg(ctx, g, dev, rank, dist, max_over_ranks, sum_over_ranks, barrier) -> dict:
     """Serving on the headline's resident graph: seeded Poisson arrivals (rate
     12/s), 1..4096 sources per query (log-uniform), digests, continuous
-    batching over 4 slots of one 64-source word each (xbtrav.serve).  Latency
+    batching over 2 slots, shortest query first, passes 1, 2 or 4 words wide
+    as the opening query needs (xbtrav.serve).  Latency
     = arrival to the query's last digest; p50/p99 are the largest over ranks,
     throughput the sum of the ranks' processed edges over the longest trace."""
     from xbtrav import replicas, serve
 
     ctx.set_tuning(words=1)
-    srv = serve.Server(ctx, slots=SERVE_LEG["slots"])
-    for s in range(SERVE_LEG["slots"]):  # warm-up: capture each slot's one-pass graph
-        srv.submit(g, g.select_sources(SEED + 99 + s, srv.rows_per_pass), want="digest")
-    srv.drain()
+    srv = serve.Server(ctx, slots=SERVE_LEG["slots"], max_words=SERVE_LEG["max_words"])
+    srv.warmup(g, SEED + 99)  # every slot and width: workspaces, scratch rows, captured pass graphs
     srv.completed.clear()
     srv.edges = 0
     srv.passes = 0
@@ -674,7 +674,9 @@ def serve_leg(ctx, g, dev, rank, dist, max_over_ranks, sum_over_ranks, barrier) 
                        "mean": max_over_ranks(out["mean_ms"]), "max": max_over_ranks(out["max_ms"])},
         "gteps": edges / secs / 1e9, "trace_seconds": secs, "queries": len(trace),
         "sources_total": int(sum(len(t[2]) for t in trace)), "arrival_rate_per_s": SERVE_LEG["rate"],
-        "k_range": [1, SERVE_LEG["kmax"]], "slots": SERVE_LEG["slots"], "sources_per_pass": srv.rows_per_pass,
+        "k_range": [1, SERVE_LEG["kmax"]], "slots": SERVE_LEG["slots"],
+        "sources_per_pass": [srv.word_bits * srv.base_words, srv.word_bits * srv.max_words],
+        "order": "shortest query first, queries waiting over 1 s first",
         "passes": out["passes"], "result": "per-source digests", "clocks": clk,
         "path": "xbtrav.serve.Server over xb_slot_launch (continuous batching, admission by free HBM)",
     }

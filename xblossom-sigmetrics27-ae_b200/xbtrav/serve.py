@@ -9,6 +9,23 @@ stream and workspace, so passes of different slots overlap on the device).  A
 query that arrives while others are on the GPU joins the next pass any slot
 starts; nothing waits for a batch to fill.
 
+Passes are filled shortest query first: the query with the fewest sources
+still to launch opens the pass, and the rest of it takes the other waiting
+queries of the same graph in the same order.  A pass costs about the same
+whatever share of its word the sources fill (every unfinished vertex is
+scanned), so a small query served behind a large one would wait for all of
+the large one's passes; shortest-first serves it in the next pass any slot
+starts.  A query that has waited longer than `age_s` since admission opens
+the next pass regardless of its size, so large queries cannot starve.
+
+With max_words above the context's words per vertex, each pass is as wide
+as the query that opens it needs (1, 2 or 4 words, never above max_words):
+a wide pass serves many sources at a lower cost per source, a narrow one
+finishes sooner, so large queries take wide passes and small ones narrow
+passes.  The context's tuning.words is switched before each launch (the
+server owns the context); every slot keeps a workspace and scratch rows for
+the widest pass it has run.
+
 Each query asks for one of two results:
   want="tables": the full int32 level / parent tables (k x n each) in device
       memory.  The tables are allocated when the query is admitted, which
@@ -50,6 +67,7 @@ class Query:
     admitted: float = None
     done_at: float = None
     rows_done: int = 0
+    rows_launched: int = 0
     passes: set = field(default_factory=set)
 
     @property
@@ -66,7 +84,8 @@ class Query:
 
 
 class Server:
-    def __init__(self, ctx, slots: int = 4, reserve_bytes: int = 4 << 30, clock=time.perf_counter):
+    def __init__(self, ctx, slots: int = 4, reserve_bytes: int = 4 << 30, clock=time.perf_counter,
+                 age_s: float = 1.0, max_words: int | None = None):
         import torch
 
         self.torch = torch
@@ -75,10 +94,17 @@ class Server:
         self.reserve = reserve_bytes
         self.clock = clock
         t = ctx.tuning()
-        self.rows_per_pass = t["word_bits"] * t["words"]
+        self.word_bits = t["word_bits"]
+        self.base_words = t["words"]
+        self.max_words = max(self.base_words, max_words or self.base_words)
+        if self.max_words not in (1, 2, 4):
+            raise ValueError("max_words must be 1, 2 or 4")
+        self.cur_words = self.base_words
+        self.rows_per_pass = self.word_bits * self.base_words
         self.dev = torch.device("cuda", ctx.device)
+        self.age_s = age_s
         self.admit_q = collections.deque()      # queries waiting for memory
-        self.rows = collections.OrderedDict()   # graph handle -> deque of (query, source index)
+        self.waiting = []                       # admitted queries with sources not yet launched
         self.slot_rows = [None] * slots         # rows of the pass in flight per slot
         self.slot_pass = [0] * slots
         self.completed = []
@@ -128,22 +154,35 @@ class Server:
 
     def _enqueue(self, q: Query) -> None:
         q.admitted = self.clock()
-        key = q.graph._h.value
-        dq = self.rows.setdefault(key, collections.deque())
-        dq.extend((q, j) for j in range(q.k))
+        self.waiting.append(q)
 
     # slots ------------------------------------------------------------------
+    def _order(self, now: float) -> list:
+        """Waiting queries in launch order: those past age_s by admission
+        time, then the rest by sources still to launch (ties: admission)."""
+        aged = sorted((q for q in self.waiting if now - q.admitted > self.age_s), key=lambda q: q.admitted)
+        rest = sorted((q for q in self.waiting if now - q.admitted <= self.age_s),
+                      key=lambda q: (q.k - q.rows_launched, q.admitted, q.qid))
+        return aged + rest
+
     def _launch(self, slot: int) -> bool:
-        """Starts a pass on an idle slot from the graph whose waiting row is oldest."""
-        best, best_t = None, None
-        for key, dq in self.rows.items():
-            if dq and (best is None or dq[0][0].admitted < best_t):
-                best, best_t = key, dq[0][0].admitted
-        if best is None:
+        """Starts a pass on an idle slot: the first query in launch order
+        opens it, other waiting queries of its graph fill the rest."""
+        if not self.waiting:
             return False
-        dq = self.rows[best]
-        take = [dq.popleft() for _ in range(min(self.rows_per_pass, len(dq)))]
-        g = take[0][0].graph
+        order = self._order(self.clock())
+        g = order[0].graph
+        cap = self._width(order[0].k - order[0].rows_launched)
+        take = []
+        for q in order:
+            if q.graph._h.value != g._h.value:
+                continue
+            n = min(cap - len(take), q.k - q.rows_launched)
+            take.extend((q, j) for j in range(q.rows_launched, q.rows_launched + n))
+            q.rows_launched += n
+            if len(take) == cap:
+                break
+        self.waiting = [q for q in self.waiting if q.rows_launched < q.k]
         src = np.array([q.sources[j] for q, j in take], dtype=np.int32)
         rows = []
         for q, j in take:
@@ -153,6 +192,33 @@ class Server:
         self.passes += 1
         self.slot_pass[slot] = self.passes
         return True
+
+    def _width(self, rows: int) -> int:
+        """Rows of the next pass for an opening query with `rows` sources
+        left: the narrowest allowed width that holds them (the widest if none
+        does); switches the context's layout when it changes."""
+        words = self.base_words
+        while words < self.max_words and rows > self.word_bits * words:
+            words *= 2
+        if words != self.cur_words:
+            self.ctx.set_tuning(words=words)
+            self.cur_words = words
+        return self.word_bits * words
+
+    def warmup(self, graph, seed: int = 1) -> None:
+        """One full pass per slot and per width, so that workspaces, scratch
+        rows and the slots' captured pass graphs exist before timing."""
+        words = self.base_words
+        while True:
+            self.ctx.set_tuning(words=words)
+            self.cur_words = words
+            for s in range(self.nslots):
+                self.ctx.slot_launch(s, graph, graph.select_sources(seed + s, self.word_bits * words), None)
+            for s in range(self.nslots):
+                self.ctx.slot_poll(s, wait=True)
+            if words >= self.max_words:
+                break
+            words *= 2
 
     def _collect(self, slot: int, wait: bool) -> bool:
         done, st, dig = self.ctx.slot_poll(slot, wait=wait)
@@ -181,7 +247,7 @@ class Server:
             if self.slot_rows[s] is None and not self._launch(s):
                 break
         busy = [s for s in range(self.nslots) if self.slot_rows[s] is not None]
-        if not busy and self.admit_q and not any(self.rows.values()):
+        if not busy and self.admit_q and not self.waiting:
             raise RuntimeError("queries wait for device memory that nothing in flight will free "
                                "(tables of finished queries are still held)")
         if wait and busy:
@@ -190,7 +256,7 @@ class Server:
         return sum(r is not None for r in self.slot_rows)
 
     def pending(self) -> bool:
-        return bool(self.admit_q) or any(self.rows.values()) or any(r is not None for r in self.slot_rows)
+        return bool(self.admit_q) or bool(self.waiting) or any(r is not None for r in self.slot_rows)
 
     def drain(self) -> None:
         while self.pending():
