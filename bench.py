@@ -52,7 +52,7 @@ WORKLOADS = {
     # serving: resident graph, Poisson arrivals (seeded rate), 1..4096 sources per query (log-uniform),
     # digests per source, continuous batching over slots; reports GTEPS and p50/p99 latency
     "serve_rmat25": dict(kind="serve", scale=25, ef=32, queries=48, rate=2.0, kmax=4096, slots=4),
-    "serve_rmat22": dict(kind="serve", scale=22, ef=16, queries=96, rate=12.0, kmax=4096, slots=2, max_words=4),
+    "serve_rmat22": dict(kind="serve", scale=22, ef=16, queries=96, rate=12.0, kmax=4096, slots=4, max_words=4),
     # the default graph with one word of sources: ncu DRAM-traffic captures (about 4 GB on the device)
     "rmat22_k64": dict(kind="rmat", scale=22, ef=16, k=64),
     # one pass of the two-word layout (2 words x 64 sources): DRAM-traffic captures
@@ -640,13 +640,13 @@ def run_serve(args, w, name) -> None:
     ctx.close()
 
 
-SERVE_LEG = dict(queries=48, rate=12.0, kmax=4096, slots=2, max_words=4)
+SERVE_LEG = dict(queries=48, rate=12.0, kmax=4096, slots=4, max_words=4)
 
 
 def serve_leg(ctx, g, dev, rank, dist, max_over_ranks, sum_over_ranks, barrier) -> dict:
     """Serving on the headline's resident graph: seeded Poisson arrivals (rate
     12/s), 1..4096 sources per query (log-uniform), digests, continuous
-    batching over 2 slots, shortest query first, passes 1, 2 or 4 words wide
+    batching over 4 slots, shortest query first, passes 1, 2 or 4 words wide
     as the opening query needs (xbtrav.serve).  Latency
     = arrival to the query's last digest; p50/p99 are the largest over ranks,
     throughput the sum of the ranks' processed edges over the longest trace."""

@@ -151,3 +151,65 @@ def test_digests_on_a_larger_graph_match_the_oracle():
     c.slots_release()
     g.close()
     c.close()
+
+
+def _path_csr(n):
+    ro = np.zeros(n + 1, np.int64)
+    ci = []
+    for v in range(n):
+        nb = [u for u in (v - 1, v + 1) if 0 <= u < n]
+        ci.extend(nb)
+        ro[v + 1] = ro[v] + len(nb)
+    return ro, np.array(ci, np.int32)
+
+
+@pytest.mark.parametrize("layout", [dict(word_bits=64, words=1), dict(word_bits=32, words=2),
+                                    dict(word_bits=64, words=4)])
+@pytest.mark.parametrize("alpha,heavy", [(256.0, 256), (1e-6, 32), (1e6, 32)])
+def test_all_digest_pass_sums_digests_in_the_table_pass(ctx, graphs, layout, alpha, heavy):
+    """A slot pass whose rows are all digest-only computes the digests inside
+    the table pass (no rows written); they equal the oracle's, with pushed
+    bits (parents searched), heavy vertices (recorded parents) and levels
+    past 255 (deep plane decode) among them."""
+    _tune(ctx, pull_alpha=alpha, heavy_degree=heavy, **layout)
+    cases = list(graphs) + [_path_csr(700)]
+    spp = layout["word_bits"] * layout["words"]
+    for ro, ci in cases:
+        g = ctx.upload_arrays(ro, ci)
+        for seed, k in ((7, spp), (8, max(1, spp // 3))):
+            src = g.select_sources(seed, k)
+            if len(ro) == 701:  # the path: include both ends and the middle
+                src = np.array([0, 699, 350][:k] + list(src[3:k]), np.int32) if k >= 3 else src
+            ctx.slot_launch(0, g, src, None)
+            done, st, dig = ctx.slot_poll(0, wait=True)
+            lv, pr, edges, _ = O.msbfs(ro, ci, src, rule=O.RULE_MINID)
+            np.testing.assert_array_equal(dig, _oracle_digest(lv, pr))
+            assert st["edges_traversed"] == edges
+        g.close()
+    ctx.slots_release()
+    _tune(ctx)
+
+
+def test_adaptive_width_server_matches_the_oracle(ctx, graphs):
+    """Shortest-first scheduling with passes 1, 2 or 4 words wide: every
+    query's tables and digests equal the oracle's."""
+    _tune(ctx)
+    dg = [ctx.upload_arrays(ro, ci) for ro, ci in graphs]
+    srv = serve.Server(ctx, slots=2, reserve_bytes=1 << 30, max_words=4)
+    qs = []
+    for i, k in enumerate([300, 3, 70, 1, 130, 256, 9]):
+        gi = i % 2
+        src = dg[gi].select_sources(2000 + i, k)
+        qs.append((gi, src, srv.submit(dg[gi], src, want="tables" if i % 3 == 1 else "digest")))
+    srv.drain()
+    for gi, src, q in qs:
+        lv, pr, _, _ = O.msbfs(*graphs[gi], src, rule=O.RULE_MINID)
+        if q.want == "tables":
+            np.testing.assert_array_equal(q.level.cpu().numpy(), lv)
+            np.testing.assert_array_equal(q.parent.cpu().numpy(), pr)
+        else:
+            np.testing.assert_array_equal(q.digest, _oracle_digest(lv, pr))
+    ctx.slots_release()
+    ctx.set_tuning(words=1)
+    for g in dg:
+        g.close()

@@ -233,10 +233,11 @@ xb_status capture_pass_levels(xb_ctx* c, BatchState* bs, const PassRes<W, NW, Of
 // Second half: the table pass through the row table and the fold into *sum.
 template <typename W, int NW, typename OffT>
 xb_status capture_pass_tables(xb_ctx* c, const PassRes<W, NW, OffT>& p, const xb_graph* g, const int32_t* src,
-                              int kb, int32_t* const* rows, xbk::PassSum* sum, cudaStream_t s) {
+                              int kb, int32_t* const* rows, xbk::PassSum* sum, cudaStream_t s,
+                              xbk::RowDigest* dig = nullptr) {
   constexpr int B = xbk::WB<W>::bits;
   int64_t launches = 0;
-  xb_status st = emit_tables<W, NW, OffT>(p, g, src, kb, rows, true, s, c->num_sms, &launches);
+  xb_status st = emit_tables<W, NW, OffT>(p, g, src, kb, rows, true, s, c->num_sms, &launches, dig);
   if (st != XB_OK) return st;
   const int hv = g->n_heavy > 0 ? 1 : 0;
   const int words = (kb + B - 1) / B;
@@ -649,9 +650,11 @@ xb_status slot_init(SlotState& sl) {
 
 // Captures the one-pass graph of a slot: clear the totals, the pass, the
 // digests of the flagged rows, and the copies of totals and digests to the
-// slot's pinned mirrors.
+// slot's pinned mirrors.  all_digest: every row of the pass is digest-only,
+// and the table pass sums the digests itself instead of writing rows for
+// k_row_digest to read.
 template <typename W, int NW, typename OffT>
-xb_status capture_slot_pass(xb_ctx* c, BatchState* bs, SlotState& sl, const xb_graph* g, int kb,
+xb_status capture_slot_pass(xb_ctx* c, BatchState* bs, SlotState& sl, const xb_graph* g, int kb, bool all_digest,
                             cudaGraphExec_t* exec) {
   constexpr int B = xbk::WB<W>::bits;
   cudaStream_t s = sl.stream;
@@ -662,11 +665,15 @@ xb_status capture_slot_pass(xb_ctx* c, BatchState* bs, SlotState& sl, const xb_g
     const PassRes<W, NW, OffT> p = capture_res<W, NW, OffT>(c, g, sl.ws, sl.ctr, sl.hpar);
     xb_status st = capture_pass_levels<W, NW, OffT>(c, bs, p, g, sl.d_src, kb, s);
     if (st != XB_OK) return st;
-    st = capture_pass_tables<W, NW, OffT>(c, p, g, sl.d_src, kb, sl.d_rows, sl.d_sum, s);
+    st = capture_pass_tables<W, NW, OffT>(c, p, g, sl.d_src, kb, sl.d_rows, sl.d_sum, s,
+                                          all_digest ? sl.d_dig : nullptr);
     if (st != XB_OK) return st;
-    const int gx = (int)std::max<int64_t>(1, std::min<int64_t>((g->n + 2047) / 2048, 64));
-    xbk::k_row_digest<<<dim3((unsigned)gx, (unsigned)kb), 256, 0, s>>>(sl.d_rows, sl.d_flags, kb, B, g->n, sl.d_dig);
-    XB_LAUNCH_CHECK("row digest");
+    if (!all_digest) {
+      const int gx = (int)std::max<int64_t>(1, std::min<int64_t>((g->n + 2047) / 2048, 64));
+      xbk::k_row_digest<<<dim3((unsigned)gx, (unsigned)kb), 256, 0, s>>>(sl.d_rows, sl.d_flags, kb, B, g->n,
+                                                                          sl.d_dig);
+      XB_LAUNCH_CHECK("row digest");
+    }
     XB_CUDA(cudaMemcpyAsync(sl.h_sum, sl.d_sum, sizeof(xbk::PassSum), cudaMemcpyDeviceToHost, s));
     XB_CUDA(cudaMemcpyAsync(sl.h_dig, sl.d_dig, sizeof(xbk::RowDigest) * kb, cudaMemcpyDeviceToHost, s));
     return XB_OK;
@@ -711,10 +718,11 @@ xb_status slot_launch(xb_ctx* c, int slot, xb_graph* g, const int32_t* sources, 
   st = grow(&sl.hpar, &cap, sizeof(int32_t) * (size_t)std::max(g->n_heavy, 1) * kHparRow, &sl.gen, "slot heavy slots");
   sl.hpar_bytes = cap;
   if (st != XB_OK) return st;
-  bool any_digest = false;
+  bool any_digest = false, all_digest = true;
   for (int j = 0; j < kb; j++) {
     if (!level_rows[j] != !parent_rows[j]) return fail(XB_ERR_ARG, "row " + std::to_string(j) + ": one of level/parent is NULL");
     any_digest |= level_rows[j] == nullptr;
+    all_digest &= level_rows[j] == nullptr;
   }
   if (any_digest) {  // SPP level rows then SPP parent rows, n_scratch entries apart
     cap = sl.scratch_bytes;
@@ -748,7 +756,7 @@ xb_status slot_launch(xb_ctx* c, int slot, xb_graph* g, const int32_t* sources, 
   std::memcpy(&abits, &c->tuning.pull_alpha, sizeof(abits));
   const std::vector<uint64_t> key = {sl.gen, (uint64_t)(uintptr_t)g, g->version, (uint64_t)kb, sizeof(W), NW,
                                      (uint64_t)heavy, abits, (uint64_t)c->tuning.level_cap,
-                                     (uint64_t)c->tuning.tile};
+                                     (uint64_t)c->tuning.tile, (uint64_t)all_digest};
   CachedGraph* hit = nullptr;
   for (auto& e : sl.cache)
     if (e.key == key) hit = &e;
@@ -770,8 +778,8 @@ xb_status slot_launch(xb_ctx* c, int slot, xb_graph* g, const int32_t* sources, 
     CachedGraph e;
     e.key = key;
     e.graphs = {g};
-    st = g->off64 ? capture_slot_pass<W, NW, int64_t>(c, bs, sl, g, kb, &e.exec)
-                  : capture_slot_pass<W, NW, int32_t>(c, bs, sl, g, kb, &e.exec);
+    st = g->off64 ? capture_slot_pass<W, NW, int64_t>(c, bs, sl, g, kb, all_digest, &e.exec)
+                  : capture_slot_pass<W, NW, int32_t>(c, bs, sl, g, kb, all_digest, &e.exec);
     if (st != XB_OK) return st;
     sl.cache.push_back(std::move(e));
     hit = &sl.cache.back();

@@ -485,7 +485,8 @@ xb_status emit_pull(const PassRes<W, NW, OffT>& p, const xb_graph* g, int cur, c
 // the parent row of the word's source s.
 template <typename W, int NW, typename OffT>
 xb_status emit_tables(const PassRes<W, NW, OffT>& p, const xb_graph* g, const int32_t* src, int kb,
-                      int32_t* const* rows, bool search_heavy, cudaStream_t s, int sms, int64_t* launches) {
+                      int32_t* const* rows, bool search_heavy, cudaStream_t s, int sms, int64_t* launches,
+                      xbk::RowDigest* dig = nullptr) {
   constexpr int B = xbk::WB<W>::bits;
   const int TAB_WARPS = p.tile == 1 ? kTabWarps1 : kTabWarps0;
   const int64_t ntiles = (p.n + 31) / 32;
@@ -503,7 +504,15 @@ xb_status emit_tables(const PassRes<W, NW, OffT>& p, const xb_graph* g, const in
     }
   }
   // all words of the pass in one launch (a tile's words share sectors)
-  if (p.tile == 1)
+  // dig: every row is digest-only; the table pass sums the digests instead
+  // of writing rows
+  if (dig && p.tile == 1)
+    xbk::k_tables<W, NW, OffT, kTabWarps1, 2, true><<<tab_grid, kTabWarps1 * 32, 0, s>>>(
+        p.n, p.ro, p.ci, p.seen, p.pl, kb, p.heavy, rows, p.ctr, p.ppos, p.pushed, src, g->d_hidx_of, p.hpar, dig);
+  else if (dig)
+    xbk::k_tables<W, NW, OffT, kTabWarps0, 4, true><<<tab_grid, kTabWarps0 * 32, 0, s>>>(
+        p.n, p.ro, p.ci, p.seen, p.pl, kb, p.heavy, rows, p.ctr, p.ppos, p.pushed, src, g->d_hidx_of, p.hpar, dig);
+  else if (p.tile == 1)
     xbk::k_tables<W, NW, OffT, kTabWarps1, 2><<<tab_grid, kTabWarps1 * 32, 0, s>>>(
         p.n, p.ro, p.ci, p.seen, p.pl, kb, p.heavy, rows, p.ctr, p.ppos, p.pushed, src, g->d_hidx_of, p.hpar);
   else

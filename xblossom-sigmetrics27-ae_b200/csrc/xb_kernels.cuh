@@ -1354,32 +1354,68 @@ __device__ __forceinline__ void vertex_levels(const W* __restrict__ seen, const 
   lvl1 = sv & p0 & ~p1 & ~hi;
 }
 
+// Per-source digest of a traversal row (serving results without tables).
+struct RowDigest {
+  unsigned long long reached;    // vertices with level >= 0
+  unsigned long long level_sum;  // sum of their levels
+  unsigned long long row_hash;   // sum of row_entry_hash over them (mod 2^64)
+  unsigned int depth;            // largest level
+  unsigned int pad;
+};
+
+// Hash of one (vertex, level, parent) entry: the splitmix64 finalizer
+// (Steele, Lea, Flood 2014) of the vertex id times the golden-ratio constant
+// XOR the (level, parent) pair packed into 64 bits.
+__host__ __device__ __forceinline__ unsigned long long row_entry_hash(int64_t v, int32_t level, int32_t parent) {
+  unsigned long long z = (unsigned long long)v * 0x9E3779B97F4A7C15ull;
+  z ^= ((unsigned long long)(uint32_t)level << 32) | (unsigned long long)(uint32_t)parent;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
 // One warp per 32-vertex tile.  Parents of bits reached by a pull step come
-// from the recorded p8 index (ci[ro[v] + p8[v][s]]).  Bits reached by a push
+// from the recorded p8 index (ci[ro[v] + p8[v][s]]).
+//
+// DIG: every row of the pass is digest-only.  Nothing is stored but the
+// parents the search finds (into the rows' parent pointers, scratch rows);
+// each (vertex, source) entry adds to its source's RowDigest instead: warp
+// reductions over the tile's 32 vertices per source, block totals in shared
+// memory, one set of global atomics per block and source (dig[row] must be
+// zero at launch).  The sums equal k_row_digest's over the rows the plain
+// variant would have written.  Bits reached by a push
 // step (and every bit of a vertex whose degree exceeds 256) are searched:
 // rounds over the flattened, still-needed adjacency (ascending within each
 // vertex), U x 32 edges per round, loads issued up front; a segmented
 // exclusive prefix OR in edge order hands each needed bit to its first
 // (= smallest-id) matching neighbour.
-template <typename W, int NW, typename OffT, int WARPS, int U>
-__global__ void __launch_bounds__(WARPS * 32, 24 / WARPS) k_tables(int64_t n, const OffT* __restrict__ ro,
+template <typename W, int NW, typename OffT, int WARPS, int U, bool DIG = false>
+__global__ void __launch_bounds__(WARPS * 32, (DIG ? 20 : 24) / WARPS) k_tables(int64_t n, const OffT* __restrict__ ro,
                                                        const int32_t* __restrict__ ci, const W* __restrict__ seen,
                                                        Planes<W, NW> pl, int kb, int heavy,
                                                        int32_t* const* __restrict__ rows, Ctrs* ctr,
                                                        const W* __restrict__ ppos, const W* __restrict__ pushed,
                                                        const int32_t* __restrict__ wsrc,
                                                        const int32_t* __restrict__ hidx_of,
-                                                       const int32_t* __restrict__ hpar) {
+                                                       const int32_t* __restrict__ hpar,
+                                                       RowDigest* __restrict__ dig = nullptr) {
   constexpr int B = WB<W>::bits;
   constexpr int ROW = B * NW;
   const int nplanes = ctr->b.nplanes;
   __shared__ int32_t s_src[NW][B];
   __shared__ int32_t* s_row[NW][2][B];
+  // DIG: block totals per source (reached, level sum, hash sum; depth)
+  __shared__ unsigned long long s_dsum[DIG ? NW * B : 1][3];
+  __shared__ unsigned int s_ddep[DIG ? NW * B : 1];
   for (int j = threadIdx.x; j < NW * B; j += blockDim.x) {
     const int w = j / B, s = j % B;
     s_src[w][s] = j < kb ? wsrc[j] : -1;
     s_row[w][0][s] = j < kb ? rows[w * 2 * B + s] : nullptr;
     s_row[w][1][s] = j < kb ? rows[w * 2 * B + B + s] : nullptr;
+    if constexpr (DIG) {
+      s_dsum[j][0] = s_dsum[j][1] = s_dsum[j][2] = 0;
+      s_ddep[j] = 0;
+    }
   }
   __syncthreads();
   const int nwords = (kb + B - 1) / B;
@@ -1587,13 +1623,43 @@ __global__ void __launch_bounds__(WARPS * 32, 24 / WARPS) k_tables(int64_t n, co
               if ((svb >> i) & 1)
                 for (int j = RP; j < nplanes; j++) lv[i] |= (int32_t)((pl.get(j, v, wi) >> (sb + i)) & 1) << j;
           }
+          if constexpr (DIG) {
 #pragma unroll
-          for (int i = 0; i < 8; i++) {
-            const int s = sb + i;
-            if (s < kbw && valid) {
-              const bool hit = (svb >> i) & 1;
-              __stcs(&s_row[wi][0][s][v], hit ? lv[i] : -1);
-              if (!((ndb >> i) & 1)) __stcs(&s_row[wi][1][s][v], hit ? pr[i] : -1);
+            for (int i = 0; i < 8; i++) {
+              const int s = sb + i;
+              const bool hit = s < kbw && valid && ((svb >> i) & 1);
+              int32_t par = pr[i];
+              // a searched parent was stored in the scratch row by this warp
+              if (hit && ((ndb >> i) & 1)) par = __ldcg(&s_row[wi][1][s][v]);
+              const unsigned long long hsh = hit ? row_entry_hash(v, lv[i], par) : 0ull;
+              const unsigned lvu = hit ? (unsigned)lv[i] : 0u;
+              // 32-bit warp reductions; the 64-bit sums are rebuilt from
+              // pieces that cannot overflow over 32 lanes
+              const unsigned cnt = __popc(__ballot_sync(0xffffffffu, hit));
+              const unsigned l0 = __reduce_add_sync(0xffffffffu, lvu & 0xFFFFu);
+              const unsigned l1 = __reduce_add_sync(0xffffffffu, lvu >> 16);
+              const unsigned dm = __reduce_max_sync(0xffffffffu, lvu);
+              const unsigned h0 = __reduce_add_sync(0xffffffffu, (unsigned)(hsh & 0xFFFFu));
+              const unsigned h1 = __reduce_add_sync(0xffffffffu, (unsigned)((hsh >> 16) & 0xFFFFu));
+              const unsigned h2 = __reduce_add_sync(0xffffffffu, (unsigned)(hsh >> 32));
+              if (lane == i && cnt) {
+                const int j = wi * B + s;
+                atomicAdd(&s_dsum[j][0], (unsigned long long)cnt);
+                atomicAdd(&s_dsum[j][1], (unsigned long long)l0 + ((unsigned long long)l1 << 16));
+                atomicAdd(&s_dsum[j][2], (unsigned long long)h0 + ((unsigned long long)h1 << 16) +
+                                             ((unsigned long long)h2 << 32));
+                atomicMax(&s_ddep[j], dm);
+              }
+            }
+          } else {
+#pragma unroll
+            for (int i = 0; i < 8; i++) {
+              const int s = sb + i;
+              if (s < kbw && valid) {
+                const bool hit = (svb >> i) & 1;
+                __stcs(&s_row[wi][0][s][v], hit ? lv[i] : -1);
+                if (!((ndb >> i) & 1)) __stcs(&s_row[wi][1][s][v], hit ? pr[i] : -1);
+              }
             }
           }
         }
@@ -1604,6 +1670,16 @@ __global__ void __launch_bounds__(WARPS * 32, 24 / WARPS) k_tables(int64_t n, co
   }
   pe = warp_sum_u64(pe);
   if (lane == 0 && pe) atomicAdd(&ctr->b.parent_edges, pe);
+  if constexpr (DIG) {
+    __syncthreads();
+    for (int j = threadIdx.x; j < kb; j += blockDim.x) {
+      if (s_dsum[j][0] == 0) continue;
+      atomicAdd(&dig[j].reached, s_dsum[j][0]);
+      atomicAdd(&dig[j].level_sum, s_dsum[j][1]);
+      atomicAdd(&dig[j].row_hash, s_dsum[j][2]);
+      atomicMax(&dig[j].depth, s_ddep[j]);
+    }
+  }
 }
 
 // Table pass for heavy vertices, scan step, for the bits a push step reached
@@ -1998,25 +2074,6 @@ __global__ void __launch_bounds__(1024) k_fifo_parents(int64_t n, const OffT* __
 // row_entry_hash(v, level[v], parent[v]), so moving a parent or a level from
 // one vertex to another changes it, while the sum keeps it independent of the
 // order the GPU visits the vertices in.
-struct RowDigest {
-  unsigned long long reached;    // vertices with level >= 0
-  unsigned long long level_sum;  // sum of their levels
-  unsigned long long row_hash;   // sum of row_entry_hash over them (mod 2^64)
-  unsigned int depth;            // largest level
-  unsigned int pad;
-};
-
-// Hash of one (vertex, level, parent) entry: the splitmix64 finalizer
-// (Steele, Lea, Flood 2014) of the vertex id times the golden-ratio constant
-// XOR the (level, parent) pair packed into 64 bits.
-__host__ __device__ __forceinline__ unsigned long long row_entry_hash(int64_t v, int32_t level, int32_t parent) {
-  unsigned long long z = (unsigned long long)v * 0x9E3779B97F4A7C15ull;
-  z ^= ((unsigned long long)(uint32_t)level << 32) | (unsigned long long)(uint32_t)parent;
-  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
-  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
-  return z ^ (z >> 31);
-}
-
 // Digests of the pass rows the flags mark; rows are in the table pass layout
 // (word wi: level rows at rows[wi*2B + b], parent rows at rows[wi*2B + B + b]).
 // blockIdx.y = row within the pass; out[row] must be zero beforehand.
