@@ -107,6 +107,10 @@ typedef struct xb_tuning {
    * 1 = two rounds in flight at every layout and 8-warp table blocks. */
   int32_t tile;
   int64_t workspace_cap;
+  /* After a pull step, push when the frontier holds fewer than n/push_beta
+   * vertices (the traversal's tail); 0 = never. */
+  float push_beta;
+  int32_t pad;
 } xb_tuning;
 
 /* ---- status ------------------------------------------------------------ */

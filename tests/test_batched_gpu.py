@@ -23,7 +23,7 @@ LAYOUTS = [
 
 
 def _tune(ctx, **kw):
-    base = dict(word_bits=64, words=1, pull_alpha=64.0, heavy_degree=256, timing=0, chains=2, tile=0)
+    base = dict(word_bits=64, words=1, pull_alpha=64.0, heavy_degree=256, timing=0, chains=2, tile=0, push_beta=0.0)
     base.update(kw)
     ctx.set_tuning(**base)
 
@@ -72,6 +72,29 @@ def test_launch_tile_one(ctx, rmat12, layout, heavy):
     res, _ = ctx.traverse_batched([(g, src)])
     _check(ro, ci, src, res[0])
     _check(ro, ci, src, ctx.traverse(g, src))
+    g.close()
+    _tune(ctx)
+
+
+@pytest.mark.parametrize("beta", [2.0, 24.0])
+@pytest.mark.parametrize("layout", [0, 4])
+@pytest.mark.parametrize("heavy", [32, 256])
+def test_tail_push_rule(ctx, rmat12, beta, layout, heavy):
+    """tuning.push_beta: after a pull step, a frontier under n/push_beta
+    vertices is pushed (parents of its bits searched by the table pass,
+    heavy ones by the heavy-vertex search): same tables as the oracle on the
+    batched and the plain path."""
+    ro, ci = rmat12
+    _tune(ctx, chains=2, heavy_degree=heavy, pull_alpha=1024.0, push_beta=beta, **LAYOUTS[layout])
+    g = ctx.upload_arrays(ro, ci)
+    src = xbtrav.select_sources_csr(ro, 91, 150)
+    res, st = ctx.traverse_batched([(g, src)])
+    _check(ro, ci, src, res[0])
+    r = ctx.traverse(g, src)
+    _check(ro, ci, src, r)
+    if beta == 2.0:  # beyond each pass's first (push) level, the tail was pushed
+        spp = LAYOUTS[layout]["word_bits"] * LAYOUTS[layout]["words"]
+        assert r.stats["push_levels"] > (len(src) + spp - 1) // spp
     g.close()
     _tune(ctx)
 

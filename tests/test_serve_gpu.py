@@ -16,7 +16,7 @@ pytestmark = pytest.mark.gpu
 
 
 def _tune(ctx, **kw):
-    base = dict(word_bits=64, words=1, pull_alpha=256.0, heavy_degree=256, timing=0, chains=2, tile=0)
+    base = dict(word_bits=64, words=1, pull_alpha=256.0, heavy_degree=256, timing=0, chains=2, tile=0, push_beta=0.0)
     base.update(kw)
     ctx.set_tuning(**base)
 

@@ -102,6 +102,7 @@ struct BatchState {
   uint64_t tick = 0;
   std::vector<CachedGraph> cache;
   int level_bound = 0;  // of the pass being captured (xbe::level_bound)
+  long long push_below = 0;  // of the pass being captured (xbe::push_below)
 };
 
 namespace {
@@ -172,7 +173,7 @@ xb_status capture_step(BatchState* bs, const PassRes<W, NW, OffT>& p, const xb_g
   cudaGraphConditionalHandle hsw;
   xb_status st = make_handle(b0, 2, cudaGraphCondAssignDefault, &hsw);
   if (st != XB_OK) return st;
-  xbk::k_step_begin<<<1, 1, 0, b0>>>(p.ctr, cur, alpha, p.nplanes_alloc, bs->level_bound, 1, hsw);
+  xbk::k_step_begin<<<1, 1, 0, b0>>>(p.ctr, cur, alpha, p.nplanes_alloc, bs->level_bound, 1, hsw, bs->push_below);
   xbk::k_zero_plane<W><<<(int)std::max<int64_t>(1, std::min<int64_t>((p.n * NW + 255) / 256, (int64_t)sms * 8)), 256,
                          0, b0>>>(p.pl.ph, p.pl.stride, p.n * NW, p.ctr);
   XB_LAUNCH_CHECK("step control");
@@ -225,6 +226,7 @@ xb_status capture_pass_levels(xb_ctx* c, BatchState* bs, const PassRes<W, NW, Of
   const float alpha = c->tuning.pull_alpha > 0 ? c->tuning.pull_alpha : 1024.0f;
   const StepShape sh = graph_shape<W, NW, OffT>(g, sms, p.tile);
   bs->level_bound = level_bound(c, p.nplanes_alloc);
+  bs->push_below = push_below(c, g);
   xb_status st = emit_pass_init<W, NW, OffT>(p, g, src, kb, s, sms, true);
   if (st != XB_OK) return st;
   return capture_level_loop<W, NW, OffT>(bs, p, g, kb, alpha, sh, s, sms);
@@ -524,11 +526,14 @@ xb_status run_batched(xb_ctx* c, const std::vector<xb_batch_item>& items, const 
                                (uint64_t)nch,
                                (uint64_t)items.size(),
                                (uint64_t)c->tuning.level_cap,
-                               (uint64_t)c->tuning.tile};
+                               (uint64_t)c->tuning.tile,
+                               0};
   {
-    uint32_t abits = 0;
+    uint32_t abits = 0, bbits = 0;
     std::memcpy(&abits, &c->tuning.pull_alpha, sizeof(abits));
+    std::memcpy(&bbits, &c->tuning.push_beta, sizeof(bbits));
     key[4] = abits;
+    key[9] = bbits;
   }
   for (const auto& it : items) {
     key.push_back((uint64_t)(uintptr_t)it.graph);
@@ -752,11 +757,12 @@ xb_status slot_launch(xb_ctx* c, int slot, xb_graph* g, const int32_t* sources, 
     sl.h_flags[j] = flag;
   }
   // cached one-pass graph
-  uint32_t abits = 0;
+  uint32_t abits = 0, bbits = 0;
   std::memcpy(&abits, &c->tuning.pull_alpha, sizeof(abits));
+  std::memcpy(&bbits, &c->tuning.push_beta, sizeof(bbits));
   const std::vector<uint64_t> key = {sl.gen, (uint64_t)(uintptr_t)g, g->version, (uint64_t)kb, sizeof(W), NW,
                                      (uint64_t)heavy, abits, (uint64_t)c->tuning.level_cap,
-                                     (uint64_t)c->tuning.tile, (uint64_t)all_digest};
+                                     (uint64_t)c->tuning.tile, (uint64_t)all_digest, bbits};
   CachedGraph* hit = nullptr;
   for (auto& e : sl.cache)
     if (e.key == key) hit = &e;

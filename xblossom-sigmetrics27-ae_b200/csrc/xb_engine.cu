@@ -306,7 +306,8 @@ xb_status run_plain(xb_ctx* c, xb_graph* g, const int32_t* d_sources, int32_t k,
     int cur = 0;
     for (;;) {
       // the device decides the step; the host reads the decision back
-      xbk::k_step_begin<<<1, 1, 0, c->stream>>>(p.ctr, cur, alpha, p.nplanes_alloc, bound, 0, 0);
+      xbk::k_step_begin<<<1, 1, 0, c->stream>>>(p.ctr, cur, alpha, p.nplanes_alloc, bound, 0, 0,
+                                                push_below(c, g));
       XB_LAUNCH_CHECK("step begin");
       XB_CUDA(cudaMemcpyAsync(c->h_ctr, p.ctr, sizeof(xbk::Ctrs), cudaMemcpyDeviceToHost, c->stream));
       XB_CUDA(cudaStreamSynchronize(c->stream));
@@ -470,6 +471,7 @@ xb_status xb_ctx_set_tuning(xb_ctx* c, const xb_tuning* t) {
   if (t->chains < 0 || t->chains > 16) return fail(XB_ERR_ARG, "chains must be in [0, 16]");
   if (t->level_cap < 0 || t->workspace_cap < 0) return fail(XB_ERR_ARG, "level_cap and workspace_cap must be >= 0");
   if (t->tile != 0 && t->tile != 1) return fail(XB_ERR_ARG, "tile must be 0 or 1");
+  if (!(t->push_beta >= 0)) return fail(XB_ERR_ARG, "push_beta must be >= 0");
   c->tuning = *t;
   if (c->tuning.chains == 0) c->tuning.chains = 4;
   return XB_OK;

@@ -219,6 +219,12 @@ inline int level_bound(const xb_ctx* c, int nplanes_alloc) {
   return (int)b;
 }
 
+// Frontier size below which a step after a pull pushes (tuning.push_beta;
+// 0 = the alpha rule alone).
+inline long long push_below(const xb_ctx* c, const xb_graph* g) {
+  return c->tuning.push_beta > 0 ? (long long)((double)g->n / (double)c->tuning.push_beta) : 0;
+}
+
 // Refuses a working-memory allocation above the context's tuning.workspace_cap.
 inline xb_status check_workspace_cap(const xb_ctx* c, size_t bytes, const char* what) {
   if (c->tuning.workspace_cap > 0 && (int64_t)bytes > c->tuning.workspace_cap)
@@ -496,7 +502,7 @@ xb_status emit_tables(const PassRes<W, NW, OffT>& p, const xb_graph* g, const in
     if (kb - wi * B <= 0) break;
     if (g->n_heavy > 0 && search_heavy) {
       // heavy vertices reached by a push step at level >= 2: search their parents
-      const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(g->n_hitems, (int64_t)sms * 8));
+      const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((g->n_hitems + 31) / 32, (int64_t)sms * 8));
       xbk::k_tables_heavy_scan<W, NW, OffT><<<grid, 256, 0, s>>>(g->d_heavy, g->d_hitems, g->n_hitems, p.ro, p.ci,
                                                                  p.seen, p.pl, wi, kTableChunk, p.hpar, p.ctr,
                                                                  p.pushed);

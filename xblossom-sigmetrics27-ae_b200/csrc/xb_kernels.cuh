@@ -1703,15 +1703,36 @@ __global__ void __launch_bounds__(256) k_tables_heavy_scan(const int32_t* __rest
   const int nplanes = ctr->b.nplanes;
   __shared__ W s_wor[8];
   __shared__ W s_claimed;
+  __shared__ int32_t s_items[32];
+  __shared__ int s_nitems;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  for (int64_t it = blockIdx.x; it < nitems; it += gridDim.x) {
-    const int2 item = items[it];
+  // groups of 32 items: the first warp checks them for needed bits at once,
+  // the block then walks only the items that have some (after a push step
+  // only few items have any, and a walk pays a dependent-load latency per
+  // item); groups small enough that every block gets some
+  for (int64_t gbase = (int64_t)blockIdx.x * 32; gbase < nitems; gbase += (int64_t)gridDim.x * 32) {
+   {
+    if (threadIdx.x == 0) s_nitems = 0;
+    __syncthreads();
+    const int64_t it = gbase + threadIdx.x;
+    bool has = false;
+    if (threadIdx.x < 32 && it < nitems) {
+      const int64_t v = hlist[items[it].x];
+      W sv, p0, p1, root, lvl1;
+      vertex_levels<W, NW>(seen, pl, nplanes, v, wi, sv, p0, p1, root, lvl1);
+      has = (sv & ~root & ~lvl1 & pushed[v * NW + wi]) != 0;
+    }
+    if (has) s_items[atomicAdd(&s_nitems, 1)] = (int32_t)threadIdx.x;
+    __syncthreads();
+   }
+   const int nlisted = s_nitems;
+   for (int li = 0; li < nlisted; li++) {
+    const int2 item = items[gbase + s_items[li]];
     const int64_t idx = item.x;
     const int64_t v = hlist[idx];
     W sv, p0, p1, root, lvl1;
     vertex_levels<W, NW>(seen, pl, nplanes, v, wi, sv, p0, p1, root, lvl1);
     const W need = sv & ~root & ~lvl1 & pushed[v * NW + wi];
-    if (!need) continue;  // uniform
     const W t0 = ~p0, t1 = ~(p0 ^ p1);
     const int64_t beg = ro[v], end = ro[v + 1];
     const int64_t c0 = beg + (int64_t)item.y * chunk;
@@ -1777,6 +1798,8 @@ __global__ void __launch_bounds__(256) k_tables_heavy_scan(const int32_t* __rest
       if (threadIdx.x == 0) atomicAdd(&ctr->b.parent_edges, pe);
       __syncthreads();
     }
+   }
+   __syncthreads();  // s_items / s_nitems are rewritten by the next group
   }
 }
 
@@ -1800,11 +1823,14 @@ static __global__ void k_pass_init(Ctrs* ctr, long long m) {
 
 // Decides the next step from the current frontier's counters lv[cur]:
 // dir = 0 push, 1 pull (frontier edges * alpha > unfinished edges), 2 done.
+// After a pull step, a frontier of fewer than push_below vertices is pushed
+// (0 = never): the tail of a traversal, where a pull would still sweep every
+// light vertex for a handful of frontier vertices.
 // Advances the level, picks the level plane to clear, bumps the stamp epoch
 // and zeroes the next frontier's counters.  A frontier still alive at
 // level_bound stops the loop with the error flag set.
 static __global__ void k_step_begin(Ctrs* ctr, int cur, float alpha, int nplanes_alloc, int level_bound,
-                                    int graph_mode, cudaGraphConditionalHandle hswitch) {
+                                    int graph_mode, cudaGraphConditionalHandle hswitch, long long push_below = 0) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   BatchCtr& b = ctr->b;
   const LevelCtr& lc = ctr->lv[cur];
@@ -1818,6 +1844,7 @@ static __global__ void k_step_begin(Ctrs* ctr, int cur, float alpha, int nplanes
   if (b.dir != 2 && b.err == 0 && alive && b.level >= level_bound) b.err = 2;
   if (b.dir != 2 && b.err == 0 && alive) {
     dir = ((double)lc.edges * (double)alpha > (double)b.m_unfinished) ? 1 : 0;
+    if (dir == 1 && b.dir == 1 && (long long)lc.n_light + lc.n_heavy < push_below) dir = 0;
     b.level += 1;
     if (b.nplanes < nplanes_alloc && (1 << b.nplanes) <= b.level) {
       b.zero_plane = b.nplanes;

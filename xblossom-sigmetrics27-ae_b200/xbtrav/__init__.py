@@ -90,6 +90,8 @@ class XbTuning(C.Structure):
         ("level_cap", C.c_int32),
         ("tile", C.c_int32),
         ("workspace_cap", C.c_int64),
+        ("push_beta", C.c_float),
+        ("pad", C.c_int32),
     ]
 
 

@@ -2,7 +2,9 @@
 
 Searches sources-per-word (32/64), words traversed together (1/2/4), the
 degree cutoff between the per-lane light pull and the per-warp heavy pull,
-the push/pull switch factor alpha, the launch tile of the pull and table
+the push/pull switch factor alpha, the tail push threshold push_beta (push
+after a pull once the frontier holds fewer than n/push_beta vertices; 0 =
+off), the launch tile of the pull and table
 kernels (xb_tuning.tile: rounds in flight per heavy-pull warp, warps per
 table block) and, for the batched path, the number of concurrent chains, by
 timing the engine's own calls (device-side CUDA events of xb_traverse or
@@ -23,10 +25,11 @@ DEFAULT_SPACE = {
     "words": [1, 2, 4],
     "heavy_degree": [128, 256, 512],
     "pull_alpha": [16.0, 64.0, 256.0, 1024.0],
+    "push_beta": [0.0, 24.0],
     "tile": [0, 1],
     "chains": [1, 2, 4, 8],
 }
-KEYS = ("word_bits", "words", "heavy_degree", "pull_alpha", "tile", "chains")
+KEYS = ("word_bits", "words", "heavy_degree", "pull_alpha", "push_beta", "tile", "chains")
 
 
 def _time_config(ctx, graph, sources, cfg: dict, reps: int, path: str) -> float:
@@ -56,7 +59,8 @@ def autotune(ctx, graph, sources, space: dict | None = None, reps: int = 5, stag
 
     staged=True searches coordinate-wise (word layout first with the current
     cutoffs, then cutoffs and alpha for the winning layout, then the launch
-    tile, then chains) instead of the full grid.
+    tail push threshold, then the launch tile, then chains) instead of the
+    full grid.
     """
     space = dict(DEFAULT_SPACE if space is None else space)
     if path != "batched":
@@ -77,6 +81,9 @@ def autotune(ctx, graph, sources, space: dict | None = None, reps: int = 5, stag
         best = min(table, key=lambda x: x[1])[0]
         for h, a in itertools.product(space["heavy_degree"], space["pull_alpha"]):
             run(dict(best, heavy_degree=h, pull_alpha=a))
+        best = min(table, key=lambda x: x[1])[0]
+        for pb in space.get("push_beta", [best.get("push_beta", 0.0)]):
+            run(dict(best, push_beta=pb))
         best = min(table, key=lambda x: x[1])[0]
         for tl in space.get("tile", [best.get("tile", 0)]):
             run(dict(best, tile=tl))
