@@ -729,7 +729,9 @@ xb_status slot_launch(xb_ctx* c, int slot, xb_graph* g, const int32_t* sources, 
     any_digest |= level_rows[j] == nullptr;
     all_digest &= level_rows[j] == nullptr;
   }
-  if (any_digest) {  // SPP level rows then SPP parent rows, n_scratch entries apart
+  // scratch rows for the digest-only sources of a mixed pass; a pass of
+  // digest-only sources sums its digests in the table pass and needs none
+  if (any_digest && !all_digest) {  // SPP level rows then SPP parent rows, n_scratch entries apart
     cap = sl.scratch_bytes;
     st = grow(&sl.scratch, &cap, sizeof(int32_t) * 2 * SPP * (size_t)g->n, &sl.gen, "slot scratch rows");
     sl.scratch_bytes = cap;
@@ -747,8 +749,10 @@ xb_status slot_launch(xb_ctx* c, int slot, xb_graph* g, const int32_t* sources, 
       lv = level_rows[j];
       pr = parent_rows[j];
       if (!lv) {
-        lv = sl.scratch + (size_t)j * sl.n_scratch;
-        pr = sl.scratch + (size_t)(SPP + j) * sl.n_scratch;
+        if (!all_digest) {
+          lv = sl.scratch + (size_t)j * sl.n_scratch;
+          pr = sl.scratch + (size_t)(SPP + j) * sl.n_scratch;
+        }
         flag = 1;
       }
     }

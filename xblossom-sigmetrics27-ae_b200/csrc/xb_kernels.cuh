@@ -1377,13 +1377,13 @@ __host__ __device__ __forceinline__ unsigned long long row_entry_hash(int64_t v,
 // One warp per 32-vertex tile.  Parents of bits reached by a pull step come
 // from the recorded p8 index (ci[ro[v] + p8[v][s]]).
 //
-// DIG: every row of the pass is digest-only.  Nothing is stored but the
-// parents the search finds (into the rows' parent pointers, scratch rows);
-// each (vertex, source) entry adds to its source's RowDigest instead: warp
-// reductions over the tile's 32 vertices per source, block totals in shared
-// memory, one set of global atomics per block and source (dig[row] must be
-// zero at launch).  The sums equal k_row_digest's over the rows the plain
-// variant would have written.  Bits reached by a push
+// DIG: every row of the pass is digest-only and nothing is stored (the row
+// pointers are not used).  Each (vertex, source) entry adds to its source's
+// RowDigest instead: warp reductions over the tile's 32 vertices per source,
+// entries whose parent is searched added by the search itself, block totals
+// in shared memory, one set of global atomics per block and source (dig[row]
+// must be zero at launch).  The sums equal k_row_digest's over the rows the
+// plain variant would have written.  Bits reached by a push
 // step (and every bit of a vertex whose degree exceeds 256) are searched:
 // rounds over the flattened, still-needed adjacency (ascending within each
 // vertex), U x 32 edges per round, loads issued up front; a segmented
@@ -1523,7 +1523,20 @@ __global__ void __launch_bounds__(WARPS * 32, (DIG ? 20 : 24) / WARPS) k_tables(
           W mine = eq & ~excl & ~s_found[wib][k];
           while (mine) {
             const int b = ffs0(mine);
-            __stcs(&s_row[wi][1][b][tile * 32 + k], col[u]);
+            if constexpr (DIG) {
+              // digest-only rows: this entry's digest terms, its level read
+              // from the owner's planes (the row pass below skips it)
+              const int64_t vk = tile * 32 + k;
+              int32_t lvl = 0;
+              for (int j = 0; j < nplanes; j++) lvl |= (int32_t)((pl.get(j, vk, wi) >> b) & 1) << j;
+              const int jrow = wi * B + b;
+              atomicAdd(&s_dsum[jrow][0], 1ull);
+              atomicAdd(&s_dsum[jrow][1], (unsigned long long)lvl);
+              atomicAdd(&s_dsum[jrow][2], row_entry_hash(vk, lvl, col[u]));
+              atomicMax(&s_ddep[jrow], (unsigned)lvl);
+            } else {
+              __stcs(&s_row[wi][1][b][tile * 32 + k], col[u]);
+            }
             mine &= mine - 1;
           }
         }
@@ -1627,11 +1640,9 @@ __global__ void __launch_bounds__(WARPS * 32, (DIG ? 20 : 24) / WARPS) k_tables(
 #pragma unroll
             for (int i = 0; i < 8; i++) {
               const int s = sb + i;
-              const bool hit = s < kbw && valid && ((svb >> i) & 1);
-              int32_t par = pr[i];
-              // a searched parent was stored in the scratch row by this warp
-              if (hit && ((ndb >> i) & 1)) par = __ldcg(&s_row[wi][1][s][v]);
-              const unsigned long long hsh = hit ? row_entry_hash(v, lv[i], par) : 0ull;
+              // searched entries were added by the search above
+              const bool hit = s < kbw && valid && ((svb >> i) & 1) && !((ndb >> i) & 1);
+              const unsigned long long hsh = hit ? row_entry_hash(v, lv[i], pr[i]) : 0ull;
               const unsigned lvu = hit ? (unsigned)lv[i] : 0u;
               // 32-bit warp reductions; the 64-bit sums are rebuilt from
               // pieces that cannot overflow over 32 lanes
