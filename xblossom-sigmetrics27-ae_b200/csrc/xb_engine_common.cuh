@@ -113,7 +113,8 @@ constexpr int kFifoGroup = 64;
 constexpr int64_t kCiPad = 16;
 
 struct WsLayout {
-  size_t seen, F, N, p01, ph, pushed, p8, touched, fl_light, fl_heavy, nl_light, nl_heavy, stamp, fbits, nbits, total;
+  size_t seen, F, N, p01, ph, pushed, p8, touched, fl_light, fl_heavy, nl_light, nl_heavy, stamp, fbits, nbits, cdone,
+      total;
   int64_t plane_stride;  // in words
   int nplanes_alloc;
 };
@@ -154,6 +155,7 @@ inline WsLayout layout_for(int64_t n, int word_bytes, int nw) {
   const size_t bw = align_up((size_t)((std::max<int64_t>(n, 1) + 31) / 32) * 4);  // one bit per vertex
   L.fbits = o; o += bw;
   L.nbits = o; o += bw;
+  L.cdone = o; o += align_up((size_t)std::max<int64_t>(n, 1));  // one byte per light chunk (at most n)
   L.total = o;
   return L;
 }
@@ -283,6 +285,7 @@ struct PassRes {
   int tile = 0;  // xb_tuning.tile: launch tile of the pull and table kernels
   size_t state_bytes = 0, plane_bytes = 0, ppos_bytes = 0;
   int64_t bit_words = 0;  // 32-bit words of a frontier bitmap
+  uint8_t* cdone = nullptr;  // light chunks with no wanted vertex for the rest of the pass
   int nplanes_alloc = 3;
 };
 
@@ -304,6 +307,7 @@ PassRes<W, NW, OffT> pass_res(const xb_graph* g, void* ws, const WsLayout& L, xb
   p.lists[0] = xbk::Lists{(int32_t*)(base + L.fl_light), (int32_t*)(base + L.fl_heavy), (uint32_t*)(base + L.fbits)};
   p.lists[1] = xbk::Lists{(int32_t*)(base + L.nl_light), (int32_t*)(base + L.nl_heavy), (uint32_t*)(base + L.nbits)};
   p.bit_words = (g->n + 31) / 32;
+  p.cdone = (uint8_t*)(base + L.cdone);
   p.stamp = (int32_t*)(base + L.stamp);
   p.ctr = ctr;
   p.hpar = hpar;
@@ -362,6 +366,7 @@ xb_status emit_pass_init(const PassRes<W, NW, OffT>& p, const xb_graph* g, const
   XB_CUDA(cudaMemsetAsync(p.pl.ph, 0, p.plane_bytes, s));
   XB_CUDA(cudaMemsetAsync(p.pushed, 0, p.state_bytes, s));
   XB_CUDA(cudaMemsetAsync(p.ppos, 0, p.ppos_bytes, s));
+  if (g->n_lchunks > 0) XB_CUDA(cudaMemsetAsync(p.cdone, 0, (size_t)g->n_lchunks, s));
   if (g->n_heavy > 0) {  // parent slots of the heavy vertices (hub pulls fold in with atomicMin)
     const int64_t hcount = (int64_t)g->n_heavy * kHparRow;
     xbk::k_fill<int32_t><<<(int)std::min<int64_t>((hcount + 255) / 256, (int64_t)sms * 8), 256, 0, s>>>(p.hpar, hcount,
@@ -449,7 +454,7 @@ xb_status emit_pull(const PassRes<W, NW, OffT>& p, const xb_graph* g, int cur, c
     if (g->n_lorder > 0) {
       xbk::k_pull_lanes<W, NW, OffT, lane_warps<NW>()><<<sh.pull_grid, lane_warps<NW>() * 32, 0, s>>>(
           g->n_lchunks, g->d_lchunk, g->d_lorder, p.ro, p.ci, F, p.seen, N, p.pl, active, p.heavy, nl, p.ctr, cur,
-          p.ppos, p.n, fl.bits);
+          p.ppos, p.n, fl.bits, p.cdone);
       (*launches)++;
     }
   } else {

@@ -867,7 +867,8 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 3) k_pull_lanes(i
                                                            W* seen, W* N, Planes<W, NW> pl, Masks<W, NW> active,
                                                            int heavy, Lists nl, Ctrs* ctr, int cur,
                                                            W* __restrict__ ppos, int64_t n,
-                                                           const uint32_t* __restrict__ fbits) {
+                                                           const uint32_t* __restrict__ fbits,
+                                                           uint8_t* __restrict__ cdone) {
   const int level = ctr->b.level;
   __shared__ int32_t s_qv[WARPS][64];
   __shared__ W s_qs[WARPS][64][NW];
@@ -890,6 +891,10 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 3) k_pull_lanes(i
     chunk = __shfl_sync(0xffffffffu, chunk, 0);
     const bool last = chunk >= nchunks;
     if (!last) {
+      // a chunk none of whose vertices wanted a live bit keeps wanting none:
+      // live bits only shrink over a pass and seen bits only grow
+      if (cdone[chunk]) continue;
+      bool chunk_want = false;
       const int64_t c0 = lchunk[chunk], c1 = lchunk[chunk + 1];
       for (int64_t t = c0; t < c1; t += 32) {
         const int64_t idx = t + lane;
@@ -906,6 +911,7 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 3) k_pull_lanes(i
           v_sweep++;
         }
         const unsigned wm = __ballot_sync(0xffffffffu, want);
+        chunk_want = chunk_want || wm != 0;
         if (want) {
           const int slot = qn + __popc(wm & ((1u << lane) - 1u));
           s_qv[wib][slot] = v;
@@ -941,6 +947,7 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 3) k_pull_lanes(i
                                         ppos, sacc, e_scan, spp, fb);
         }
       }
+      if (!chunk_want && lane == 0) cdone[chunk] = 1;
     }
     if (last) {
       // the list is exhausted: drain the partial queue
@@ -1438,9 +1445,25 @@ __global__ void __launch_bounds__(WARPS * 32, (DIG ? 20 : 24) / WARPS) k_tables(
     const int kbw = min(B, kb - wi * B);
     const int64_t v = tile * 32 + lane;
     const bool valid = v < n;
+    // a tile no source of this word reached (isolated vertices, small
+    // components): every entry is -1, nothing else to read; in other tiles
+    // an unreached lane skips its loads the same way
+    const bool reached = valid && seen[v * NW + wi] != 0;
+    if (!__any_sync(0xffffffffu, reached)) {
+      if constexpr (!DIG) {
+        if (valid) {
+#pragma unroll 4
+          for (int s = 0; s < kbw; s++) {
+            __stcs(&s_row[wi][0][s][v], -1);
+            __stcs(&s_row[wi][1][s][v], -1);
+          }
+        }
+      }
+      continue;
+    }
     W sv = 0, p0 = 0, p1 = 0, root = 0, lvl1 = 0;
     int64_t beg = 0, dg = 0;
-    if (valid) {
+    if (reached) {
       vertex_levels<W, NW>(seen, pl, nplanes, v, wi, sv, p0, p1, root, lvl1);
       beg = ro[v];
       dg = (int64_t)ro[v + 1] - beg;
@@ -1448,7 +1471,7 @@ __global__ void __launch_bounds__(WARPS * 32, (DIG ? 20 : 24) / WARPS) k_tables(
     const bool is_heavy = dg > heavy;
     const bool has_p8 = dg <= kP8MaxDegree;
     W pw = 0;
-    if (valid && !is_heavy && has_p8) pw = pushed[v * NW + wi];
+    if (reached && !is_heavy && has_p8) pw = pushed[v * NW + wi];
     // bits whose parent must be searched (level-1 bits: the source itself)
     const W need = (valid && !is_heavy) ? (sv & ~root & ~lvl1 & (has_p8 ? pw : ~(W)0)) : (W)0;
     s_need[wib][lane] = need;
@@ -1559,7 +1582,7 @@ __global__ void __launch_bounds__(WARPS * 32, (DIG ? 20 : 24) / WARPS) k_tables(
       // parent sources: recorded position (light, pulled; bit-sliced in 8
       // planes), recorded id (heavy), searched (written above), the source
       // itself (levels 0 and 1)
-      const bool use_pp = valid && !is_heavy && has_p8;
+      const bool use_pp = reached && !is_heavy && has_p8;
       const W* prow = ppos + (v * NW + wi) * 8;
       const int32_t* hrow = is_heavy ? hpar + (int64_t)hidx_of[v] * ROW + wi * B : nullptr;
       // the first kCiCache neighbours of the vertex: most recorded positions
@@ -1587,7 +1610,7 @@ __global__ void __launch_bounds__(WARPS * 32, (DIG ? 20 : 24) / WARPS) k_tables(
         L[1] = half32<W>(p1, h);
 #pragma unroll
         for (int j = 2; j < RP; j++)
-          L[j] = (valid && j < nplanes)
+          L[j] = (reached && j < nplanes)
                      ? reinterpret_cast<const uint32_t*>(pl.ph + (int64_t)(j - 2) * pl.stride + v * NW + wi)[h]
                      : 0u;
 #pragma unroll
