@@ -25,17 +25,24 @@ namespace {
 
 __global__ void k_alt_init(int64_t n, const int32_t* __restrict__ mate, int32_t* level, int32_t* parent,
                            int32_t* owner, int32_t* cand, int32_t* front, int32_t* fcount, int32_t* bad) {
-  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
-    const int32_t m = mate[v];
-    cand[v] = INT32_MAX;
-    if (m < -1 || m >= n || m == v || (m >= 0 && mate[m] != v)) atomicAdd(bad, 1);
-    if (m < 0) {
-      level[v] = 0;
-      parent[v] = owner[v] = (int32_t)v;
-      front[atomicAdd(fcount, 1)] = (int32_t)v;
-    } else {
-      level[v] = parent[v] = owner[v] = -1;
+  // warp-uniform rounds, so the frontier appends go out one atomic per warp
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t b0 = (int64_t)blockIdx.x * blockDim.x; b0 < n; b0 += stride) {
+    const int64_t v = b0 + threadIdx.x;
+    bool app = false;
+    if (v < n) {
+      const int32_t m = mate[v];
+      cand[v] = INT32_MAX;
+      if (m < -1 || m >= n || m == v || (m >= 0 && mate[m] != v)) atomicAdd(bad, 1);
+      if (m < 0) {
+        level[v] = 0;
+        parent[v] = owner[v] = (int32_t)v;
+        app = true;
+      } else {
+        level[v] = parent[v] = owner[v] = -1;
+      }
     }
+    xbk::warp_append(app, (int32_t)v, front, fcount);
   }
 }
 
@@ -88,18 +95,27 @@ __global__ void k_alt_resolve(const int32_t* __restrict__ touched, const int32_t
                               const int32_t* __restrict__ mate, const int32_t* __restrict__ cand, int32_t d,
                               int32_t* level, int32_t* parent, int32_t* owner, int32_t* next, int32_t* ncount) {
   const int32_t tcount = *tcount_p;
-  for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < tcount; i += gridDim.x * blockDim.x) {
-    const int32_t w = touched[i], x = mate[w];
-    const int32_t cw = cand[w], cx = cand[x];
-    if (!(cx == INT32_MAX || cw < cx || (cw == cx && w < x))) continue;  // x is the inner one
-    const int32_t r = owner[cw];
-    level[w] = 2 * d + 1;
-    parent[w] = cw;
-    owner[w] = r;
-    level[x] = 2 * d + 2;
-    parent[x] = w;
-    owner[x] = r;
-    next[atomicAdd(ncount, 1)] = x;
+  // warp-uniform rounds: the next frontier takes one atomic per warp
+  for (int32_t b0 = blockIdx.x * blockDim.x; b0 < tcount; b0 += gridDim.x * blockDim.x) {
+    const int32_t i = b0 + (int32_t)threadIdx.x;
+    bool app = false;
+    int32_t x = 0;
+    if (i < tcount) {
+      const int32_t w = touched[i];
+      x = mate[w];
+      const int32_t cw = cand[w], cx = cand[x];
+      if (cx == INT32_MAX || cw < cx || (cw == cx && w < x)) {  // else x is the inner one
+        const int32_t r = owner[cw];
+        level[w] = 2 * d + 1;
+        parent[w] = cw;
+        owner[w] = r;
+        level[x] = 2 * d + 2;
+        parent[x] = w;
+        owner[x] = r;
+        app = true;
+      }
+    }
+    xbk::warp_append(app, x, next, ncount);
   }
 }
 

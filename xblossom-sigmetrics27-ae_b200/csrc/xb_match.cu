@@ -101,15 +101,22 @@ template <typename OffT>
 __global__ void k_mm_init(int64_t n, const OffT* __restrict__ ro, const int32_t* __restrict__ mate, int32_t* st,
                           int32_t* pred, int32_t* base, int32_t* lock, int32_t* head, int32_t* front,
                           int32_t* fcount) {
-  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
-    const bool has_edge = ro[v + 1] > ro[v];
-    const bool exposed = mate[v] < 0;
-    st[v] = exposed ? mm_state((int32_t)v, kOuter) : -1;
-    pred[v] = -1;
-    base[v] = (int32_t)v;
-    lock[v] = 0;
-    head[v] = -1;
-    if (exposed && has_edge) front[atomicAdd(fcount, 1)] = (int32_t)v;  // isolated roots grow nothing
+  // warp-uniform rounds, so the frontier appends go out one atomic per warp
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t b0 = (int64_t)blockIdx.x * blockDim.x; b0 < n; b0 += stride) {
+    const int64_t v = b0 + threadIdx.x;
+    bool app = false;
+    if (v < n) {
+      const bool has_edge = ro[v + 1] > ro[v];
+      const bool exposed = mate[v] < 0;
+      st[v] = exposed ? mm_state((int32_t)v, kOuter) : -1;
+      pred[v] = -1;
+      base[v] = (int32_t)v;
+      lock[v] = 0;
+      head[v] = -1;
+      app = exposed && has_edge;  // isolated roots grow nothing
+    }
+    xbk::warp_append(app, (int32_t)v, front, fcount);
   }
 }
 
@@ -122,17 +129,24 @@ __global__ void k_mm_init(int64_t n, const OffT* __restrict__ ro, const int32_t*
 template <typename OffT>
 __global__ void k_mm_reinit(int64_t n, const OffT* __restrict__ ro, int32_t* st, int32_t* pred, int32_t* base,
                             const int32_t* __restrict__ lock, int32_t* head, int32_t* front, int32_t* fcount) {
-  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
-    head[v] = -1;
-    const int32_t sv = st[v];
-    if (sv == -1) continue;
-    if (lock[sv >> 2]) {
-      st[v] = -1;
-      pred[v] = -1;
-      base[v] = (int32_t)v;
-    } else if ((sv & 3) == kOuter && ro[v + 1] > ro[v]) {
-      front[atomicAdd(fcount, 1)] = (int32_t)v;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t b0 = (int64_t)blockIdx.x * blockDim.x; b0 < n; b0 += stride) {
+    const int64_t v = b0 + threadIdx.x;
+    bool app = false;
+    if (v < n) {
+      head[v] = -1;
+      const int32_t sv = st[v];
+      if (sv != -1) {
+        if (lock[sv >> 2]) {
+          st[v] = -1;
+          pred[v] = -1;
+          base[v] = (int32_t)v;
+        } else {
+          app = (sv & 3) == kOuter && ro[v + 1] > ro[v];
+        }
+      }
     }
+    xbk::warp_append(app, (int32_t)v, front, fcount);  // one atomic per warp
   }
 }
 
