@@ -365,7 +365,6 @@ xb_status emit_pass_init(const PassRes<W, NW, OffT>& p, const xb_graph* g, const
   XB_CUDA(cudaMemsetAsync(p.pl.p01, 0, 2 * p.plane_bytes, s));
   XB_CUDA(cudaMemsetAsync(p.pl.ph, 0, p.plane_bytes, s));
   XB_CUDA(cudaMemsetAsync(p.pushed, 0, p.state_bytes, s));
-  XB_CUDA(cudaMemsetAsync(p.ppos, 0, p.ppos_bytes, s));
   if (g->n_lchunks > 0) XB_CUDA(cudaMemsetAsync(p.cdone, 0, (size_t)g->n_lchunks, s));
   if (g->n_heavy > 0) {  // parent slots of the heavy vertices (hub pulls fold in with atomicMin)
     const int64_t hcount = (int64_t)g->n_heavy * kHparRow;
@@ -374,7 +373,7 @@ xb_status emit_pass_init(const PassRes<W, NW, OffT>& p, const xb_graph* g, const
   }
   xbk::k_pass_init<<<1, 1, 0, s>>>(p.ctr, (long long)g->m);
   xbk::k_init_batch<W, NW, OffT><<<1, 256, 0, s>>>(src, kb, p.ro, p.buf[0], p.seen, p.pl, active_mask<W, NW>(kb),
-                                                   p.heavy, p.lists[0], p.ctr);
+                                                   p.heavy, p.lists[0], p.ctr, p.ppos);
   XB_LAUNCH_CHECK("pass init");
   return XB_OK;
 }
@@ -400,7 +399,7 @@ xb_status emit_push(const PassRes<W, NW, OffT>& p, const xb_graph* g, int cur, c
   }
   xbk::k_push_finalize<W, NW, OffT><<<sh.finalize_grid, 256, 0, s>>>(p.touched, p.ro, N, p.seen, p.pl,
                                                                      active_mask<W, NW>(kb), p.heavy, nl, p.ctr, cur,
-                                                                     p.pushed, fl.bits, p.bit_words);
+                                                                     p.pushed, fl.bits, p.bit_words, p.ppos);
   (*launches)++;
   XB_LAUNCH_CHECK("push step");
   return XB_OK;

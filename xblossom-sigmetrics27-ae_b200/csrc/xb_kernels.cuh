@@ -260,6 +260,17 @@ __device__ __forceinline__ W warp_or(W x) {
   return x;
 }
 
+// Zeroes the position-plane row of (v, word i).  Rows are not cleared per
+// pass: each is zeroed (or written whole) when its vertex first gets bits of
+// that word -- here for sources and pushed vertices, by the pull otherwise --
+// and rows of words a vertex never reaches are never read.
+template <typename W>
+__device__ __forceinline__ void ppos_zero_row(W* ppos, int64_t v, int nw, int i) {
+  W* r = ppos + (v * nw + i) * 8;
+#pragma unroll
+  for (int k = 0; k < 8; k++) r[k] = 0;
+}
+
 // Per-lane counter increments, kept in registers until the kernel ends.
 template <typename W, int NW>
 struct StatAcc {
@@ -331,7 +342,8 @@ __device__ __forceinline__ void flush_stats(StatAcc<W, NW>& acc, LevelCtr* nctr,
 // Batch initialisation: one block; thread t owns source slot t.
 template <typename W, int NW, typename OffT>
 __global__ void k_init_batch(const int32_t* __restrict__ src, int kb, const OffT* __restrict__ ro, W* F,
-                             W* seen, Planes<W, NW> pl, Masks<W, NW> active, int heavy, Lists fl, Ctrs* ctr) {
+                             W* seen, Planes<W, NW> pl, Masks<W, NW> active, int heavy, Lists fl, Ctrs* ctr,
+                             W* ppos = nullptr) {
   constexpr int B = WB<W>::bits;
   const int t = threadIdx.x;
   int32_t v = -1;
@@ -340,6 +352,7 @@ __global__ void k_init_batch(const int32_t* __restrict__ src, int kb, const OffT
     const W bit = (W)1 << (t % B);
     atomicOr(&F[(int64_t)v * NW + t / B], bit);
     atomicOr(&seen[(int64_t)v * NW + t / B], bit);
+    if (ppos) ppos_zero_row<W>(ppos, v, NW, t / B);  // sources sharing a row write the same zeros
   }
   __syncthreads();
   bool first = t < kb;
@@ -475,7 +488,8 @@ __global__ void k_push_heavy(const int32_t* __restrict__ list, const int32_t* __
 template <typename W, int NW, typename OffT>
 __global__ void k_push_finalize(const int32_t* __restrict__ touched, const OffT* __restrict__ ro, const W* N,
                                 W* seen, Planes<W, NW> pl, Masks<W, NW> active, int heavy, Lists nl, Ctrs* ctr,
-                                int cur, W* pushed, uint32_t* consumed_bits, int64_t bit_words) {
+                                int cur, W* pushed, uint32_t* consumed_bits, int64_t bit_words,
+                                W* ppos = nullptr) {
   const int level = ctr->b.level;
   LevelCtr* nctr = &ctr->lv[cur ^ 1];
   const int32_t cnt = nctr->n_touched;
@@ -498,6 +512,7 @@ __global__ void k_push_finalize(const int32_t* __restrict__ touched, const OffT*
         // bits reached by a push step have no recorded parent index: the
         // table pass searches their parents
         pushed[(int64_t)w * NW + i] |= nw[i];
+        if (ppos && nw[i] && !sw[i]) ppos_zero_row<W>(ppos, w, NW, i);  // first bits of this word
       }
       dg = deg_of(ro, w);
     } else {
@@ -850,9 +865,15 @@ __device__ __forceinline__ void pull_lane_vertex(bool act, int32_t v, const W (&
       N[(int64_t)v * NW + i] = acc[i];
       if (rec && acc[i]) {
         W* prow = ppos + ((int64_t)v * NW + i) * 8;
+        if (sw[i] == 0) {
+          // the vertex's first bits of this word: the row is written whole
 #pragma unroll
-        for (int k = 0; k < 8; k++)
-          if (pp(i, k)) prow[k] |= pp(i, k);
+          for (int k = 0; k < 8; k++) prow[k] = pp(i, k);
+        } else {
+#pragma unroll
+          for (int k = 0; k < 8; k++)
+            if (pp(i, k)) prow[k] |= pp(i, k);
+        }
       }
     }
   }
