@@ -171,3 +171,24 @@ def test_adaptive_width_warmup_visits_every_width():
 def test_max_words_validated():
     with pytest.raises(ValueError):
         _server(max_words=3)
+
+
+def test_refused_launch_keeps_its_sources_waiting():
+    srv, ctx, clk = _server()
+    g = FakeGraph(1)
+    real = ctx.slot_launch
+    calls = {"n": 0}
+
+    def refuse_once(slot, gr, src, rows):
+        calls["n"] += 1
+        if calls["n"] == 1:
+            raise RuntimeError("XB_ERR_OOM")
+        real(slot, gr, src, rows)
+
+    ctx.slot_launch = refuse_once
+    q = srv.submit(g, np.arange(0, 100), want="digest")
+    with pytest.raises(RuntimeError):
+        srv.step()
+    assert q.rows_launched == 0 and srv.waiting == [q]
+    srv.drain()
+    assert q.done and sorted(np.concatenate([x[2] for x in ctx.launches]).tolist()) == list(range(100))

@@ -182,12 +182,18 @@ class Server:
             q.rows_launched += n
             if len(take) == cap:
                 break
-        self.waiting = [q for q in self.waiting if q.rows_launched < q.k]
         src = np.array([q.sources[j] for q, j in take], dtype=np.int32)
         rows = []
         for q, j in take:
             rows.append(None if q.want == "digest" else (q.level[j].data_ptr(), q.parent[j].data_ptr()))
-        self.ctx.slot_launch(slot, g, src, rows)
+        try:
+            self.ctx.slot_launch(slot, g, src, rows)
+        except Exception:
+            # a pass the library refused: its sources wait again
+            for q, j in take:
+                q.rows_launched = min(q.rows_launched, j)
+            raise
+        self.waiting = [q for q in self.waiting if q.rows_launched < q.k]
         self.slot_rows[slot] = take
         self.passes += 1
         self.slot_pass[slot] = self.passes
