@@ -52,7 +52,8 @@ WORKLOADS = {
     # serving: resident graph, Poisson arrivals (seeded rate), 1..4096 sources per query (log-uniform),
     # digests per source, continuous batching over slots; reports GTEPS and p50/p99 latency
     "serve_rmat25": dict(kind="serve", scale=25, ef=32, queries=48, rate=2.0, kmax=4096, slots=2, max_words=2),
-    "serve_rmat22": dict(kind="serve", scale=22, ef=16, queries=96, rate=12.0, kmax=4096, slots=4, max_words=4),
+    "serve_rmat22": dict(kind="serve", scale=22, ef=16, queries=96, rate=12.0, kmax=4096, slots=4, max_words=4,
+                         express=1),
     # the default graph with one word of sources: ncu DRAM-traffic captures (about 4 GB on the device)
     "rmat22_k64": dict(kind="rmat", scale=22, ef=16, k=64),
     # one pass of the two-word layout (2 words x 64 sources): DRAM-traffic captures
@@ -608,7 +609,7 @@ def run_serve(args, w, name) -> None:
     g = ctx.upload(csr)
     del csr
     slots = args.chains or w["slots"]
-    srv = serve.Server(ctx, slots=slots, max_words=w.get("max_words", 1))
+    srv = serve.Server(ctx, slots=slots, max_words=w.get("max_words", 1), express=w.get("express", 0))
     # warm-up: one full pass per slot and width (workspaces, scratch, captured pass graphs)
     srv.warmup(g, SEED + 99)
     srv.completed.clear()
@@ -629,6 +630,7 @@ def run_serve(args, w, name) -> None:
                    "graph": f"rmat scale {w['scale']} ef {w['ef']} a/b/c/d .57/.19/.19/.05",
                    "queries": len(trace), "sources_total": int(sum(ks)), "k_range": [1, w["kmax"]],
                    "arrival_rate_per_s": w["rate"], "slots": slots, "max_words": srv.max_words,
+                   "express_slots": srv.express,
                    "result": "per-source digests"},
         "path": "xbtrav.serve.Server over xb_slot_launch (continuous batching)",
         "latency_ms": {"p50": out["p50_ms"], "p99": out["p99_ms"], "mean": out["mean_ms"], "max": out["max_ms"]},
@@ -640,20 +642,22 @@ def run_serve(args, w, name) -> None:
     ctx.close()
 
 
-SERVE_LEG = dict(queries=48, rate=12.0, kmax=4096, slots=4, max_words=4)
+SERVE_LEG = dict(queries=48, rate=12.0, kmax=4096, slots=4, max_words=4, express=1)
 
 
 def serve_leg(ctx, g, dev, rank, dist, max_over_ranks, sum_over_ranks, barrier) -> dict:
     """Serving on the headline's resident graph: seeded Poisson arrivals (rate
     12/s), 1..4096 sources per query (log-uniform), digests, continuous
-    batching over 4 slots, shortest query first, passes 1, 2 or 4 words wide
+    batching over 4 slots (one an express lane at high stream priority for
+    small queries), shortest query first, passes 1, 2 or 4 words wide
     as the opening query needs (xbtrav.serve).  Latency
     = arrival to the query's last digest; p50/p99 are the largest over ranks,
     throughput the sum of the ranks' processed edges over the longest trace."""
     from xbtrav import replicas, serve
 
     ctx.set_tuning(words=1)
-    srv = serve.Server(ctx, slots=SERVE_LEG["slots"], max_words=SERVE_LEG["max_words"])
+    srv = serve.Server(ctx, slots=SERVE_LEG["slots"], max_words=SERVE_LEG["max_words"],
+                       express=SERVE_LEG["express"])
     srv.warmup(g, SEED + 99)  # every slot and width: workspaces, scratch rows, captured pass graphs
     srv.completed.clear()
     srv.edges = 0
@@ -667,6 +671,8 @@ def serve_leg(ctx, g, dev, rank, dist, max_over_ranks, sum_over_ranks, barrier) 
     clk = clocks.stop()
     barrier()
     ctx.slots_release()
+    for s in range(SERVE_LEG["slots"]):
+        ctx.slot_set_priority(s, 0)
     secs = max_over_ranks(out["seconds"])
     edges = sum_over_ranks(srv.edges)
     return {
@@ -676,7 +682,7 @@ def serve_leg(ctx, g, dev, rank, dist, max_over_ranks, sum_over_ranks, barrier) 
         "sources_total": int(sum(len(t[2]) for t in trace)), "arrival_rate_per_s": SERVE_LEG["rate"],
         "k_range": [1, SERVE_LEG["kmax"]], "slots": SERVE_LEG["slots"],
         "sources_per_pass": [srv.word_bits * srv.base_words, srv.word_bits * srv.max_words],
-        "order": "shortest query first, queries waiting over 1 s first",
+        "order": "shortest query first, queries waiting over 1 s first; 1 express slot (high priority, small queries)",
         "passes": out["passes"], "result": "per-source digests", "clocks": clk,
         "path": "xbtrav.serve.Server over xb_slot_launch (continuous batching, admission by free HBM)",
     }

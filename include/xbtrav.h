@@ -314,6 +314,12 @@ xb_status xb_slot_poll(xb_ctx* ctx, int32_t slot, int32_t* done, xb_stats* stats
 xb_status xb_slot_wait(xb_ctx* ctx, int32_t slot, xb_stats* stats, xb_row_digest* digests);
 /* Frees every slot's device memory (all slots must be idle). */
 xb_status xb_slots_release(xb_ctx* ctx);
+/* Stream priority of a slot: 0 = default, 1 = the device's greatest; an
+ * idle slot only.  Passes on a priority-1 slot have their kernels scheduled
+ * ahead of the other slots' (a serving loop's express lane for small
+ * queries).  Kept across xb_slots_release.  No counterpart in the
+ * reference (it has no serving path). */
+xb_status xb_slot_set_priority(xb_ctx* ctx, int32_t slot, int32_t priority);
 
 /* ---- weighted: multi-source shortest paths ------------------------------ */
 /* Attaches int32 edge weights to a resident graph, one per column index

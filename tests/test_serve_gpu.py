@@ -213,3 +213,37 @@ def test_adaptive_width_server_matches_the_oracle(ctx, graphs):
     ctx.set_tuning(words=1)
     for g in dg:
         g.close()
+
+
+def test_slot_priority_and_express_lane(ctx, graphs):
+    """xb_slot_set_priority: a priority-1 slot runs the same passes (digests
+    equal the oracle's), the setting is refused on a busy slot and for bad
+    arguments; a server with an express slot gives every query the oracle's
+    results."""
+    _tune(ctx)
+    ro, ci = graphs[0]
+    g = ctx.upload_arrays(ro, ci)
+    ctx.slot_set_priority(0, 1)
+    src = g.select_sources(31, 64)
+    ctx.slot_launch(0, g, src, None)
+    with pytest.raises(xbtrav.XbError):
+        ctx.slot_set_priority(0, 0)  # busy
+    _, _, dig = ctx.slot_poll(0, wait=True)
+    lv, pr, _, _ = O.msbfs(ro, ci, src, rule=O.RULE_MINID)
+    np.testing.assert_array_equal(dig, _oracle_digest(lv, pr))
+    for bad in ((0, 2), (-1, 0), (99, 1)):
+        with pytest.raises(xbtrav.XbError):
+            ctx.slot_set_priority(*bad)
+    ctx.slot_set_priority(0, 0)
+    srv = serve.Server(ctx, slots=3, max_words=4, express=1)
+    qs = [(s, srv.submit(g, s, want="digest")) for s in (g.select_sources(40 + i, k) for i, k in
+                                                             enumerate([500, 3, 64, 1, 200, 17]))]
+    srv.drain()
+    for s, q in qs:
+        lv, pr, _, _ = O.msbfs(ro, ci, s, rule=O.RULE_MINID)
+        np.testing.assert_array_equal(q.digest, _oracle_digest(lv, pr))
+    ctx.slots_release()
+    for slot in range(3):
+        ctx.slot_set_priority(slot, 0)
+    ctx.set_tuning(words=1)
+    g.close()

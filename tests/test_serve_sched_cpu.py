@@ -36,6 +36,11 @@ class FakeCtx:
     def set_tuning(self, **kw):
         self.words = kw.get("words", self.words)
 
+    def slot_set_priority(self, slot, priority):
+        assert slot not in self.inflight
+        self.priority = getattr(self, "priority", {})
+        self.priority[slot] = priority
+
     def slot_launch(self, slot, g, src, rows):
         assert slot not in self.inflight
         assert 1 <= len(src) <= 64 * self.words  # a pass holds at most one layout's sources
@@ -55,9 +60,9 @@ class Clock:
         return self.t
 
 
-def _server(slots=1, age_s=1.0, max_words=None):
+def _server(slots=1, age_s=1.0, max_words=None, express=0):
     ctx, clk = FakeCtx(), Clock()
-    return serve.Server(ctx, slots=slots, clock=clk, age_s=age_s, max_words=max_words), ctx, clk
+    return serve.Server(ctx, slots=slots, clock=clk, age_s=age_s, max_words=max_words, express=express), ctx, clk
 
 
 def _origin(srcs, queries):
@@ -192,3 +197,26 @@ def test_refused_launch_keeps_its_sources_waiting():
     assert q.rows_launched == 0 and srv.waiting == [q]
     srv.drain()
     assert q.done and sorted(np.concatenate([x[2] for x in ctx.launches]).tolist()) == list(range(100))
+
+
+def test_express_slot_takes_only_passes_opened_by_small_queries():
+    srv, ctx, clk = _server(slots=2, max_words=4, express=1)
+    assert ctx.priority == {0: 1, 1: 0}
+    g = FakeGraph(1)
+    big = srv.submit(g, np.arange(0, 600), want="digest")
+    srv.step()  # slot 0 (express) finds no small query; slot 1 takes a wide pass
+    assert [x[0] for x in ctx.launches] == [1] and len(ctx.launches[0][2]) == 256
+    small = srv.submit(g, np.arange(5000, 5010), want="digest")
+    srv.step()  # slot 1's pass is collected; the express slot opens a one-word pass with the small query
+    express = [x for x in ctx.launches if x[0] == 0]
+    assert express and _origin(express[0][2], [big, small])[:10] == [small.qid] * 10
+    assert len(express[0][2]) == 64  # the rest of the word filled from the large query
+    srv.drain()
+    assert big.done and small.done
+    launched = np.concatenate([x[2] for x in ctx.launches]).tolist()
+    assert sorted(launched) == sorted(list(range(600)) + list(range(5000, 5010)))
+
+
+def test_express_needs_an_ordinary_slot():
+    with pytest.raises(ValueError):
+        _server(slots=1, express=1)

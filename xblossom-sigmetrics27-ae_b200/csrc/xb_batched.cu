@@ -64,6 +64,7 @@ constexpr int kSlotMaxRows = 256;  // 64 sources x 4 words
 
 struct SlotState {
   bool init = false, busy = false;
+  int priority = 0;  // 1: the slot's stream has the device's greatest priority (xb_slot_set_priority)
   int kb = 0;
   void* ws = nullptr;
   size_t ws_bytes = 0;
@@ -630,12 +631,24 @@ void slot_free(SlotState& sl) {
     if (p) cudaFreeHost(p);
   if (sl.done) cudaEventDestroy(sl.done);
   if (sl.stream) cudaStreamDestroy(sl.stream);
+  const int prio = sl.priority;  // a setting, kept across releases
   sl = SlotState();
+  sl.priority = prio;
+}
+
+// The slot's stream: default priority, or the device's greatest.  A captured
+// pass graph launched into it runs its kernels at the stream's priority.
+xb_status slot_stream(SlotState& sl) {
+  int least = 0, greatest = 0;
+  XB_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+  XB_CUDA(cudaStreamCreateWithPriority(&sl.stream, cudaStreamNonBlocking, sl.priority ? greatest : 0));
+  return XB_OK;
 }
 
 xb_status slot_init(SlotState& sl) {
   if (sl.init) return XB_OK;
-  XB_CUDA(cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking));
+  xb_status st = slot_stream(sl);
+  if (st != XB_OK) return st;
   XB_CUDA(cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming));
   XB_CUDA(cudaMalloc(&sl.d_src, sizeof(int32_t) * kSlotMaxRows));
   XB_CUDA(cudaMallocHost(&sl.h_src, sizeof(int32_t) * kSlotMaxRows));
@@ -1008,6 +1021,27 @@ extern "C" xb_status xb_slot_wait(xb_ctx* c, int32_t slot, xb_stats* stats, xb_r
     return fail(XB_ERR_CUDA, std::string("slot pass: ") + cudaGetErrorString(e));
   }
   return xbe::slot_collect(sl, stats, digests);
+}
+
+extern "C" xb_status xb_slot_set_priority(xb_ctx* c, int32_t slot, int32_t priority) {
+  xbi::clear_error();
+  if (!c) return fail(XB_ERR_ARG, "null context");
+  if (slot < 0 || slot >= xbe::kMaxSlots) return fail(XB_ERR_ARG, "slot out of range");
+  if (priority != 0 && priority != 1) return fail(XB_ERR_ARG, "priority must be 0 or 1");
+  XB_CUDA(cudaSetDevice(c->device));
+  xb_status st = xbe::make_state(c);
+  if (st != XB_OK) return st;
+  xbe::SlotState& sl = c->batch->slots[slot];
+  if (sl.busy) return fail(XB_ERR_STATE, "slot " + std::to_string(slot) + " has a pass in flight");
+  if (sl.priority == priority) return XB_OK;
+  sl.priority = priority;
+  if (sl.stream) {  // an initialised slot gets a new stream; its captured passes stay valid
+    XB_CUDA(cudaStreamSynchronize(sl.stream));
+    XB_CUDA(cudaStreamDestroy(sl.stream));
+    sl.stream = nullptr;
+    return xbe::slot_stream(sl);
+  }
+  return XB_OK;
 }
 
 extern "C" xb_status xb_slots_release(xb_ctx* c) {

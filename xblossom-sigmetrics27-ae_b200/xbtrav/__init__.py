@@ -168,6 +168,7 @@ def lib() -> C.CDLL:
         "xb_slot_poll": (i32, [vp, i32, P(i32), P(XbStats), vp]),
         "xb_slot_wait": (i32, [vp, i32, P(XbStats), vp]),
         "xb_slots_release": (i32, [vp]),
+        "xb_slot_set_priority": (i32, [vp, i32, i32]),
         "xb_graph_set_weights": (i32, [vp, vp, i64]),
         "xb_multi_sssp": (i32, [vp, vp, vp, i32, vp, u32, P(XbStats)]),
         "xb_max_match": (i32, [vp, vp, vp, u32, P(XbStats)]),
@@ -665,6 +666,11 @@ class Context:
 
     def slots_release(self) -> None:
         _check(lib().xb_slots_release(self._h))
+
+    def slot_set_priority(self, slot: int, priority: int) -> None:
+        """Stream priority of an idle slot (xb_slot_set_priority): 0 default,
+        1 the device's greatest."""
+        _check(lib().xb_slot_set_priority(self._h, slot, priority))
 
     def close(self) -> None:
         if self._h and self._h.value:

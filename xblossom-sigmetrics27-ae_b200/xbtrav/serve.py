@@ -9,6 +9,11 @@ stream and workspace, so passes of different slots overlap on the device).  A
 query that arrives while others are on the GPU joins the next pass any slot
 starts; nothing waits for a batch to fill.
 
+With express > 0, the first `express` slots run at the device's greatest
+stream priority (xb_slot_set_priority) and only take one-word passes opened
+by a query that fits one: a small query neither waits for a slot behind the
+wide passes of large ones nor yields the SMs to them while it runs.
+
 Passes are filled shortest query first: the query with the fewest sources
 still to launch opens the pass, and the rest of it takes the other waiting
 queries of the same graph in the same order.  A pass costs about the same
@@ -85,7 +90,7 @@ class Query:
 
 class Server:
     def __init__(self, ctx, slots: int = 4, reserve_bytes: int = 4 << 30, clock=time.perf_counter,
-                 age_s: float = 1.0, max_words: int | None = None):
+                 age_s: float = 1.0, max_words: int | None = None, express: int = 0):
         import torch
 
         self.torch = torch
@@ -103,6 +108,11 @@ class Server:
         self.rows_per_pass = self.word_bits * self.base_words
         self.dev = torch.device("cuda", ctx.device)
         self.age_s = age_s
+        if not 0 <= express < slots:
+            raise ValueError("express must leave at least one ordinary slot")
+        self.express = express
+        for s in range(slots):
+            ctx.slot_set_priority(s, 1 if s < express else 0)
         self.admit_q = collections.deque()      # queries waiting for memory
         self.waiting = []                       # admitted queries with sources not yet launched
         self.slot_rows = [None] * slots         # rows of the pass in flight per slot
@@ -167,10 +177,18 @@ class Server:
 
     def _launch(self, slot: int) -> bool:
         """Starts a pass on an idle slot: the first query in launch order
-        opens it, other waiting queries of its graph fill the rest."""
+        opens it, other waiting queries of its graph fill the rest.  An
+        express slot takes only one-word passes opened by a query that fits
+        one."""
         if not self.waiting:
             return False
         order = self._order(self.clock())
+        if slot < self.express:
+            narrow = self.word_bits * self.base_words
+            small = [q for q in order if q.k - q.rows_launched <= narrow]
+            if not small:
+                return False
+            order = small + [q for q in order if q.k - q.rows_launched > narrow]  # the rest fills the word
         g = order[0].graph
         cap = self._width(order[0].k - order[0].rows_launched)
         take = []
@@ -250,8 +268,8 @@ class Server:
                 self._collect(s, wait=False)
         self._admit()
         for s in range(self.nslots):
-            if self.slot_rows[s] is None and not self._launch(s):
-                break
+            if self.slot_rows[s] is None and not self._launch(s) and s >= self.express:
+                break  # nothing waits (an express slot may only lack small queries)
         busy = [s for s in range(self.nslots) if self.slot_rows[s] is not None]
         if not busy and self.admit_q and not self.waiting:
             raise RuntimeError("queries wait for device memory that nothing in flight will free "
