@@ -51,7 +51,8 @@ WORKLOADS = {
     "multi128": dict(kind="multi", instances=128, k=0),
     # serving: resident graph, Poisson arrivals (seeded rate), 1..4096 sources per query (log-uniform),
     # digests per source, continuous batching over slots; reports GTEPS and p50/p99 latency
-    "serve_rmat25": dict(kind="serve", scale=25, ef=32, queries=48, rate=2.0, kmax=4096, slots=2, max_words=2),
+    "serve_rmat25": dict(kind="serve", scale=25, ef=32, queries=48, rate=2.0, kmax=4096, slots=3, max_words=2,
+                         express=1),
     "serve_rmat22": dict(kind="serve", scale=22, ef=16, queries=96, rate=12.0, kmax=4096, slots=4, max_words=4,
                          express=1),
     # the default graph with one word of sources: ncu DRAM-traffic captures (about 4 GB on the device)
@@ -603,8 +604,9 @@ def run_serve(args, w, name) -> None:
     ctx = xbtrav.Context(0)
     # passes start at one word (64 sources: low latency); max_words lets large
     # queries open wider passes where per-slot memory allows (workspace +
-    # scratch rows: 28 GB per slot at scale 25 with one word, 56 GB with two,
-    # so that graph runs two slots of at most two words)
+    # scratch rows where a pass mixes tables and digests: about 20 GB per
+    # two-word slot at scale 25, so that graph runs three slots of at most two
+    # words)
     ctx.set_tuning(words=1)
     g = ctx.upload(csr)
     del csr
