@@ -603,10 +603,10 @@ def run_serve(args, w, name) -> None:
     info = csr.info()
     ctx = xbtrav.Context(0)
     # passes start at one word (64 sources: low latency); max_words lets large
-    # queries open wider passes where per-slot memory allows (workspace +
-    # scratch rows where a pass mixes tables and digests: about 20 GB per
-    # two-word slot at scale 25, so that graph runs three slots of at most two
-    # words)
+    # queries open wider passes where per-slot memory allows (a two-word slot's
+    # workspace is about 20 GB at scale 25, plus scratch rows only for passes
+    # that mix tables and digests), so that graph runs three slots of at most
+    # two words
     ctx.set_tuning(words=1)
     g = ctx.upload(csr)
     del csr
