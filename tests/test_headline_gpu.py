@@ -3,7 +3,7 @@
 The default benchmark workload is R-MAT scale 22 / edge factor 16 (seed
 0x5EED), 1024 sources drawn with seed 0x5EED + 1, traversed by
 xb_traverse_batched at the context's default tuning (64-bit words, four per
-vertex = 256 sources per pass, 4 chains, heavy cutoff 256, pull factor 1024).
+vertex = 256 sources per pass, 4 chains, heavy cutoff 256, pull factor 256).
 These tests run exactly that call and compare a spread sample of source rows
 bit-exactly with the CPU oracle (levels and min-id parents): every pass, every
 word of a pass and bit positions 0 and 63 of each word, plus seeded random

@@ -224,7 +224,7 @@ template <typename W, int NW, typename OffT>
 xb_status capture_pass_levels(xb_ctx* c, BatchState* bs, const PassRes<W, NW, OffT>& p, const xb_graph* g,
                               const int32_t* src, int kb, cudaStream_t s) {
   const int sms = c->num_sms;
-  const float alpha = c->tuning.pull_alpha > 0 ? c->tuning.pull_alpha : 1024.0f;
+  const float alpha = c->tuning.pull_alpha > 0 ? c->tuning.pull_alpha : 256.0f;
   const StepShape sh = graph_shape<W, NW, OffT>(g, sms, p.tile);
   bs->level_bound = level_bound(c, p.nplanes_alloc);
   bs->push_below = push_below(c, g);

@@ -291,7 +291,7 @@ xb_status run_plain(xb_ctx* c, xb_graph* g, const int32_t* d_sources, int32_t k,
   PassRes<W, NW, OffT> p = pass_res<W, NW, OffT>(g, c->ws, L, c->d_ctr, g->d_hpar, heavy);
   p.tile = c->tuning.tile;
   const int sms = c->num_sms;
-  const float alpha = c->tuning.pull_alpha > 0 ? c->tuning.pull_alpha : 1024.0f;
+  const float alpha = c->tuning.pull_alpha > 0 ? c->tuning.pull_alpha : 256.0f;
   ClassTimer timer{c, st, c->tuning.timing != 0};
   const StepShape mx = max_shape<W, NW, OffT>(g, sms, p.tile);
   const int bound = level_bound(c, p.nplanes_alloc);
@@ -429,9 +429,11 @@ xb_status xb_ctx_create(int32_t device, xb_ctx** out) {
   XB_CUDA(cudaEventCreate(&c->evc1));
   c->tuning.word_bits = 64;
   c->tuning.words = 4;  // 256 sources per pass: one gather of a whole 32-byte sector serves them all
-  // pull unless the frontier's edges are under 1/1024 of the unfinished edges:
-  // pull steps record parents as they go, push steps leave them to a search
-  c->tuning.pull_alpha = 1024.0f;
+  // pull unless the frontier's edges are under 1/256 of the unfinished edges:
+  // pull steps record parents as they go, push steps leave them to a search;
+  // a small source set's first level is still pushed (a pull there scans the
+  // whole graph for a few frontier vertices)
+  c->tuning.pull_alpha = 256.0f;
   c->tuning.heavy_degree = 256;
   c->tuning.timing = 0;
   c->tuning.chains = 4;
