@@ -781,11 +781,14 @@ def main() -> None:
     def batched_step():
         return ctx.traverse_batched([(g, src_dev)], outputs=[(level, parent)])[1]
 
-    def timed(step, steps, sampler=None):
-        """steps of `step` between CUDA events on the engine's stream; returns (ms, summed stats)."""
+    def timed(step, steps, label, sampler=None):
+        """steps of `step` between CUDA events on the engine's stream; returns
+        (ms, summed stats).  The steps run inside an NVTX range named `label`
+        (a profiler can capture one leg's launches with --nvtx-include)."""
         barrier()
         if sampler is not None:
             sampler.start()
+        torch.cuda.nvtx.range_push(label)
         ev0 = torch.cuda.Event(enable_timing=True)
         ev1 = torch.cuda.Event(enable_timing=True)
         agg = {"edges_traversed": 0, "class_ms": [0.0, 0.0, 0.0], "class_bytes": [0, 0, 0],
@@ -805,6 +808,7 @@ def main() -> None:
             agg["pull_levels"] += s["pull_levels"]
         with torch.cuda.stream(stream):
             ev1.record(stream)
+        torch.cuda.nvtx.range_pop()
         barrier()
         clk = sampler.stop() if sampler is not None else None
         return max_over_ranks(ev0.elapsed_time(ev1)), agg, clk
@@ -813,20 +817,20 @@ def main() -> None:
     ctx.set_tuning(timing=0)
     for _ in range(args.warmup):
         plain_step()
-    plain_ms, plain_agg, _ = timed(plain_step, args.steps)
+    plain_ms, plain_agg, _ = timed(plain_step, args.steps, "plain")
     plain_gteps = sum_over_ranks(plain_agg["edges_traversed"]) / (plain_ms / 1e3) / 1e9
 
     # the plain path with one word (64 sources) per launch sequence
     tun0 = ctx.tuning()
     ctx.set_tuning(words=1)
     plain_step()
-    pw_ms, pw_agg, _ = timed(plain_step, max(1, min(args.steps, 3)))
+    pw_ms, pw_agg, _ = timed(plain_step, max(1, min(args.steps, 3)), "plain_one_word")
     plain_word_gteps = sum_over_ranks(pw_agg["edges_traversed"]) / (pw_ms / 1e3) / 1e9
     ctx.set_tuning(words=tun0["words"])
 
     # per-kernel-class device times of the same kernels (one step, event-timed per class)
     ctx.set_tuning(timing=1)
-    _, cls_agg, _ = timed(plain_step, 1)
+    _, cls_agg, _ = timed(plain_step, 1, "plain_classes")
     ctx.set_tuning(timing=0)
 
     # batched path: the whole step is one CUDA-graph launch
@@ -840,7 +844,7 @@ def main() -> None:
         clocks.start()
         for _ in range(args.warmup):
             batched_step()
-        b_ms, b_agg, _ = timed(batched_step, args.steps)
+        b_ms, b_agg, _ = timed(batched_step, args.steps, "batched")
         clk = clocks.stop()
     edges_total = sum_over_ranks(b_agg["edges_traversed"])
     value = edges_total / (b_ms / 1e3) / 1e9

@@ -110,7 +110,14 @@ typedef struct xb_tuning {
   /* After a pull step, push when the frontier holds fewer than n/push_beta
    * vertices (the traversal's tail); 0 = never. */
   float push_beta;
-  int32_t pad;
+  /* How a call's sources are grouped into passes: 0 (default) = by source
+   * degree, highest first (sources whose traversals grow alike share a
+   * pass's level steps: fewer steps with few live lanes); 1 = in the order
+   * given.  Output rows stay where the caller asked for them either way.
+   * xb_traverse_batched with host output tables keys its captured copies
+   * on the grouping, so a stream of calls with host tables and new source
+   * lists recaptures under 0 and reuses one graph under 1. */
+  int32_t source_order;
 } xb_tuning;
 
 /* ---- status ------------------------------------------------------------ */

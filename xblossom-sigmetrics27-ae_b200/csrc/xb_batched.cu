@@ -385,7 +385,15 @@ xb_status run_batched(xb_ctx* c, const std::vector<xb_batch_item>& items, const 
   for (const xb_graph* g : graphs) {
     st = ensure_heavy(const_cast<xb_graph*>(g), heavy);
     if (st != XB_OK) return st;
-    const auto& v = by_graph[g];
+    auto& v = by_graph[g];
+    if (c->tuning.source_order == 0 && v.size() > (size_t)SPP) {  // passes grouped by source degree
+      std::vector<int64_t> order(v.size());
+      for (size_t j = 0; j < v.size(); j++) order[j] = (int64_t)j;
+      order_by_degree(g, order, [&](int64_t j) { return (int64_t)hsrc[v[j].item][v[j].idx]; });
+      std::vector<RowDst> sorted(v.size());
+      for (size_t j = 0; j < v.size(); j++) sorted[j] = v[order[j]];
+      v.swap(sorted);
+    }
     for (size_t j0 = 0; j0 < v.size(); j0 += SPP) {
       PassPlan pp;
       pp.g = g;
@@ -536,6 +544,7 @@ xb_status run_batched(xb_ctx* c, const std::vector<xb_batch_item>& items, const 
     key[4] = abits;
     key[9] = bbits;
   }
+  bool any_host = false;
   for (const auto& it : items) {
     key.push_back((uint64_t)(uintptr_t)it.graph);
     key.push_back(it.graph->version);
@@ -544,8 +553,14 @@ xb_status run_batched(xb_ctx* c, const std::vector<xb_batch_item>& items, const 
     if (!(it.flags & XB_OUT_DEVICE) && it.k > 0) {
       key.push_back((uint64_t)(uintptr_t)it.level);
       key.push_back((uint64_t)(uintptr_t)it.parent);
+      any_host = true;
     }
   }
+  // the captured host copies follow the rows' pass grouping, which depends
+  // on the sources when they are grouped by degree
+  if (any_host && c->tuning.source_order == 0)
+    for (const auto& pp : plan)
+      for (const auto& r : pp.rows) key.push_back(((uint64_t)(uint32_t)r.item << 32) | (uint32_t)r.idx);
   CachedGraph* hit = nullptr;
   for (auto& e : bs->cache)
     if (e.key == key) hit = &e;

@@ -256,8 +256,8 @@ xb_status ensure_heavy(xb_graph* g, int thr) {
 }
 
 template <typename W, int NW, typename OffT>
-xb_status run_plain(xb_ctx* c, xb_graph* g, const int32_t* d_sources, int32_t k, int32_t* level_out,
-                    int32_t* parent_out, bool out_dev, bool fifo, xb_stats* st) {
+xb_status run_plain(xb_ctx* c, xb_graph* g, const int32_t* d_sources, const int64_t* perm, int32_t k,
+                    int32_t* level_out, int32_t* parent_out, bool out_dev, bool fifo, xb_stats* st) {
   constexpr int B = xbk::WB<W>::bits;
   constexpr int SPP = B * NW;  // sources per pass
   const int64_t n = g->n;
@@ -279,10 +279,17 @@ xb_status run_plain(xb_ctx* c, xb_graph* g, const int32_t* d_sources, int32_t k,
     std::vector<int32_t*> rows((size_t)(npass * 2 * SPP));
     for (int64_t j = 0; j < npass; j++) {
       const int kb = (int)std::min<int64_t>(SPP, k - j * SPP);
-      if (out_dev)
-        fill_rows<W, NW>(rows.data() + j * 2 * SPP, kb, level_out + j * SPP * n, parent_out + j * SPP * n, n);
-      else
-        fill_rows<W, NW>(rows.data() + j * 2 * SPP, kb, c->d_stage, c->d_stage + (size_t)SPP * n, n);
+      int32_t** pr = rows.data() + j * 2 * SPP;
+      if (!out_dev) {
+        fill_rows<W, NW>(pr, kb, c->d_stage, c->d_stage + (size_t)SPP * n, n);
+        continue;
+      }
+      fill_rows<W, NW>(pr, kb, level_out, parent_out, 0);  // nullptr past kb
+      for (int i = 0; i < kb; i++) {  // each source's row where the caller put it
+        const int64_t r = perm[j * SPP + i];
+        pr[(i / B) * 2 * B + i % B] = level_out + r * n;
+        pr[(i / B) * 2 * B + B + i % B] = parent_out + r * n;
+      }
     }
     XB_CUDA(cudaMemcpyAsync(c->d_rows, rows.data(), sizeof(int32_t*) * rows.size(), cudaMemcpyHostToDevice,
                             c->stream));
@@ -361,11 +368,18 @@ xb_status run_plain(xb_ctx* c, xb_graph* g, const int32_t* d_sources, int32_t k,
       XB_LAUNCH_CHECK("fifo parents");
     }
     timer.end(1, launches);
-    if (!out_dev) {
-      XB_CUDA(cudaMemcpyAsync(level_out + k0 * n, lv_base, sizeof(int32_t) * (size_t)kb * n, cudaMemcpyDeviceToHost,
-                              c->stream));
-      XB_CUDA(cudaMemcpyAsync(parent_out + k0 * n, pr_base, sizeof(int32_t) * (size_t)kb * n, cudaMemcpyDeviceToHost,
-                              c->stream));
+    if (!out_dev) {  // runs of consecutive caller rows become one copy each
+      for (int j = 0; j < kb;) {
+        const int64_t r0 = perm[k0 + j];
+        int e = j + 1;
+        while (e < kb && perm[k0 + e] == r0 + (e - j)) e++;
+        const size_t bytes = sizeof(int32_t) * (size_t)(e - j) * (size_t)n;
+        XB_CUDA(cudaMemcpyAsync(level_out + r0 * n, lv_base + (size_t)j * n, bytes, cudaMemcpyDeviceToHost,
+                                c->stream));
+        XB_CUDA(cudaMemcpyAsync(parent_out + r0 * n, pr_base + (size_t)j * n, bytes, cudaMemcpyDeviceToHost,
+                                c->stream));
+        j = e;
+      }
     }
     XB_CUDA(cudaMemcpyAsync(c->h_ctr, p.ctr, sizeof(xbk::Ctrs), cudaMemcpyDeviceToHost, c->stream));
     XB_CUDA(cudaStreamSynchronize(c->stream));
@@ -390,13 +404,12 @@ xb_status run_plain(xb_ctx* c, xb_graph* g, const int32_t* d_sources, int32_t k,
 }
 
 template <typename W, typename OffT>
-xb_status dispatch_nw(xb_ctx* c, xb_graph* g, const int32_t* d_src, int32_t k, int32_t* lv, int32_t* pr, bool od,
-                      bool fifo,
-                      xb_stats* st) {
+xb_status dispatch_nw(xb_ctx* c, xb_graph* g, const int32_t* d_src, const int64_t* perm, int32_t k, int32_t* lv,
+                      int32_t* pr, bool od, bool fifo, xb_stats* st) {
   switch (c->tuning.words) {
-    case 1: return run_plain<W, 1, OffT>(c, g, d_src, k, lv, pr, od, fifo, st);
-    case 2: return run_plain<W, 2, OffT>(c, g, d_src, k, lv, pr, od, fifo, st);
-    case 4: return run_plain<W, 4, OffT>(c, g, d_src, k, lv, pr, od, fifo, st);
+    case 1: return run_plain<W, 1, OffT>(c, g, d_src, perm, k, lv, pr, od, fifo, st);
+    case 2: return run_plain<W, 2, OffT>(c, g, d_src, perm, k, lv, pr, od, fifo, st);
+    case 4: return run_plain<W, 4, OffT>(c, g, d_src, perm, k, lv, pr, od, fifo, st);
     default: return fail(XB_ERR_ARG, "tuning.words must be 1, 2 or 4");
   }
 }
@@ -474,6 +487,7 @@ xb_status xb_ctx_set_tuning(xb_ctx* c, const xb_tuning* t) {
   if (t->level_cap < 0 || t->workspace_cap < 0) return fail(XB_ERR_ARG, "level_cap and workspace_cap must be >= 0");
   if (t->tile != 0 && t->tile != 1) return fail(XB_ERR_ARG, "tile must be 0 or 1");
   if (!(t->push_beta >= 0)) return fail(XB_ERR_ARG, "push_beta must be >= 0");
+  if (t->source_order != 0 && t->source_order != 1) return fail(XB_ERR_ARG, "source_order must be 0 or 1");
   c->tuning = *t;
   if (c->tuning.chains == 0) c->tuning.chains = 4;
   return XB_OK;
@@ -710,14 +724,25 @@ xb_status xb_traverse(xb_ctx* c, const xb_graph* gc, const int32_t* sources, int
     if (hs[i] < 0 || hs[i] >= g->n) return fail(XB_ERR_ARG, "source " + std::to_string(i) + " out of range");
   xb_status s = xbe::ensure_sources(c, k);
   if (s != XB_OK) return s;
+  // pass grouping: perm[i] = the caller's row of the i-th source traversed
+  std::vector<int64_t> perm((size_t)k);
+  for (int32_t i = 0; i < k; i++) perm[i] = i;
+  if (c->tuning.source_order == 0 && k > c->tuning.word_bits * c->tuning.words) {
+    xbe::order_by_degree(g, perm, [&](int64_t i) { return (int64_t)hs[i]; });
+    std::vector<int32_t> ps((size_t)k);
+    for (int32_t i = 0; i < k; i++) ps[i] = hs[perm[i]];
+    hs.swap(ps);
+  }
   XB_CUDA(cudaMemcpyAsync(c->d_src, hs.data(), sizeof(int32_t) * k, cudaMemcpyHostToDevice, c->stream));
   XB_CUDA(cudaEventRecord(c->ev0, c->stream));
+  const int64_t* pm = perm.data();
   if (c->tuning.word_bits == 64) {
-    s = g->off64 ? xbe::dispatch_nw<unsigned long long, int64_t>(c, g, c->d_src, k, level, parent, out_dev, fifo, st)
-                 : xbe::dispatch_nw<unsigned long long, int32_t>(c, g, c->d_src, k, level, parent, out_dev, fifo, st);
+    s = g->off64
+            ? xbe::dispatch_nw<unsigned long long, int64_t>(c, g, c->d_src, pm, k, level, parent, out_dev, fifo, st)
+            : xbe::dispatch_nw<unsigned long long, int32_t>(c, g, c->d_src, pm, k, level, parent, out_dev, fifo, st);
   } else {
-    s = g->off64 ? xbe::dispatch_nw<unsigned int, int64_t>(c, g, c->d_src, k, level, parent, out_dev, fifo, st)
-                 : xbe::dispatch_nw<unsigned int, int32_t>(c, g, c->d_src, k, level, parent, out_dev, fifo, st);
+    s = g->off64 ? xbe::dispatch_nw<unsigned int, int64_t>(c, g, c->d_src, pm, k, level, parent, out_dev, fifo, st)
+                 : xbe::dispatch_nw<unsigned int, int32_t>(c, g, c->d_src, pm, k, level, parent, out_dev, fifo, st);
   }
   if (s != XB_OK) {
     cudaStreamSynchronize(c->stream);

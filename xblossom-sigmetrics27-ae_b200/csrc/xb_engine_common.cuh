@@ -227,6 +227,17 @@ inline long long push_below(const xb_ctx* c, const xb_graph* g) {
   return c->tuning.push_beta > 0 ? (long long)((double)g->n / (double)c->tuning.push_beta) : 0;
 }
 
+// Stable order of count sources by out-degree, highest first (the pass
+// grouping of tuning.source_order 0).  key(i) gives the i-th source's vertex.
+template <typename Key>
+void order_by_degree(const xb_graph* g, std::vector<int64_t>& order, Key key) {
+  const int64_t* ro = g->h_ro.data();
+  std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t b) {
+    const int64_t va = key(a), vb = key(b);
+    return ro[va + 1] - ro[va] > ro[vb + 1] - ro[vb];
+  });
+}
+
 // Refuses a working-memory allocation above the context's tuning.workspace_cap.
 inline xb_status check_workspace_cap(const xb_ctx* c, size_t bytes, const char* what) {
   if (c->tuning.workspace_cap > 0 && (int64_t)bytes > c->tuning.workspace_cap)

@@ -91,7 +91,7 @@ class XbTuning(C.Structure):
         ("tile", C.c_int32),
         ("workspace_cap", C.c_int64),
         ("push_beta", C.c_float),
-        ("pad", C.c_int32),
+        ("source_order", C.c_int32),
     ]
 
 
