@@ -213,6 +213,11 @@ xb_status xb_graph_info(const xb_graph* g, int64_t* n, int64_t* m, int64_t* max_
 /* Width of the graph's device row offsets: 4 or 8 bytes. */
 xb_status xb_graph_offset_bytes(const xb_graph* g, int32_t* bytes);
 xb_status xb_select_sources(const xb_graph* g, uint64_t seed, int32_t k, int32_t* out);
+/* The pass grouping of tuning.source_order 0: order[i] = the index (into
+ * sources) of the i-th source to traverse, by out-degree, highest first,
+ * ties in the given order.  For host schedulers that split a query over
+ * several passes themselves (xb_slot_launch).  No reference counterpart. */
+xb_status xb_graph_source_order(const xb_graph* g, const int32_t* sources, int32_t k, int32_t* order);
 
 /* ---- traversal ---------------------------------------------------------- */
 /* Plain per-call path (the drop-in).  k sources; level and parent receive

@@ -17,9 +17,13 @@ class _Handle:
 
 
 class FakeGraph:
-    def __init__(self, h, n=100):
+    def __init__(self, h, n=100, order=None):
         self._h = _Handle(h)
         self.n = n
+        self.order = order  # source_order(src) -> order(src); None = as given
+
+    def source_order(self, src):
+        return np.arange(len(src), dtype=np.int32) if self.order is None else self.order(src)
 
 
 class FakeCtx:
@@ -45,11 +49,13 @@ class FakeCtx:
         assert slot not in self.inflight
         assert 1 <= len(src) <= 64 * self.words  # a pass holds at most one layout's sources
         self.launches.append((slot, g._h.value, np.array(src)))
-        self.inflight[slot] = len(src)
+        self.inflight[slot] = np.array(src)
 
     def slot_poll(self, slot, wait=False):
-        k = self.inflight.pop(slot)
-        return True, {"edges_traversed": 10 * k}, np.zeros((k, 4), np.int64)
+        src = self.inflight.pop(slot)
+        dig = np.zeros((len(src), 4), np.int64)
+        dig[:, 0] = src  # each digest row names its source
+        return True, {"edges_traversed": 10 * len(src)}, dig
 
 
 class Clock:
@@ -220,3 +226,29 @@ def test_express_slot_takes_only_passes_opened_by_small_queries():
 def test_express_needs_an_ordinary_slot():
     with pytest.raises(ValueError):
         _server(slots=1, express=1)
+
+
+def test_query_over_several_passes_launches_in_the_graphs_order():
+    """A 150-source query (three one-word passes) launches its sources in the
+    order the graph's source_order gives; every digest lands at its source's
+    row of the query."""
+    srv, ctx, clk = _server()
+    g = FakeGraph(1, order=lambda src: np.argsort(-np.asarray(src), kind="stable").astype(np.int32))
+    src = np.random.default_rng(3).permutation(np.arange(500, 650)).astype(np.int32)
+    q = srv.submit(g, src, want="digest")
+    srv.drain()
+    launched = np.concatenate([s for _, _, s in ctx.launches])
+    np.testing.assert_array_equal(launched, np.sort(src)[::-1])
+    assert [len(s) for _, _, s in ctx.launches] == [64, 64, 22]
+    np.testing.assert_array_equal(q.digest[:, 0], src)
+
+
+def test_one_word_query_keeps_its_order():
+    """A query that fits one word is launched as given (one pass either way)."""
+    srv, ctx, clk = _server()
+    g = FakeGraph(1, order=lambda src: np.arange(len(src))[::-1].astype(np.int32))
+    src = np.arange(10, 74).astype(np.int32)
+    q = srv.submit(g, src, want="digest")
+    srv.drain()
+    np.testing.assert_array_equal(ctx.launches[0][2], src)
+    np.testing.assert_array_equal(q.digest[:, 0], src)

@@ -132,3 +132,17 @@ def test_source_order_validated(ctx):
     with pytest.raises(xbtrav.XbError):
         ctx.set_tuning(source_order=2)
     _tune(ctx, 0)
+
+
+def test_source_order_api_is_the_degree_grouping(ctx, rmat12):
+    """xb_graph_source_order: indices by out-degree, highest first, ties in
+    the given order; out-of-range sources are refused."""
+    ro, ci = rmat12
+    g = ctx.upload_arrays(ro, ci)
+    src = _sources(ro, 6, 400)
+    deg = np.diff(np.asarray(ro))[src]
+    np.testing.assert_array_equal(g.source_order(src), np.argsort(-deg, kind="stable"))
+    assert len(g.source_order(np.zeros(0, np.int32))) == 0
+    with pytest.raises(xbtrav.XbError):
+        g.source_order(np.array([0, g.n], np.int32))
+    g.close()

@@ -203,14 +203,14 @@ def test_autotuner_picks_a_config_that_keeps_parity(ctx, tmp_path):
     src = xbtrav.select_sources_csr(ro, 32, 96)
     g = ctx.upload(csr)
     space = {"word_bits": [64, 32], "words": [1, 2], "heavy_degree": [128, 256], "pull_alpha": [64.0, 256.0],
-             "push_beta": [0.0, 24.0], "tile": [0, 1], "chains": [1, 2]}
+             "push_beta": [0.0, 24.0], "tile": [0, 1], "source_order": [0, 1], "chains": [1, 2]}
     for path in ("plain", "batched"):
         # the first stage keeps the current cutoffs: start inside the space
         _tune(ctx, heavy_degree=256, pull_alpha=256.0, chains=2)
         best, table = autotune.autotune(ctx, g, src, space=space, reps=1, path=path)
         assert all(best[k] in space[k] for k in space if path == "batched" or k != "chains")
         assert best == {k: ctx.tuning()[k] for k in best}
-        assert len(table) >= 4 + 4 + 2 + 2
+        assert len(table) >= 4 + 4 + 2 + 2 + 2
         r = ctx.traverse(g, src)
         lv, pr, _, _ = O.msbfs(ro, ci, src)
         np.testing.assert_array_equal(r.level, lv)

@@ -690,6 +690,20 @@ xb_status xb_select_sources(const xb_graph* g, uint64_t seed, int32_t k, int32_t
   return xbi::select_sources(g->n, g->h_ro.data(), seed, k, out);
 }
 
+xb_status xb_graph_source_order(const xb_graph* g, const int32_t* sources, int32_t k, int32_t* order) {
+  xbi::clear_error();
+  if (!g) return fail(XB_ERR_ARG, "null graph");
+  if (k < 0) return fail(XB_ERR_ARG, "negative source count");
+  if (k > 0 && (!sources || !order)) return fail(XB_ERR_ARG, "null sources or order");
+  for (int32_t i = 0; i < k; i++)
+    if (sources[i] < 0 || sources[i] >= g->n) return fail(XB_ERR_ARG, "source " + std::to_string(i) + " out of range");
+  std::vector<int64_t> perm((size_t)k);
+  for (int32_t i = 0; i < k; i++) perm[i] = i;
+  xbe::order_by_degree(g, perm, [&](int64_t i) { return (int64_t)sources[i]; });
+  for (int32_t i = 0; i < k; i++) order[i] = (int32_t)perm[i];
+  return XB_OK;
+}
+
 xb_status xb_traverse(xb_ctx* c, const xb_graph* gc, const int32_t* sources, int32_t k, int32_t mode,
                       const int32_t* matching, int32_t* level, int32_t* parent, int32_t* owner, uint32_t flags,
                       xb_stats* st) {

@@ -162,6 +162,7 @@ def lib() -> C.CDLL:
         "xb_graph_free": (i32, [vp]),
         "xb_graph_info": (i32, [vp, P(i64), P(i64), P(i64)]),
         "xb_select_sources": (i32, [vp, u64, i32, vp]),
+        "xb_graph_source_order": (i32, [vp, vp, i32, vp]),
         "xb_traverse": (i32, [vp, vp, vp, i32, i32, vp, vp, vp, vp, u32, P(XbStats)]),
         "xb_traverse_batched": (i32, [vp, P(XbBatchItem), i32, P(XbStats)]),
         "xb_slot_launch": (i32, [vp, i32, vp, vp, i32, vp, vp]),
@@ -343,6 +344,14 @@ class Graph:
     def select_sources(self, seed: int, k: int) -> np.ndarray:
         out = np.zeros(k, np.int32)
         _check(lib().xb_select_sources(self._h, seed, k, out.ctypes.data))
+        return out
+
+    def source_order(self, sources) -> np.ndarray:
+        """The engine's pass grouping of `sources` (xb_graph_source_order):
+        indices into sources by out-degree, highest first, ties in order."""
+        src = np.ascontiguousarray(sources, dtype=np.int32)
+        out = np.zeros(len(src), np.int32)
+        _check(lib().xb_graph_source_order(self._h, src.ctypes.data, len(src), out.ctypes.data))
         return out
 
     @property

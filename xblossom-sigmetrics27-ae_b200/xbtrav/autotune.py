@@ -6,7 +6,8 @@ the push/pull switch factor alpha, the tail push threshold push_beta (push
 after a pull once the frontier holds fewer than n/push_beta vertices; 0 =
 off), the launch tile of the pull and table
 kernels (xb_tuning.tile: rounds in flight per heavy-pull warp, warps per
-table block) and, for the batched path, the number of concurrent chains, by
+table block), the grouping of sources into passes (xb_tuning.source_order:
+by out-degree or as given) and, for the batched path, the number of concurrent chains, by
 timing the engine's own calls (device-side CUDA events of xb_traverse or
 xb_traverse_batched, median of `reps` runs) on the workload's sources.  The
 reference has no tuner; its only knobs are compile-time buffer ratios and a
@@ -27,9 +28,10 @@ DEFAULT_SPACE = {
     "pull_alpha": [16.0, 64.0, 256.0, 1024.0],
     "push_beta": [0.0, 24.0],
     "tile": [0, 1],
+    "source_order": [0, 1],
     "chains": [1, 2, 4, 8],
 }
-KEYS = ("word_bits", "words", "heavy_degree", "pull_alpha", "push_beta", "tile", "chains")
+KEYS = ("word_bits", "words", "heavy_degree", "pull_alpha", "push_beta", "tile", "source_order", "chains")
 
 
 def _time_config(ctx, graph, sources, cfg: dict, reps: int, path: str) -> float:
@@ -59,8 +61,8 @@ def autotune(ctx, graph, sources, space: dict | None = None, reps: int = 5, stag
 
     staged=True searches coordinate-wise (word layout first with the current
     cutoffs, then cutoffs and alpha for the winning layout, then the launch
-    tail push threshold, then the launch tile, then chains) instead of the
-    full grid.
+    tail push threshold, then the launch tile, then the source grouping,
+    then chains) instead of the full grid.
     """
     space = dict(DEFAULT_SPACE if space is None else space)
     if path != "batched":
@@ -87,6 +89,9 @@ def autotune(ctx, graph, sources, space: dict | None = None, reps: int = 5, stag
         best = min(table, key=lambda x: x[1])[0]
         for tl in space.get("tile", [best.get("tile", 0)]):
             run(dict(best, tile=tl))
+        best = min(table, key=lambda x: x[1])[0]
+        for so in space.get("source_order", [best.get("source_order", 0)]):
+            run(dict(best, source_order=so))
         best = min(table, key=lambda x: x[1])[0]
         for ch in space["chains"]:
             run(dict(best, chains=ch))

@@ -31,6 +31,12 @@ passes.  The context's tuning.words is switched before each launch (the
 server owns the context); every slot keeps a workspace and scratch rows for
 the widest pass it has run.
 
+A query of more than one word's sources launches them grouped by
+out-degree, highest first (xb_graph_source_order, the grouping the library's
+own calls use under tuning.source_order 0): its passes then hold sources
+whose traversals grow alike.  Rows, tables and digests stay at the
+positions of the query's source list.
+
 Each query asks for one of two results:
   want="tables": the full int32 level / parent tables (k x n each) in device
       memory.  The tables are allocated when the query is admitted, which
@@ -74,6 +80,7 @@ class Query:
     rows_done: int = 0
     rows_launched: int = 0
     passes: set = field(default_factory=set)
+    order: np.ndarray = None  # launch position -> row of sources / tables / digest
 
     @property
     def k(self) -> int:
@@ -108,6 +115,9 @@ class Server:
         self.rows_per_pass = self.word_bits * self.base_words
         self.dev = torch.device("cuda", ctx.device)
         self.age_s = age_s
+        # a query over several passes launches its sources grouped by degree,
+        # as the library's own calls do (xb_tuning.source_order 0)
+        self.group = t.get("source_order", 0) == 0
         if not 0 <= express < slots:
             raise ValueError("express must leave at least one ordinary slot")
         self.express = express
@@ -133,6 +143,8 @@ class Server:
                 raise ValueError("the query's tables can never fit into device memory; ask for want='digest'")
         q = Query(self._next, graph, src, want, self.clock() if arrival is None else arrival)
         self._next += 1
+        q.order = (graph.source_order(src) if self.group and q.k > self.word_bits
+                   else np.arange(q.k, dtype=np.int32))
         if q.k == 0:
             q.admitted = q.done_at = q.arrival
             self.completed.append(q)
@@ -200,10 +212,11 @@ class Server:
             q.rows_launched += n
             if len(take) == cap:
                 break
-        src = np.array([q.sources[j] for q, j in take], dtype=np.int32)
+        src = np.array([q.sources[q.order[j]] for q, j in take], dtype=np.int32)
         rows = []
         for q, j in take:
-            rows.append(None if q.want == "digest" else (q.level[j].data_ptr(), q.parent[j].data_ptr()))
+            r = int(q.order[j])
+            rows.append(None if q.want == "digest" else (q.level[r].data_ptr(), q.parent[r].data_ptr()))
         try:
             self.ctx.slot_launch(slot, g, src, rows)
         except Exception:
@@ -252,7 +265,7 @@ class Server:
         self.edges += st["edges_traversed"]
         for r, (q, j) in enumerate(self.slot_rows[slot]):
             if q.want == "digest":
-                q.digest[j] = dig[r]
+                q.digest[q.order[j]] = dig[r]
             q.rows_done += 1
             if q.rows_done == q.k:
                 q.done_at = now
