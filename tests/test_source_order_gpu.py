@@ -135,13 +135,19 @@ def test_source_order_validated(ctx):
 
 
 def test_source_order_api_is_the_degree_grouping(ctx, rmat12):
-    """xb_graph_source_order: indices by out-degree, highest first, ties in
-    the given order; out-of-range sources are refused."""
+    """xb_graph_source_order: indices by out-degree, highest first, equal
+    degrees by the sum of the neighbours' degrees, highest first, then in the
+    given order; out-of-range sources are refused."""
     ro, ci = rmat12
+    ro, ci = np.asarray(ro), np.asarray(ci)
     g = ctx.upload_arrays(ro, ci)
     src = _sources(ro, 6, 400)
-    deg = np.diff(np.asarray(ro))[src]
-    np.testing.assert_array_equal(g.source_order(src), np.argsort(-deg, kind="stable"))
+    dall = np.diff(ro)
+    deg = dall[src]
+    r2 = np.array([dall[ci[ro[s]:ro[s + 1]]].sum() for s in src])
+    want = np.lexsort((np.arange(len(src)), -r2, -deg))
+    np.testing.assert_array_equal(g.source_order(src), want)
+    assert (np.diff(deg[want]) <= 0).all()
     assert len(g.source_order(np.zeros(0, np.int32))) == 0
     with pytest.raises(xbtrav.XbError):
         g.source_order(np.array([0, g.n], np.int32))

@@ -389,7 +389,9 @@ xb_status run_batched(xb_ctx* c, const std::vector<xb_batch_item>& items, const 
     if (c->tuning.source_order == 0 && v.size() > (size_t)SPP) {  // passes grouped by source degree
       std::vector<int64_t> order(v.size());
       for (size_t j = 0; j < v.size(); j++) order[j] = (int64_t)j;
-      order_by_degree(g, order, [&](int64_t j) { return (int64_t)hsrc[v[j].item][v[j].idx]; });
+      st = order_by_degree(const_cast<xb_graph*>(g), order,
+                           [&](int64_t j) { return (int64_t)hsrc[v[j].item][v[j].idx]; });
+      if (st != XB_OK) return st;
       std::vector<RowDst> sorted(v.size());
       for (size_t j = 0; j < v.size(); j++) sorted[j] = v[order[j]];
       v.swap(sorted);

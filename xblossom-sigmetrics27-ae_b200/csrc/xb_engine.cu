@@ -134,6 +134,32 @@ xb_status ensure_fifo(xb_ctx* c, size_t ints) {
   return XB_OK;
 }
 
+xb_status ensure_reach2(xb_graph* g) {
+  if ((int64_t)g->h_reach2.size() == g->n) return XB_OK;
+  if (!g->ctx) return fail(XB_ERR_STATE, "the graph's context was destroyed");
+  xb_ctx* c = g->ctx;
+  XB_CUDA(cudaSetDevice(c->device));
+  long long* d = nullptr;
+  if (cudaMalloc(&d, sizeof(long long) * (size_t)g->n) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(XB_ERR_OOM, "neighbour degree sum allocation failed");
+  }
+  std::vector<int64_t> h((size_t)g->n);
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((g->n + 7) / 8, (int64_t)c->num_sms * 8));
+  if (g->off64)
+    xbk::k_reach2<int64_t><<<grid, 256, 0, c->stream>>>(g->n, (const int64_t*)g->d_ro, g->d_ci, d);
+  else
+    xbk::k_reach2<int32_t><<<grid, 256, 0, c->stream>>>(g->n, (const int32_t*)g->d_ro, g->d_ci, d);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(h.data(), d, sizeof(long long) * (size_t)g->n, cudaMemcpyDeviceToHost,
+                                            c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  cudaFree(d);
+  if (e != cudaSuccess) return fail(XB_ERR_CUDA, std::string("neighbour degree sums: ") + cudaGetErrorString(e));
+  g->h_reach2.swap(h);
+  return XB_OK;
+}
+
 xb_status ensure_heavy(xb_graph* g, int thr) {
   if (g->heavy_thr == thr) return XB_OK;
   // heavy vertices by falling degree (ties by ascending id): every heavy
@@ -690,8 +716,9 @@ xb_status xb_select_sources(const xb_graph* g, uint64_t seed, int32_t k, int32_t
   return xbi::select_sources(g->n, g->h_ro.data(), seed, k, out);
 }
 
-xb_status xb_graph_source_order(const xb_graph* g, const int32_t* sources, int32_t k, int32_t* order) {
+xb_status xb_graph_source_order(const xb_graph* gc, const int32_t* sources, int32_t k, int32_t* order) {
   xbi::clear_error();
+  xb_graph* g = const_cast<xb_graph*>(gc);  // the neighbour degree sums are cached on first use
   if (!g) return fail(XB_ERR_ARG, "null graph");
   if (k < 0) return fail(XB_ERR_ARG, "negative source count");
   if (k > 0 && (!sources || !order)) return fail(XB_ERR_ARG, "null sources or order");
@@ -699,7 +726,10 @@ xb_status xb_graph_source_order(const xb_graph* g, const int32_t* sources, int32
     if (sources[i] < 0 || sources[i] >= g->n) return fail(XB_ERR_ARG, "source " + std::to_string(i) + " out of range");
   std::vector<int64_t> perm((size_t)k);
   for (int32_t i = 0; i < k; i++) perm[i] = i;
-  xbe::order_by_degree(g, perm, [&](int64_t i) { return (int64_t)sources[i]; });
+  if (k > 0) {
+    const xb_status s = xbe::order_by_degree(g, perm, [&](int64_t i) { return (int64_t)sources[i]; });
+    if (s != XB_OK) return s;
+  }
   for (int32_t i = 0; i < k; i++) order[i] = (int32_t)perm[i];
   return XB_OK;
 }
@@ -742,7 +772,8 @@ xb_status xb_traverse(xb_ctx* c, const xb_graph* gc, const int32_t* sources, int
   std::vector<int64_t> perm((size_t)k);
   for (int32_t i = 0; i < k; i++) perm[i] = i;
   if (c->tuning.source_order == 0 && k > c->tuning.word_bits * c->tuning.words) {
-    xbe::order_by_degree(g, perm, [&](int64_t i) { return (int64_t)hs[i]; });
+    s = xbe::order_by_degree(g, perm, [&](int64_t i) { return (int64_t)hs[i]; });
+    if (s != XB_OK) return s;
     std::vector<int32_t> ps((size_t)k);
     for (int32_t i = 0; i < k; i++) ps[i] = hs[perm[i]];
     hs.swap(ps);

@@ -93,6 +93,7 @@ struct xb_graph {
   int32_t heavy_thr = -1;
   uint64_t version = 0;  // bumped whenever the heavy-vertex arrays are rebuilt
   int32_t* d_w = nullptr;  // edge weights (xb_graph_set_weights), one per colIndices entry
+  std::vector<int64_t> h_reach2;  // per vertex, its neighbours' degree sum (computed on first use)
 };
 
 namespace xbe {
@@ -162,6 +163,8 @@ inline WsLayout layout_for(int64_t n, int word_bytes, int nw) {
 
 // Builds (or keeps) the graph's heavy-vertex arrays for cutoff thr.
 xb_status ensure_heavy(xb_graph* g, int thr);
+// Fills g->h_reach2 (once per graph) on the graph's context's device.
+xb_status ensure_reach2(xb_graph* g);
 
 // Releases the batched path's resources of a context.
 void batch_state_free(BatchState* b);
@@ -227,15 +230,22 @@ inline long long push_below(const xb_ctx* c, const xb_graph* g) {
   return c->tuning.push_beta > 0 ? (long long)((double)g->n / (double)c->tuning.push_beta) : 0;
 }
 
-// Stable order of count sources by out-degree, highest first (the pass
-// grouping of tuning.source_order 0).  key(i) gives the i-th source's vertex.
+// Stable order of sources by out-degree, highest first, equal degrees by
+// their neighbours' degree sum, highest first (the pass grouping of
+// tuning.source_order 0: a pass's sources then reach the graph's core at the
+// same level).  key(i) gives the i-th source's vertex.
 template <typename Key>
-void order_by_degree(const xb_graph* g, std::vector<int64_t>& order, Key key) {
+xb_status order_by_degree(xb_graph* g, std::vector<int64_t>& order, Key key) {
+  const xb_status s = ensure_reach2(g);
+  if (s != XB_OK) return s;
   const int64_t* ro = g->h_ro.data();
+  const int64_t* r2 = g->h_reach2.data();
   std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t b) {
     const int64_t va = key(a), vb = key(b);
-    return ro[va + 1] - ro[va] > ro[vb + 1] - ro[vb];
+    const int64_t da = ro[va + 1] - ro[va], db = ro[vb + 1] - ro[vb];
+    return da != db ? da > db : r2[va] > r2[vb];
   });
+  return XB_OK;
 }
 
 // Refuses a working-memory allocation above the context's tuning.workspace_cap.

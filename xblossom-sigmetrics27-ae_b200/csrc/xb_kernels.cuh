@@ -2190,4 +2190,25 @@ static __global__ void __launch_bounds__(256) k_row_digest(int32_t* const* __res
   }
 }
 
+// Per vertex v, the sum of its neighbours' degrees (the CSR entries a
+// traversal from v reads at its second level): the tie-break of the pass
+// grouping by source degree.  Warp per vertex; the loop bound is uniform
+// over the warp, so the shuffle reduction runs with every lane.
+template <typename OffT>
+__global__ void k_reach2(int64_t n, const OffT* __restrict__ ro, const int32_t* __restrict__ ci,
+                         long long* __restrict__ out) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t v = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < n; v += warps) {
+    const int64_t b = (int64_t)ro[v], e = (int64_t)ro[v + 1];
+    long long s = 0;
+    for (int64_t i = b + lane; i < e; i += 32) {
+      const int32_t u = ci[i];
+      s += (long long)(ro[u + 1] - ro[u]);
+    }
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (lane == 0) out[v] = s;
+  }
+}
+
 }  // namespace xbk

@@ -244,7 +244,10 @@ class Server:
 
     def warmup(self, graph, seed: int = 1) -> None:
         """One full pass per slot and per width, so that workspaces, scratch
-        rows and the slots' captured pass graphs exist before timing."""
+        rows and the slots' captured pass graphs exist before timing (and the
+        graph's source grouping data, computed on its first use)."""
+        if self.group:
+            graph.source_order(graph.select_sources(seed, 2))
         words = self.base_words
         while True:
             self.ctx.set_tuning(words=words)
