@@ -226,7 +226,9 @@ xb_status xb_graph_source_order(const xb_graph* g, const int32_t* sources, int32
  * parent is itself; -1 unreached).  Sources are processed in passes of
  * tuning.word_bits * tuning.words sources (64-bit words, four per vertex by
  * default: 256 sources per pass), one pass per launch sequence, with a
- * host-side level loop.
+ * host-side level loop; with more sources than one pass holds, they are
+ * grouped into passes as tuning.source_order says (by degree by default) and
+ * every source's rows still land at its index in `sources`.
  * In plain mode matching and owner must be NULL.
  * XB_MODE_ALTERNATING: the alternating forest of `matching` (n ints, -1 =
  * exposed) grown from every exposed vertex, the expansion of the reference's
