@@ -277,14 +277,15 @@ typedef struct xb_batch_item {
 /* Batched path (the reference has none: its engine runs one source set per
  * host-driven loop, xblossom_gpu_engine_10.cu:72-185).  All queries of the
  * batch -- on one graph or several, of any sizes -- run as ONE CUDA-graph
- * launch: the sources of queries on the same graph are packed 64 (or 32) per
- * word regardless of which query they come from, the words ("passes") are
+ * launch: the sources of queries on the same graph are packed into passes of
+ * tuning.word_bits * tuning.words regardless of which query they come from
+ * (grouped by degree under tuning.source_order 0), the passes are
  * spread over tuning.chains concurrent chains, and each pass's level loop runs
  * on the device (conditional WHILE / SWITCH nodes pick push or pull per level
  * from the frontier counters; no host round trip per level).  The launch is
  * cached: calls with the same queries shape (graphs, k per query, flags and,
- * for host outputs, the output pointers) reuse it; sources and device output
- * pointers may change freely between such calls.  Results are identical to
+ * for host outputs, the output pointers and the sources' grouping) reuse it;
+ * sources and device output pointers may change freely between such calls.  Results are identical to
  * xb_traverse's.  stats (may be NULL) sums over the whole batch. */
 xb_status xb_traverse_batched(xb_ctx* ctx, const xb_batch_item* items, int32_t nitems,
                               xb_stats* stats);
