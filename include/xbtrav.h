@@ -111,7 +111,8 @@ typedef struct xb_tuning {
    * vertices (the traversal's tail); 0 = never. */
   float push_beta;
   /* How a call's sources are grouped into passes: 0 (default) = by source
-   * degree, highest first (sources whose traversals grow alike share a
+   * degree, highest first, equal degrees by their neighbours' degree sum
+   * (xb_graph_source_order; sources whose traversals grow alike share a
    * pass's level steps: fewer steps with few live lanes); 1 = in the order
    * given.  Output rows stay where the caller asked for them either way.
    * xb_traverse_batched with host output tables keys its captured copies
