@@ -119,6 +119,13 @@ class DGraph {
   DGraph& operator=(const DGraph&) = delete;
   const xb_graph* get() const { return g_; }
   Context& ctx() const { return *ctx_; }
+  // The engine's pass grouping of `sources` (xb_graph_source_order): indices
+  // into sources by degree, highest first, ties by the neighbours' degree sum.
+  std::vector<int32_t> SourceOrder(const std::vector<int32_t>& sources) const {
+    std::vector<int32_t> order(sources.size());
+    check(xb_graph_source_order(g_, sources.data(), (int32_t)sources.size(), order.data()));
+    return order;
+  }
 
  private:
   Context* ctx_;
