@@ -831,7 +831,8 @@ def main() -> None:
         clk = sampler.stop() if sampler is not None else None
         return max_over_ranks(ev0.elapsed_time(ev1)), agg, clk
 
-    # plain per-call path (the drop-in): one word per launch sequence, host level loop
+    # plain per-call path (the drop-in): one pass of the layout's words per launch
+    # sequence, host level loop
     ctx.set_tuning(timing=0)
     for _ in range(args.warmup):
         plain_step()
@@ -949,7 +950,7 @@ def main() -> None:
     if rank == 0:
         path_desc = (f"xb_traverse_batched (one CUDA-graph launch per step, device level loop, "
                      f"{tun['chains']} chains, {tun['word_bits']} sources per word x {tun['words']})"
-                     if args.path == "batched" else "xb_traverse (host level loop, one word per launch sequence)")
+                     if args.path == "batched" else "xb_traverse (host level loop, one pass per launch sequence)")
         agg = b_agg if args.path == "batched" else plain_agg
         line = {
             "metric": METRIC, "value": headline, "unit": "GTEPS",
