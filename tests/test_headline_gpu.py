@@ -7,7 +7,8 @@ vertex = 256 sources per pass, 4 chains, heavy cutoff 256, pull factor 256).
 These tests run exactly that call and compare a spread sample of source rows
 bit-exactly with the CPU oracle (levels and min-id parents): every pass, every
 word of a pass and bit positions 0 and 63 of each word, plus seeded random
-rows.  The plain path (xb_traverse) on the same inputs must give identical
+rows (positions in the engine's pass grouping, xb_graph_source_order, mapped
+to the caller's rows).  The plain path (xb_traverse) on the same inputs must give identical
 tables in full.  The uneven 128-graph workload is checked the same way on
 sampled queries, and R-MAT 20 at the default tuning (hubs above degree 4096,
 so the chunked hub pull runs inside the captured level loop) in full.
@@ -71,7 +72,11 @@ def test_headline_batched_and_plain_rmat22_k1024(rmat22):
     pr_b = torch.empty_like(lv_b)
     _, st = ctx.traverse_batched([(g, src_dev)], outputs=[(lv_b, pr_b)])
     assert st["batches"] == 4
-    rows = _sample_rows(1024, 256, 8, 2024)
+    # traversal positions (pass, word, bit) -> the caller's rows through the
+    # pass grouping, which the engine applies to these 1024 sources
+    order = g.source_order(src).astype(np.int64)
+    assert np.array_equal(np.sort(order), np.arange(1024))
+    rows = np.unique(order[_sample_rows(1024, 256, 8, 2024)])
     assert len(rows) >= 40
     _check_rows(ro, ci, src, rows, lv_b, pr_b)
     # the plain per-call path on the same inputs: identical tables in full
